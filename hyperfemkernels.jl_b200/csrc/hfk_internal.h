@@ -1,0 +1,148 @@
+// Internal definitions of the B200 engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/hfk.h"
+
+namespace hfk {
+
+// ---- error handling: every ABI entry point returns a status and records the message ----------
+void set_error(const std::string& msg);
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define HFK_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::hfk::Error{HFK_ERR_CUDA, std::string("HyperFEMKernels: CUDA error: ") +       \
+                                           cudaGetErrorString(e_) + " at " #call};          \
+  } while (0)
+#define HFK_REQUIRE(cond, code, msg)                                       \
+  do {                                                                     \
+    if (!(cond)) throw ::hfk::Error{code, std::string("HyperFEMKernels: ") + (msg)}; \
+  } while (0)
+
+// ---- a device buffer owned by a handle ---------------------------------------------------
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void resize(size_t m) {
+    if (m == n && p) return;
+    release();
+    if (m) HFK_CUDA(cudaMalloc(&p, m * sizeof(T)));
+    n = m;
+  }
+  void upload(const T* h, size_t m, cudaStream_t s) {
+    resize(m);
+    if (m) HFK_CUDA(cudaMemcpyAsync(p, h, m * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) HFK_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+};
+
+// max supported nodes / points per direction in the tensor-product kernels
+constexpr int MAXQ = 6;
+
+// 1D tables (tensor order), passed by value to kernels (constant bank, broadcast reads)
+template <typename R>
+struct Tab1D {
+  R N1[MAXQ * MAXQ];   // N1[a * Q + i]: basis i at 1D point a
+  R dN1[MAXQ * MAXQ];
+  R w1[MAXQ];          // 1D weights (unused when the product weights are passed)
+};
+
+// Per-problem read-only data the cell kernels take (device pointers), passed by value.
+struct CellData {
+  const int32_t* ids;     // (ndl, ncells) cell-major, tensor node order, ldof = c*nn + n
+  const int32_t* cells;   // list of cells (one colour) or nullptr for 0..ncells-1
+  int ncells_list;
+  int ncells;
+  const double* geo;      // 10 per cell: iJt (column-major 3x3) and |det Jt| at the first point
+  const uint8_t* affine;  // per cell
+  const double* coords;   // (3, 8, ncells)
+  const double* dMt;      // (8, 3, np) tensor point order
+  const double* w;        // (np) tensor point order
+  int law;                // HFK_LAW_*
+  double lam, mu, body[3];
+};
+
+// State of a matrix-free level in a precision
+template <typename R>
+struct LevelState {
+  DBuf<R> x, dvals;
+};
+
+}  // namespace hfk
+
+// The opaque handles of the ABI
+struct hfk_problem {
+  int D = 3, nn = 0, nc = 3, np = 0, ng = 8, ndl = 0, ncells = 0;
+  int Q = 0, P = 0;             // tensor-product structure (0 = none)
+  int64_t nfree = 0, ndir = 0;
+  int law = 0;
+  double params[5] = {0, 0, 0, 0, 0};
+  cudaStream_t stream = nullptr;      // launch stream (own_stream or the caller's)
+  cudaStream_t own_stream = nullptr;
+  int device = 0;
+  // host copies of the construction data
+  std::vector<int> nodeperm, pointperm;   // tensor index -> caller index
+  std::vector<int32_t> h_ids;             // caller order
+  std::vector<double> h_w;                // caller point order
+  std::vector<double> h_N1, h_dN1;        // P x Q (a * Q + i)
+  // device data (tensor order)
+  hfk::DBuf<int32_t> ids;                 // (ndl, ncells)
+  hfk::DBuf<double> geo, coords, dMt, w, Nt, dNt;  // Nt (nn, np), dNt (nn, 3, np) tensor order
+  hfk::DBuf<uint8_t> affine;
+  // colours
+  int ncolors = 0;
+  std::vector<int32_t> h_color_of;        // per cell, 1-based
+  std::vector<int> color_start;           // ncolors + 1 offsets into cells_by_color
+  hfk::DBuf<int32_t> cells_by_color;
+  // sparsity pattern (CSC, 0-based int32 internally) and positions (tensor order, 1-based, 0 = none)
+  int64_t nnz = 0;
+  hfk::DBuf<int64_t> colptr;              // 1-based (Julia SparseMatrixCSC)
+  hfk::DBuf<int64_t> rowval;
+  hfk::DBuf<int32_t> nzpos;               // (ndl*ndl, ncells)
+  hfk::DBuf<double> nzval;
+  // current state (FP64) and its FP32 copy
+  hfk::DBuf<double> x, dvals;
+  hfk::DBuf<float> x32, dvals32;
+  bool prepared = false;
+  int mf_mode = HFK_MF_RECOMPUTE;
+  // stored tangents (reference formulation: T, iJt, dV per point)
+  hfk::DBuf<double> T, iJtq, dVq;
+  // nodal blocks
+  int nblocks = 0;
+  hfk::DBuf<int32_t> block_of;            // (nn, ncells) tensor order, 0 = none
+  hfk::DBuf<int32_t> bdofs;               // (3, nblocks) 1-based, 0 = fixed
+  hfk::DBuf<double> B, Binv;              // (9, nblocks)
+  hfk::DBuf<float> Binv32;
+  bool blocks_ok = false;
+  // staging for host pointers
+  hfk::DBuf<double> stage_in, stage_in2, stage_out;
+  hfk::DBuf<int64_t> stage_l;
+  hfk::DBuf<float> tmp32a, tmp32b;
+  // error flag for numerical checks
+  hfk::DBuf<int> flag;
+  // timing of the last kernel sequence (CUDA events)
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int launches = 0;
+};

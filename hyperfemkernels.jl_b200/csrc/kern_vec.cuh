@@ -1,0 +1,377 @@
+// Vector-level kernels: reductions, nodal blocks (extraction, inversion, application), the fused
+// Chebyshev steps, transfers between levels, dense coarse solve. All memory-bound: grid-stride
+// loops sized to the SM count, coalesced along the free-dof vectors.
+#pragma once
+#include "hfk_internal.h"
+#include "pointwise.cuh"
+
+namespace hfk {
+
+// ---- deterministic two-stage reductions ------------------------------------------------------
+constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+template <typename R>
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void block_sum_store(double v, double* out) {
+  __shared__ double ws[32];
+  v = warp_sum<double>(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (blockDim.x >> 5) ? ws[lane] : 0.0;
+    v = warp_sum<double>(v);
+    if (lane == 0) *out = v;
+  }
+  __syncthreads();
+}
+
+// partial[k * gridDim.x + block] for up to 3 dot products x_k . y_k
+template <typename R>
+__global__ void dots_kernel(int64_t n, int k, const R* a0, const R* b0, const R* a1, const R* b1, const R* a2,
+                            const R* b2, double* partial) {
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    s0 += (double)a0[i] * (double)b0[i];
+    if (k > 1) s1 += (double)a1[i] * (double)b1[i];
+    if (k > 2) s2 += (double)a2[i] * (double)b2[i];
+  }
+  block_sum_store(s0, partial + blockIdx.x);
+  if (k > 1) block_sum_store(s1, partial + gridDim.x + blockIdx.x);
+  if (k > 2) block_sum_store(s2, partial + 2 * gridDim.x + blockIdx.x);
+}
+
+__global__ void finish_sums_kernel(int nparts, int k, const double* partial, double* out) {
+  for (int j = 0; j < k; ++j) {
+    double s = 0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += partial[j * nparts + i];
+    block_sum_store(s, out + j);
+  }
+}
+
+// ---- elementwise ----------------------------------------------------------------------------
+template <typename R>
+__global__ void fill_kernel(int64_t n, R v, R* x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = v;
+}
+template <typename A, typename B>
+__global__ void convert_kernel(int64_t n, const A* x, B* y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) y[i] = (B)x[i];
+}
+// y = a x + b y
+template <typename R>
+__global__ void axpby_kernel(int64_t n, R a, const R* x, R b, R* y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+// z = a x + b y
+template <typename R>
+__global__ void axpbyz_kernel(int64_t n, R a, const R* x, R b, const R* y, R* z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) z[i] = a * x[i] + b * y[i];
+}
+// CG update: x += alpha p; rold = r; r -= alpha q
+__global__ void cg_update_kernel(int64_t n, double alpha, const double* p, const double* q, double* x, double* r,
+                                 double* rold) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ri = r[i];
+    if (rold) rold[i] = ri;
+    x[i] += alpha * p[i];
+    r[i] = ri - alpha * q[i];
+  }
+}
+
+// ---- nodal blocks ---------------------------------------------------------------------------
+// B_blk[ci,cj] += sum_q sum_{K,K'} dN^[n,K,q] Dh_q[(ci,K),(cj,K')] dN^[n,K',q] over the nodes of the
+// cells of one colour (blocks_from_tangents!, src/preconditioners.jl:250-280, with the tangent
+// pulled back once per point as in the assembly kernel).
+struct BlockIO {
+  const double* u;
+  const double* dvals;
+  const double* dNt;       // (nn, 3, np) tensor order
+  const int32_t* block_of; // (nn, ncells)
+  double* B;               // (9, nblocks)
+  int np, nn;
+};
+
+__global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
+  extern __shared__ __align__(16) double sm[];
+  const int np = io.np, nn = io.nn, ndl = 3 * nn;
+  double* xl = sm;               // ndl
+  double* Hs = xl + ndl;         // 9 np
+  double* iJs = Hs + 9 * np;     // 9 np
+  double* dVs = iJs + 9 * np;    // np
+  double* Dh = dVs + np;         // 81 np
+  const int li = blockIdx.x;
+  if (li >= cd.ncells_list) return;
+  const int cell = cd.cells ? cd.cells[li] : li;
+  const int32_t* gid = cd.ids + (size_t)cell * ndl;
+  for (int j = threadIdx.x; j < ndl; j += blockDim.x) {
+    const int32_t id = gid[j];
+    xl[j] = id > 0 ? io.u[id - 1] : (id < 0 ? io.dvals[-id - 1] : 0.0);
+  }
+  __syncthreads();
+  const double* A = io.dNt;
+  for (int q = threadIdx.x; q < np; q += blockDim.x) {
+    double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int n = 0; n < nn; ++n) {
+      const double a0 = A[n + nn * (3 * q)], a1 = A[n + nn * (1 + 3 * q)], a2 = A[n + nn * (2 + 3 * q)];
+      for (int c = 0; c < 3; ++c) {
+        const double x = xl[c * nn + n];
+        G[c][0] += x * a0;
+        G[c][1] += x * a1;
+        G[c][2] += x * a2;
+      }
+    }
+    double Jt[9], iJ[9], det;
+    if (cd.affine[cell]) {
+      for (int i = 0; i < 9; ++i) iJ[i] = cd.geo[(size_t)cell * 10 + i];
+      det = cd.geo[(size_t)cell * 10 + 9];
+    } else {
+      point_jacobian_dev(cd, cell, q, Jt);
+      det = det3(Jt);
+      inv3(Jt, det, iJ);
+      det = fabs(det);
+    }
+    for (int c = 0; c < 3; ++c)
+      for (int J = 0; J < 3; ++J) Hs[q * 9 + c + 3 * J] = iJ[J] * G[c][0] + iJ[J + 3] * G[c][1] + iJ[J + 6] * G[c][2];
+    for (int i = 0; i < 9; ++i) iJs[q * 9 + i] = iJ[i];
+    dVs[q] = cd.w[q] * det;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < np * 9; e += blockDim.x) {
+    const int q = e / 9, ck = e % 9, c = ck / 3, k = ck % 3;
+    double T[81];
+    law_tangent(cd.law, cd.lam, cd.mu, Hs + q * 9, T);
+    const double* iJ = iJs + q * 9;
+    double X[3][3];
+    for (int J = 0; J < 3; ++J)
+      for (int Kp = 0; Kp < 3; ++Kp) {
+        double s = 0;
+        for (int L = 0; L < 3; ++L) s += T[(c * 3 + J) + 9 * (k * 3 + L)] * iJ[L + 3 * Kp];
+        X[J][Kp] = s;
+      }
+    for (int K = 0; K < 3; ++K)
+      for (int Kp = 0; Kp < 3; ++Kp) {
+        double s = 0;
+        for (int J = 0; J < 3; ++J) s += iJ[J + 3 * K] * X[J][Kp];
+        Dh[q * 81 + (c * 3 + K) + 9 * (k * 3 + Kp)] = dVs[q] * s;
+      }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nn * 9; e += blockDim.x) {
+    const int n = e / 9, ck = e % 9, ci = ck / 3, cj = ck % 3;
+    const int blk = io.block_of[n + (size_t)nn * cell];
+    if (blk == 0) continue;
+    double s = 0;
+    for (int q = 0; q < np; ++q) {
+      const double a0 = A[n + nn * (3 * q)], a1 = A[n + nn * (1 + 3 * q)], a2 = A[n + nn * (2 + 3 * q)];
+      const double* D = Dh + q * 81 + ci * 3 + 9 * (cj * 3);
+      s += a0 * (D[0] * a0 + D[9] * a1 + D[18] * a2) + a1 * (D[1] * a0 + D[10] * a1 + D[19] * a2) +
+           a2 * (D[2] * a0 + D[11] * a1 + D[20] * a2);
+    }
+    io.B[(size_t)(blk - 1) * 9 + ci + 3 * cj] += s;
+  }
+}
+
+// _invert_blocks! (src/preconditioners.jl:312-327): fixed components -> identity rows/columns
+__global__ void invert_blocks_kernel(int nb, const int32_t* dofs, const double* B, double* Binv, float* Binv32,
+                                     int* bad) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    double M[9];
+    bool fin = true;
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) {
+        const bool fixed = dofs[3 * b + i] == 0 || dofs[3 * b + j] == 0;
+        M[i + 3 * j] = fixed ? (i == j ? 1.0 : 0.0) : B[9 * (size_t)b + i + 3 * j];
+        fin &= isfinite(M[i + 3 * j]);
+      }
+    double Mi[9];
+    if (fin) {
+      inv3(M, det3(M), Mi);
+      for (int i = 0; i < 9; ++i) fin &= isfinite(Mi[i]);
+    } else {
+      for (int i = 0; i < 9; ++i) Mi[i] = M[i];
+    }
+    if (!fin) atomicOr(bad, 1);
+    for (int i = 0; i < 9; ++i) {
+      Binv[9 * (size_t)b + i] = Mi[i];
+      if (Binv32) Binv32[9 * (size_t)b + i] = (float)Mi[i];
+    }
+  }
+}
+
+// y[dofs] = Binv r[dofs] (ldiv!, src/preconditioners.jl:329-344)
+template <typename R>
+__global__ void blocks_apply_kernel(int nb, const int32_t* dofs, const R* Binv, const R* r, R* y) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const int d0 = dofs[3 * b], d1 = dofs[3 * b + 1], d2 = dofs[3 * b + 2];
+    const R r0 = d0 ? r[d0 - 1] : R(0), r1 = d1 ? r[d1 - 1] : R(0), r2 = d2 ? r[d2 - 1] : R(0);
+    const R* M = Binv + 9 * (size_t)b;
+    if (d0) y[d0 - 1] = M[0] * r0 + M[3] * r1 + M[6] * r2;
+    if (d1) y[d1 - 1] = M[1] * r0 + M[4] * r1 + M[7] * r2;
+    if (d2) y[d2 - 1] = M[2] * r0 + M[5] * r1 + M[8] * r2;
+  }
+}
+
+// ---- Chebyshev (smooth!, src/smoothers.jl:116-146), fused per nodal block ----------------------
+// start: r = rhs (zero guess) or r = rhs - Ax (z holds Ax); d = Binv r / theta; x = d or x += d
+template <typename R>
+__global__ void cheb_start_kernel(int nb, const int32_t* dofs, const R* Binv, const R* rhs, const R* Ax, R* r, R* d,
+                                  R* x, R inv_theta, int zero_guess) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
+    R rr[3];
+    for (int i = 0; i < 3; ++i) {
+      rr[i] = 0;
+      if (dd[i]) {
+        R v = rhs[dd[i] - 1];
+        if (!zero_guess) v -= Ax[dd[i] - 1];
+        r[dd[i] - 1] = v;
+        rr[i] = v;
+      }
+    }
+    const R* M = Binv + 9 * (size_t)b;
+    for (int i = 0; i < 3; ++i) {
+      if (!dd[i]) continue;
+      const R z = M[i] * rr[0] + M[i + 3] * rr[1] + M[i + 6] * rr[2];
+      const R di = z * inv_theta;
+      d[dd[i] - 1] = di;
+      x[dd[i] - 1] = zero_guess ? di : x[dd[i] - 1] + di;
+    }
+  }
+}
+// step: r -= z (z = A d); if more: d = c1 d + c2 Binv r; x += d
+template <typename R>
+__global__ void cheb_step_kernel(int nb, const int32_t* dofs, const R* Binv, const R* z, R* r, R* d, R* x, R c1, R c2,
+                                 int update_d) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
+    R rr[3];
+    for (int i = 0; i < 3; ++i) {
+      rr[i] = 0;
+      if (dd[i]) {
+        const R v = r[dd[i] - 1] - z[dd[i] - 1];
+        r[dd[i] - 1] = v;
+        rr[i] = v;
+      }
+    }
+    if (!update_d) continue;
+    const R* M = Binv + 9 * (size_t)b;
+    for (int i = 0; i < 3; ++i) {
+      if (!dd[i]) continue;
+      const R zz = M[i] * rr[0] + M[i + 3] * rr[1] + M[i + 6] * rr[2];
+      const R dn = c1 * d[dd[i] - 1] + c2 * zz;
+      d[dd[i] - 1] = dn;
+      x[dd[i] - 1] += dn;
+    }
+  }
+}
+
+// ---- transfers (src/transfers.jl) ------------------------------------------------------------
+struct XferData {
+  const int32_t* ids_f;   // (3 NF, ncells) fine level, tensor order
+  const int32_t* ids_c;   // (3 NC, ncells) coarse level
+  const double* E;        // (NF, NC) column-major, tensor orders
+  const double* Einj;     // (NC, NF)
+  const int32_t* mult;    // per fine free dof
+  const int32_t* cells;   // colour list or nullptr
+  int ncells_list, NF, NC;
+};
+
+// prolongate_cells! (src/transfers.jl:179-193): fine value = E * coarse local values, inserted
+template <typename R>
+__global__ void prolongate_kernel(XferData t, const R* xc, R* yf) {
+  const int per = 3 * t.NF;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)t.ncells_list * per;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int li = (int)(e / per), j = (int)(e % per);
+    const int cell = t.cells ? t.cells[li] : li;
+    const int32_t idf = t.ids_f[(size_t)cell * per + j];
+    if (idf <= 0) continue;
+    const int comp = j / t.NF, f = j % t.NF;
+    const int32_t* ic = t.ids_c + (size_t)cell * 3 * t.NC + comp * t.NC;
+    double s = 0;
+    for (int c = 0; c < t.NC; ++c) {
+      const double w = t.E[f + (size_t)t.NF * c];
+      const int32_t id = ic[c];
+      if (w != 0.0 && id > 0) s += w * (double)xc[id - 1];
+    }
+    yf[idf - 1] = (R)s;
+  }
+}
+
+// restrict_cells! (src/transfers.jl:195-213): E^T (yf / multiplicity), scatter-add (coloured)
+template <typename R>
+__global__ void restrict_kernel(XferData t, const R* yf, R* yc) {
+  const int per = 3 * t.NC;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)t.ncells_list * per;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int li = (int)(e / per), j = (int)(e % per);
+    const int cell = t.cells ? t.cells[li] : li;
+    const int32_t idc = t.ids_c[(size_t)cell * per + j];
+    if (idc <= 0) continue;
+    const int comp = j / t.NC, c = j % t.NC;
+    const int32_t* iff = t.ids_f + (size_t)cell * 3 * t.NF + comp * t.NF;
+    double s = 0;
+    for (int f = 0; f < t.NF; ++f) {
+      const double w = t.E[f + (size_t)t.NF * c];
+      const int32_t id = iff[f];
+      if (w != 0.0 && id > 0) s += w * ((double)yf[id - 1] / t.mult[id - 1]);
+    }
+    yc[idc - 1] += (R)s;
+  }
+}
+
+// inject_field! (src/transfers.jl:295-313)
+__global__ void inject_kernel(XferData t, int ncells, const double* xf, const double* df, double* xc, double* dc) {
+  const int per = 3 * t.NC;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)ncells * per;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int cell = (int)(e / per), j = (int)(e % per);
+    const int comp = j / t.NC, c = j % t.NC;
+    const int32_t* iff = t.ids_f + (size_t)cell * 3 * t.NF + comp * t.NF;
+    double v = 0;
+    for (int f = 0; f < t.NF; ++f) {
+      const double w = t.Einj[c + (size_t)t.NC * f];
+      if (w == 0.0) continue;
+      const int32_t id = iff[f];
+      v += w * (id > 0 ? xf[id - 1] : df[-id - 1]);
+    }
+    const int32_t idc = t.ids_c[(size_t)cell * per + j];
+    if (idc > 0) xc[idc - 1] = v;
+    else if (idc < 0) dc[-idc - 1] = v;
+  }
+}
+
+// ---- dense coarse solve -----------------------------------------------------------------------
+// CSC (1-based) -> dense column-major n x n
+__global__ void csc_to_dense_kernel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                                    double* A) {
+  for (int64_t c = blockIdx.x; c < n; c += gridDim.x)
+    for (int64_t k = colptr[c] - 1 + threadIdx.x; k < colptr[c + 1] - 1; k += blockDim.x)
+      A[(rowval[k] - 1) + n * c] = nzval[k];
+}
+// lower triangle -> full symmetric
+__global__ void symmetrize_lower_kernel(int64_t n, double* A) {
+  for (int64_t c = blockIdx.x; c < n; c += gridDim.x)
+    for (int64_t r = threadIdx.x; r < c; r += blockDim.x) A[r + n * c] = A[c + n * r];
+}
+// y = A x, A dense column-major symmetric (rows read as columns): one warp per output
+__global__ void symv_kernel(int64_t n, const double* A, const double* x, double* y) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < n;
+       row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const double* col = A + n * row;  // column `row` == row `row` (symmetric)
+    double s = 0;
+    for (int64_t k = lane; k < n; k += 32) s += col[k] * x[k];
+    s = warp_sum<double>(s);
+    if (lane == 0) y[row] = s;
+  }
+}
+
+}  // namespace hfk

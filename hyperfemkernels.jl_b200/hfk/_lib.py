@@ -1,0 +1,125 @@
+"""ctypes binding of ``libhfk.so`` (the C ABI declared in ``include/hfk.h``).
+
+This is the Python stand-in for the ``ccall``s the Julia host makes. Vector arguments may be numpy
+arrays (host memory) or CUDA tensors/arrays exposing ``data_ptr()`` (device memory); the library
+detects which. There is no CPU fallback: loading fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhfk.so")
+
+HFK_OK = 0
+LAW_SVK = 1
+LAW_LINEAR_ELASTIC = 2
+MF_STORED = 0
+MF_RECOMPUTE = 1
+FP64 = 0
+FP32 = 1
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+_pi = ctypes.POINTER(ctypes.c_int)
+_pi64 = ctypes.POINTER(ctypes.c_int64)
+_pd = ctypes.POINTER(ctypes.c_double)
+
+# name -> argtypes (every function returns int)
+SIGNATURES = {
+    "hfk_version": [],
+    "hfk_problem_create": [ctypes.POINTER(_vp), _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i, _vp, _i],
+    "hfk_problem_destroy": [_vp],
+    "hfk_problem_set_params": [_vp, _vp, _i],
+    "hfk_problem_set_stream": [_vp, _vp],
+    "hfk_problem_info": [_vp, _pi64, _pi, _pi, _pi, _pi64],
+    "hfk_launch_count": [_vp, _pi64],
+    "hfk_colors": [_vp, _vp],
+    "hfk_pattern_build": [_vp, _pi64],
+    "hfk_pattern_get": [_vp, _vp, _vp],
+    "hfk_nonzero_positions": [_vp, _vp],
+    "hfk_residual": [_vp, _vp, _vp, _vp],
+    "hfk_jacobian": [_vp, _vp, _vp, _vp],
+    "hfk_mf_prepare": [_vp, _vp, _vp, _i],
+    "hfk_mf_apply": [_vp, _vp, _vp],
+    "hfk_mf_apply_f32": [_vp, _vp, _vp],
+    "hfk_blocks_update": [_vp, _pi],
+    "hfk_blocks_apply": [_vp, _vp, _vp],
+    "hfk_blocks_get": [_vp, _pi, _vp, _vp, _vp],
+    "hfk_eigenvalue_bounds": [_vp, _i, _vp, _pd, _pd],
+    "hfk_hessenberg_eigvals": [_i, _vp, _vp, _vp],
+    "hfk_chebyshev_smooth": [_vp, _d, _d, _i, _vp, _vp, _i, _vp],
+    "hfk_transfer_create": [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp],
+    "hfk_transfer_destroy": [_vp],
+    "hfk_prolongate": [_vp, _vp, _vp],
+    "hfk_restrict": [_vp, _vp, _vp],
+    "hfk_inject": [_vp, _vp, _vp, _vp, _vp],
+    "hfk_pmg_create": [ctypes.POINTER(_vp), _i, _vp, _vp, _i, _d, _d, _i, _i, _i],
+    "hfk_pmg_destroy": [_vp],
+    "hfk_pmg_update": [_vp, _vp, _vp, _pi],
+    "hfk_pmg_vcycle": [_vp, _vp, _vp],
+    "hfk_pmg_level_info": [_vp, _i, _pd, _pd, _pd, _pd],
+    "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
+}
+
+_LIB = None
+
+
+class HFKError(RuntimeError):
+    """An error status from the library (message prefixed "HyperFEMKernels: ")."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib():
+    """The loaded library; raises if ``libhfk.so`` was not built (no silent fallback)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"HyperFEMKernels: {LIB_PATH} is missing; build it with __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.hfk_last_error.argtypes = []
+        L.hfk_last_error.restype = ctypes.c_char_p
+        _LIB = L
+    return _LIB
+
+
+def call(name, *args):
+    """Call an ABI function and raise ``HFKError`` on a non-zero status."""
+    L = lib()
+    rc = getattr(L, name)(*args)
+    if rc != HFK_OK:
+        raise HFKError(rc, L.hfk_last_error().decode())
+    return rc
+
+
+def ptr(a, dtype=np.float64):
+    """Address of a numpy array (checked dtype/contiguity) or a CUDA tensor (``data_ptr()``)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        import torch  # only when a tensor is passed
+
+        want = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32,
+                np.int64: torch.int64}[np.dtype(dtype).type]
+        if a.dtype != want or not a.is_contiguous():
+            raise TypeError(f"HyperFEMKernels: expected a contiguous {want} tensor")
+        return ctypes.c_void_p(a.data_ptr())
+    if not isinstance(a, np.ndarray):
+        raise TypeError("HyperFEMKernels: expected a numpy array or a CUDA tensor")
+    if a.dtype != np.dtype(dtype):
+        raise TypeError(f"HyperFEMKernels: expected dtype {np.dtype(dtype)}, got {a.dtype}")
+    if not (a.flags.c_contiguous or a.flags.f_contiguous):
+        raise TypeError("HyperFEMKernels: expected a contiguous array")
+    return ctypes.c_void_p(a.ctypes.data)

@@ -1,0 +1,327 @@
+"""Solver layer: ``BlockJacobi``, ``Chebyshev``, ``Prolongation``, ``PMultigrid``, ``MatrixFreeSolver``.
+
+Mirrors the reference's solver API (HyperFEMKernels ``src/preconditioners.jl``, ``src/smoothers.jl``,
+``src/transfers.jl``, ``src/pmultigrid.jl``, ``src/solvers.jl``) over the engine: the smoothers,
+V-cycle and Krylov iterations run on the GPU (``hfk_pmg_*``, ``hfk_solve_cg``). The Krylov method is
+an FP64 (flexible) CG with the true-residual stopping test ``||b - J x|| <= atol + rtol ||b||``.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr
+from .fespace import VectorLagrangeSpace, transfer_matrices
+from .operator import KernelOperator, MatrixFreeJacobian, Problem
+
+
+@dataclasses.dataclass(frozen=True)
+class Chebyshev:
+    """``Chebyshev(; degree = 2, range = 20.0, inflate = 1.1, eig_iters = 10)`` (src/smoothers.jl:21-33)."""
+
+    degree: int = 2
+    range: float = 20.0
+    inflate: float = 1.1
+    eig_iters: int = 10
+
+    def __post_init__(self):
+        if self.degree < 1:
+            raise ValueError("HyperFEMKernels: Chebyshev: degree must be ≥ 1")
+        if not self.range > 1:
+            raise ValueError("HyperFEMKernels: Chebyshev: range must be > 1")
+        if self.inflate < 1:
+            raise ValueError("HyperFEMKernels: Chebyshev: inflate must be ≥ 1")
+        if self.eig_iters < 2:
+            raise ValueError("HyperFEMKernels: Chebyshev: eig_iters must be ≥ 2")
+
+
+def chebyshev_damping(c: Chebyshev) -> float:
+    """Damping of the smoother on its interval, 1/T_k(theta/delta) (src/smoothers.jl:35-40)."""
+    b = 1.0
+    a = b / c.range
+    th, de = (b + a) / 2, (b - a) / 2
+    return 1.0 / math.cosh(c.degree * math.acosh(th / de))
+
+
+def chebyshev_start(n: int) -> np.ndarray:
+    """Fixed start vector of the eigenvalue estimate (src/smoothers.jl:68-71)."""
+    i = np.arange(1, n + 1, dtype=float)
+    v = np.sin(1.0 + 0.7 * i) + 0.3 * np.cos(2.3 * i)
+    return v / np.linalg.norm(v)
+
+
+class BlockJacobi:
+    """Preconditioner slot: inverse nodal block diagonal of the prepared tangent (src/preconditioners.jl:116)."""
+
+
+class BlockJacobiState:
+    def __init__(self, mf: MatrixFreeJacobian):
+        self.mf = mf
+        self.nbuild = 0
+        self.update(mf)
+
+    def update(self, mf: MatrixFreeJacobian):
+        self.mf = mf
+        ok = ctypes.c_int()
+        call("hfk_blocks_update", mf.op.problem.h, ctypes.byref(ok))
+        self.ok = bool(ok.value)
+        self.nbuild += 1
+        return self
+
+    def ldiv(self, y, r):
+        """``ldiv!(y, st, r)`` (src/preconditioners.jl:329-344)."""
+        call("hfk_blocks_apply", self.mf.op.problem.h, ptr(r), ptr(y))
+        return y
+
+    def blocks(self):
+        """(dofs (nb, 3) 1-based, B (nb, 3, 3), Binv (nb, 3, 3))."""
+        nb = ctypes.c_int()
+        call("hfk_blocks_get", self.mf.op.problem.h, ctypes.byref(nb), None, None, None)
+        n = nb.value
+        dofs = np.zeros(3 * n, dtype=np.int32)
+        B = np.zeros(9 * n)
+        Bi = np.zeros(9 * n)
+        call("hfk_blocks_get", self.mf.op.problem.h, ctypes.byref(nb), ptr(dofs, np.int32), ptr(B), ptr(Bi))
+        return (dofs.reshape(n, 3), B.reshape(n, 3, 3).transpose(0, 2, 1), Bi.reshape(n, 3, 3).transpose(0, 2, 1))
+
+
+def eigenvalue_bounds(mf: MatrixFreeJacobian, prec: BlockJacobiState, k: int = 10, b=None):
+    """``eigenvalue_bounds(mf, prec; k, b)`` (src/preconditioners.jl:374-389): (lmin, lmax)."""
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+    call("hfk_eigenvalue_bounds", mf.op.problem.h, k, ptr(bb) if bb is not None else None, ctypes.byref(lo),
+         ctypes.byref(hi))
+    return lo.value, hi.value
+
+
+def hessenberg_eigvals(H: np.ndarray):
+    """Eigenvalues of an upper Hessenberg matrix (the library's host QR iteration)."""
+    n = H.shape[0]
+    Hf = np.asfortranarray(H, dtype=np.float64)
+    re, im = np.zeros(n), np.zeros(n)
+    call("hfk_hessenberg_eigvals", n, ptr(Hf), ptr(re), ptr(im))
+    return re + 1j * im
+
+
+class Prolongation:
+    """``Prolongation(Uc, Uf)`` (src/transfers.jl:133-154) between two operators' problems on one mesh."""
+
+    def __init__(self, coarse: Problem, fine: Problem):
+        Qf, Qc = fine.space.Q, coarse.space.Q
+        self.E, self.Einj = transfer_matrices(Qf, Qc)
+        h = ctypes.c_void_p()
+        call("hfk_transfer_create", ctypes.byref(h), fine.h, coarse.h, ptr(self.E), ptr(self.Einj))
+        self.h = h
+        self.fine, self.coarse = fine, coarse
+        self.nf, self.nc = fine.nfree, coarse.nfree
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().hfk_transfer_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def prolongate(self, yf, xc):
+        """``prolongate!(yf, P, xc)`` (src/transfers.jl:238-245)."""
+        call("hfk_prolongate", self.h, ptr(xc), ptr(yf))
+        return yf
+
+    def restrict(self, yc, yf):
+        """``restrict!(yc, P, yf)`` (src/transfers.jl:252-259)."""
+        call("hfk_restrict", self.h, ptr(yf), ptr(yc))
+        return yc
+
+    def inject(self, xc, dc, xf, df):
+        """``inject!(xc, dc, P, xf, df)`` (src/transfers.jl:285-313)."""
+        call("hfk_inject", self.h, ptr(xf), ptr(df), ptr(xc), ptr(dc))
+        return xc, dc
+
+
+class PMultigrid:
+    """``PMultigrid(spaces; smoother = Chebyshev(), coarse = LUSolver(), coarse_every = 1)`` (src/pmultigrid.jl:256-267).
+
+    ``spaces`` lists the trial spaces of the levels, finest first (same mesh, same closed Dirichlet
+    boundary, nested orders). The coarsest level is assembled and factorised on the GPU (dense
+    Cholesky, FP64). ``precision`` "fp64" or "fp32" (smoothers and products of the levels above
+    the coarse one; the eigenvalue estimate and the coarse solve stay FP64).
+    """
+
+    def __init__(self, spaces, smoother: Chebyshev = Chebyshev(), coarse_every: int = 1, precision: str = "fp64"):
+        if len(spaces) < 2:
+            raise ValueError("HyperFEMKernels: PMultigrid needs at least two levels")
+        if coarse_every < 1:
+            raise ValueError("HyperFEMKernels: PMultigrid: coarse_every must be ≥ 1")
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("HyperFEMKernels: precision must be 'fp64' or 'fp32'")
+        self.spaces = list(spaces)
+        self.smoother = smoother
+        self.coarse_every = coarse_every
+        self.precision = precision
+
+
+class PMultigridState:
+    def __init__(self, prec: PMultigrid, mf: MatrixFreeJacobian):
+        self.prec = prec
+        op = mf.op
+        # level operators captured from the working operator's forms, with the working quadrature
+        # (the coarse operators integrate with the fine measure, src/pmultigrid.jl:244-247)
+        self.problems = [op.problem]
+        for U in prec.spaces[1:]:
+            self.problems.append(Problem(U, op.quad, op.res))
+        self.P = [Prolongation(self.problems[l + 1], self.problems[l]) for l in range(len(self.problems) - 1)]
+        L = len(self.problems)
+        lv = (ctypes.c_void_p * L)(*[p.h.value for p in self.problems])
+        tr = (ctypes.c_void_p * (L - 1))(*[t.h.value for t in self.P])
+        h = ctypes.c_void_p()
+        c = prec.smoother
+        call("hfk_pmg_create", ctypes.byref(h), L, lv, tr, c.degree, c.range, c.inflate, c.eig_iters, prec.coarse_every,
+             _lib.FP32 if prec.precision == "fp32" else _lib.FP64)
+        self.h = h
+        self.ncycle = 0
+        self.nbuild = 0
+        self.update(mf)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().hfk_pmg_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def update(self, mf: MatrixFreeJacobian):
+        """``preconditioner_update!`` (src/pmultigrid.jl:298-313): levels follow the operator's state."""
+        for p in self.problems[1:]:
+            p.set_params(mf.op.res)
+        ok = ctypes.c_int()
+        x = mf.x
+        call("hfk_pmg_update", self.h, ptr(x), ptr(mf.op.dirichlet_values()), ctypes.byref(ok))
+        self.ok = bool(ok.value)
+        self.nbuild += 1
+        return self
+
+    def ldiv(self, y, r):
+        """``ldiv!(y, st, r)`` (src/pmultigrid.jl:331-338): one V-cycle (NaN when not ok)."""
+        self.ncycle += 1
+        call("hfk_pmg_vcycle", self.h, ptr(r), ptr(y))
+        return y
+
+    def level_info(self, level: int):
+        a, b, lo, hi = (ctypes.c_double() for _ in range(4))
+        call("hfk_pmg_level_info", self.h, level, ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(a), ctypes.byref(b))
+        return dict(lmin=lo.value, lmax=hi.value, a=a.value, b=b.value)
+
+
+@dataclasses.dataclass
+class MatrixFreeSolver:
+    """``MatrixFreeSolver(; krylov, rtol, atol, maxiter, preconditioner)`` (src/solvers.jl:33-53).
+
+    ``krylov`` is "fcg" (flexible CG, for variable preconditioners such as a mixed-precision
+    V-cycle) or "cg".
+    """
+
+    krylov: str = "fcg"
+    rtol: float = 1e-8
+    atol: float = 0.0
+    maxiter: int = 500
+    preconditioner: object = None
+
+    def __post_init__(self):
+        if self.krylov not in ("fcg", "cg"):
+            raise ValueError(f"HyperFEMKernels: MatrixFreeSolver: krylov must be 'fcg' or 'cg' (got {self.krylov!r})")
+        if not (0 <= self.rtol < 1):
+            raise ValueError(f"HyperFEMKernels: the relative tolerance must be in [0, 1) (got {self.rtol})")
+        if self.atol < 0:
+            raise ValueError("HyperFEMKernels: MatrixFreeSolver: atol must be ≥ 0")
+        if self.maxiter <= 0:
+            raise ValueError("HyperFEMKernels: MatrixFreeSolver: maxiter must be positive")
+
+
+class MatrixFreeSolverNS:
+    def __init__(self, solver: MatrixFreeSolver, mf: MatrixFreeJacobian):
+        if not mf.prepared:
+            raise RuntimeError("HyperFEMKernels: the MatrixFreeJacobian has not been prepared "
+                               "(call jacobian!(mf, op, x) before numerical_setup)")
+        self.solver, self.mf = solver, mf
+        p = solver.preconditioner
+        if p is None:
+            self.prec = None
+        elif isinstance(p, PMultigrid):
+            self.prec = PMultigridState(p, mf)
+        else:
+            raise TypeError("HyperFEMKernels: unsupported preconditioner slot")
+        self.rtol = solver.rtol
+        self.iters, self.converged, self.indefinite, self.rnorm, self.nsetup = 0, True, False, float("nan"), 1
+
+    def update(self, mf):
+        self.mf = mf
+        self.nsetup += 1
+        if self.prec is not None:
+            self.prec.update(mf)
+        return self
+
+
+def symbolic_setup(ls: MatrixFreeSolver, mf):
+    if not isinstance(mf, MatrixFreeJacobian):
+        raise TypeError("HyperFEMKernels: MatrixFreeSolver applies a MatrixFreeJacobian; build the KernelOperator "
+                        "with jacobian = 'matrixfree'")
+    return ls
+
+
+def numerical_setup(ss: MatrixFreeSolver, mf: MatrixFreeJacobian) -> MatrixFreeSolverNS:
+    return MatrixFreeSolverNS(ss, mf)
+
+
+def numerical_setup_update(ns: MatrixFreeSolverNS, mf: MatrixFreeJacobian) -> MatrixFreeSolverNS:
+    """``numerical_setup!(ns, mf)`` (src/solvers.jl:106-109)."""
+    return ns.update(mf)
+
+
+def solve(x, ns: MatrixFreeSolverNS, b):
+    """``solve!(x, ns, b)`` (src/solvers.jl:111-159); x is the initial guess on input."""
+    s = ns.solver
+    it, conv, ind, rel = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    prec = ns.prec.h if ns.prec is not None else None
+    call("hfk_solve_cg", ns.mf.op.problem.h, prec, ptr(b), ptr(x), ns.rtol, s.atol, s.maxiter,
+         1 if s.krylov == "fcg" else 0, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(ind), ctypes.byref(rel))
+    ns.iters, ns.converged, ns.indefinite, ns.rnorm = it.value, bool(conv.value), bool(ind.value), rel.value
+    return x
+
+
+# hooks read by a Newton solver (src/solvers.jl:164-174)
+def linear_converged(ns):
+    return ns.converged
+
+
+def linear_iterations(ns):
+    return ns.iters
+
+
+def linear_indefinite(ns):
+    return ns.indefinite
+
+
+def set_tolerance(ns, rtol):
+    if rtol is None:
+        ns.rtol = ns.solver.rtol
+    else:
+        if not (0 <= rtol < 1):
+            raise ValueError(f"HyperFEMKernels: the relative tolerance must be in [0, 1) (got {rtol})")
+        ns.rtol = float(rtol)
+    return ns
+
+
+def tolerance(ns):
+    return ns.rtol
+
+
+def preconditioner_builds(ns):
+    return 0 if ns.prec is None else ns.prec.nbuild

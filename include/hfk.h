@@ -1,0 +1,176 @@
+/* hfk.h - C ABI of the B200 engine for HyperFEMKernels' hot path.
+ *
+ * The reference (MultiSimOLab/HyperFEMKernels.jl) is Julia; its host side keeps capturing and
+ * lowering the Gridap weak form and calls these functions with `ccall` in place of its own
+ * element loops. Citations are file:line in the reference repository.
+ *
+ * Conventions (those of the reference's arrays, so that Julia passes them without copies):
+ *  - arrays are column-major with the reference's logical shapes;
+ *  - cell_dof_ids is (ndl, ncells) Int32 with ndl = 3*nn and ldof = c*nn + n (the CONTIG layout of
+ *    FieldTable, src/tables.jl:181-182); > 0 = free dof id (1-based), < 0 = -(Dirichlet index);
+ *  - free-dof vectors have length nfree, Dirichlet vectors length ndir;
+ *  - CSC patterns are Julia's SparseMatrixCSC{Float64,Int}: colptr/rowval Int64 1-based;
+ *  - every vector argument may be a host pointer or a device pointer (CUDA device or managed
+ *    memory); the library detects which and copies host data through its own device buffers;
+ *  - every function returns HFK_OK (0) or an error code; hfk_last_error() gives the message,
+ *    prefixed "HyperFEMKernels: " like the reference's exceptions;
+ *  - numerical failure (a non-finite tangent, an indefinite level) is a status output, not an
+ *    error code (src/pmultigrid.jl:331-335, src/solvers.jl:114-121);
+ *  - a handle is not reentrant: calls on one handle must not overlap (src/assembly.jl:363-367).
+ *    Each handle launches on its own CUDA stream (hfk_problem_set_stream to choose it).
+ */
+#ifndef HFK_H
+#define HFK_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HFK_OK 0
+#define HFK_ERR_ARG 1
+#define HFK_ERR_CUDA 2
+#define HFK_ERR_STATE 3
+#define HFK_ERR_UNSUPPORTED 4
+#define HFK_ERR_NUMERIC 5
+#define HFK_ERR_PATTERN 6
+#define HFK_ERR_INTERNAL 7
+
+/* pointwise laws the host recognised from the captured tree (src/tree.jl:253-283) */
+#define HFK_LAW_SVK 1            /* St Venant-Kirchhoff P(F) = F S(E); params lambda, mu[, body x y z] */
+#define HFK_LAW_LINEAR_ELASTIC 2 /* sigma = lambda tr(H) I + mu (H + H'); params lambda, mu[, body] */
+
+/* matrix-free formulations */
+#define HFK_MF_STORED 0    /* reference partial assembly: T, inv(Jt), dV stored per point (src/matrixfree.jl:14-23) */
+#define HFK_MF_RECOMPUTE 1 /* tangent re-evaluated from the state at every product (no per-point storage) */
+
+typedef struct hfk_problem hfk_problem;
+typedef struct hfk_transfer hfk_transfer;
+typedef struct hfk_pmg hfk_pmg;
+
+/* Message of the last error on this thread. */
+const char* hfk_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+int hfk_version(void);
+
+/* ---- operator: one volume group of a 3-component Lagrangian field on hexahedra ----------------
+ * Replaces the construction of KernelOperator (src/assembly.jl:630-666) for a group whose law the
+ * host recognised: the field layout (FieldLayout/cell_dof_matrix, src/assembly.jl:20-30,
+ * src/tables.jl:329-342), the geometry (GeoTable, src/tables.jl:42-106), the reference tables
+ * (FieldTable, src/tables.jl:171-237), and the tensor-product structure found numerically from xq
+ * and Nt (TPTable, src/tensorproduct.jl:55-91). Cells are coloured at construction
+ * (color_cells, src/coloring.jl:4-28).
+ *   nn nodes per cell (Q^3), np quadrature points (P^3), ng geometry nodes (8: trilinear map)
+ *   xq (3, np) reference points; w (np) weights; Nt (nn, np); dNt (nn, 3, np); dMt (ng, 3, np)
+ *   coords (3, ng, ncells) vertex coordinates; cell_dof_ids (3*nn, ncells) */
+int hfk_problem_create(hfk_problem** out, int nn, int np, int ng, int ncells, const double* xq, const double* w,
+                       const double* Nt, const double* dNt, const double* dMt, const double* coords,
+                       const int32_t* cell_dof_ids, int64_t nfree, int64_t ndir, int law, const double* params,
+                       int nparams);
+int hfk_problem_destroy(hfk_problem* p);
+/* Cheap update(op, res, jac) of the same structure: new law parameters, tables/pattern/colours kept
+ * (src/assembly.jl:693-744). */
+int hfk_problem_set_params(hfk_problem* p, const double* params, int nparams);
+/* Launch on `stream` (a cudaStream_t) from now on; NULL restores the handle's own stream. */
+int hfk_problem_set_stream(hfk_problem* p, void* stream);
+int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolors, int64_t* nnz);
+/* Number of kernels this handle launched so far (launch accounting for benchmarks). */
+int hfk_launch_count(hfk_problem* p, int64_t* count);
+
+/* Colour of every cell, 1-based (color_cells, src/coloring.jl:4-28; bit-exact greedy first fit). */
+int hfk_colors(hfk_problem* p, int32_t* color_of_cell);
+
+/* Sparsity pattern of the Jacobian and the positions of the element entries
+ * (sparsity/full_keys!/cell_positions!, src/assembly.jl:773-899). Built on the GPU;
+ * identical to the reference's sorted-key construction. */
+int hfk_pattern_build(hfk_problem* p, int64_t* nnz);
+/* sparsity_pattern(op) (src/assembly.jl:768): colptr (nfree+1), rowval (nnz), 1-based. */
+int hfk_pattern_get(hfk_problem* p, int64_t* colptr, int64_t* rowval);
+/* nonzero_positions(op) (src/assembly.jl:771): (ndl*ndl, ncells) Int32, 1-based, 0 = not stored;
+ * entry ii + ndl*jj of a cell = (test ii, trial jj). */
+int hfk_nonzero_positions(hfk_problem* p, int32_t* nzpos);
+
+/* residual!(b, op, x) (src/assembly.jl:909-916): b (nfree) = assembled residual at the free values
+ * x and Dirichlet values dvals. FP64. */
+int hfk_residual(hfk_problem* p, const double* x, const double* dvals, double* b);
+/* jacobian!(A, op, x) (src/assembly.jl:918-927): nzval (nnz) of the CSC Jacobian in rowval order
+ * (zero-filled, then the fused element kernels and the colour-by-colour scatter). FP64. */
+int hfk_jacobian(hfk_problem* p, const double* x, const double* dvals, double* nzval);
+
+/* prepare!(mf, x) / jacobian!(mf, op, x) (src/matrixfree.jl:97-100, :140-159): bind the state.
+ * mode HFK_MF_STORED stores T, inv(Jt), dV per point as the reference does; HFK_MF_RECOMPUTE keeps
+ * only the state and re-evaluates the tangent inside every product. */
+int hfk_mf_prepare(hfk_problem* p, const double* x, const double* dvals, int mode);
+/* mul!(y, mf, dx) (src/matrixfree.jl:246-260): y = J(x) dx on free dofs (Dirichlet increments zero),
+ * sum-factorised. FP64. */
+int hfk_mf_apply(hfk_problem* p, const double* dx, double* y);
+/* The same product in FP32 (state, increment and result in FP32; mixed-precision smoothers). */
+int hfk_mf_apply_f32(hfk_problem* p, const float* dx, float* y);
+
+/* BlockJacobi nodal blocks of the prepared tangent (field_blocks/block_diagonal!/invert_blocks!,
+ * src/preconditioners.jl:151-327); ok = 0 if a block is not finite. */
+int hfk_blocks_update(hfk_problem* p, int* ok);
+/* ldiv!(y, BlockJacobiState, r) (src/preconditioners.jl:329-344). */
+int hfk_blocks_apply(hfk_problem* p, const double* r, double* y);
+/* Blocks as the reference stores them: dofs (3, nblocks) 1-based (0 = fixed component), B and Binv
+ * (3, 3, nblocks). Any output may be NULL; nblocks is always written. */
+int hfk_blocks_get(hfk_problem* p, int* nblocks, int32_t* dofs, double* B, double* Binv);
+
+/* eigenvalue_bounds(mf, BlockJacobi; k, b) (src/preconditioners.jl:374-389): Ritz bounds of the
+ * block-preconditioned tangent after k Arnoldi steps from `start` (NULL = the Chebyshev start vector
+ * sin(1+0.7i)+0.3cos(2.3i), src/smoothers.jl:68-71). FP64. */
+int hfk_eigenvalue_bounds(hfk_problem* p, int k, const double* start, double* lmin, double* lmax);
+/* Eigenvalues (real, imaginary parts) of an n x n upper Hessenberg matrix (column-major), the eigvals
+ * call of eigenvalue_bounds (src/preconditioners.jl:386); host only. */
+int hfk_hessenberg_eigvals(int n, const double* H, double* re, double* im);
+/* smooth!(x, ChebyshevState, rhs; zero_guess, residual) (src/smoothers.jl:116-146) on [a, b]:
+ * `degree` steps; residual may be NULL. FP64. */
+int hfk_chebyshev_smooth(hfk_problem* p, double a, double b, int degree, const double* rhs, double* x,
+                         int zero_guess, double* residual);
+
+/* ---- transfers between nested levels on one mesh (src/transfers.jl) --------------------------
+ * E (nn_f, nn_c): coarse basis at the fine nodes; Einj (nn_c, nn_f): fine basis at the coarse
+ * nodes (TransferField, src/transfers.jl:57-131). */
+int hfk_transfer_create(hfk_transfer** out, hfk_problem* fine, hfk_problem* coarse, const double* E,
+                        const double* Einj);
+int hfk_transfer_destroy(hfk_transfer* t);
+/* prolongate!(yf, P, xc) (src/transfers.jl:238-245) */
+int hfk_prolongate(hfk_transfer* t, const double* xc, double* yf);
+/* restrict!(yc, P, yf) (src/transfers.jl:252-259) */
+int hfk_restrict(hfk_transfer* t, const double* yf, double* yc);
+/* inject!(xc, dc, P, xf, df) (src/transfers.jl:285-313) */
+int hfk_inject(hfk_transfer* t, const double* xf, const double* df, double* xc, double* dc);
+
+/* ---- p-multigrid (src/pmultigrid.jl) ---------------------------------------------------------
+ * levels[0] is the working level (its state is bound by hfk_pmg_update), levels[nlevels-1] the
+ * assembled coarse level (solved by a dense Cholesky factorisation on the GPU, in place of the
+ * reference's LUSolver); transfers[l] goes from level l+1 to level l. Chebyshev(degree, range,
+ * inflate, eig_iters) as src/smoothers.jl:21-33. precision HFK_FP64 or HFK_FP32: the arithmetic of
+ * the smoothers and products on the levels above the coarse one (the coarse solve is always FP64). */
+#define HFK_FP64 0
+#define HFK_FP32 1
+int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_transfer* const* transfers,
+                   int degree, double range, double inflate, int eig_iters, int coarse_every, int precision);
+int hfk_pmg_destroy(hfk_pmg* m);
+/* update_levels! + smoother updates (src/pmultigrid.jl:168-221, :298-313): inject the fine state
+ * (x, dvals), prepare every level, extract blocks and intervals, assemble and factorise the coarse
+ * level every coarse_every updates. ok = 0 when a level is not usable (NaN tangent, indefinite). */
+int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok);
+/* ldiv!(y, PMultigridState, r) (src/pmultigrid.jl:316-338): one V-cycle; NaN when not ok. */
+int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y);
+/* Interval and Ritz values of a level's smoother. */
+int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
+
+/* ---- Krylov (src/solvers.jl) ----------------------------------------------------------------
+ * MatrixFreeSolver.solve! (src/solvers.jl:111-159) with an FP64 (flexible) CG on the prepared
+ * operator `op` preconditioned by `prec` (NULL = none): stops when ||b - J x|| <= atol + rtol ||b||
+ * (true residual). flexible != 0 uses the Polak-Ribiere beta (a variable preconditioner, e.g. a
+ * mixed-precision V-cycle). x is the initial guess on input. A non-positive curvature stops with
+ * converged = 0 and indefinite = 1; an unusable preconditioner returns at once, iters = 0. */
+int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                 int flexible, int* iters, int* converged, int* indefinite, double* relres);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,62 @@
+"""The C ABI library loads and exports every symbol that include/hfk.h declares (no GPU needed)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+
+from hfk import _lib
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "hfk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(hfk_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_every_declared_symbol_is_exported_and_bound():
+    L = _lib.lib()
+    names = declared_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in _lib.SIGNATURES or n == "hfk_last_error", f"{n} has no ctypes signature"
+
+
+def test_version_and_error_prefix():
+    L = _lib.lib()
+    assert L.hfk_version() >= 100
+    with pytest.raises(_lib.HFKError) as e:
+        _lib.call("hfk_problem_create", None, 0, 0, 0, 0, None, None, None, None, None, None, None, 0, 0, 1, None, 0)
+    assert str(e.value).startswith("HyperFEMKernels: ")
+    assert e.value.code == 1
+
+
+def test_hessenberg_eigenvalues_match_lapack():
+    # the eigvals call of eigenvalue_bounds (src/preconditioners.jl:386) in the library's host code
+    from hfk.solvers import hessenberg_eigvals
+
+    rng = np.random.default_rng(0)
+    for n in (1, 2, 3, 5, 10, 20):
+        for sym in (False, True):
+            A = rng.standard_normal((n, n))
+            if sym:
+                A = A @ A.T + n * np.eye(n)
+            H = np.triu(A, -1)
+            ev = np.sort_complex(hessenberg_eigvals(H))
+            ref = np.sort_complex(np.linalg.eigvals(H))
+            assert np.allclose(ev, ref, atol=1e-9 * max(1, np.abs(ref).max())), (n, ev, ref)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the failure mode without a GPU")
+def test_operations_fail_loudly_without_a_device():
+    from conftest import svk_space
+    from hfk.forms import svk_residual, svk_jacobian
+    from hfk.operator import KernelOperator
+
+    V = svk_space(order=2)
+    with pytest.raises(_lib.HFKError) as e:
+        KernelOperator(svk_residual(), svk_jacobian(), V)
+    assert "CUDA" in str(e.value)

@@ -1,0 +1,281 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle on seeded inputs.
+
+Tolerances: FP64 results agree with the oracle to <= 1e-12 relative (different summation order:
+sum factorisation vs dense tables, GPU vs CPU reductions); integer results (colours, pattern,
+positions) are bit-exact. FP32 products are checked against the FP64 oracle at 2e-6 relative.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import reldiff, svk_space, svk_state
+
+import oracle as O
+from hfk import forms
+from hfk.fespace import CartesianMesh, Quadrature, VectorLagrangeSpace
+from hfk.operator import KernelOperator, MatrixFreeJacobian
+from hfk import solvers as S
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+def make(order=2, n=(3, 2, 2), perturb=0.0, law="svk", body=(0.0, 0.0, 0.0), faces=("x0", "x1"), jac="assembled"):
+    V = svk_space(n=n, order=order, perturb=perturb, faces=faces)
+    deg = 2 * order
+    if law == "svk":
+        res, jf = forms.svk_residual(2.0, 1.0, deg, body), forms.svk_jacobian(2.0, 1.0, deg)
+        olaw = O.LAW_SVK
+    else:
+        res, jf = forms.linear_elastic_residual(2.0, 1.0, deg, body), forms.linear_elastic_jacobian(2.0, 1.0, deg)
+        olaw = O.LAW_LINEAR
+    op = KernelOperator(res, jf, V, V, jacobian=jac)
+    orc = O.OracleProblem(V, Quadrature.gauss(deg), olaw, (2.0, 1.0) + tuple(body))
+    return V, op, orc
+
+
+CASES = [(1, 0.0), (2, 0.0), (2, 0.2), (3, 0.0), (4, 0.0)]
+
+
+@pytest.mark.parametrize("order,perturb", CASES)
+def test_colours_bit_exact(order, perturb):
+    V, op, orc = make(order, perturb=perturb)
+    assert np.array_equal(op.problem.colors(), orc.colors)
+
+
+@pytest.mark.parametrize("order,perturb", [(1, 0.0), (2, 0.0), (2, 0.2)])
+def test_pattern_and_positions_bit_exact(order, perturb):
+    V, op, orc = make(order, perturb=perturb)
+    colptr, rowval = op.pattern_julia()
+    ocp, orv = orc.pattern()
+    assert np.array_equal(colptr, ocp) and np.array_equal(rowval, orv)
+    assert np.array_equal(op.nonzero_positions(), orc.nzpos)
+
+
+@pytest.mark.parametrize("order,perturb", CASES)
+@pytest.mark.parametrize("law", ["svk", "linear"])
+def test_residual_parity(order, perturb, law):
+    V, op, orc = make(order, perturb=perturb, law=law, body=(0.3, -0.2, 0.5))
+    x = svk_state(V, amp=1e-2)
+    b = op.residual(np.zeros(V.nfree), x)
+    assert reldiff(b, orc.residual(x, V.dirichlet_values)) < TOL64
+
+
+@pytest.mark.parametrize("order,perturb", [(1, 0.0), (2, 0.0), (2, 0.2)])
+@pytest.mark.parametrize("law", ["svk", "linear"])
+def test_jacobian_parity(order, perturb, law):
+    V, op, orc = make(order, perturb=perturb, law=law)
+    x = svk_state(V, amp=1e-2)
+    A = op.allocate_jacobian(x)
+    op.jacobian(A, x)
+    ref = orc.jacobian_values(x, V.dirichlet_values)
+    assert reldiff(A.data, ref) < TOL64
+    # a second assembly into the same matrix (zero-fill) gives the same values
+    op.jacobian(A, x)
+    assert reldiff(A.data, ref) < TOL64
+
+
+@pytest.mark.parametrize("order,perturb", CASES)
+@pytest.mark.parametrize("mode", ["recompute", "stored"])
+def test_matrix_free_product_parity(order, perturb, mode):
+    V, op, orc = make(order, perturb=perturb, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op, mode)
+    op.jacobian(mf, x)
+    orc.mf_prepare(x, V.dirichlet_values)
+    dx = np.random.default_rng(1).standard_normal(V.nfree)
+    y = mf.mul(np.zeros(V.nfree), dx)
+    assert reldiff(y, orc.mf_apply(dx)) < TOL64
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_matrix_free_fp32_error_bounded(order):
+    V, op, orc = make(order, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    orc.mf_prepare(x, V.dirichlet_values)
+    dx = np.random.default_rng(1).standard_normal(V.nfree)
+    y32 = mf.mul_f32(np.zeros(V.nfree, dtype=np.float32), dx.astype(np.float32))
+    assert reldiff(y32.astype(np.float64), orc.mf_apply(dx)) < 2e-6
+
+
+def test_device_pointers_and_host_pointers_agree():
+    import torch
+
+    V, op, orc = make(2, jac="matrixfree")
+    x = svk_state(V)
+    b_host = op.residual(np.zeros(V.nfree), x)
+    xd = torch.from_numpy(x).cuda()
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).cuda()
+    bd = torch.zeros(V.nfree, dtype=torch.float64, device="cuda")
+    op.residual(bd, xd, dd)
+    assert np.array_equal(bd.cpu().numpy(), b_host)
+
+
+def test_blocks_parity():
+    V, op, orc = make(2, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    st = S.BlockJacobiState(mf)
+    assert st.ok
+    orc.mf_prepare(x, V.dirichlet_values)
+    od, oB, oBi = orc.blocks()
+    gd, gB, gBi = st.blocks()
+    assert np.array_equal(gd, od)
+    assert reldiff(gB, oB) < TOL64 and reldiff(gBi, oBi) < 1e-11
+    r = np.random.default_rng(3).standard_normal(V.nfree)
+    assert reldiff(st.ldiv(np.zeros(V.nfree), r), orc.blocks_apply(r)) < 1e-11
+
+
+def test_eigenvalue_bounds_and_chebyshev_parity():
+    V, op, orc = make(2, n=(3, 3, 2), jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    st = S.BlockJacobiState(mf)
+    orc.mf_prepare(x, V.dirichlet_values)
+    ocheb = O.OracleChebyshev(orc, degree=3)
+    lo, hi = S.eigenvalue_bounds(mf, st, 10)
+    assert abs(hi - ocheb.lmax) < 1e-9 * ocheb.lmax and abs(lo - ocheb.lmin) < 1e-8 * ocheb.lmax
+    rhs = np.random.default_rng(0).standard_normal(V.nfree)
+    xg = np.zeros(V.nfree)
+    rg = np.zeros(V.nfree)
+    from hfk._lib import call, ptr
+
+    call("hfk_chebyshev_smooth", op.problem.h, ocheb.a, ocheb.b, 3, ptr(rhs), ptr(xg), 1, ptr(rg))
+    xo, ro = ocheb.smooth(None, rhs, zero_guess=True, want_residual=True)
+    assert reldiff(xg, xo) < 1e-11 and reldiff(rg, ro) < 1e-10
+
+
+@pytest.mark.parametrize("qf,qc", [(2, 1), (4, 2), (3, 2)])
+def test_transfers_parity(qf, qc):
+    m = CartesianMesh((2, 3, 2))
+    Vf = VectorLagrangeSpace(m, qf, ("x0", "x1"))
+    Vc = VectorLagrangeSpace(m, qc, ("x0", "x1"))
+    q = Quadrature.gauss(2 * qf)
+    opf = KernelOperator(forms.svk_residual(degree=2 * qf), forms.svk_jacobian(degree=2 * qf), Vf)
+    opc = KernelOperator(forms.svk_residual(degree=2 * qf), forms.svk_jacobian(degree=2 * qf), Vc)
+    P = S.Prolongation(opc.problem, opf.problem)
+    T = O.OracleTransfer(Vf, Vc)
+    rng = np.random.default_rng(0)
+    xc, yf = rng.standard_normal(Vc.nfree), rng.standard_normal(Vf.nfree)
+    assert reldiff(P.prolongate(np.zeros(Vf.nfree), xc), T.prolongate(xc)) < 1e-14
+    assert reldiff(P.restrict(np.zeros(Vc.nfree), yf), T.restrict(yf)) < 1e-14
+    df = rng.standard_normal(Vf.ndir)
+    xi, di = P.inject(np.zeros(Vc.nfree), np.zeros(Vc.ndir), yf, df)
+    oxi, odi = T.inject(yf, df, Vc.nfree, Vc.ndir)
+    assert reldiff(xi, oxi) < 1e-14 and reldiff(di, odi) < 1e-14
+
+
+def _pmg_case(n, orders, law="linear"):
+    m = CartesianMesh((n, n, n))
+    g = lambda x: np.stack([0.01 * x[:, 0], -0.02 * x[:, 1] * x[:, 2], 0.005 + 0 * x[:, 0]], axis=1)
+    Vs = [VectorLagrangeSpace(m, o, "boundary", g=g if l == 0 else None) for l, o in enumerate(orders)]
+    deg = 2 * orders[0]
+    body = (0.3, -0.2, 0.5)
+    if law == "linear":
+        res, jac = forms.linear_elastic_residual(2.0, 1.0, deg, body), forms.linear_elastic_jacobian(2.0, 1.0, deg)
+    else:
+        res, jac = forms.svk_residual(2.0, 1.0, deg, body), forms.svk_jacobian(2.0, 1.0, deg)
+    return Vs, res, jac
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vcycle_parity_with_oracle(precision):
+    Vs, res, jac = _pmg_case(3, (2, 1), "svk")
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = svk_state(Vs[0], amp=0.0, disp=0.0)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=2), precision=precision), mf)
+    assert st.ok
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_SVK, (2.0, 1.0, 0.3, -0.2, 0.5), degree=2)
+    mg.update(x, Vs[0].dirichlet_values)
+    info = st.level_info(0)
+    assert abs(info["b"] - mg.smoothers[0].b) < 1e-9 * mg.smoothers[0].b
+    r = np.random.default_rng(2).standard_normal(Vs[0].nfree)
+    y = st.ldiv(np.zeros(Vs[0].nfree), r)
+    tol = 1e-9 if precision == "fp64" else 1e-5
+    assert reldiff(y, mg.ldiv(r)) < tol
+
+
+@pytest.mark.parametrize("orders", [(2, 1), (3, 1), (4, 2, 1)])
+def test_pmg_solve_matches_direct_and_iterations_bounded(orders):
+    # test/solvers/test_pmultigrid.jl:37-51
+    its = []
+    for n in (2, 4):
+        Vs, res, jac = _pmg_case(n, orders)
+        op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+        x = np.zeros(Vs[0].nfree)
+        mf = op.allocate_jacobian(x)
+        op.jacobian(mf, x)
+        b = -op.residual(np.zeros(Vs[0].nfree), x)
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-10, maxiter=200, preconditioner=S.PMultigrid(Vs))
+        ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf)
+        dx = S.solve(np.zeros(Vs[0].nfree), ns, b)
+        assert S.linear_converged(ns)
+        ref_op = KernelOperator(res, jac, Vs[0])
+        A = ref_op.allocate_jacobian(x)
+        ref_op.jacobian(A, x)
+        ref = sp.linalg.spsolve(A.tocsc(), b)
+        assert reldiff(dx, ref) < 1e-8
+        its.append(S.linear_iterations(ns))
+    assert all(i <= 30 for i in its)
+    assert its[1] <= 1.4 * its[0] + 2
+
+
+def test_mixed_precision_solve_reaches_fp64_tolerance():
+    Vs, res, jac = _pmg_case(4, (2, 1), "svk")
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = np.zeros(Vs[0].nfree)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    b = -op.residual(np.zeros(Vs[0].nfree), x)
+    for prec in ("fp64", "fp32"):
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, preconditioner=S.PMultigrid(Vs, precision=prec))
+        ns = S.numerical_setup(ls, mf)
+        dx = S.solve(np.zeros(Vs[0].nfree), ns, b)
+        assert S.linear_converged(ns)
+        r = b - mf @ dx
+        assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b) * 1.01
+
+
+def test_nan_state_makes_the_preconditioner_fail_as_a_status():
+    # test/solvers/test_pmultigrid.jl:117-133: a NaN tangent gives ok = false, NaN from ldiv, failed solve
+    Vs, res, jac = _pmg_case(2, (2, 1), "svk")
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = np.zeros(Vs[0].nfree)
+    x[5] = np.nan
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, preconditioner=S.PMultigrid(Vs))
+    ns = S.numerical_setup(ls, mf)
+    assert not ns.prec.ok
+    y = ns.prec.ldiv(np.zeros(Vs[0].nfree), np.ones(Vs[0].nfree))
+    assert np.all(np.isnan(y))
+    dx = S.solve(np.zeros(Vs[0].nfree), ns, np.ones(Vs[0].nfree))
+    assert not S.linear_converged(ns) and S.linear_iterations(ns) == 0
+
+
+def test_update_changes_parameters_keeps_structure():
+    V, op, orc = make(2)
+    x = svk_state(V, amp=1e-2)
+    op2 = op.update(forms.svk_residual(4.0, 0.5, 4), forms.svk_jacobian(4.0, 0.5, 4))
+    assert op2.problem is op.problem
+    orc.set_params((4.0, 0.5))
+    assert reldiff(op2.residual(np.zeros(V.nfree), x), orc.residual(x, V.dirichlet_values)) < TOL64
+
+
+def test_single_cell_and_all_dirichlet_but_one_node():
+    m = CartesianMesh((1, 1, 1))
+    V = VectorLagrangeSpace(m, 2, "boundary")  # one interior node: 3 free dofs
+    op = KernelOperator(forms.svk_residual(), forms.svk_jacobian(), V)
+    orc = O.OracleProblem(V, Quadrature.gauss(4))
+    x = np.array([0.01, -0.02, 0.03])
+    assert reldiff(op.residual(np.zeros(3), x), orc.residual(x, V.dirichlet_values)) < TOL64
+    A = op.allocate_jacobian(x)
+    op.jacobian(A, x)
+    assert reldiff(A.data, orc.jacobian_values(x, V.dirichlet_values)) < TOL64
