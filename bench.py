@@ -1,0 +1,351 @@
+"""Benchmark of the hot path: matrix-free SVK Jacobian-vector product, Q2 hexahedra on a 64^3 cube.
+
+One step = one J(x)·dx over the whole mesh (6.34 M free dofs), FP64, tangent re-evaluated from the
+state inside the product (sum factorisation). Inputs are resident in HBM for `value`; `e2e` runs the
+same product through the public C ABI with pinned host buffers (dx copied in, y copied out every
+step). Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`--impl reference` times the CPU restatement of the reference algorithm (the oracle: the
+reference's stored-tangent matrix-free product, OpenMP over all host cores) on a bounded sample of
+the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hyperfemkernels.jl_b200"))
+
+METRIC = "Q2 SVK Jacobian GDOF/s (matrix-free J*v, FP64)"
+UNIT = "GDOF/s"
+N_CELLS = 64
+ORDER = 2
+WORKLOAD = "MF Jacobian-vector product, SVK (lambda=2, mu=1), Q2 hexahedra, 64^3 unit cube, Gauss 3^3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS, help="cells per direction")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def build_case(n, order=ORDER, seed=0):
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+
+    m = CartesianMesh((n, n, n))
+    g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
+    V = VectorLagrangeSpace(m, order, ("x0", "x1"), g=g)
+    rng = np.random.default_rng(seed)
+    x, _ = V.interpolate(lambda p: np.stack([0.05 * p[:, 0], 0 * p[:, 0], 0 * p[:, 0]], axis=1))
+    x = x + rng.uniform(-1e-3, 1e-3, V.nfree)
+    dx = np.random.default_rng(seed + 1).standard_normal(V.nfree)
+    return V, x, dx
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [s.strip() for s in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def jv_flops_per_cell(Q, P):
+    """FP64 flops of one recompute J*v cell: 6 interpolations, 3 contractions, pointwise law."""
+    interp = 2 * (2 * P * Q**3 + 3 * P**2 * Q**2 + 3 * P**3 * Q)  # x, y, z sweeps (FMA = 2)
+    contract = 2 * (3 * P**3 * Q + 3 * P**2 * Q**2 + 2 * P * Q**3)
+    pointwise = P**3 * (2 * (27 + 27 + 18 + 27 + 27 + 27 + 27) + 60)  # grads, F'F, F'Hd, Hd S, F W, pull-back
+    return 6 * interp + 3 * contract + pointwise
+
+
+def engine(args):
+    import torch
+    import torch.distributed as dist
+
+    from hfk import _lib, forms
+    from hfk.operator import KernelOperator, MatrixFreeJacobian
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    V, x, dx = build_case(args.n)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V, jacobian="matrixfree")
+    stream = torch.cuda.current_stream()
+    op.problem.set_stream(stream.cuda_stream)
+    n = V.nfree
+    dev = torch.device("cuda", local)
+    xd = torch.from_numpy(x).to(dev)
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+    dxd = torch.from_numpy(dx).to(dev)
+    yd = torch.zeros(n, dtype=torch.float64, device=dev)
+    mf = MatrixFreeJacobian(op, "recompute")
+    mf.prepare(xd, dd)
+    h = op.problem.h
+
+    def step():
+        _lib.call("hfk_mf_apply", h, _lib.ptr(dxd), _lib.ptr(yd))
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- headline: device-resident FP64 J*v ----
+    step()
+    torch.cuda.synchronize()
+    l0 = op.problem.launches()
+    with ClockSampler(local) as clk:
+        ms = timed(step, args.steps, args.warmup)
+    launches = (op.problem.launches() - l0) // (args.steps + args.warmup) * args.steps
+    ms_step = ms / args.steps
+    value = world * n / (ms_step * 1e-3) / 1e9
+    clocks = clk.summary()
+
+    # ---- e2e: host (pinned) buffers through the public ABI, H2D + D2H inside every step ----
+    dxh = torch.from_numpy(dx).pin_memory()
+    yh = torch.zeros(n, dtype=torch.float64).pin_memory()
+
+    def step_e2e():
+        _lib.call("hfk_mf_apply", h, _lib.ptr(dxh), _lib.ptr(yh))
+
+    ms_e2e = timed(step_e2e, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
+    e2e = {"value": world * n / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+           "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e}
+
+    # ---- roofline of the dominant kernel (colour launches of the J*v cell kernel) ----
+    ncells = V.mesh.ncells
+    alg_bytes = 4 * V.ndl * ncells + 8 * n * 3 + 8 * V.ndir + 81 * ncells  # ids, u, dx, y, dvals, geometry
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm, src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        hbm, src = 6650.0, "fallback"
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    flops = jv_flops_per_cell(3, 3) * ncells
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "peak_source": src, "bytes_per_launch": alg_bytes,
+                "fp64_tflops": flops / (ms_step * 1e-3) / 1e12, "fp64_flops_per_launch": flops,
+                "note": "recompute J*v is FP64-issue bound; hbm frac uses the algorithmic bytes"}
+
+    extra = {}
+    if not args.no_extra and rank == 0:
+        # reference formulation on the GPU: stored tangents (T, inv(Jt), dV per point)
+        mfs = MatrixFreeJacobian(op, "stored")
+        mfs.prepare(xd, dd)
+        ms_s = timed(step, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
+        stored_bytes = 8 * 91 * 27 * ncells + 8 * n * 2 + 4 * V.ndl * ncells
+        extra["jv_stored_fp64"] = {"gdofs": n / (ms_s * 1e-3) / 1e9, "ms": ms_s,
+                                   "hbm_frac": stored_bytes / (ms_s * 1e-3) / 1e9 / hbm}
+        mf.prepare(xd, dd)
+        dx32 = dxd.float()
+        y32 = torch.zeros(n, dtype=torch.float32, device=dev)
+
+        def step32():
+            _lib.call("hfk_mf_apply_f32", h, _lib.ptr(dx32, np.float32), _lib.ptr(y32, np.float32))
+
+        ms32 = timed(step32, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
+        step()
+        torch.cuda.synchronize()
+        err32 = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
+        extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
+        extra.update(assembly_case(torch, dev, stream, timed))
+
+    cpu = cpu_baseline_sample() if rank == 0 and not args.no_cpu else None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "cells": ncells, "free_dofs_per_gpu": n, "order": ORDER,
+                           "quadrature_points_per_cell": 27, "parallelism": f"replicas x{world}",
+                           "l2": f"inputs larger than L2 ({alg_bytes / 1e6:.0f} MB per step)",
+                           "state": "u = 0.05 x e_x + U(-1e-3, 1e-3), dx ~ N(0,1), seeds 0/1"},
+                "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+                "cpu_baseline": cpu, "extra": extra}
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def assembly_case(torch, dev, stream, timed):
+    """Secondary: Q2 SVK 20x10x10 residual + CSC Jacobian (the reference's CPU-runnable case)."""
+    from hfk import _lib, forms
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.operator import KernelOperator
+
+    m = CartesianMesh((20, 10, 10))
+    g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
+    V = VectorLagrangeSpace(m, 2, ("x0", "x1"), g=g)
+    rng = np.random.default_rng(0)
+    x, _ = V.interpolate(lambda p: np.stack([0.05 * p[:, 0], 0 * p[:, 0], 0 * p[:, 0]], axis=1))
+    x = x + rng.uniform(-1e-3, 1e-3, V.nfree)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
+    op.problem.set_stream(stream.cuda_stream)
+    op.sparsity_pattern()
+    nnz = op.sparsity_pattern().nnz
+    xd = torch.from_numpy(x).to(dev)
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+    nz = torch.zeros(nnz, dtype=torch.float64, device=dev)
+    b = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
+    h = op.problem.h
+
+    def jac():
+        _lib.call("hfk_jacobian", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
+
+    def res():
+        _lib.call("hfk_residual", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(b))
+
+    ms_j = timed(jac, 10, 3) / 10
+    ms_r = timed(res, 10, 3) / 10
+    return {"assembly_q2_20x10x10": {"free_dofs": V.nfree, "nnz": int(nnz), "jacobian_ms": ms_j, "residual_ms": ms_r,
+                                     "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
+                                     "jacobian_qps": 27 * V.mesh.ncells / (ms_j * 1e-3)}}
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline_sample(budget_s=15.0):
+    """Oracle (CPU restatement, stored-tangent J*v as the reference) on a bounded sample: Q2 24^3."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hfk.fespace import Quadrature
+
+    nsub = 24
+    V, x, dx = build_case(nsub)
+    p = O.OracleProblem(V, Quadrature.gauss(4))
+    p.mf_prepare(x, V.dirichlet_values)
+    p.mf_apply(dx)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        p.mf_apply(dx)
+        k += 1
+        if time.perf_counter() - t0 > budget_s or k >= 50:
+            break
+    t = (time.perf_counter() - t0) / k
+    return {"value": V.nfree / t / 1e9, "unit": UNIT, "cores": O.lib().o_max_threads(), "kind": "port",
+            "sample": f"Q2 {nsub}^3 ({V.nfree} free dofs), {k} stored-tangent J*v applies, OpenMP all host cores"}
+
+
+def reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hfk.fespace import Quadrature
+
+    # bounded sample of the workload per step: Q2 24^3 (1/19 of the cells), the reference's formulation
+    nsub = 24
+    V, x, dx = build_case(nsub)
+    p = O.OracleProblem(V, Quadrature.gauss(4))
+    p.mf_prepare(x, V.dirichlet_values)
+    for _ in range(max(1, args.warmup)):
+        p.mf_apply(dx)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p.mf_apply(dx)
+    t = (time.perf_counter() - t0) / args.steps
+    value = V.nfree / t / 1e9
+    cores = O.lib().o_max_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": f"Q2 {nsub}^3 per step"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"Q2 {nsub}^3 ({V.nfree} free dofs) stored-tangent J*v per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        reference(a)
+    else:
+        engine(a)

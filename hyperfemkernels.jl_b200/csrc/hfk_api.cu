@@ -144,8 +144,16 @@ bool detect_tp(hfk_problem* p, const double* xq, const double* Nt) {
   p->h_N1.assign(P * Q, 0);
   p->h_dN1.assign(P * Q, 0);
   std::vector<double> n1(Q), dn1(Q);
+  // the 1D basis is evaluated at the unrounded coordinate of each 1D point (the rounding only
+  // identifies equal coordinates; evaluating at the rounded value would perturb the tables by ~1e-12)
   for (int a = 0; a < P; ++a) {
-    lagrange1d(Q, xs[a], n1.data(), dn1.data());
+    double xa = xs[a];
+    for (int q = 0; q < p->np; ++q)
+      if (std::round(xq[3 * q] * 1e12) / 1e12 == xs[a]) {
+        xa = xq[3 * q];
+        break;
+      }
+    lagrange1d(Q, xa, n1.data(), dn1.data());
     for (int i = 0; i < Q; ++i) {
       p->h_N1[a * Q + i] = n1[i];
       p->h_dN1[a * Q + i] = dn1[i];
@@ -1054,6 +1062,11 @@ struct hfk_pmg {
 
 namespace {
 
+// every level launches on level 0's stream (which the caller may have changed since)
+void pmg_bind_stream(hfk_pmg* m) {
+  for (int l = 1; l < m->L; ++l) m->lv[l]->stream = m->lv[0]->stream;
+}
+
 void coarse_factor(hfk_pmg* m) {
   hfk_problem* c = m->lv[m->L - 1];
   pattern_build_dev(c);
@@ -1263,8 +1276,12 @@ int hfk_problem_create(hfk_problem** out, int nn, int np, int ng, int ncells, co
 int hfk_problem_destroy(hfk_problem* p) {
   HFK_API_BEGIN
   if (!p) return HFK_OK;
-  cudaStreamSynchronize(p->stream);
-  if (p->own_stream) cudaStreamDestroy(p->own_stream);
+  // only the handle's own stream is touched: `stream` may be a caller's or a hierarchy's stream, and
+  // freeing device memory waits for the device anyway
+  if (p->own_stream) {
+    cudaStreamSynchronize(p->own_stream);
+    cudaStreamDestroy(p->own_stream);
+  }
   delete p;
   HFK_API_END
 }
@@ -1618,6 +1635,11 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
     m->tr.push_back(transfers[l]);
     require_tp(levels[l]);
   }
+  // one stream for the whole hierarchy: the V-cycle moves data between levels
+  for (int l = 1; l < nlevels; ++l) {
+    HFK_CUDA(cudaStreamSynchronize(levels[l]->stream));
+    levels[l]->stream = levels[0]->stream;
+  }
   m->degree = degree;
   m->range = range;
   m->inflate = inflate;
@@ -1658,7 +1680,12 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
 
 int hfk_pmg_destroy(hfk_pmg* m) {
   HFK_API_BEGIN
-  if (m && m->solver) cusolverDnDestroy(m->solver);
+  if (m) {
+    cudaStreamSynchronize(m->lv[0]->stream);
+    // the coarser levels go back to their own streams (levels must outlive their hierarchy)
+    for (int l = 1; l < m->L; ++l) m->lv[l]->stream = m->lv[l]->own_stream;
+    if (m->solver) cusolverDnDestroy(m->solver);
+  }
   delete m;
   HFK_API_END
 }
@@ -1666,6 +1693,7 @@ int hfk_pmg_destroy(hfk_pmg* m) {
 int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   HFK_API_BEGIN
   HFK_REQUIRE(m && x && ok, HFK_ERR_ARG, "null argument");
+  pmg_bind_stream(m);
   hfk_problem* p0 = m->lv[0];
   const bool f32 = m->precision == HFK_FP32;
   // level 0 state: the Newton's tangent (prepared in recompute mode)
@@ -1739,6 +1767,7 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y) {
   HFK_API_BEGIN
   HFK_REQUIRE(m && r && y, HFK_ERR_ARG, "null argument");
   HFK_REQUIRE(m->built, HFK_ERR_STATE, "PMultigrid: call hfk_pmg_update first");
+  pmg_bind_stream(m);
   hfk_problem* p0 = m->lv[0];
   const double* dr = dev_in(r, p0->nfree, m->top_r, p0->stream);
   double* dy = dev_out(y, p0->nfree, m->top_y);
@@ -1766,6 +1795,10 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
   HFK_REQUIRE(atol >= 0 && maxiter > 0, HFK_ERR_ARG, "atol must be >= 0 and maxiter > 0");
   HFK_REQUIRE(op->prepared, HFK_ERR_STATE, "the operator has not been prepared");
   const int64_t n = op->nfree;
+  if (prec) {
+    HFK_REQUIRE(prec->lv[0] == op, HFK_ERR_ARG, "the preconditioner's working level is not this operator");
+    pmg_bind_stream(prec);
+  }
   cudaStream_t s = op->stream;
   *iters = 0;
   *converged = 0;

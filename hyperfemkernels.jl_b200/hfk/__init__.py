@@ -15,13 +15,11 @@ __all__ = ["fespace", "forms", "CartesianMesh", "Quadrature", "VectorLagrangeSpa
 
 def __getattr__(name):
     # the classes that call the library load it lazily, so that fespace/forms import without a GPU build
+    import importlib
+
     if name in ("KernelOperator", "MatrixFreeJacobian", "Problem"):
-        from . import operator
-
-        return getattr(operator, name)
-    if name in ("MatrixFreeSolver", "PMultigrid", "Chebyshev", "BlockJacobi", "Prolongation", "solvers",
-                "chebyshev_damping", "eigenvalue_bounds"):
-        from . import solvers
-
-        return solvers if name == "solvers" else getattr(solvers, name)
+        return getattr(importlib.import_module(__name__ + ".operator"), name)
+    if name in ("MatrixFreeSolver", "PMultigrid", "Chebyshev", "BlockJacobi", "Prolongation", "chebyshev_damping",
+                "eigenvalue_bounds"):
+        return getattr(importlib.import_module(__name__ + ".solvers"), name)
     raise AttributeError(name)

@@ -149,6 +149,7 @@ int hfk_inject(hfk_transfer* t, const double* xf, const double* df, double* xc, 
  * the smoothers and products on the levels above the coarse one (the coarse solve is always FP64). */
 #define HFK_FP64 0
 #define HFK_FP32 1
+/* The hierarchy runs every level on level 0's stream while it exists; destroy it before its levels. */
 int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_transfer* const* transfers,
                    int degree, double range, double inflate, int eig_iters, int coarse_every, int precision);
 int hfk_pmg_destroy(hfk_pmg* m);

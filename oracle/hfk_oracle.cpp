@@ -464,7 +464,15 @@ bool build_tp(Problem& p) {
   p.dN1.assign(P * Q, 0);
   std::vector<double> n1(Q), dn1(Q);
   for (int a = 0; a < P; ++a) {
-    lagrange1d(Q, xs[a], n1.data(), dn1.data());
+    // evaluated at the unrounded coordinate (the reference evaluates at the 12-digit-rounded one,
+    // src/tensorproduct.jl:64-71, a ~1e-12 perturbation of the sum-factorised path)
+    double xa = xs[a];
+    for (int q = 0; q < p.np; ++q)
+      if (std::round(p.xq[3 * q] * 1e12) / 1e12 == xs[a]) {
+        xa = p.xq[3 * q];
+        break;
+      }
+    lagrange1d(Q, xa, n1.data(), dn1.data());
     for (int i = 0; i < Q; ++i) {
       p.N1[a + P * i] = n1[i];
       p.dN1[a + P * i] = dn1[i];
