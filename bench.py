@@ -193,7 +193,8 @@ def engine(args):
 
     # ---- roofline of the dominant kernel (colour launches of the J*v cell kernel) ----
     ncells = V.mesh.ncells
-    alg_bytes = 4 * V.ndl * ncells + 8 * n * 3 + 8 * V.ndir + 81 * ncells  # ids, u, dx, y, dvals, geometry
+    # ids, dx read, y read+write, F per point (prepared deformation gradient), per-cell geometry
+    alg_bytes = 4 * V.ndl * ncells + 8 * n * 3 + 72 * 27 * ncells + 81 * ncells
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -205,7 +206,7 @@ def engine(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "peak_source": src, "bytes_per_launch": alg_bytes,
                 "fp64_tflops": flops / (ms_step * 1e-3) / 1e12, "fp64_flops_per_launch": flops,
-                "note": "recompute J*v is FP64-issue bound; hbm frac uses the algorithmic bytes"}
+                "note": "recompute J*v is latency/FP64-issue bound; hbm frac uses the algorithmic bytes"}
 
     extra = {}
     if not args.no_extra and rank == 0:
@@ -237,7 +238,7 @@ def engine(args):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "cells": ncells, "free_dofs_per_gpu": n, "order": ORDER,
                            "quadrature_points_per_cell": 27, "parallelism": f"replicas x{world}",
-                           "l2": f"inputs larger than L2 ({alg_bytes / 1e6:.0f} MB per step)",
+                           "l2": f"inputs larger than L2 ({alg_bytes / 1e6:.0f} MB read per step, L2 126 MB)",
                            "state": "u = 0.05 x e_x + U(-1e-3, 1e-3), dx ~ N(0,1), seeds 0/1"},
                 "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
                 "cpu_baseline": cpu, "extra": extra}

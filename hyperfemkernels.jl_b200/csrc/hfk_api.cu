@@ -233,7 +233,7 @@ template <int Q, int P, int MODE, typename R>
 void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
   constexpr int WARPS = 4;
   using S = TPShape<Q, P>;
-  const size_t smem = cell_smem_bytes<Q, P, MODE, R>(WARPS);
+  const size_t smem = cell_smem_bytes<Q, P, R>(WARPS);
   static bool attr = false;
   if (!attr) {
     HFK_CUDA(cudaFuncSetAttribute(cell_kernel<Q, P, MODE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -360,25 +360,13 @@ void require_tp(hfk_problem* p) {
               "the cells have no tensor-product structure (sum-factorised kernels need Q^3 nodes and P^3 Gauss points)");
 }
 
-void bind_state(hfk_problem* p, const double* x, const double* dvals, bool f32) {
+void bind_state(hfk_problem* p, const double* x, const double* dvals) {
   const double* dx = dev_in(x, p->nfree, p->stage_in, p->stream);
   const double* dd = dev_in(dvals, p->ndir, p->stage_in2, p->stream);
   p->x.resize(p->nfree);
   p->dvals.resize(std::max<int64_t>(p->ndir, 1));
   if (p->nfree) HFK_CUDA(cudaMemcpyAsync(p->x.p, dx, p->nfree * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
   if (p->ndir) HFK_CUDA(cudaMemcpyAsync(p->dvals.p, dd, p->ndir * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
-  if (f32) {
-    p->x32.resize(p->nfree);
-    p->dvals32.resize(std::max<int64_t>(p->ndir, 1));
-    if (p->nfree) {
-      convert_kernel<double, float><<<vec_grid(p->nfree), 256, 0, p->stream>>>(p->nfree, p->x.p, p->x32.p);
-      check_launch(p);
-    }
-    if (p->ndir) {
-      convert_kernel<double, float><<<vec_grid(p->ndir), 256, 0, p->stream>>>(p->ndir, p->dvals.p, p->dvals32.p);
-      check_launch(p);
-    }
-  }
 }
 
 // ---- reductions -------------------------------------------------------------------------------
@@ -407,8 +395,6 @@ void mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
   HFK_CUDA(cudaMemsetAsync(y, 0, p->nfree * sizeof(double), p->stream));
   CellIO<double> io{};
-  io.u = p->x.p;
-  io.dvals = p->dvals.p;
   io.dx = dx;
   io.y = y;
   if (p->mf_mode == HFK_MF_STORED) {
@@ -417,29 +403,45 @@ void mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
     io.dVq = p->dVq.p;
     run_cells<MODE_JV_STORED, double>(p, io);
   } else {
+    io.Fq = p->Fq.p;
     run_cells<MODE_JV, double>(p, io);
   }
 }
 
+// the FP32 copy of the stored deformation gradients (made on first use after a prepare)
+void ensure_F32(hfk_problem* p) {
+  if (p->Fq32_valid) return;
+  HFK_REQUIRE(p->Fq.p, HFK_ERR_STATE, "the FP32 product needs a prepared tangent (recompute mode)");
+  p->Fq32.resize(p->Fq.n);
+  convert_kernel<double, float><<<vec_grid((int64_t)p->Fq.n), 256, 0, p->stream>>>((int64_t)p->Fq.n, p->Fq.p, p->Fq32.p);
+  check_launch(p);
+  p->Fq32_valid = true;
+}
+
 void mf_apply_dev32(hfk_problem* p, const float* dx, float* y) {
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
-  if (p->x32.n != (size_t)p->nfree) {
-    p->x32.resize(p->nfree);
-    p->dvals32.resize(std::max<int64_t>(p->ndir, 1));
-    convert_kernel<double, float><<<vec_grid(p->nfree), 256, 0, p->stream>>>(p->nfree, p->x.p, p->x32.p);
-    check_launch(p);
-    if (p->ndir) {
-      convert_kernel<double, float><<<vec_grid(p->ndir), 256, 0, p->stream>>>(p->ndir, p->dvals.p, p->dvals32.p);
-      check_launch(p);
-    }
-  }
+  HFK_REQUIRE(p->mf_mode == HFK_MF_RECOMPUTE, HFK_ERR_STATE, "the FP32 product needs the recompute formulation");
+  ensure_F32(p);
   HFK_CUDA(cudaMemsetAsync(y, 0, p->nfree * sizeof(float), p->stream));
   CellIO<float> io{};
-  io.u = p->x32.p;
-  io.dvals = p->dvals32.p;
   io.dx = dx;
   io.y = y;
+  io.Fq = p->Fq32.p;
   run_cells<MODE_JV, float>(p, io);
+}
+
+// prepare in the recompute formulation: F = I + grad u at every point of every cell (from x, dvals)
+void prepare_F(hfk_problem* p) {
+  require_tp(p);
+  p->Fq.resize((size_t)9 * p->np * p->ncells);
+  CellIO<double> io{};
+  io.u = p->x.p;
+  io.dvals = p->dvals.p;
+  io.Fout = p->Fq.p;
+  dispatch_cell<MODE_PREP_F, double>(p, nullptr, p->ncells, io);
+  p->Fq32_valid = false;
+  p->mf_mode = HFK_MF_RECOMPUTE;
+  p->prepared = true;
 }
 
 template <typename R>
@@ -1399,8 +1401,7 @@ int hfk_mf_prepare(hfk_problem* p, const double* x, const double* dvals, int mod
   HFK_REQUIRE(p && x && (dvals || p->ndir == 0), HFK_ERR_ARG, "null argument");
   HFK_REQUIRE(mode == HFK_MF_STORED || mode == HFK_MF_RECOMPUTE, HFK_ERR_ARG, "unknown matrix-free mode");
   require_tp(p);
-  bind_state(p, x, dvals, false);
-  p->x32.release();
+  bind_state(p, x, dvals);
   p->mf_mode = mode;
   if (mode == HFK_MF_STORED) {
     const size_t npq = (size_t)p->np * p->ncells;
@@ -1411,10 +1412,14 @@ int hfk_mf_prepare(hfk_problem* p, const double* x, const double* dvals, int mod
     store_tangents_kernel<<<vec_grid((int64_t)npq), 256, 0, p->stream>>>(cd, p->x.p, p->dvals.p, p->dNt.p, p->nn,
                                                                           p->np, p->T.p, p->iJtq.p, p->dVq.p);
     check_launch(p);
+    p->Fq.release();
+    p->Fq32.release();
+    p->Fq32_valid = false;
   } else {
     p->T.release();
     p->iJtq.release();
     p->dVq.release();
+    prepare_F(p);
   }
   p->prepared = true;
   HFK_CUDA(cudaStreamSynchronize(p->stream));
@@ -1696,11 +1701,9 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   pmg_bind_stream(m);
   hfk_problem* p0 = m->lv[0];
   const bool f32 = m->precision == HFK_FP32;
-  // level 0 state: the Newton's tangent (prepared in recompute mode)
-  bind_state(p0, x, dvals, f32);
-  p0->mf_mode = HFK_MF_RECOMPUTE;
-  p0->prepared = true;
-  if (!f32) p0->x32.release();
+  // level 0 state: the Newton's tangent (prepared in the recompute formulation)
+  bind_state(p0, x, dvals);
+  prepare_F(p0);
   // inject level by level and prepare (update_levels!, src/pmultigrid.jl:197-204)
   for (int l = 0; l + 1 < m->L; ++l) {
     hfk_problem* f = m->lv[l];
@@ -1708,22 +1711,13 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     c->x.resize(c->nfree);
     c->dvals.resize(std::max<int64_t>(c->ndir, 1));
     inject_dev(m->tr[l], f->x.p, f->dvals.p, c->x.p, c->dvals.p);
-    c->mf_mode = HFK_MF_RECOMPUTE;
-    c->prepared = true;
-    if (f32 && l + 1 < m->L - 1) {
-      c->x32.resize(c->nfree);
-      c->dvals32.resize(std::max<int64_t>(c->ndir, 1));
-      convert_kernel<double, float><<<vec_grid(c->nfree), 256, 0, c->stream>>>(c->nfree, c->x.p, c->x32.p);
-      check_launch(c);
-      if (c->ndir) {
-        convert_kernel<double, float><<<vec_grid(c->ndir), 256, 0, c->stream>>>(c->ndir, c->dvals.p, c->dvals32.p);
-        check_launch(c);
-      }
+    if (l + 1 < m->L - 1) {
+      prepare_F(c);
     } else {
-      c->x32.release();
+      c->prepared = true;  // the coarse level is assembled
     }
-    HFK_CUDA(cudaStreamSynchronize(f->stream));
   }
+  (void)f32;
   // smoothers: blocks and intervals (smoother_update!, src/smoothers.jl:86-107)
   bool all_ok = true;
   for (int l = 0; l + 1 < m->L; ++l) {

@@ -122,11 +122,14 @@ struct hfk_problem {
   hfk::DBuf<int64_t> rowval;
   hfk::DBuf<int32_t> nzpos;               // (ndl*ndl, ncells)
   hfk::DBuf<double> nzval;
-  // current state (FP64) and its FP32 copy
+  // current state (FP64)
   hfk::DBuf<double> x, dvals;
-  hfk::DBuf<float> x32, dvals32;
   bool prepared = false;
   int mf_mode = HFK_MF_RECOMPUTE;
+  // deformation gradient per point (recompute formulation), FP64 and its FP32 copy
+  hfk::DBuf<double> Fq;
+  hfk::DBuf<float> Fq32;
+  bool Fq32_valid = false;
   // stored tangents (reference formulation: T, iJt, dV per point)
   hfk::DBuf<double> T, iJtq, dVq;
   // nodal blocks

@@ -1,59 +1,86 @@
-// Sum-factorised cell kernels: residual, matrix-free Jacobian product (tangent recomputed from the
-// state, or read from stored per-point tangents) for a 3-component Lagrangian field on hexahedra.
+// Sum-factorised cell kernels for a 3-component Lagrangian field on hexahedra:
+//   MODE_RESIDUAL  residual of the law at the state u (gathers u)
+//   MODE_PREP_F    deformation gradient F = I + grad u at every point, stored (gathers u)
+//   MODE_JV        J(u) dx with the tangent re-evaluated from the stored F (gathers dx)
+//   MODE_JV_STORED J(u) dx with the reference's stored per-point tangents T, inv(Jt), dV
 //
 // Mapping: a warp holds CPW = 32 / M^2 cells (M = max(P, Q)); the M^2 lanes of a cell own the
-// tensor lines of each sum-factorisation sweep (x lines (j,k), then y lines (a,k), then z lines
-// (a,b)), so every sweep reads each input once and writes P (or 3P) outputs from registers. Lane
-// (a,b) then owns the P points (a,b,c) for the pointwise law. Cells of one colour share no free
-// dof, so the scatter is a plain read-modify-write (colour-by-colour launches), or an atomicAdd
-// when one launch covers all cells.
+// tensor lines of each sum-factorisation sweep (x lines (j,k), y lines (a,k), z lines (a,b)), so
+// every sweep reads each input once and writes P (or 3P) outputs from registers. Lane (a,b) owns
+// the P points (a,b,c): it loads its z column of the y-sweep into registers and writes the point
+// coefficients back in place (each lane only touches addresses of its own column), which keeps
+// the shared footprint of a cell small (occupancy). Cells of one colour share no free dof, so the
+// scatter is a plain read-modify-write (colour-by-colour launches), or atomicAdd in one launch.
 //
 // Reference: tp_interpolate!/tp_contract! (src/tensorproduct.jl:125-224), apply_cells!
-// (src/matrixfree.jl:341-396), element_residual_mm! (src/assembly.jl:1219-1241); the tangent of
-// SVK is the exact derivative the factorised form evaluates (src/factorforms.jl:316-322).
+// (src/matrixfree.jl:341-396), element_residual_mm! (src/assembly.jl:1219-1241); the SVK tangent
+// is the exact derivative the factorised form evaluates (src/factorforms.jl:316-322).
 #pragma once
 #include "hfk_internal.h"
 #include "pointwise.cuh"
 
 namespace hfk {
 
-enum CellMode { MODE_RESIDUAL = 0, MODE_JV = 1, MODE_JV_STORED = 2 };
+enum CellMode { MODE_RESIDUAL = 0, MODE_JV = 1, MODE_JV_STORED = 2, MODE_PREP_F = 3 };
 
 template <int Q, int P>
 struct TPShape {
   static constexpr int NN = Q * Q * Q;
   static constexpr int NP = P * P * P;
   static constexpr int M = P > Q ? P : Q;
-  static constexpr int TPC = M * M;        // lanes per cell
-  static constexpr int CPW = 32 / TPC;     // cells per warp
+  static constexpr int TPC = M * M;     // lanes per cell
+  static constexpr int CPW = 32 / TPC;  // cells per warp
   static_assert(CPW >= 1, "a cell must fit in a warp (max(P,Q) <= 5)");
+  static_assert(3 * Q <= 4 * P, "the in-place z contraction needs 3Q <= 4P");
 };
 
-// shared-memory layout of one cell (in units of R), see the phase comments in the kernel
-template <int Q, int P, int MODE>
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// Shared layout of one cell, in units of R:
+//   YR  [rows][P*P]: y-sweep out (3 fields x 3 kinds x Q rows), then the point coefficients in
+//       place (3 comps x 4 slots x P rows), then the z-contraction out (3 comps x 3 kinds x Q rows)
+//   xl  [3][NN] local values;  XS [2][P*Q*Q] x-sweep out
+//   the y-contraction out (3 comps x 2 x P*Q*Q) uses the tail: YR rows past 9Q, then xl and XS
+template <int Q, int P>
 struct CellSmem {
-  using S = TPShape<Q, P>;
-  static constexpr int NF = MODE == MODE_JV ? 6 : 3;            // gathered fields
-  static constexpr int XL = NF * S::NN;                          // local values
-  static constexpr int XR = (6 * P * Q * Q > 12 * S::NP - XL ? 6 * P * Q * Q : 12 * S::NP - XL);  // x-sweep / y-contraction
-  static constexpr int YR0 = NF * 3 * Q * P * P;
-  static constexpr int YR = YR0 > 9 * Q * P * P ? YR0 : 9 * Q * P * P;                      // y-sweep / z-contraction
-  static constexpr int VALS = XL + XR + YR;                      // R elements
+  static constexpr int NN = Q * Q * Q, NP = P * P * P;
+  static constexpr int YR = cmax(9 * Q * P * P, 12 * NP);
+  static constexpr int XL = 3 * NN;
+  static constexpr int XS0 = 2 * P * Q * Q;
+  static constexpr int TAIL0 = YR - 9 * Q * P * P + XL + XS0;
+  static constexpr int XS = TAIL0 >= 6 * P * Q * Q ? XS0 : XS0 + (6 * P * Q * Q - TAIL0);
+  static constexpr int VALS = YR + XL + XS;
 };
 
-// bytes of one cell's shared region, rounded up to 16 so that every region starts aligned
-template <int Q, int P, int MODE, typename R>
+// Bytes of one cell's shared region. With several cells per warp the region stride is padded to
+// TPC * sizeof(R) modulo 128 bytes, so the lanes of consecutive cells (each reading TPC consecutive
+// words) fall on consecutive banks instead of the same ones.
+template <int Q, int P, typename R>
 __host__ __device__ constexpr size_t cell_region_bytes() {
-  return (((size_t)CellSmem<Q, P, MODE>::VALS * sizeof(R) + (size_t)3 * TPShape<Q, P>::NN * sizeof(int32_t)) + 15) /
-         16 * 16;
+  size_t raw = (size_t)CellSmem<Q, P>::VALS * sizeof(R) + (size_t)3 * TPShape<Q, P>::NN * sizeof(int32_t);
+  raw = (raw + sizeof(R) - 1) / sizeof(R) * sizeof(R);
+  if (TPShape<Q, P>::CPW > 1) {
+    const size_t target = ((size_t)TPShape<Q, P>::TPC * sizeof(R)) % 128;
+    while (raw % 128 != target) raw += sizeof(R);
+  }
+  return raw;
+}
+
+// resident CTAs per SM the register allocation of a mode targets (measured on B200: the stored
+// formulation prefers fewer, larger register files; the recompute product more warps)
+template <int MODE>
+constexpr int cell_min_blocks() {
+  return MODE == MODE_JV_STORED ? 2 : (MODE == MODE_JV ? 4 : 3);
 }
 
 template <typename R>
 struct CellIO {
-  const R* u;       // state free values (MODE_RESIDUAL, MODE_JV)
+  const R* u;       // state free values (MODE_RESIDUAL, MODE_PREP_F)
   const R* dvals;   // state Dirichlet values
   const R* dx;      // increment (MODE_JV, MODE_JV_STORED)
   R* y;             // output (scatter-add)
+  const R* Fq;      // stored F (MODE_JV): (cell*9 + i)*NP + q
+  R* Fout;          // MODE_PREP_F output, same layout
   const double* T;  // stored tangents (cell*81 + i)*NP + q
   const double* iJtq;
   const double* dVq;
@@ -61,50 +88,59 @@ struct CellIO {
 };
 
 template <int Q, int P, int MODE, typename R>
-__global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, CellIO<R> io) {
+__global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(CellData cd, Tab1D<R> tab, CellIO<R> io) {
   using S = TPShape<Q, P>;
-  using L = CellSmem<Q, P, MODE>;
+  using L = CellSmem<Q, P>;
   constexpr int NN = S::NN, NP = S::NP, TPC = S::TPC, CPW = S::CPW;
   constexpr int NDL = 3 * NN;
-  constexpr int NF = L::NF;
+  constexpr int PP = P * P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int slot = lane / TPC;        // cell slot in the warp
-  const bool active = slot < CPW;     // lanes past CPW * TPC idle (every phase is guarded by t)
-  const int t = active ? lane - slot * TPC : (1 << 20);  // lane within the cell
-  // per-cell regions
-  const int cell_index_base = (blockIdx.x * nwarps + warp) * CPW;
-  const size_t per_cell_bytes = cell_region_bytes<Q, P, MODE, R>();
-  unsigned char* base = smem_raw + (size_t)(warp * CPW + (active ? slot : 0)) * per_cell_bytes;
-  R* xl = reinterpret_cast<R*>(base);     // [NF][NN]
-  R* xr = xl + L::XL;                     // x-sweep out [2][P][Q][Q], later y-contraction out [3][2][P][Q][Q]
-  R* yr = xr + L::XR;                     // y-sweep out [NF][3][Q][P*P], later z-contraction out [3][3][Q][P*P]
-  R* rh = xl;                             // pointwise coefficients [3][4][P][P*P] (aliases xl + xr)
-  int32_t* sid = reinterpret_cast<int32_t*>(yr + L::YR);
+  const int slot = lane / TPC;
+  const bool active = slot < CPW;  // lanes past CPW * TPC idle: every phase is guarded by t
+  const int t = active ? lane - slot * TPC : (1 << 20);
+  unsigned char* base = smem_raw + (size_t)(warp * CPW + (active ? slot : 0)) * cell_region_bytes<Q, P, R>();
+  R* yr = reinterpret_cast<R*>(base);
+  R* xl = yr + L::YR;
+  R* xs = xl + L::XL;
+  R* tail = yr + 9 * Q * PP;  // y-contraction out (contiguous over the YR tail, xl, xs)
+  int32_t* sid = reinterpret_cast<int32_t*>(yr + L::VALS);
 
-  const int list_index = cell_index_base + (active ? slot : 0);
+  const int list_index = (blockIdx.x * nwarps + warp) * CPW + (active ? slot : 0);
   const bool has_cell = active && list_index < cd.ncells_list;
   const int cell = has_cell ? (cd.cells ? cd.cells[list_index] : list_index) : 0;
 
-  // ---- gather (gather_cell!, src/assembly.jl:1060-1070; dx: zero at Dirichlet dofs) -------
+  // ---- gather (gather_cell!, src/assembly.jl:1060-1070; increments are zero at Dirichlet dofs) ----
   if (has_cell) {
     const int32_t* gid = cd.ids + (size_t)cell * NDL;
+#pragma unroll 3
     for (int j = t; j < NDL; j += TPC) {
-      int32_t id = gid[j];
+      const int32_t id = gid[j];
       sid[j] = id;
-      if (MODE == MODE_RESIDUAL || MODE == MODE_JV)
+      if (MODE == MODE_RESIDUAL || MODE == MODE_PREP_F)
         xl[j] = id > 0 ? io.u[id - 1] : (id < 0 ? io.dvals[-id - 1] : R(0));
-      if (MODE == MODE_JV) xl[NDL + j] = id > 0 ? io.dx[id - 1] : R(0);
-      if (MODE == MODE_JV_STORED) xl[j] = id > 0 ? io.dx[id - 1] : R(0);
+      else
+        xl[j] = id > 0 ? io.dx[id - 1] : R(0);
+    }
+  }
+  // geometry of an affine cell (cell_geometry, src/assembly.jl:1100-1107), loaded early
+  double iJc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, detc = 0;
+  bool aff = false;
+  if (has_cell && MODE != MODE_JV_STORED) {
+    aff = cd.affine[cell];
+    if (aff) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) iJc[i] = cd.geo[(size_t)cell * 10 + i];
+      detc = cd.geo[(size_t)cell * 10 + 9];
     }
   }
   __syncwarp();
 
-  // ---- interpolation sweeps per field (tp_interpolate! 3D, reference gradients only) ---------
+  // ---- interpolation sweeps (tp_interpolate! 3D, reference gradients only) ------------------
 #pragma unroll 1
-  for (int f = 0; f < NF; ++f) {
+  for (int f = 0; f < 3; ++f) {
     const R* uf = xl + f * NN;
     if (t < Q * Q) {  // x lines (j, k)
       const int j = t % Q, k = t / Q;
@@ -119,8 +155,8 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
           s += tab.N1[a * Q + i] * v[i];
           ds += tab.dN1[a * Q + i] * v[i];
         }
-        xr[a + P * (j + Q * k)] = s;
-        xr[P * Q * Q + a + P * (j + Q * k)] = ds;
+        xs[a + P * (j + Q * k)] = s;
+        xs[P * Q * Q + a + P * (j + Q * k)] = ds;
       }
     }
     __syncwarp();
@@ -129,8 +165,8 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
       R va[Q], vb[Q];
 #pragma unroll
       for (int j = 0; j < Q; ++j) {
-        va[j] = xr[a + P * (j + Q * k)];
-        vb[j] = xr[P * Q * Q + a + P * (j + Q * k)];
+        va[j] = xs[a + P * (j + Q * k)];
+        vb[j] = xs[P * Q * Q + a + P * (j + Q * k)];
       }
 #pragma unroll
       for (int b = 0; b < P; ++b) {
@@ -142,57 +178,53 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
           e0 += tab.N1[b * Q + j] * vb[j];
         }
         const int ab = a + P * b;
-        yr[((f * 3 + 0) * Q + k) * P * P + ab] = c0;
-        yr[((f * 3 + 1) * Q + k) * P * P + ab] = d0;
-        yr[((f * 3 + 2) * Q + k) * P * P + ab] = e0;
+        yr[((f * 3 + 0) * Q + k) * PP + ab] = c0;
+        yr[((f * 3 + 1) * Q + k) * PP + ab] = d0;
+        yr[((f * 3 + 2) * Q + k) * PP + ab] = e0;
       }
     }
     __syncwarp();
   }
 
-  // ---- pointwise phase: lane (a, b) owns the points (a, b, c) ------------------------------
-  // affine cells: one inverse Jacobian per cell (cell_geometry, src/assembly.jl:1100-1107)
-  double iJc[9], detc = 0;
-  bool aff = false;
-  if (has_cell && MODE != MODE_JV_STORED) {
-    aff = cd.affine[cell];
-    if (aff) {
-#pragma unroll
-      for (int i = 0; i < 9; ++i) iJc[i] = cd.geo[(size_t)cell * 10 + i];
-      detc = cd.geo[(size_t)cell * 10 + 9];
-    }
-  }
-  if (has_cell && t < P * P) {
+  // ---- pointwise phase: lane (a, b) owns the points (a, b, c) --------------------------------
+  if (t < PP) {
     const int ab = t;
+    R yc[3][3][Q];  // this lane's column of the y-sweep: [field][kind][k]
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int kind = 0; kind < 3; ++kind)
+#pragma unroll
+        for (int k = 0; k < Q; ++k) yc[f][kind][k] = yr[((f * 3 + kind) * Q + k) * PP + ab];
 #pragma unroll 1
     for (int c = 0; c < P; ++c) {
-      const int q = ab + P * P * c;
-      // z sweep of every field at this point: reference gradients G[f][K]
-      R G[NF][3];
+      const int q = ab + PP * c;
+      R G[3][3];  // z sweep: reference gradients G[f][K]
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
+      for (int f = 0; f < 3; ++f) {
         R g1 = 0, g2 = 0, g3 = 0;
 #pragma unroll
         for (int k = 0; k < Q; ++k) {
-          const R cv = yr[((f * 3 + 0) * Q + k) * P * P + ab];
-          const R dv = yr[((f * 3 + 1) * Q + k) * P * P + ab];
-          const R ev = yr[((f * 3 + 2) * Q + k) * P * P + ab];
           const R n = tab.N1[c * Q + k], dn = tab.dN1[c * Q + k];
-          g1 += n * ev;
-          g2 += n * dv;
-          g3 += dn * cv;
+          g1 += n * yc[f][2][k];
+          g2 += n * yc[f][1][k];
+          g3 += dn * yc[f][0][k];
         }
         G[f][0] = g1;
         G[f][1] = g2;
         G[f][2] = g3;
       }
-      // geometry at the point
-      R iJ[9], dV;
+      R iJ[9], dV = 0;
       if (MODE == MODE_JV_STORED) {
+        if (has_cell) {
 #pragma unroll
-        for (int i = 0; i < 9; ++i) iJ[i] = (R)io.iJtq[((size_t)cell * 9 + i) * NP + q];
-        dV = (R)io.dVq[(size_t)cell * NP + q];
-      } else if (aff) {
+          for (int i = 0; i < 9; ++i) iJ[i] = (R)io.iJtq[((size_t)cell * 9 + i) * NP + q];
+          dV = (R)io.dVq[(size_t)cell * NP + q];
+        } else {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) iJ[i] = 0;
+        }
+      } else if (aff || !has_cell) {
 #pragma unroll
         for (int i = 0; i < 9; ++i) iJ[i] = (R)iJc[i];
         dV = (R)(cd.w[q] * detc);
@@ -205,65 +237,85 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
         for (int i = 0; i < 9; ++i) iJ[i] = (R)iJd[i];
         dV = (R)(cd.w[q] * fabs(det));
       }
-      R out[3][3];   // R^[comp][K] = dV sum_J iJt[J,K] P[comp,J]
-      R outv[3];     // value coefficients (body force of the residual)
+      R H[9];
+      phys_grad<R, 3>(iJ, G, 0, H);
+      if (MODE == MODE_PREP_F) {
+        if (has_cell) {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) io.Fout[((size_t)cell * 9 + i) * NP + q] = H[i] + ((i % 4) == 0 ? R(1) : R(0));
+        }
+        continue;
+      }
+      R out[3][3];
+      R outv[3] = {0, 0, 0};
       if (MODE == MODE_RESIDUAL) {
-        R H[9];
-        phys_grad<R>(iJ, G, 0, H);
         R Pm[9];
         law_stress<R>(cd.law, (R)cd.lam, (R)cd.mu, H, Pm);
         pull_back<R>(iJ, Pm, dV, out);
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) outv[cc] = -dV * (R)cd.body[cc];
       } else if (MODE == MODE_JV) {
-        R H[9], Hd[9], dP[9];
-        phys_grad<R>(iJ, G, 0, H);
-        phys_grad<R>(iJ, G, 3, Hd);
-        law_dstress<R>(cd.law, (R)cd.lam, (R)cd.mu, H, Hd, dP);
+        R Fm[9], dP[9];
+        if (has_cell) {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) Fm[i] = io.Fq[((size_t)cell * 9 + i) * NP + q];
+        } else {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) Fm[i] = (i % 4) == 0 ? R(1) : R(0);
+        }
+        law_dstress_F<R>(cd.law, (R)cd.lam, (R)cd.mu, Fm, H, dP);
         pull_back<R>(iJ, dP, dV, out);
       } else {
-        // stored tangent: su = physical gradients of dx, sv = dV T su (apply_cells!, src/matrixfree.jl:367-375)
-        R Hd[9], sv[9];
-        phys_grad<R>(iJ, G, 0, Hd);
-        const double* Tq = io.T + (size_t)cell * 81 * NP + q;
+        // stored tangent: sv = dV T su (apply_cells!, src/matrixfree.jl:367-375)
+        R sv[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
           R s = 0;
+          if (has_cell) {
+            const double* Tq = io.T + (size_t)cell * 81 * NP + q;
 #pragma unroll
-          for (int j = 0; j < 9; ++j) s += (R)Tq[(size_t)(i + 9 * j) * NP] * Hd[(j / 3) + 3 * (j % 3)];
+            for (int j = 0; j < 9; ++j) s += (R)Tq[(size_t)(i + 9 * j) * NP] * H[(j / 3) + 3 * (j % 3)];
+          }
           sv[(i / 3) + 3 * (i % 3)] = s;
         }
         pull_back<R>(iJ, sv, dV, out);
       }
-      // store coefficients of this point (rh aliases xl/xr, whose last reads precede the last sync)
+      // point coefficients written in place into this lane's own column of YR
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
+        yr[((cc * 4 + 0) * P + c) * PP + ab] = outv[cc];
 #pragma unroll
-        for (int K = 0; K < 3; ++K) rh[((cc * 4 + 1 + K) * P + c) * P * P + ab] = out[cc][K];
-        rh[((cc * 4 + 0) * P + c) * P * P + ab] = MODE == MODE_RESIDUAL ? outv[cc] : R(0);
+        for (int K = 0; K < 3; ++K) yr[((cc * 4 + 1 + K) * P + c) * PP + ab] = out[cc][K];
       }
     }
   }
+  if (MODE == MODE_PREP_F) return;
   __syncwarp();
 
-  // ---- contraction (tp_contract! 3D): z, then y, then x ------------------------------------
-  if (t < P * P) {  // z lines (a, b) -> t0, t1, t2 [k]
+  // ---- contraction (tp_contract! 3D): z (in place, per lane column), y, x -------------------
+  if (t < PP) {
     const int ab = t;
 #pragma unroll 1
     for (int cc = 0; cc < 3; ++cc) {
+      // the z-contraction rows of cc overlap only coefficient rows of cc or of earlier components
+      R rv[4][P];
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int c = 0; c < P; ++c) rv[s][c] = yr[((cc * 4 + s) * P + c) * PP + ab];
 #pragma unroll
       for (int k = 0; k < Q; ++k) {
         R t0 = 0, t1 = 0, t2 = 0;
 #pragma unroll
         for (int c = 0; c < P; ++c) {
           const R n = tab.N1[c * Q + k], dn = tab.dN1[c * Q + k];
-          t0 += n * rh[((cc * 4 + 0) * P + c) * P * P + ab] + dn * rh[((cc * 4 + 3) * P + c) * P * P + ab];
-          t1 += n * rh[((cc * 4 + 1) * P + c) * P * P + ab];
-          t2 += n * rh[((cc * 4 + 2) * P + c) * P * P + ab];
+          t0 += n * rv[0][c] + dn * rv[3][c];
+          t1 += n * rv[1][c];
+          t2 += n * rv[2][c];
         }
-        yr[((cc * 3 + 0) * Q + k) * P * P + ab] = t0;
-        yr[((cc * 3 + 1) * Q + k) * P * P + ab] = t1;
-        yr[((cc * 3 + 2) * Q + k) * P * P + ab] = t2;
+        yr[((cc * 3 + 0) * Q + k) * PP + ab] = t0;
+        yr[((cc * 3 + 1) * Q + k) * PP + ab] = t1;
+        yr[((cc * 3 + 2) * Q + k) * PP + ab] = t2;
       }
     }
   }
@@ -275,9 +327,9 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
       R v0[P], v1[P], v2[P];
 #pragma unroll
       for (int b = 0; b < P; ++b) {
-        v0[b] = yr[((cc * 3 + 0) * Q + k) * P * P + a + P * b];
-        v1[b] = yr[((cc * 3 + 1) * Q + k) * P * P + a + P * b];
-        v2[b] = yr[((cc * 3 + 2) * Q + k) * P * P + a + P * b];
+        v0[b] = yr[((cc * 3 + 0) * Q + k) * PP + a + P * b];
+        v1[b] = yr[((cc * 3 + 1) * Q + k) * PP + a + P * b];
+        v2[b] = yr[((cc * 3 + 2) * Q + k) * PP + a + P * b];
       }
 #pragma unroll
       for (int j = 0; j < Q; ++j) {
@@ -287,40 +339,62 @@ __global__ void __launch_bounds__(128) cell_kernel(CellData cd, Tab1D<R> tab, Ce
           s0 += tab.N1[b * Q + j] * v0[b] + tab.dN1[b * Q + j] * v2[b];
           s1 += tab.N1[b * Q + j] * v1[b];
         }
-        xr[(cc * 2 + 0) * P * Q * Q + a + P * (j + Q * k)] = s0;
-        xr[(cc * 2 + 1) * P * Q * Q + a + P * (j + Q * k)] = s1;
+        tail[(cc * 2 + 0) * P * Q * Q + a + P * (j + Q * k)] = s0;
+        tail[(cc * 2 + 1) * P * Q * Q + a + P * (j + Q * k)] = s1;
       }
     }
   }
   __syncwarp();
-  if (has_cell && t < Q * Q) {  // x lines (j, k) -> r[i], scatter of free test rows
+  if (has_cell && t < Q * Q) {  // x lines (j, k) -> r[i]; scatter of the free test rows
     const int j = t % Q, k = t / Q;
-#pragma unroll 1
+    R r[3][Q];
+#pragma unroll
     for (int cc = 0; cc < 3; ++cc) {
       R v0[P], v1[P];
 #pragma unroll
       for (int a = 0; a < P; ++a) {
-        v0[a] = xr[(cc * 2 + 0) * P * Q * Q + a + P * (j + Q * k)];
-        v1[a] = xr[(cc * 2 + 1) * P * Q * Q + a + P * (j + Q * k)];
+        v0[a] = tail[(cc * 2 + 0) * P * Q * Q + a + P * (j + Q * k)];
+        v1[a] = tail[(cc * 2 + 1) * P * Q * Q + a + P * (j + Q * k)];
       }
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
         R s = 0;
 #pragma unroll
         for (int a = 0; a < P; ++a) s += tab.N1[a * Q + i] * v0[a] + tab.dN1[a * Q + i] * v1[a];
-        const int32_t id = sid[cc * NN + i + Q * j + Q * Q * k];
-        if (id > 0) {
-          if (io.atomic) atomicAdd(&io.y[id - 1], s);
-          else io.y[id - 1] += s;
-        }
+        r[cc][i] = s;
       }
+    }
+    if (io.atomic) {
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const int32_t id = sid[cc * NN + i + Q * j + Q * Q * k];
+          if (id > 0) atomicAdd(&io.y[id - 1], r[cc][i]);
+        }
+    } else {
+      R old[3][Q];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const int32_t id = sid[cc * NN + i + Q * j + Q * Q * k];
+          old[cc][i] = id > 0 ? io.y[id - 1] : R(0);
+        }
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const int32_t id = sid[cc * NN + i + Q * j + Q * Q * k];
+          if (id > 0) io.y[id - 1] = old[cc][i] + r[cc][i];
+        }
     }
   }
 }
 
-template <int Q, int P, int MODE, typename R>
+template <int Q, int P, typename R>
 constexpr size_t cell_smem_bytes(int warps) {
-  return (size_t)warps * TPShape<Q, P>::CPW * cell_region_bytes<Q, P, MODE, R>();
+  return (size_t)warps * TPShape<Q, P>::CPW * cell_region_bytes<Q, P, R>();
 }
 
 }  // namespace hfk

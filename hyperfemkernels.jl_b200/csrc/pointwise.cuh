@@ -100,20 +100,14 @@ __device__ __forceinline__ void law_stress(int law, R lam, R mu, const R* H, R* 
     for (int J = 0; J < 3; ++J) Pm[c + 3 * J] = F[c] * S[3 * J] + F[c + 3] * S[1 + 3 * J] + F[c + 6] * S[2 + 3 * J];
 }
 
-// Directional derivative dP = (dP/dF)[Hd] at F = I + H
+// Directional derivative dP = (dP/dF)[Hd] at the deformation gradient F (stored per point)
 // SVK: dP = Hd S + F (lam tr(F'Hd) I + mu (Hd'F + F'Hd))
 template <typename R>
-__device__ __forceinline__ void law_dstress(int law, R lam, R mu, const R* H, const R* Hd, R* dP) {
+__device__ __forceinline__ void law_dstress_F(int law, R lam, R mu, const R* F, const R* Hd, R* dP) {
   if (law == HFK_LAW_LINEAR_ELASTIC) {
     law_stress<R>(law, lam, mu, Hd, dP);
     return;
   }
-  R F[9];
-#pragma unroll
-  for (int i = 0; i < 9; ++i) F[i] = H[i];
-  F[0] += R(1);
-  F[4] += R(1);
-  F[8] += R(1);
   R C[9], M[9];
 #pragma unroll
   for (int I = 0; I < 3; ++I)

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libhfk.so")
+LIB_PATH = os.environ.get("HFK_LIB", os.path.join(_HERE, "libhfk.so"))
 
 HFK_OK = 0
 LAW_SVK = 1
