@@ -54,6 +54,7 @@ SIGNATURES = {
     "hfk_eigenvalue_bounds": [_vp, _i, _vp, _pd, _pd],
     "hfk_hessenberg_eigvals": [_i, _vp, _vp, _vp],
     "hfk_chebyshev_smooth": [_vp, _d, _d, _i, _vp, _vp, _i, _vp],
+    "hfk_chebyshev_smooth_noalloc": [_vp, _d, _d, _i, _vp, _vp, _i, _vp],
     "hfk_transfer_create": [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp],
     "hfk_transfer_destroy": [_vp],
     "hfk_prolongate": [_vp, _vp, _vp],

@@ -128,6 +128,21 @@ int hfk_hessenberg_eigvals(int n, const double* H, double* re, double* im);
 int hfk_chebyshev_smooth(hfk_problem* p, double a, double b, int degree, const double* rhs, double* x,
                          int zero_guess, double* residual);
 
+/* Allocation-free smooth!: the same smoothing as hfk_chebyshev_smooth, for callers that cannot allocate
+ * device memory once their solver is set up (a host drawing every GPU buffer from a fixed, pre-sized
+ * pool, or an application that forbids allocation after set-up; cudaMalloc/cudaFree synchronise the
+ * device and can fail once memory is committed). No counterpart in the reference. It allocates
+ * nothing: its three work vectors live in one file-scope device array sized for
+ * HFK_NOALLOC_MAX_DOFS free dofs (3 * 2^19 doubles = 12 MiB, held on every GPU that loads the
+ * library until the process exits); larger operators are rejected with HFK_ERR_ARG. rhs, x and
+ * residual (NULL allowed) must be device pointers. The first call on a device does the set-up (it
+ * resolves the array's device address with cudaGetSymbolAddress); make that first call before any
+ * stream capture. Every call shares the array and starts by clearing it; calls that overlap on the
+ * GPU (from other streams or threads) race on it. The call returns after the smoothing has finished. */
+#define HFK_NOALLOC_MAX_DOFS 524288
+int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, int degree, const double* rhs, double* x,
+                                 int zero_guess, double* residual);
+
 /* ---- transfers between nested levels on one mesh (src/transfers.jl) --------------------------
  * E (nn_f, nn_c): coarse basis at the fine nodes; Einj (nn_c, nn_f): fine basis at the coarse
  * nodes (TransferField, src/transfers.jl:57-131). */

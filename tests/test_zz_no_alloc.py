@@ -1,0 +1,84 @@
+"""The allocation-free smoother entry point (hfk_chebyshev_smooth_noalloc).
+
+It serves callers that cannot allocate device memory once their solver is set up (a host that draws
+every GPU buffer from a fixed pool, or an application that forbids allocation after set-up). Its
+output must match the allocating entry point hfk_chebyshev_smooth, on two calls in a row (the
+shared scratch array keeps the previous call's contents, so the second call checks that nothing
+leaks from the first). This file is collected last, so a run that stops at the first failure has
+already run every other test.
+"""
+import numpy as np
+import pytest
+
+from conftest import reldiff, svk_space, svk_state
+
+from hfk import _lib, forms
+from hfk._lib import call, ptr
+from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+from hfk.operator import KernelOperator, MatrixFreeJacobian
+from hfk import solvers as S
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12  # the FP64 tolerance of the parity tests
+
+
+def _prepared_operator():
+    V = svk_space(n=(3, 3, 2), order=2)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V, jacobian="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    st = S.BlockJacobiState(mf)
+    assert st.ok
+    lmin, lmax = S.eigenvalue_bounds(mf, st, 10)
+    b = 1.1 * lmax
+    return V, op, b / 20.0, b
+
+
+def test_noalloc_smoother_matches_the_allocating_one_twice():
+    import torch
+
+    V, op, a, b = _prepared_operator()
+    n = V.nfree
+    rng = np.random.default_rng(7)
+    rhs1 = torch.from_numpy(rng.standard_normal(n)).cuda()
+    rhs2 = torch.from_numpy(rng.standard_normal(n)).cuda()
+    h = op.problem.h
+    x_ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r_ref = torch.zeros_like(x_ref)
+    x_na = torch.zeros_like(x_ref)
+    r_na = torch.zeros_like(x_ref)
+    # first call: zero initial guess, with the residual
+    call("hfk_chebyshev_smooth", h, a, b, 3, ptr(rhs1), ptr(x_ref), 1, ptr(r_ref))
+    call("hfk_chebyshev_smooth_noalloc", h, a, b, 3, ptr(rhs1), ptr(x_na), 1, ptr(r_na))
+    torch.cuda.synchronize()
+    assert reldiff(x_na.cpu().numpy(), x_ref.cpu().numpy()) < TOL64
+    assert reldiff(r_na.cpu().numpy(), r_ref.cpu().numpy()) < TOL64
+    # second call in a row: the previous solution as initial guess, another right-hand side, no residual
+    call("hfk_chebyshev_smooth", h, a, b, 4, ptr(rhs2), ptr(x_ref), 0, None)
+    call("hfk_chebyshev_smooth_noalloc", h, a, b, 4, ptr(rhs2), ptr(x_na), 0, None)
+    torch.cuda.synchronize()
+    assert reldiff(x_na.cpu().numpy(), x_ref.cpu().numpy()) < TOL64
+    assert float(torch.linalg.norm(x_na)) > 0
+
+
+def test_noalloc_smoother_rejects_host_pointers_and_too_many_dofs():
+    V, op, a, b = _prepared_operator()
+    rhs = np.ones(V.nfree)
+    x = np.zeros(V.nfree)
+    with pytest.raises(_lib.HFKError) as e:
+        call("hfk_chebyshev_smooth_noalloc", op.problem.h, a, b, 2, ptr(rhs), ptr(x), 1, None)
+    assert "device pointers" in str(e.value)
+    # Q1 on a 64^3 mesh: 823 875 nodes, beyond the stated maximum of free dofs
+    m = CartesianMesh((64, 64, 64))
+    big = VectorLagrangeSpace(m, 1, ("x0", "x1"))
+    assert big.nfree > 524288
+    opb = KernelOperator(forms.svk_residual(2.0, 1.0, 2), forms.svk_jacobian(2.0, 1.0, 2), big)
+    import torch
+
+    r = torch.ones(big.nfree, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(r)
+    with pytest.raises(_lib.HFKError) as e:
+        call("hfk_chebyshev_smooth_noalloc", opb.problem.h, a, b, 2, ptr(r), ptr(y), 1, None)
+    assert e.value.code == 1 and "at most 524288 free dofs" in str(e.value)
