@@ -230,6 +230,7 @@ def engine(args):
         err32 = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
         extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
         extra.update(assembly_case(torch, dev, stream, timed))
+        extra.update(newton_case())
 
     cpu = cpu_baseline_sample() if rank == 0 and not args.no_cpu else None
     if rank == 0:
@@ -281,6 +282,36 @@ def assembly_case(torch, dev, stream, timed):
     return {"assembly_q2_20x10x10": {"free_dofs": V.nfree, "nnz": int(nnz), "jacobian_ms": ms_j, "residual_ms": ms_r,
                                      "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
                                      "jacobian_qps": 27 * V.mesh.ncells / (ms_j * 1e-3)}}
+
+
+def newton_case(n=16, loads=(0.1, 0.325, 0.55, 0.775, 1.0)):
+    """Secondary: matrix-free Newton on SVK Q4 16^3 (823 875 dofs), load factor 0.1-1.0 in 5 steps,
+    flexible CG + p-multigrid 4 -> 2 -> 1 (Chebyshev degree 4, assembled Q1 coarse), every linear
+    solve to 1e-8 relative; plain FP64 vs FP32 smoothers/products under the FP64 outer loop."""
+    from hfk import forms
+    from hfk import solvers as S
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.newton import newton_solve
+    from hfk.operator import KernelOperator
+
+    m = CartesianMesh((n, n, n))
+    gfun = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
+    Vs = [VectorLagrangeSpace(m, o, ("x0", "x1"), g=gfun if o == 4 else None) for o in (4, 2, 1)]
+    g_full = Vs[0].dirichlet_values.copy()
+    res, jac = forms.svk_residual(2.0, 1.0, 8), forms.svk_jacobian(2.0, 1.0, 8)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, maxiter=300,
+                                preconditioner=S.PMultigrid(Vs, S.Chebyshev(degree=4), precision=prec))
+        newton_solve(op, ls, g_full, loads[:1], rtol_newton=1e-8)  # warm-up (kernel attributes, handles)
+        x, st = newton_solve(op, ls, g_full, loads, rtol_newton=1e-8)
+        out[prec] = {"seconds": st.seconds, "newton_iters": st.newton_iters, "krylov_iters": st.krylov_iters,
+                     "converged": st.converged, "final_residual": st.residual_norms[-1], "pmg": st.pmg,
+                     "residual_norms": [float(f"{r:.3e}") for r in st.residual_norms]}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
+    return {"newton_pmg_svk_q4_16": {"free_dofs": Vs[0].nfree, "levels": "Q4 -> Q2 -> Q1 (dense Cholesky)",
+                                     "loads": list(loads), **out}}
 
 
 def cpu_threads():

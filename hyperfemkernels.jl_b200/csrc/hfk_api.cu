@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -273,8 +274,25 @@ void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R
 }
 
 // Run a cell kernel colour by colour (deterministic scatter)
+// Scatter policy: colour by colour (deterministic) unless the colours are too small to fill the
+// GPU, then one launch over all cells with atomicAdd (an order-dependent last bit). A colour needs
+// about 4 warps per SM to hide the gather latency.
+bool use_atomic_scatter(const hfk_problem* p) {
+  if (p->scatter == HFK_SCATTER_COLOURED) return false;
+  if (p->scatter == HFK_SCATTER_ATOMIC) return true;
+  const int m = std::max(p->Q, p->P);
+  const int cpw = m > 0 ? std::max(1, 32 / (m * m)) : 1;
+  const int64_t per_colour = p->ncolors ? p->ncells / p->ncolors : p->ncells;
+  return per_colour < (int64_t)sm_count() * 4 * cpw;
+}
+
 template <int MODE, typename R>
 void run_cells(hfk_problem* p, CellIO<R> io) {
+  if (use_atomic_scatter(p)) {
+    io.atomic = 1;
+    dispatch_cell<MODE, R>(p, nullptr, p->ncells, io);
+    return;
+  }
   io.atomic = 0;
   for (int c = 0; c < p->ncolors; ++c) {
     const int n = p->color_start[c + 1] - p->color_start[c];
@@ -371,10 +389,6 @@ void bind_state(hfk_problem* p, const double* x, const double* dvals) {
 }
 
 // ---- reductions -------------------------------------------------------------------------------
-struct Reducer {
-  DBuf<double> partial, out;
-  double host[3];
-};
 
 template <typename R>
 void dots(hfk_problem* p, Reducer& red, int64_t n, int k, const R* a0, const R* b0, const R* a1 = nullptr,
@@ -632,6 +646,45 @@ void cheb_smooth_dev(hfk_problem* p, ChebWork<R>& w, double a, double b, int deg
   if (residual) HFK_CUDA(cudaMemcpyAsync(residual, w.r.p, n * sizeof(R), cudaMemcpyDeviceToDevice, p->stream));
 }
 
+// The same smoothing with the coefficients read from device memory (`coef`, see
+// cheb_start_dev_kernel): used by the V-cycle, which is captured once in a CUDA graph.
+template <typename R>
+void cheb_smooth_coef(hfk_problem* p, ChebWork<R>& w, const double* coef, int degree, const R* rhs, R* x,
+                      bool zero_guess, R* residual) {
+  const int64_t n = p->nfree;
+  w.ensure(n);
+  if (!zero_guess) mf_apply_any<R>(p, x, w.z.p);
+  cheb_start_dev_kernel<R><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, binv_of<R>(p), rhs,
+                                                                        w.z.p, w.r.p, w.d.p, x, coef,
+                                                                        zero_guess ? 1 : 0);
+  check_launch(p);
+  for (int i = 1; i <= degree; ++i) {
+    if (i == degree && !residual) break;
+    mf_apply_any<R>(p, w.d.p, w.z.p);
+    const bool last = i == degree;
+    cheb_step_dev_kernel<R><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, binv_of<R>(p), w.z.p,
+                                                                          w.r.p, w.d.p, x, coef, i, last ? 0 : 1);
+    check_launch(p);
+    if (last) break;
+  }
+  if (residual) HFK_CUDA(cudaMemcpyAsync(residual, w.r.p, n * sizeof(R), cudaMemcpyDeviceToDevice, p->stream));
+}
+
+// Chebyshev coefficients of smooth! (src/smoothers.jl:116-146) on [a, b]: [1/theta, c1_1, c2_1, ...]
+std::vector<double> chebyshev_coefficients(double a, double b, int degree) {
+  const double th = (b + a) / 2, de = (b - a) / 2, sg = th / de;
+  std::vector<double> c(1 + 2 * (size_t)degree, 0.0);
+  c[0] = 1.0 / th;
+  double rho = 1.0 / sg;
+  for (int i = 1; i < degree; ++i) {
+    const double rn = 1.0 / (2 * sg - rho);
+    c[2 * i - 1] = rn * rho;
+    c[2 * i] = 2 * rn / de;
+    rho = rn;
+  }
+  return c;
+}
+
 // ---- small dense eigenvalues (Francis double-shift QR on a Hessenberg matrix) ---------------------
 // The eigvals call of eigenvalue_bounds (src/preconditioners.jl:386); real and imaginary parts.
 bool hessenberg_eigvals(int n, std::vector<double> H /* column-major n x n */, double* re, double* im) {
@@ -745,7 +798,7 @@ bool hessenberg_eigvals(int n, std::vector<double> H /* column-major n x n */, d
 }
 
 struct EigWork {
-  DBuf<double> V, t, w;
+  DBuf<double> V, t, w, Hd;
   Reducer red;
 };
 
@@ -757,37 +810,44 @@ void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev,
   ew.V.resize((size_t)(k + 1) * n);
   ew.t.resize(n);
   ew.w.resize(n);
+  ew.Hd.resize((size_t)(k + 2) * (k + 1));
+  ew.Hd.zero(p->stream);
+  ew.red.partial.resize((size_t)3 * RED_BLOCKS);
   std::vector<double> H((size_t)(k + 1) * k, 0.0);
-  double nb;
-  dots<double>(p, ew.red, n, 1, start_dev, start_dev, nullptr, nullptr, nullptr, nullptr, &nb);
-  nb = std::sqrt(nb);
-  axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0 / nb, start_dev, 0.0, start_dev, ew.V.p);
+  const int ld = k + 1;
+  double* Hd = ew.Hd.p;
+  double* nrm = Hd + (size_t)ld * k;  // scratch scalar past the Hessenberg matrix
+  auto dot_to = [&](const double* x, const double* y, double* out) {
+    dots_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, p->stream>>>(n, 1, x, y, nullptr, nullptr, nullptr, nullptr,
+                                                                    ew.red.partial.p);
+    check_launch(p);
+    finish_sums_kernel<<<1, 1024, 0, p->stream>>>(RED_BLOCKS, 1, ew.red.partial.p, out);
+    check_launch(p);
+  };
+  dot_to(start_dev, start_dev, nrm);
+  sqrt_dev_kernel<<<1, 1, 0, p->stream>>>(nrm);
   check_launch(p);
-  int steps = k;
+  scale_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, nrm, start_dev, ew.V.p);
+  check_launch(p);
   for (int j = 0; j < k; ++j) {
     double* vj = ew.V.p + (size_t)j * n;
     blocks_apply_dev<double>(p, vj, ew.t.p);
     mf_apply_dev(p, ew.t.p, ew.w.p);
-    for (int i = 0; i <= j; ++i) {
-      double hij;
-      dots<double>(p, ew.red, n, 1, ew.V.p + (size_t)i * n, ew.w.p, nullptr, nullptr, nullptr, nullptr, &hij);
-      H[i + (size_t)(k + 1) * j] = hij;
-      axpby_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, -hij, ew.V.p + (size_t)i * n, 1.0, ew.w.p);
+    for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, coefficients written into H on the device
+      double* hij = Hd + i + (size_t)ld * j;
+      dot_to(ew.V.p + (size_t)i * n, ew.w.p, hij);
+      axpy_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, hij, -1.0, ew.V.p + (size_t)i * n, ew.w.p);
       check_launch(p);
     }
-    double hn;
-    dots<double>(p, ew.red, n, 1, ew.w.p, ew.w.p, nullptr, nullptr, nullptr, nullptr, &hn);
-    hn = std::sqrt(hn);
-    H[j + 1 + (size_t)(k + 1) * j] = hn;
-    if (hn == 0) {
-      steps = j + 1;
-      break;
-    }
-    axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0 / hn, ew.w.p, 0.0, ew.w.p,
-                                                              ew.V.p + (size_t)(j + 1) * n);
+    double* hn = Hd + (j + 1) + (size_t)ld * j;
+    dot_to(ew.w.p, ew.w.p, hn);
+    sqrt_dev_kernel<<<1, 1, 0, p->stream>>>(hn);
+    check_launch(p);
+    scale_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, hn, ew.w.p, ew.V.p + (size_t)(j + 1) * n);
     check_launch(p);
   }
-  (void)steps;
+  HFK_CUDA(cudaMemcpyAsync(H.data(), Hd, sizeof(double) * (size_t)ld * k, cudaMemcpyDeviceToHost, p->stream));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
   // breakdown truncation (src/preconditioners.jl:379-385)
   int jj = k;
   for (int i = 1; i < k; ++i) {
@@ -1054,13 +1114,31 @@ struct hfk_pmg {
   int since = 0, nupdate = 0, nbuild = 0;
   std::vector<std::unique_ptr<LevelWork<double>>> w64;
   std::vector<std::unique_ptr<LevelWork<float>>> w32;
-  // coarse: dense inverse of the assembled coarse tangent
-  DBuf<double> Ainv, cb, cx;
+  // coarse: dense Cholesky factor (lower) of the assembled coarse tangent
+  DBuf<double> Lc, cb, cx;
   bool coarse_ok = false;
-  EigWork ew;
-  DBuf<double> start;
+  std::vector<std::unique_ptr<EigWork>> ew;          // per level (no reallocation between levels)
+  std::vector<std::unique_ptr<DBuf<double>>> start;  // per level: the fixed Arnoldi start vector
+  DBuf<double> potrf_work;
+  DBuf<int> potrf_info;
   DBuf<double> top_r, top_y;
   cusolverDnHandle_t solver = nullptr;
+  cublasHandle_t blas = nullptr;
+  DBuf<unsigned char> blas_ws;
+  double t_potrf = 0;
+  // Chebyshev coefficients per level on the device (rewritten at every update)
+  std::vector<std::unique_ptr<DBuf<double>>> coef;
+  // the V-cycle as a CUDA graph, captured on the second cycle and replayed until a level's law
+  // parameters change (the coefficients and states it reads live in fixed device buffers)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int cycles_since_update = 0;
+  std::vector<double> graph_params;
+  // statistics: times in ms (host wall clock for the update phases, CUDA events for the cycles)
+  double t_update = 0, t_coarse = 0, t_blocks = 0, t_eig = 0, t_cycle = 0;
+  int64_t ncycles = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool ev_pending = false;
 };
 
 namespace {
@@ -1076,10 +1154,10 @@ void coarse_factor(hfk_pmg* m) {
   jacobian_dev(c, c->x.p, c->dvals.p, c->nzval.p);
   const int64_t n = c->nfree;
   HFK_REQUIRE(n <= 40000, HFK_ERR_UNSUPPORTED, "the dense coarse solve supports up to 40000 coarse dofs");
-  m->Ainv.resize((size_t)n * n);
-  m->Ainv.zero(c->stream);
+  m->Lc.resize((size_t)n * n);
+  m->Lc.zero(c->stream);
   csc_to_dense_kernel<<<(int)std::min<int64_t>(n, 65535), 128, 0, c->stream>>>(n, c->colptr.p, c->rowval.p, c->nzval.p,
-                                                                                m->Ainv.p);
+                                                                                m->Lc.p);
   check_launch(c);
   if (!m->solver) {
     if (cusolverDnCreate(&m->solver) != CUSOLVER_STATUS_SUCCESS)
@@ -1087,37 +1165,52 @@ void coarse_factor(hfk_pmg* m) {
   }
   cusolverDnSetStream(m->solver, c->stream);
   int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Ainv.p, (int)n, &lwork) !=
+  if (cusolverDnDpotrf_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Lc.p, (int)n, &lwork) !=
       CUSOLVER_STATUS_SUCCESS)
     throw Error{HFK_ERR_CUDA, "HyperFEMKernels: potrf_bufferSize failed"};
-  int lwork2 = 0;
-  cusolverDnDpotri_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Ainv.p, (int)n, &lwork2);
-  DBuf<double> work;
-  work.resize(std::max(lwork, lwork2) + 1);
-  DBuf<int> info;
-  info.resize(1);
-  cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Ainv.p, (int)n, work.p, lwork, info.p);
+  if (m->potrf_work.n < (size_t)lwork + 1) m->potrf_work.resize((size_t)lwork + 1);
+  m->potrf_info.resize(1);
+  DBuf<double>& work = m->potrf_work;
+  DBuf<int>& info = m->potrf_info;
+  cudaEvent_t e0, e1;
+  HFK_CUDA(cudaEventCreate(&e0));
+  HFK_CUDA(cudaEventCreate(&e1));
+  HFK_CUDA(cudaEventRecord(e0, c->stream));
+  cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Lc.p, (int)n, work.p, lwork, info.p);
+  HFK_CUDA(cudaEventRecord(e1, c->stream));
   int h_info = 0;
   HFK_CUDA(cudaMemcpyAsync(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HFK_CUDA(cudaStreamSynchronize(c->stream));
-  if (h_info != 0) {
-    m->coarse_ok = false;
-    return;
-  }
-  cusolverDnDpotri(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Ainv.p, (int)n, work.p, lwork2, info.p);
-  HFK_CUDA(cudaMemcpyAsync(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  HFK_CUDA(cudaStreamSynchronize(c->stream));
-  symmetrize_lower_kernel<<<(int)std::min<int64_t>(n, 65535), 256, 0, c->stream>>>(n, m->Ainv.p);
-  check_launch(c);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  m->t_potrf += ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the lower triangle now holds the Cholesky factor L (A = L L^T); the cycle applies A^-1 by two
+  // triangular solves
   m->coarse_ok = h_info == 0;
-  m->nbuild++;
+  if (m->coarse_ok) m->nbuild++;
 }
 
+// x = A^-1 b with the Cholesky factor: L y = b, L^T x = y (cuBLAS triangular solves, FP64)
 void coarse_solve(hfk_pmg* m, const double* b, double* x) {
   hfk_problem* c = m->lv[m->L - 1];
   const int64_t n = c->nfree;
-  symv_kernel<<<vec_grid(n * 32), 256, 0, c->stream>>>(n, m->Ainv.p, b, x);
-  check_launch(c);
+  if (!m->blas) {
+    if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
+    // a fixed workspace, so that the captured cycle never asks cuBLAS to allocate
+    m->blas_ws.resize(32u << 20);
+    if (cublasSetWorkspace(m->blas, m->blas_ws.p, m->blas_ws.n) != CUBLAS_STATUS_SUCCESS)
+      throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasSetWorkspace failed"};
+  }
+  cublasSetStream(m->blas, c->stream);
+  HFK_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  const double one = 1.0;
+  if (cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
+                  m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS ||
+      cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
+                  m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS)
+    throw Error{HFK_ERR_CUDA, "HyperFEMKernels: triangular solve of the coarse level failed"};
 }
 
 template <typename R>
@@ -1137,7 +1230,7 @@ void vcycle_dev(hfk_pmg* m, int l) {
   hfk_problem* p = m->lv[l];
   LevelWork<R>& w = level_work<R>(m, l);
   // pre-smoothing from zero, with the residual for the restriction
-  cheb_smooth_dev<R>(p, w.cheb, m->a[l], m->b[l], m->degree, w.b.p, w.x.p, true, w.r.p);
+  cheb_smooth_coef<R>(p, w.cheb, m->coef[l]->p, m->degree, w.b.p, w.x.p, true, w.r.p);
   if (l + 1 == m->L - 1) {
     hfk_problem* c = m->lv[l + 1];
     LevelWork<R>& wc = level_work<R>(m, l + 1);
@@ -1161,7 +1254,53 @@ void vcycle_dev(hfk_pmg* m, int l) {
   axpby_kernel<R><<<vec_grid(p->nfree), 256, 0, p->stream>>>(p->nfree, R(1), w.e.p, R(1), w.x.p);
   check_launch(p);
   // post-smoothing with the same polynomial (symmetric cycle)
-  cheb_smooth_dev<R>(p, w.cheb, m->a[l], m->b[l], m->degree, w.b.p, w.x.p, false, nullptr);
+  cheb_smooth_coef<R>(p, w.cheb, m->coef[l]->p, m->degree, w.b.p, w.x.p, false, nullptr);
+}
+
+void pmg_drop_graph(hfk_pmg* m) {
+  if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  m->graph_exec = nullptr;
+  m->graph = nullptr;
+  m->cycles_since_update = 0;
+}
+
+void pmg_collect_cycle_time(hfk_pmg* m) {
+  if (!m->ev_pending) return;
+  HFK_CUDA(cudaEventSynchronize(m->ev1));
+  float ms = 0;
+  HFK_CUDA(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+  m->t_cycle += ms;
+  m->ev_pending = false;
+}
+
+// one V-cycle from level_work(0).b into level_work(0).x, replayed from a CUDA graph once captured
+void pmg_cycle_on_buffers(hfk_pmg* m) {
+  hfk_problem* p0 = m->lv[0];
+  cudaStream_t s = p0->stream;
+  if (!m->graph_exec && m->cycles_since_update >= 1) {
+    // every buffer exists (the first cycle after the update ran uncaptured): capture the cycle
+    HFK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      if (m->precision == HFK_FP32) vcycle_dev<float>(m, 0);
+      else vcycle_dev<double>(m, 0);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    HFK_CUDA(cudaStreamEndCapture(s, &m->graph));
+    HFK_CUDA(cudaGraphInstantiate(&m->graph_exec, m->graph, 0));
+  }
+  if (m->graph_exec) {
+    HFK_CUDA(cudaGraphLaunch(m->graph_exec, s));
+  } else if (m->precision == HFK_FP32) {
+    vcycle_dev<float>(m, 0);
+  } else {
+    vcycle_dev<double>(m, 0);
+  }
+  m->cycles_since_update++;
 }
 
 // ldiv!(y, PMultigridState, r) on device vectors
@@ -1173,19 +1312,28 @@ void pmg_apply_dev(hfk_pmg* m, const double* r, double* y) {
     check_launch(p0);
     return;
   }
+  pmg_collect_cycle_time(m);
+  if (!m->ev0) {
+    HFK_CUDA(cudaEventCreate(&m->ev0));
+    HFK_CUDA(cudaEventCreate(&m->ev1));
+  }
+  HFK_CUDA(cudaEventRecord(m->ev0, p0->stream));
   if (m->precision == HFK_FP32) {
     LevelWork<float>& w = *m->w32[0];
     convert_kernel<double, float><<<vec_grid(n), 256, 0, p0->stream>>>(n, r, w.b.p);
     check_launch(p0);
-    vcycle_dev<float>(m, 0);
+    pmg_cycle_on_buffers(m);
     convert_kernel<float, double><<<vec_grid(n), 256, 0, p0->stream>>>(n, w.x.p, y);
     check_launch(p0);
   } else {
     LevelWork<double>& w = *m->w64[0];
     HFK_CUDA(cudaMemcpyAsync(w.b.p, r, n * sizeof(double), cudaMemcpyDeviceToDevice, p0->stream));
-    vcycle_dev<double>(m, 0);
+    pmg_cycle_on_buffers(m);
     HFK_CUDA(cudaMemcpyAsync(y, w.x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, p0->stream));
   }
+  HFK_CUDA(cudaEventRecord(m->ev1, p0->stream));
+  m->ev_pending = true;
+  m->ncycles++;
 }
 
 }  // namespace
@@ -1301,6 +1449,14 @@ int hfk_problem_set_stream(hfk_problem* p, void* stream) {
   HFK_REQUIRE(p, HFK_ERR_ARG, "null handle");
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+  HFK_API_END
+}
+
+int hfk_problem_set_scatter(hfk_problem* p, int mode) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && (mode == HFK_SCATTER_AUTO || mode == HFK_SCATTER_COLOURED || mode == HFK_SCATTER_ATOMIC),
+              HFK_ERR_ARG, "scatter mode must be HFK_SCATTER_AUTO, _COLOURED or _ATOMIC");
+  p->scatter = mode;
   HFK_API_END
 }
 
@@ -1675,6 +1831,12 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
       m->w64.push_back(std::move(w));
     }
   }
+  for (int l = 0; l < nlevels; ++l) {
+    m->coef.push_back(std::make_unique<DBuf<double>>());
+    m->coef.back()->resize(1 + 2 * (size_t)degree);
+    m->ew.push_back(std::make_unique<EigWork>());
+    m->start.push_back(std::make_unique<DBuf<double>>());
+  }
   const int64_t nc = levels[nlevels - 1]->nfree;
   m->cb.resize(nc);
   m->cx.resize(nc);
@@ -1691,6 +1853,10 @@ int hfk_pmg_destroy(hfk_pmg* m) {
     // the coarser levels go back to their own streams (levels must outlive their hierarchy)
     for (int l = 1; l < m->L; ++l) m->lv[l]->stream = m->lv[l]->own_stream;
     if (m->solver) cusolverDnDestroy(m->solver);
+    if (m->blas) cublasDestroy(m->blas);
+    pmg_drop_graph(m);
+    if (m->ev0) cudaEventDestroy(m->ev0);
+    if (m->ev1) cudaEventDestroy(m->ev1);
   }
   delete m;
   HFK_API_END
@@ -1700,6 +1866,20 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   HFK_API_BEGIN
   HFK_REQUIRE(m && x && ok, HFK_ERR_ARG, "null argument");
   pmg_bind_stream(m);
+  pmg_collect_cycle_time(m);
+  {
+    // the captured cycle bakes in the levels' law parameters: capture again if they changed
+    std::vector<double> prm;
+    for (auto* lv : m->lv) prm.insert(prm.end(), lv->params, lv->params + 5);
+    if (prm != m->graph_params) {
+      pmg_drop_graph(m);
+      m->graph_params = prm;
+    }
+  }
+  const auto t_start = std::chrono::steady_clock::now();
+  auto ms_since = [](std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+  };
   hfk_problem* p0 = m->lv[0];
   const bool f32 = m->precision == HFK_FP32;
   // level 0 state: the Newton's tangent (prepared in the recompute formulation)
@@ -1724,18 +1904,23 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   for (int l = 0; l + 1 < m->L; ++l) {
     hfk_problem* p = m->lv[l];
     int bok = 0;
+    auto tb = std::chrono::steady_clock::now();
     blocks_update_dev(p, &bok);
+    m->t_blocks += ms_since(tb);
     if (!bok) {
       m->lok[l] = 0;
       all_ok = false;
       continue;
     }
-    std::vector<double> v;
-    chebyshev_start_vector(p->nfree, v);
-    DBuf<double> sv;
-    sv.upload(v.data(), v.size(), p->stream);
+    if (m->start[l]->n != (size_t)p->nfree) {
+      std::vector<double> v;
+      chebyshev_start_vector(p->nfree, v);
+      m->start[l]->upload(v.data(), v.size(), p->stream);
+    }
     double lmin = 0, lmax = 0;
-    eig_bounds_dev(p, m->ew, m->eig_iters, sv.p, &lmin, &lmax);
+    auto te = std::chrono::steady_clock::now();
+    eig_bounds_dev(p, *m->ew[l], m->eig_iters, m->start[l]->p, &lmin, &lmax);
+    m->t_eig += ms_since(te);
     m->lmin[l] = lmin;
     m->lmax[l] = lmax;
     const bool lok = std::isfinite(lmax) && lmax > 0 && lmin > 0;
@@ -1743,11 +1928,17 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     all_ok &= lok;
     m->b[l] = m->inflate * lmax;
     m->a[l] = m->b[l] / m->range;
+    const std::vector<double> c = chebyshev_coefficients(m->a[l], m->b[l], m->degree);
+    m->coef[l]->upload(c.data(), c.size(), p->stream);
+    if (f32) ensure_F32(p);
   }
   // coarse level (every coarse_every updates)
   m->since++;
   if (!m->built || m->since >= m->coarse_every) {
+    auto tc = std::chrono::steady_clock::now();
     coarse_factor(m);
+    HFK_CUDA(cudaStreamSynchronize(p0->stream));
+    m->t_coarse += ms_since(tc);
     m->since = 0;
   }
   all_ok &= m->coarse_ok;
@@ -1755,6 +1946,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   m->built = true;
   m->nupdate++;
   *ok = all_ok;
+  m->t_update += ms_since(t_start);
   HFK_API_END
 }
 
@@ -1769,6 +1961,22 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y) {
   pmg_apply_dev(m, dr, dy);
   finish_out(y, dy, p0->nfree, p0->stream);
   HFK_CUDA(cudaStreamSynchronize(p0->stream));
+  HFK_API_END
+}
+
+int hfk_pmg_stats(hfk_pmg* m, double* out) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && out, HFK_ERR_ARG, "null argument");
+  pmg_collect_cycle_time(m);
+  out[0] = (double)m->nupdate;
+  out[1] = (double)m->nbuild;
+  out[2] = (double)m->ncycles;
+  out[3] = m->t_update;
+  out[4] = m->t_coarse;
+  out[5] = m->t_blocks;
+  out[6] = m->t_eig;
+  out[7] = m->t_cycle;
+  out[8] = m->t_potrf;
   HFK_API_END
 }
 
@@ -1805,7 +2013,8 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
     HFK_CUDA(cudaStreamSynchronize(s));
     return HFK_OK;
   }
-  DBuf<double> db, dx, r, z, pp, q, rold;
+  hfk::CGWork& cw = op->cg;
+  DBuf<double>&db = cw.b, &dx = cw.x, &r = cw.r, &z = cw.z, &pp = cw.p, &q = cw.q, &rold = cw.rold;
   const double* bd = dev_in(b, n, db, s);
   double* xd = x;
   if (!is_device_ptr(x)) {
@@ -1818,7 +2027,7 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
   pp.resize(n);
   q.resize(n);
   if (flexible) rold.resize(n);
-  Reducer red;
+  Reducer& red = cw.red;
   double res[3];
   // r = b - A x
   mf_apply_dev(op, xd, q.p);

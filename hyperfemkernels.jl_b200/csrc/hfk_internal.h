@@ -84,6 +84,18 @@ struct CellData {
   double lam, mu, body[3];
 };
 
+// Work of the two-stage reductions (partial sums and the result)
+struct Reducer {
+  DBuf<double> partial, out;
+  double host[3];
+};
+
+// Work vectors of the Krylov solve, kept with the operator between solves
+struct CGWork {
+  DBuf<double> b, x, r, z, p, q, rold;
+  Reducer red;
+};
+
 // State of a matrix-free level in a precision
 template <typename R>
 struct LevelState {
@@ -148,4 +160,6 @@ struct hfk_problem {
   // timing of the last kernel sequence (CUDA events)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int launches = 0;
+  int scatter = HFK_SCATTER_AUTO;
+  hfk::CGWork cg;
 };

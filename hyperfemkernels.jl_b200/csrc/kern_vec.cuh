@@ -272,6 +272,79 @@ __global__ void cheb_step_kernel(int nb, const int32_t* dofs, const R* Binv, con
   }
 }
 
+// The same two steps with the coefficients read from device memory (coef = [1/theta, c1_1, c2_1,
+// c1_2, c2_2, ...], written by the host at every update), so that a V-cycle captured once in a CUDA
+// graph stays valid when the smoothing interval changes.
+template <typename R>
+__global__ void cheb_start_dev_kernel(int nb, const int32_t* dofs, const R* Binv, const R* rhs, const R* Ax, R* r,
+                                      R* d, R* x, const double* coef, int zero_guess) {
+  const R inv_theta = (R)coef[0];
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
+    R rr[3];
+    for (int i = 0; i < 3; ++i) {
+      rr[i] = 0;
+      if (dd[i]) {
+        R v = rhs[dd[i] - 1];
+        if (!zero_guess) v -= Ax[dd[i] - 1];
+        r[dd[i] - 1] = v;
+        rr[i] = v;
+      }
+    }
+    const R* M = Binv + 9 * (size_t)b;
+    for (int i = 0; i < 3; ++i) {
+      if (!dd[i]) continue;
+      const R di = (M[i] * rr[0] + M[i + 3] * rr[1] + M[i + 6] * rr[2]) * inv_theta;
+      d[dd[i] - 1] = di;
+      x[dd[i] - 1] = zero_guess ? di : x[dd[i] - 1] + di;
+    }
+  }
+}
+template <typename R>
+__global__ void cheb_step_dev_kernel(int nb, const int32_t* dofs, const R* Binv, const R* z, R* r, R* d, R* x,
+                                     const double* coef, int step, int update_d) {
+  const R c1 = update_d ? (R)coef[2 * step - 1] : R(0), c2 = update_d ? (R)coef[2 * step] : R(0);
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
+    R rr[3];
+    for (int i = 0; i < 3; ++i) {
+      rr[i] = 0;
+      if (dd[i]) {
+        const R v = r[dd[i] - 1] - z[dd[i] - 1];
+        r[dd[i] - 1] = v;
+        rr[i] = v;
+      }
+    }
+    if (!update_d) continue;
+    const R* M = Binv + 9 * (size_t)b;
+    for (int i = 0; i < 3; ++i) {
+      if (!dd[i]) continue;
+      const R dn = c1 * d[dd[i] - 1] + c2 * (M[i] * rr[0] + M[i + 3] * rr[1] + M[i + 6] * rr[2]);
+      d[dd[i] - 1] = dn;
+      x[dd[i] - 1] += dn;
+    }
+  }
+}
+
+// ---- Arnoldi without host synchronisation: scalars stay on the device -----------------------
+// y += sign * (*alpha) * x
+__global__ void axpy_dev_kernel(int64_t n, const double* alpha, double sign, const double* x, double* y) {
+  const double a = sign * *alpha;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+// *s = sqrt(*s)
+__global__ void sqrt_dev_kernel(double* s) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *s = sqrt(*s);
+}
+// y = x / *s (0 when *s is 0: the breakdown is decided on the host from the Hessenberg matrix)
+__global__ void scale_dev_kernel(int64_t n, const double* s, const double* x, double* y) {
+  const double v = *s;
+  const double inv = v != 0.0 ? 1.0 / v : 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i] * inv;
+}
+
 // ---- transfers (src/transfers.jl) ------------------------------------------------------------
 struct XferData {
   const int32_t* ids_f;   // (3 NF, ncells) fine level, tensor order
@@ -356,22 +429,4 @@ __global__ void csc_to_dense_kernel(int64_t n, const int64_t* colptr, const int6
     for (int64_t k = colptr[c] - 1 + threadIdx.x; k < colptr[c + 1] - 1; k += blockDim.x)
       A[(rowval[k] - 1) + n * c] = nzval[k];
 }
-// lower triangle -> full symmetric
-__global__ void symmetrize_lower_kernel(int64_t n, double* A) {
-  for (int64_t c = blockIdx.x; c < n; c += gridDim.x)
-    for (int64_t r = threadIdx.x; r < c; r += blockDim.x) A[r + n * c] = A[c + n * r];
-}
-// y = A x, A dense column-major symmetric (rows read as columns): one warp per output
-__global__ void symv_kernel(int64_t n, const double* A, const double* x, double* y) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < n;
-       row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-    const double* col = A + n * row;  // column `row` == row `row` (symmetric)
-    double s = 0;
-    for (int64_t k = lane; k < n; k += 32) s += col[k] * x[k];
-    s = warp_sum<double>(s);
-    if (lane == 0) y[row] = s;
-  }
-}
-
 }  // namespace hfk

@@ -21,6 +21,9 @@ MF_STORED = 0
 MF_RECOMPUTE = 1
 FP64 = 0
 FP32 = 1
+SCATTER_AUTO = 0
+SCATTER_COLOURED = 1
+SCATTER_ATOMIC = 2
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -38,6 +41,7 @@ SIGNATURES = {
     "hfk_problem_set_params": [_vp, _vp, _i],
     "hfk_problem_set_stream": [_vp, _vp],
     "hfk_problem_info": [_vp, _pi64, _pi, _pi, _pi, _pi64],
+    "hfk_problem_set_scatter": [_vp, _i],
     "hfk_launch_count": [_vp, _pi64],
     "hfk_colors": [_vp, _vp],
     "hfk_pattern_build": [_vp, _pi64],
@@ -65,6 +69,7 @@ SIGNATURES = {
     "hfk_pmg_update": [_vp, _vp, _vp, _pi],
     "hfk_pmg_vcycle": [_vp, _vp, _vp],
     "hfk_pmg_level_info": [_vp, _i, _pd, _pd, _pd, _pd],
+    "hfk_pmg_stats": [_vp, _vp],
     "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
 }
 

@@ -26,6 +26,7 @@ class NewtonStats:
     residual_norms: list = dataclasses.field(default_factory=list)
     converged: bool = True
     seconds: float = 0.0
+    pmg: dict = None  # p-multigrid counters and times (PMultigridState.stats)
 
 
 def newton_solve(op: KernelOperator, solver: S.MatrixFreeSolver, g_full: np.ndarray, loads, x0=None, *,
@@ -80,4 +81,6 @@ def newton_solve(op: KernelOperator, solver: S.MatrixFreeSolver, g_full: np.ndar
             break
     torch.cuda.synchronize()
     st.seconds = time.perf_counter() - t0
+    if ns is not None and ns.prec is not None and hasattr(ns.prec, "stats"):
+        st.pmg = ns.prec.stats()
     return x, st

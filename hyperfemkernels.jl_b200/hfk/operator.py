@@ -59,6 +59,11 @@ class Problem:
     def set_stream(self, stream_handle: int | None):
         call("hfk_problem_set_stream", self.h, ctypes.c_void_p(stream_handle or 0))
 
+    def set_scatter(self, mode: str):
+        """"auto" (default), "coloured" (deterministic) or "atomic" for the sum-factorised kernels."""
+        m = {"auto": _lib.SCATTER_AUTO, "coloured": _lib.SCATTER_COLOURED, "atomic": _lib.SCATTER_ATOMIC}[mode]
+        call("hfk_problem_set_scatter", self.h, m)
+
     def launches(self) -> int:
         c = ctypes.c_int64()
         call("hfk_launch_count", self.h, ctypes.byref(c))

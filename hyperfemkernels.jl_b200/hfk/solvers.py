@@ -214,6 +214,14 @@ class PMultigridState:
         call("hfk_pmg_vcycle", self.h, ptr(r), ptr(y))
         return y
 
+    def stats(self):
+        """Counters and times (ms): updates, coarse builds, cycles, update/coarse/blocks/eig/cycle time."""
+        out = np.zeros(9)
+        call("hfk_pmg_stats", self.h, ptr(out))
+        keys = ("updates", "coarse_builds", "cycles", "t_update_ms", "t_coarse_ms", "t_blocks_ms", "t_eig_ms",
+                "t_cycle_ms", "t_potrf_ms")
+        return dict(zip(keys, out.tolist()))
+
     def level_info(self, level: int):
         a, b, lo, hi = (ctypes.c_double() for _ in range(4))
         call("hfk_pmg_level_info", self.h, level, ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(a), ctypes.byref(b))

@@ -74,6 +74,15 @@ int hfk_problem_set_params(hfk_problem* p, const double* params, int nparams);
 /* Launch on `stream` (a cudaStream_t) from now on; NULL restores the handle's own stream. */
 int hfk_problem_set_stream(hfk_problem* p, void* stream);
 int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolors, int64_t* nnz);
+/* Scatter of the sum-factorised kernels (residual, products): colour by colour with plain
+ * read-modify-writes (deterministic, the reference's race-free colouring, src/coloring.jl:1-3), or
+ * one launch over all cells with FP64 atomics (the summation order, hence the last bit, varies
+ * between runs). AUTO (default) colours unless the colours are too small to fill the GPU. The
+ * assembled Jacobian and the nodal blocks always scatter by colour. */
+#define HFK_SCATTER_AUTO 0
+#define HFK_SCATTER_COLOURED 1
+#define HFK_SCATTER_ATOMIC 2
+int hfk_problem_set_scatter(hfk_problem* p, int mode);
 /* Number of kernels this handle launched so far (launch accounting for benchmarks). */
 int hfk_launch_count(hfk_problem* p, int64_t* count);
 
@@ -158,8 +167,8 @@ int hfk_inject(hfk_transfer* t, const double* xf, const double* df, double* xc, 
 
 /* ---- p-multigrid (src/pmultigrid.jl) ---------------------------------------------------------
  * levels[0] is the working level (its state is bound by hfk_pmg_update), levels[nlevels-1] the
- * assembled coarse level (solved by a dense Cholesky factorisation on the GPU, in place of the
- * reference's LUSolver); transfers[l] goes from level l+1 to level l. Chebyshev(degree, range,
+ * assembled coarse level (solved by a dense Cholesky factorisation on the GPU and two triangular
+ * solves per cycle, in place of the reference's LUSolver); transfers[l] goes from level l+1 to level l. Chebyshev(degree, range,
  * inflate, eig_iters) as src/smoothers.jl:21-33. precision HFK_FP64 or HFK_FP32: the arithmetic of
  * the smoothers and products on the levels above the coarse one (the coarse solve is always FP64). */
 #define HFK_FP64 0
@@ -174,6 +183,11 @@ int hfk_pmg_destroy(hfk_pmg* m);
 int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok);
 /* ldiv!(y, PMultigridState, r) (src/pmultigrid.jl:316-338): one V-cycle; NaN when not ok. */
 int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y);
+/* Counters and times (ms) of a hierarchy: out[9] = updates, coarse factorisations, V-cycles, time in
+ * updates, in coarse assembly + factorisation, in block extraction, in eigenvalue estimates, in
+ * V-cycles, in the Cholesky factorisation alone. The
+ * V-cycle is replayed from a CUDA graph captured on the second cycle after each update. */
+int hfk_pmg_stats(hfk_pmg* m, double* out);
 /* Interval and Ritz values of a level's smoother. */
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
 

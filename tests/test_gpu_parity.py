@@ -105,6 +105,7 @@ def test_device_pointers_and_host_pointers_agree():
     import torch
 
     V, op, orc = make(2, jac="matrixfree")
+    op.problem.set_scatter("coloured")  # deterministic summation order: bit-identical results
     x = svk_state(V)
     b_host = op.residual(np.zeros(V.nfree), x)
     xd = torch.from_numpy(x).cuda()
@@ -112,6 +113,22 @@ def test_device_pointers_and_host_pointers_agree():
     bd = torch.zeros(V.nfree, dtype=torch.float64, device="cuda")
     op.residual(bd, xd, dd)
     assert np.array_equal(bd.cpu().numpy(), b_host)
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_atomic_and_coloured_scatter_agree(order):
+    V, op, orc = make(order, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    dx = np.random.default_rng(5).standard_normal(V.nfree)
+    out = {}
+    for mode in ("coloured", "atomic"):
+        op.problem.set_scatter(mode)
+        out[mode] = (mf.mul(np.zeros(V.nfree), dx), op.residual(np.zeros(V.nfree), x))
+    assert reldiff(out["atomic"][0], out["coloured"][0]) < 1e-14
+    assert reldiff(out["atomic"][1], out["coloured"][1]) < 1e-13
+    assert reldiff(out["coloured"][0], orc.jacobian(x, V.dirichlet_values) @ dx) < TOL64
 
 
 def test_blocks_parity():
@@ -278,3 +295,32 @@ def test_single_cell_and_all_dirichlet_but_one_node():
     A = op.allocate_jacobian(x)
     op.jacobian(A, x)
     assert reldiff(A.data, orc.jacobian_values(x, V.dirichlet_values)) < TOL64
+
+
+def test_newton_pmg_load_stepping_matches_oracle_newton():
+    # the canonical Newton loop (test/solvers/test_pmultigrid.jl:86-115): same trajectory as the oracle
+    from hfk.newton import newton_solve
+
+    m = CartesianMesh((3, 3, 3))
+    gfun = [lambda x: 0 * x, lambda x: np.tile([0.1, 0.0, 0.0], (len(x), 1))]
+    Vs = [VectorLagrangeSpace(m, o, ("x0", "x1"), g=gfun if o == 2 else None) for o in (2, 1)]
+    g_full = Vs[0].dirichlet_values.copy()
+    res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    loads = [0.5, 1.0]
+    for prec in ("fp64", "fp32"):
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-10, preconditioner=S.PMultigrid(Vs, S.Chebyshev(degree=3),
+                                                                                      precision=prec))
+        x, st = newton_solve(op, ls, g_full, loads, rtol_newton=1e-10)
+        assert st.converged and st.newton_iters >= 2
+        # oracle Newton with a direct solve of the assembled tangent
+        orc = O.OracleProblem(Vs[0], Quadrature.gauss(4))
+        xo = np.zeros(Vs[0].nfree)
+        for lam in loads:
+            d = lam * g_full
+            for _ in range(20):
+                r = orc.residual(xo, d)
+                if np.linalg.norm(r) < 1e-13:
+                    break
+                xo = xo - sp.linalg.spsolve(orc.jacobian(xo, d).tocsc(), r)
+        assert reldiff(x.cpu().numpy(), xo) < 1e-8
