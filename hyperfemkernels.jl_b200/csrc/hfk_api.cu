@@ -21,6 +21,7 @@
 #include "hfk_internal.h"
 #include "kern_assembly.cuh"
 #include "kern_cell.cuh"
+#include "kern_mlp.cuh"
 #include "kern_vec.cuh"
 
 using namespace hfk;
@@ -1095,6 +1096,14 @@ void inject_dev(hfk_transfer* t, const double* xf, const double* df, double* xc,
 }
 }  // namespace
 
+// The learned correction's network (FP32 master weights, BF16 copy, Adam moments)
+struct hfk_mlp {
+  DBuf<float> w, m1, m2, grad, loss;
+  DBuf<__nv_bfloat16> wb;
+  int64_t steps = 0;
+  cudaStream_t stream = nullptr;
+};
+
 template <typename R>
 struct LevelWork {
   DBuf<R> b, x, r, e;
@@ -1126,6 +1135,12 @@ struct hfk_pmg {
   cublasHandle_t blas = nullptr;
   DBuf<unsigned char> blas_ws;
   double t_potrf = 0;
+  // learned correction after each cycle (null = plain cycle) and its work buffers
+  hfk_mlp* mlp = nullptr;
+  DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_u, ml_scal;
+  DBuf<float> ml_feats, ml_out;
+  DBuf<int> ml_accepted;
+  int64_t ml_tried = 0;
   // Chebyshev coefficients per level on the device (rewritten at every update)
   std::vector<std::unique_ptr<DBuf<double>>> coef;
   // the V-cycle as a CUDA graph, captured on the second cycle and replayed until a level's law
@@ -1303,6 +1318,80 @@ void pmg_cycle_on_buffers(hfk_pmg* m) {
   m->cycles_since_update++;
 }
 
+// sum of squares of x into *out (device), sync-free
+void sumsq_to(hfk_problem* p, Reducer& red, int64_t n, const double* x, double* out) {
+  red.partial.resize((size_t)3 * RED_BLOCKS);
+  dots_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, p->stream>>>(n, 1, x, x, nullptr, nullptr, nullptr, nullptr,
+                                                                  red.partial.p);
+  check_launch(p);
+  finish_sums_kernel<<<1, 1024, 0, p->stream>>>(RED_BLOCKS, 1, red.partial.p, out);
+  check_launch(p);
+}
+
+__global__ void rms_kernel(int k, double* v, double inv_n) {
+  if (blockIdx.x == 0 && threadIdx.x < k) v[threadIdx.x] = sqrt(v[threadIdx.x] * inv_n);
+}
+
+// Features of the fine level for the residual r and the cycle output y: s = r - A y, scales
+// [rms s, rms Binv s, rms r, rms y], |s|^2 kept in ml_scal[4]. Returns the block count.
+int mlp_prepare_features(hfk_pmg* m, const double* r, const double* y) {
+  hfk_problem* p = m->lv[0];
+  const int64_t n = p->nfree;
+  const int nb = p->nblocks;
+  m->ml_s.resize(n);
+  m->ml_t.resize(n);
+  m->ml_q.resize(n);
+  m->ml_scal.resize(8);
+  m->ml_feats.resize((size_t)nb * MLP_IN);
+  Reducer& red = m->ew[0]->red;
+  mf_apply_dev(p, y, m->ml_q.p);
+  axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0, r, -1.0, m->ml_q.p, m->ml_s.p);
+  check_launch(p);
+  blocks_apply_dev<double>(p, m->ml_s.p, m->ml_t.p);
+  sumsq_to(p, red, n, m->ml_s.p, m->ml_scal.p + 0);
+  sumsq_to(p, red, n, m->ml_t.p, m->ml_scal.p + 1);
+  sumsq_to(p, red, n, r, m->ml_scal.p + 2);
+  sumsq_to(p, red, n, y, m->ml_scal.p + 3);
+  HFK_CUDA(cudaMemcpyAsync(m->ml_scal.p + 4, m->ml_scal.p, sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  rms_kernel<<<1, 32, 0, p->stream>>>(4, m->ml_scal.p, 1.0 / (double)std::max<int64_t>(n, 1));
+  check_launch(p);
+  const float ll = (float)std::log(std::max(p->params[0], 1e-300)), lm = (float)std::log(std::max(p->params[1], 1e-300));
+  mlp_features_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, p->Binv.p, m->ml_s.p, r, y, m->ml_scal.p,
+                                                            ll, lm, m->ml_feats.p);
+  check_launch(p);
+  return nb;
+}
+
+// y += delta = MLP(features) if that reduces the residual |r - A y| (the acceptance rule)
+void mlp_correct(hfk_pmg* m, const double* r, double* y) {
+  hfk_problem* p = m->lv[0];
+  const int64_t n = p->nfree;
+  const int nb = mlp_prepare_features(m, r, y);
+  m->ml_out.resize((size_t)nb * MLP_OUT);
+  m->ml_delta.resize(n);
+  m->ml_u.resize(n);
+  static bool attr = false;
+  if (!attr) {
+    HFK_CUDA(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(MLP_NPARAM * sizeof(float))));
+    attr = true;
+  }
+  mlp_forward_kernel<<<vec_grid(nb, 128), 128, MLP_NPARAM * sizeof(float), p->stream>>>(nb, m->mlp->wb.p, m->ml_feats.p,
+                                                                                       m->ml_out.p);
+  check_launch(p);
+  HFK_CUDA(cudaMemsetAsync(m->ml_delta.p, 0, n * sizeof(double), p->stream));
+  mlp_scatter_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, m->ml_out.p, m->ml_scal.p, m->ml_delta.p);
+  check_launch(p);
+  mf_apply_dev(p, m->ml_delta.p, m->ml_q.p);
+  axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0, m->ml_s.p, -1.0, m->ml_q.p, m->ml_u.p);
+  check_launch(p);
+  sumsq_to(p, m->ew[0]->red, n, m->ml_u.p, m->ml_scal.p + 5);
+  m->ml_accepted.resize(1);
+  mlp_accept_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, m->ml_scal.p + 4, m->ml_delta.p, y, m->ml_accepted.p);
+  check_launch(p);
+  m->ml_tried++;
+}
+
 // ldiv!(y, PMultigridState, r) on device vectors
 void pmg_apply_dev(hfk_pmg* m, const double* r, double* y) {
   hfk_problem* p0 = m->lv[0];
@@ -1331,6 +1420,7 @@ void pmg_apply_dev(hfk_pmg* m, const double* r, double* y) {
     pmg_cycle_on_buffers(m);
     HFK_CUDA(cudaMemcpyAsync(y, w.x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, p0->stream));
   }
+  if (m->mlp) mlp_correct(m, r, y);
   HFK_CUDA(cudaEventRecord(m->ev1, p0->stream));
   m->ev_pending = true;
   m->ncycles++;
@@ -1990,9 +2080,12 @@ int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double
   HFK_API_END
 }
 
-int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
-                 int flexible, int* iters, int* converged, int* indefinite, double* relres) {
-  HFK_API_BEGIN
+}  // extern "C"
+
+namespace {
+// MatrixFreeSolver.solve! (src/solvers.jl:111-159): FP64 (flexible) CG, true-residual stopping test
+void solve_cg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                  int flexible, int* iters, int* converged, int* indefinite, double* relres) {
   HFK_REQUIRE(op && b && x && iters && converged, HFK_ERR_ARG, "null argument");
   HFK_REQUIRE(rtol >= 0 && rtol < 1, HFK_ERR_ARG, "the relative tolerance must be in [0, 1)");
   HFK_REQUIRE(atol >= 0 && maxiter > 0, HFK_ERR_ARG, "atol must be >= 0 and maxiter > 0");
@@ -2011,7 +2104,7 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
     if (is_device_ptr(x)) HFK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
     else std::fill(x, x + n, 0.0);
     HFK_CUDA(cudaStreamSynchronize(s));
-    return HFK_OK;
+    return;
   }
   hfk::CGWork& cw = op->cg;
   DBuf<double>&db = cw.b, &dx = cw.x, &r = cw.r, &z = cw.z, &pp = cw.p, &q = cw.q, &rold = cw.rold;
@@ -2095,6 +2188,14 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
   *iters = it;
   *converged = conv;
   if (indefinite) *indefinite = indef;
+}
+}  // namespace
+
+extern "C" {
+int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                 int flexible, int* iters, int* converged, int* indefinite, double* relres) {
+  HFK_API_BEGIN
+  solve_cg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres);
   HFK_API_END
 }
 
@@ -2192,3 +2293,212 @@ extern "C" int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, 
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   HFK_API_END
 }
+
+// =================================================================================================
+// Learned correction: the network, its training, and its place after the V-cycle
+// =================================================================================================
+namespace {
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+void mlp_upload(hfk_mlp* m, const float* w_host) {
+  m->w.upload(w_host, MLP_NPARAM, m->stream);
+  m->wb.resize(MLP_NPARAM);
+  mlp_to_bf16_kernel<<<vec_grid(MLP_NPARAM), 256, 0, m->stream>>>(MLP_NPARAM, m->w.p, m->wb.p);
+  HFK_CUDA(cudaGetLastError());
+}
+
+void mlp_grad_dev(hfk_mlp* m, const float* feats, const float* targets, int64_t n, float* grad, float* loss) {
+  static bool attr = false;
+  if (!attr) {
+    HFK_CUDA(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_grad_smem_bytes()));
+    attr = true;
+  }
+  HFK_CUDA(cudaMemsetAsync(grad, 0, MLP_NPARAM * sizeof(float), m->stream));
+  HFK_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), m->stream));
+  const int64_t chunks = (n + MLP_CHUNK - 1) / MLP_CHUNK;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count() * 2));
+  mlp_grad_kernel<<<grid, 128, mlp_grad_smem_bytes(), m->stream>>>(n, m->wb.p, feats, targets,
+                                                                   1.0f / (float)std::max<int64_t>(n, 1), grad, loss);
+  HFK_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+extern "C" {
+
+int hfk_mlp_create(hfk_mlp** out, uint64_t seed) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(out, HFK_ERR_ARG, "null output handle");
+  auto m = std::make_unique<hfk_mlp>();
+  HFK_CUDA(cudaStreamCreate(&m->stream));
+  // uniform Glorot initialisation from a seeded generator; biases zero
+  std::vector<float> w(MLP_NPARAM, 0.f);
+  uint64_t s = seed;
+  auto fill = [&](int off, int fan_out, int fan_in) {
+    const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+    for (int i = 0; i < fan_out * fan_in; ++i) {
+      const double u = (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0);
+      w[off + i] = (float)((2 * u - 1) * lim);
+    }
+  };
+  fill(MLP_OW1, MLP_W, MLP_IN);
+  fill(MLP_OW2, MLP_W, MLP_W);
+  fill(MLP_OW3, MLP_OUT, MLP_W);
+  for (int i = 0; i < MLP_NW3; ++i) w[MLP_OW3 + i] *= 0.1f;  // start close to the plain cycle
+  mlp_upload(m.get(), w.data());
+  m->m1.resize(MLP_NPARAM);
+  m->m2.resize(MLP_NPARAM);
+  m->grad.resize(MLP_NPARAM);
+  m->loss.resize(1);
+  m->m1.zero(m->stream);
+  m->m2.zero(m->stream);
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  *out = m.release();
+  HFK_API_END
+}
+
+int hfk_mlp_destroy(hfk_mlp* m) {
+  HFK_API_BEGIN
+  if (m) {
+    cudaStreamSynchronize(m->stream);
+    cudaStreamDestroy(m->stream);
+    delete m;
+  }
+  HFK_API_END
+}
+
+int hfk_mlp_num_params(void) { return MLP_NPARAM; }
+
+int hfk_mlp_get_weights(hfk_mlp* m, float* w) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && w, HFK_ERR_ARG, "null argument");
+  HFK_CUDA(cudaMemcpyAsync(w, m->w.p, MLP_NPARAM * sizeof(float), cudaMemcpyDefault, m->stream));
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  HFK_API_END
+}
+
+int hfk_mlp_set_weights(hfk_mlp* m, const float* w) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && w, HFK_ERR_ARG, "null argument");
+  std::vector<float> h(MLP_NPARAM);
+  HFK_CUDA(cudaMemcpy(h.data(), w, MLP_NPARAM * sizeof(float), cudaMemcpyDefault));
+  mlp_upload(m, h.data());
+  m->m1.zero(m->stream);
+  m->m2.zero(m->stream);
+  m->steps = 0;
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  HFK_API_END
+}
+
+int hfk_mlp_forward(hfk_mlp* m, const float* feats, int64_t n, float* out) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && feats && out && n >= 0, HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(is_device_ptr(feats) && is_device_ptr(out), HFK_ERR_ARG, "features and outputs must be device pointers");
+  HFK_CUDA(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(MLP_NPARAM * sizeof(float))));
+  if (n) mlp_forward_kernel<<<vec_grid(n, 128), 128, MLP_NPARAM * sizeof(float), m->stream>>>(n, m->wb.p, feats, out);
+  HFK_CUDA(cudaGetLastError());
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  HFK_API_END
+}
+
+int hfk_mlp_grad(hfk_mlp* m, const float* feats, const float* targets, int64_t n, float* grad, float* loss) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && feats && targets && grad && loss && n > 0, HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(is_device_ptr(feats) && is_device_ptr(targets), HFK_ERR_ARG, "samples must be device pointers");
+  mlp_grad_dev(m, feats, targets, n, m->grad.p, m->loss.p);
+  HFK_CUDA(cudaMemcpyAsync(grad, m->grad.p, MLP_NPARAM * sizeof(float), cudaMemcpyDefault, m->stream));
+  HFK_CUDA(cudaMemcpyAsync(loss, m->loss.p, sizeof(float), cudaMemcpyDefault, m->stream));
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  HFK_API_END
+}
+
+int hfk_mlp_train(hfk_mlp* m, const float* feats, const float* targets, int64_t n, int steps, int64_t batch, float lr,
+                  float* last_loss) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && feats && targets && n > 0 && steps >= 0 && batch > 0 && lr > 0, HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(is_device_ptr(feats) && is_device_ptr(targets), HFK_ERR_ARG, "samples must be device pointers");
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  int64_t start = 0;
+  for (int it = 0; it < steps; ++it) {
+    const int64_t nb = std::min(batch, n - start);
+    mlp_grad_dev(m, feats + start * MLP_IN, targets + start * MLP_OUT, nb, m->grad.p, m->loss.p);
+    m->steps++;
+    const float c1 = 1.f - std::pow(b1, (float)m->steps), c2 = 1.f - std::pow(b2, (float)m->steps);
+    mlp_adam_kernel<<<vec_grid(MLP_NPARAM), 256, 0, m->stream>>>(MLP_NPARAM, m->w.p, m->wb.p, m->grad.p, m->m1.p,
+                                                                  m->m2.p, lr, b1, b2, eps, c1, c2);
+    HFK_CUDA(cudaGetLastError());
+    start += nb;
+    if (start >= n) start = 0;
+  }
+  if (last_loss) HFK_CUDA(cudaMemcpyAsync(last_loss, m->loss.p, sizeof(float), cudaMemcpyDefault, m->stream));
+  HFK_CUDA(cudaStreamSynchronize(m->stream));
+  HFK_API_END
+}
+
+int hfk_pmg_set_mlp(hfk_pmg* m, hfk_mlp* net) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m, HFK_ERR_ARG, "null handle");
+  m->mlp = net;
+  m->ml_accepted.resize(1);
+  m->ml_accepted.zero(m->lv[0]->stream);
+  m->ml_tried = 0;
+  HFK_CUDA(cudaStreamSynchronize(m->lv[0]->stream));
+  HFK_API_END
+}
+
+int hfk_pmg_mlp_stats(hfk_pmg* m, int64_t* tried, int64_t* accepted) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && tried && accepted, HFK_ERR_ARG, "null argument");
+  int acc = 0;
+  if (m->ml_accepted.p) {
+    HFK_CUDA(cudaMemcpyAsync(&acc, m->ml_accepted.p, sizeof(int), cudaMemcpyDeviceToHost, m->lv[0]->stream));
+    HFK_CUDA(cudaStreamSynchronize(m->lv[0]->stream));
+  }
+  *tried = m->ml_tried;
+  *accepted = acc;
+  HFK_API_END
+}
+
+int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets, int* nsamples, double rtol) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && r && feats && targets && nsamples && rtol > 0 && rtol < 1, HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(m->built && m->ok, HFK_ERR_STATE, "PMultigrid: call hfk_pmg_update first (with a usable hierarchy)");
+  HFK_REQUIRE(is_device_ptr(r) && is_device_ptr(feats) && is_device_ptr(targets), HFK_ERR_ARG,
+              "hfk_pmg_mlp_sample takes device pointers");
+  pmg_bind_stream(m);
+  hfk_problem* p = m->lv[0];
+  const int64_t n = p->nfree;
+  DBuf<double> y, e;
+  y.resize(n);
+  e.resize(n);
+  hfk_mlp* net = m->mlp;
+  m->mlp = nullptr;  // plain cycle
+  try {
+    pmg_apply_dev(m, r, y.p);
+    const int nb = mlp_prepare_features(m, r, y.p);
+    // the remaining error e = A^-1 s, by an accurate solve preconditioned by the plain cycle
+    HFK_CUDA(cudaMemsetAsync(e.p, 0, n * sizeof(double), p->stream));
+    int its = 0, conv = 0, ind = 0;
+    double rel = 0;
+    solve_cg_dev(p, m, m->ml_s.p, e.p, rtol, 0.0, 500, 1, &its, &conv, &ind, &rel);
+    HFK_REQUIRE(conv, HFK_ERR_NUMERIC, "the target solve of a training sample did not converge");
+    mlp_targets_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, e.p, m->ml_scal.p, targets);
+    check_launch(p);
+    HFK_CUDA(cudaMemcpyAsync(feats, m->ml_feats.p, (size_t)nb * MLP_IN * sizeof(float), cudaMemcpyDeviceToDevice,
+                             p->stream));
+    HFK_CUDA(cudaStreamSynchronize(p->stream));
+    *nsamples = nb;
+  } catch (...) {
+    m->mlp = net;
+    throw;
+  }
+  m->mlp = net;
+  HFK_API_END
+}
+
+}  // extern "C"

@@ -71,6 +71,17 @@ SIGNATURES = {
     "hfk_pmg_level_info": [_vp, _i, _pd, _pd, _pd, _pd],
     "hfk_pmg_stats": [_vp, _vp],
     "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
+    "hfk_mlp_create": [ctypes.POINTER(_vp), ctypes.c_uint64],
+    "hfk_mlp_destroy": [_vp],
+    "hfk_mlp_num_params": [],
+    "hfk_mlp_get_weights": [_vp, _vp],
+    "hfk_mlp_set_weights": [_vp, _vp],
+    "hfk_mlp_forward": [_vp, _vp, _i64, _vp],
+    "hfk_mlp_grad": [_vp, _vp, _vp, _i64, _vp, _vp],
+    "hfk_mlp_train": [_vp, _vp, _vp, _i64, _i, _i64, ctypes.c_float, _vp],
+    "hfk_pmg_set_mlp": [_vp, _vp],
+    "hfk_pmg_mlp_stats": [_vp, _pi64, _pi64],
+    "hfk_pmg_mlp_sample": [_vp, _vp, _vp, _vp, _pi, _d],
 }
 
 _LIB = None

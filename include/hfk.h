@@ -191,6 +191,35 @@ int hfk_pmg_stats(hfk_pmg* m, double* out);
 /* Interval and Ritz values of a level's smoother. */
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
 
+/* ---- learned correction (no counterpart in the reference) ------------------------------------
+ * A per-node MLP (16 -> 64 -> 64 -> 3, tanh, BF16 weights read by the forward pass, FP32 master
+ * weights, FP32 accumulation) whose output, scaled, is added to the V-cycle's result after each cycle
+ * only if it reduces the FP64 residual |r - A y| (the plain cycle stays the fallback). Features per
+ * node: residual after the cycle s, its block-Jacobi value, the cycle's input r and output y (each
+ * group scaled by its RMS), log lambda, log mu. Training pairs (features, remaining error A^-1 s)
+ * come from the plain cycle (hfk_pmg_mlp_sample); training is Adam on the GPU (hfk_mlp_train). */
+typedef struct hfk_mlp hfk_mlp;
+int hfk_mlp_create(hfk_mlp** out, uint64_t seed);
+int hfk_mlp_destroy(hfk_mlp* m);
+/* Number of parameters (flat vector: W1 (64x16 row-major), b1, W2 (64x64), b2, W3 (3x64), b3). */
+int hfk_mlp_num_params(void);
+int hfk_mlp_get_weights(hfk_mlp* m, float* w);
+int hfk_mlp_set_weights(hfk_mlp* m, const float* w);
+/* out (n x 3) = MLP(feats (n x 16)), device pointers. */
+int hfk_mlp_forward(hfk_mlp* m, const float* feats, int64_t n, float* out);
+/* Gradient of the mean squared error over n samples (device samples; grad may be host memory). */
+int hfk_mlp_grad(hfk_mlp* m, const float* feats, const float* targets, int64_t n, float* grad, float* loss);
+/* `steps` Adam steps on consecutive minibatches of `batch` samples (wrapping), learning rate lr. */
+int hfk_mlp_train(hfk_mlp* m, const float* feats, const float* targets, int64_t n, int steps, int64_t batch, float lr,
+                  float* last_loss);
+/* Attach (or detach with NULL) the network to a hierarchy's cycle. */
+int hfk_pmg_set_mlp(hfk_pmg* m, hfk_mlp* net);
+/* Corrections tried and accepted since the network was attached. */
+int hfk_pmg_mlp_stats(hfk_pmg* m, int64_t* tried, int64_t* accepted);
+/* One set of training samples for the residual r (device): features (nblocks x 16) and targets
+ * (nblocks x 3, the remaining error after the plain cycle, solved to rtol); nsamples = nblocks. */
+int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets, int* nsamples, double rtol);
+
 /* ---- Krylov (src/solvers.jl) ----------------------------------------------------------------
  * MatrixFreeSolver.solve! (src/solvers.jl:111-159) with an FP64 (flexible) CG on the prepared
  * operator `op` preconditioned by `prec` (NULL = none): stops when ||b - J x|| <= atol + rtol ||b||

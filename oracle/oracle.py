@@ -436,3 +436,59 @@ def pcg(apply_op, b, prec=None, rtol=1e-8, atol=0.0, maxiter=500, x0=None):
         p = zn + beta * p
         r, z, rz = rn, zn, rzn
     return x, it, False, np.linalg.norm(r) / nb
+
+
+# ---------------------------------------------------------------------------------------------
+# MLP of the learned correction (the engine's hfk_mlp_*): numpy forward/backward with the same
+# parameter layout and the BF16 rounding of the weights the GPU forward pass reads.
+
+MLP_IN, MLP_W, MLP_OUT = 16, 64, 3
+
+
+def bf16_round(w):
+    """Round float32 values to bfloat16 (round to nearest even), returned as float32."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    b = w.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32)
+
+
+def mlp_unpack(w):
+    o = 0
+    W1 = w[o:o + MLP_W * MLP_IN].reshape(MLP_W, MLP_IN); o += MLP_W * MLP_IN
+    b1 = w[o:o + MLP_W]; o += MLP_W
+    W2 = w[o:o + MLP_W * MLP_W].reshape(MLP_W, MLP_W); o += MLP_W * MLP_W
+    b2 = w[o:o + MLP_W]; o += MLP_W
+    W3 = w[o:o + MLP_OUT * MLP_W].reshape(MLP_OUT, MLP_W); o += MLP_OUT * MLP_W
+    b3 = w[o:o + MLP_OUT]
+    return W1, b1, W2, b2, W3, b3
+
+
+def mlp_forward(w, X):
+    """Outputs (n x 3) for features X (n x 16), weights rounded to BF16, float64 arithmetic."""
+    W1, b1, W2, b2, W3, b3 = (a.astype(np.float64) for a in mlp_unpack(bf16_round(w)))
+    a1 = np.tanh(X @ W1.T + b1)
+    a2 = np.tanh(a1 @ W2.T + b2)
+    return a2 @ W3.T + b3
+
+
+def mlp_grad(w, X, T):
+    """(gradient of mean_s |out_s - t_s|^2 w.r.t. the flat weights, loss), BF16-rounded forward."""
+    W1, b1, W2, b2, W3, b3 = (a.astype(np.float64) for a in mlp_unpack(bf16_round(w)))
+    n = X.shape[0]
+    a1 = np.tanh(X @ W1.T + b1)
+    a2 = np.tanh(a1 @ W2.T + b2)
+    out = a2 @ W3.T + b3
+    e = out - T
+    loss = float((e * e).sum() / n)
+    d3 = 2 * e / n
+    gW3 = d3.T @ a2
+    gb3 = d3.sum(0)
+    d2 = (d3 @ W3) * (1 - a2 * a2)
+    gW2 = d2.T @ a1
+    gb2 = d2.sum(0)
+    d1 = (d2 @ W2) * (1 - a1 * a1)
+    gW1 = d1.T @ X
+    gb1 = d1.sum(0)
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
+    return g, loss

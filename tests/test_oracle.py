@@ -268,3 +268,25 @@ def test_pmg_solve_matches_direct_and_is_h_independent():
         its.append(it)
     assert all(i <= 30 for i in its)
     assert its[1] <= 1.4 * its[0] + 2
+
+
+def test_oracle_mlp_gradient_matches_finite_differences():
+    # pins the CPU reference of the learned correction's network (its gradient checks the GPU kernels)
+    rng = np.random.default_rng(0)
+    w = O.bf16_round((0.1 * rng.standard_normal(5443)).astype(np.float32)).astype(np.float64)
+    X = rng.standard_normal((40, 16))
+    T = rng.standard_normal((40, 3))
+    g, _ = O.mlp_grad(w.astype(np.float32), X, T)
+
+    def loss(wv):
+        W1, b1, W2, b2, W3, b3 = O.mlp_unpack(wv)
+        a1 = np.tanh(X @ W1.T + b1)
+        a2 = np.tanh(a1 @ W2.T + b2)
+        return (((a2 @ W3.T + b3) - T) ** 2).sum() / len(X)
+
+    for i in (3, 700, 1030, 2500, 5100, 5300, 5442):
+        e = np.zeros_like(w)
+        e[i] = 1e-6
+        fd = (loss(w + e) - loss(w - e)) / 2e-6
+        assert abs(g[i] - fd) <= 1e-6 * max(1.0, abs(fd))
+    assert np.array_equal(O.bf16_round(np.float32([1.0, 1.00390625, -2.5])), np.float32([1.0, 1.0, -2.5]))
