@@ -22,6 +22,7 @@
 #include "kern_assembly.cuh"
 #include "kern_cell.cuh"
 #include "kern_mlp.cuh"
+#include "kern_seg.cuh"
 #include "kern_vec.cuh"
 
 using namespace hfk;
@@ -227,6 +228,7 @@ CellData cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) 
   cd.law = p->law;
   cd.lam = p->params[0];
   cd.mu = p->params[1];
+  cd.cell_lm = p->cell_lm.p;
   for (int c = 0; c < 3; ++c) cd.body[c] = p->params[2 + c];
   return cd;
 }
@@ -406,6 +408,65 @@ void dots(hfk_problem* p, Reducer& red, int64_t n, int k, const R* a0, const R* 
     for (int i = 0; i < k; ++i) res[i] = red.host[i];
 }
 
+// ---- segments (independent problems in one handle) -------------------------------------------
+// The chunks of the segmented reductions, built on first use (one segment: [0, nfree)).
+void ensure_seg_items(hfk_problem* p) {
+  if (p->items_built) return;
+  if (p->seg_off.empty()) p->seg_off = {0, p->nfree};
+  std::vector<int64_t> lo, hi;
+  std::vector<int32_t> first(p->nseg + 1);
+  for (int s = 0; s < p->nseg; ++s) {
+    first[s] = (int32_t)lo.size();
+    for (int64_t a = p->seg_off[s]; a < p->seg_off[s + 1]; a += SEG_CHUNK) {
+      lo.push_back(a);
+      hi.push_back(std::min<int64_t>(a + SEG_CHUNK, p->seg_off[s + 1]));
+    }
+  }
+  first[p->nseg] = (int32_t)lo.size();
+  p->nitems = (int)lo.size();
+  if (lo.empty()) {
+    lo.push_back(0);
+    hi.push_back(0);
+  }
+  p->item_lo.upload(lo.data(), lo.size(), p->stream);
+  p->item_hi.upload(hi.data(), hi.size(), p->stream);
+  p->item_first.upload(first.data(), first.size(), p->stream);
+  p->seg_off_d.upload(p->seg_off.data(), p->seg_off.size(), p->stream);
+  p->seg_partial.resize((size_t)3 * std::max(p->nitems, 1));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  p->items_built = true;
+}
+
+const int32_t* seg_dof_map(const hfk_problem* p) { return p->nseg > 1 ? p->seg_of_dof.p : nullptr; }
+const int32_t* seg_block_map(const hfk_problem* p) { return p->nseg > 1 ? p->seg_of_block.p : nullptr; }
+
+// Per-segment sums of up to three products a_j . b_j into out[s * stride + j] (device), sync-free
+template <typename R>
+void seg_dots(hfk_problem* p, int k, double* out, int stride, const R* a0, const R* b0, const R* a1 = nullptr,
+              const R* b1 = nullptr, const R* a2 = nullptr, const R* b2 = nullptr) {
+  ensure_seg_items(p);
+  if (p->nitems) {
+    seg_dots_kernel<R><<<p->nitems, RED_THREADS, 0, p->stream>>>(k, p->item_lo.p, p->item_hi.p, a0, b0, a1, b1, a2, b2,
+                                                                  p->seg_partial.p);
+    check_launch(p);
+  }
+  seg_finish_kernel<<<p->nseg, RED_THREADS, 0, p->stream>>>(k, p->item_first.p, p->seg_partial.p, out, stride);
+  check_launch(p);
+}
+
+// segment of every nodal block (the segment of its first free dof)
+void build_seg_of_block(hfk_problem* p, const std::vector<int32_t>& dofs) {
+  if (p->nseg <= 1) return;
+  std::vector<int32_t> sb(std::max(p->nblocks, 1), 0);
+  for (int b = 0; b < p->nblocks; ++b) {
+    int32_t d = 0;
+    for (int c = 0; c < 3 && !d; ++c) d = dofs[3 * (size_t)b + c];
+    const int64_t i = (int64_t)d - 1;
+    sb[b] = (int32_t)(std::upper_bound(p->seg_off.begin(), p->seg_off.end(), i) - p->seg_off.begin()) - 1;
+  }
+  p->seg_of_block.upload(sb.data(), sb.size(), p->stream);
+}
+
 // ---- matrix-free products on device vectors ---------------------------------------------------
 void mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
@@ -499,7 +560,7 @@ __global__ void store_tangents_kernel(CellData cd, const double* u, const double
     double H[9], Tq[81];
     for (int c = 0; c < 3; ++c)
       for (int J = 0; J < 3; ++J) H[c + 3 * J] = iJ[J] * G[c][0] + iJ[J + 3] * G[c][1] + iJ[J + 6] * G[c][2];
-    law_tangent(cd.law, cd.lam, cd.mu, H, Tq);
+    law_tangent(cd.law, cd.lam_of(cell), cd.mu_of(cell), H, Tq);
     for (int i = 0; i < 81; ++i) T[((size_t)cell * 81 + i) * np + q] = Tq[i];
     for (int i = 0; i < 9; ++i) iJtq[((size_t)cell * 9 + i) * np + q] = iJ[i];
     dVq[(size_t)cell * np + q] = cd.w[q] * det;
@@ -547,6 +608,7 @@ void build_block_structure(hfk_problem* p) {
   p->nblocks = (int)keys.size();
   p->block_of.upload(block_of.data(), block_of.size(), p->stream);
   p->bdofs.upload(dofs.data(), dofs.size(), p->stream);
+  build_seg_of_block(p, dofs);
   p->B.resize(9 * (size_t)std::max(p->nblocks, 1));
   p->Binv.resize(9 * (size_t)std::max(p->nblocks, 1));
   p->Binv32.resize(9 * (size_t)std::max(p->nblocks, 1));
@@ -649,14 +711,17 @@ void cheb_smooth_dev(hfk_problem* p, ChebWork<R>& w, double a, double b, int deg
 
 // The same smoothing with the coefficients read from device memory (`coef`, see
 // cheb_start_dev_kernel): used by the V-cycle, which is captured once in a CUDA graph.
+// With segments, coef holds one coefficient set per segment (stride 1 + 2 degree).
 template <typename R>
 void cheb_smooth_coef(hfk_problem* p, ChebWork<R>& w, const double* coef, int degree, const R* rhs, R* x,
                       bool zero_guess, R* residual) {
   const int64_t n = p->nfree;
+  const int cstride = 1 + 2 * degree;
+  const int32_t* segb = seg_block_map(p);
   w.ensure(n);
   if (!zero_guess) mf_apply_any<R>(p, x, w.z.p);
   cheb_start_dev_kernel<R><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, binv_of<R>(p), rhs,
-                                                                        w.z.p, w.r.p, w.d.p, x, coef,
+                                                                        w.z.p, w.r.p, w.d.p, x, coef, segb, cstride,
                                                                         zero_guess ? 1 : 0);
   check_launch(p);
   for (int i = 1; i <= degree; ++i) {
@@ -664,7 +729,8 @@ void cheb_smooth_coef(hfk_problem* p, ChebWork<R>& w, const double* coef, int de
     mf_apply_any<R>(p, w.d.p, w.z.p);
     const bool last = i == degree;
     cheb_step_dev_kernel<R><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, binv_of<R>(p), w.z.p,
-                                                                          w.r.p, w.d.p, x, coef, i, last ? 0 : 1);
+                                                                          w.r.p, w.d.p, x, coef, segb, cstride, i,
+                                                                          last ? 0 : 1);
     check_launch(p);
     if (last) break;
   }
@@ -800,35 +866,33 @@ bool hessenberg_eigvals(int n, std::vector<double> H /* column-major n x n */, d
 
 struct EigWork {
   DBuf<double> V, t, w, Hd;
-  Reducer red;
 };
 
-// eigenvalue_bounds (src/preconditioners.jl:374-389): k Arnoldi steps (modified Gram-Schmidt) on
-// J P^-1 from b, breakdown truncation, Ritz values of the Hessenberg matrix
-void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev, double* lmin, double* lmax) {
+// eigenvalue_bounds (src/preconditioners.jl:374-389) of every segment at once: k Arnoldi steps
+// (modified Gram-Schmidt) on J P^-1 from the start vector with per-segment inner products, so that
+// each segment builds its own Hessenberg matrix (a block-diagonal operator keeps the segments'
+// Krylov spaces apart); breakdown truncation and Ritz values per segment on the host. One copy
+// of the Hessenberg matrices to the host, no other synchronisation.
+void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev, std::vector<double>& lmin,
+                    std::vector<double>& lmax) {
   const int64_t n = p->nfree;
-  k = (int)std::min<int64_t>(k, n);
+  const int ns = p->nseg;
+  k = (int)std::max<int64_t>(1, std::min<int64_t>(k, n));
+  const int ld = k + 1;
+  const int hs = ld * (k + 1);  // per segment: H (ld x k) and one scratch column
   ew.V.resize((size_t)(k + 1) * n);
   ew.t.resize(n);
   ew.w.resize(n);
-  ew.Hd.resize((size_t)(k + 2) * (k + 1));
+  ew.Hd.resize((size_t)hs * ns);
   ew.Hd.zero(p->stream);
-  ew.red.partial.resize((size_t)3 * RED_BLOCKS);
-  std::vector<double> H((size_t)(k + 1) * k, 0.0);
-  const int ld = k + 1;
   double* Hd = ew.Hd.p;
-  double* nrm = Hd + (size_t)ld * k;  // scratch scalar past the Hessenberg matrix
-  auto dot_to = [&](const double* x, const double* y, double* out) {
-    dots_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, p->stream>>>(n, 1, x, y, nullptr, nullptr, nullptr, nullptr,
-                                                                    ew.red.partial.p);
-    check_launch(p);
-    finish_sums_kernel<<<1, 1024, 0, p->stream>>>(RED_BLOCKS, 1, ew.red.partial.p, out);
-    check_launch(p);
-  };
-  dot_to(start_dev, start_dev, nrm);
-  sqrt_dev_kernel<<<1, 1, 0, p->stream>>>(nrm);
+  const int32_t* seg = seg_dof_map(p);
+  const int sg = std::max(1, (ns + 255) / 256);
+  double* nrm = Hd + (size_t)ld * k;  // scratch scalar past each Hessenberg matrix
+  seg_dots<double>(p, 1, nrm, hs, start_dev, start_dev);
+  seg_sqrt_kernel<<<sg, 256, 0, p->stream>>>(ns, nrm, hs);
   check_launch(p);
-  scale_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, nrm, start_dev, ew.V.p);
+  seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, nrm, hs, start_dev, ew.V.p);
   check_launch(p);
   for (int j = 0; j < k; ++j) {
     double* vj = ew.V.p + (size_t)j * n;
@@ -836,52 +900,61 @@ void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev,
     mf_apply_dev(p, ew.t.p, ew.w.p);
     for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, coefficients written into H on the device
       double* hij = Hd + i + (size_t)ld * j;
-      dot_to(ew.V.p + (size_t)i * n, ew.w.p, hij);
-      axpy_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, hij, -1.0, ew.V.p + (size_t)i * n, ew.w.p);
+      seg_dots<double>(p, 1, hij, hs, ew.V.p + (size_t)i * n, ew.w.p);
+      seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, ew.V.p + (size_t)i * n, ew.w.p);
       check_launch(p);
     }
     double* hn = Hd + (j + 1) + (size_t)ld * j;
-    dot_to(ew.w.p, ew.w.p, hn);
-    sqrt_dev_kernel<<<1, 1, 0, p->stream>>>(hn);
+    seg_dots<double>(p, 1, hn, hs, ew.w.p, ew.w.p);
+    seg_sqrt_kernel<<<sg, 256, 0, p->stream>>>(ns, hn, hs);
     check_launch(p);
-    scale_dev_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, hn, ew.w.p, ew.V.p + (size_t)(j + 1) * n);
+    seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hn, hs, ew.w.p, ew.V.p + (size_t)(j + 1) * n);
     check_launch(p);
   }
-  HFK_CUDA(cudaMemcpyAsync(H.data(), Hd, sizeof(double) * (size_t)ld * k, cudaMemcpyDeviceToHost, p->stream));
+  std::vector<double> Hall((size_t)hs * ns);
+  HFK_CUDA(cudaMemcpyAsync(Hall.data(), Hd, sizeof(double) * Hall.size(), cudaMemcpyDeviceToHost, p->stream));
   HFK_CUDA(cudaStreamSynchronize(p->stream));
-  // breakdown truncation (src/preconditioners.jl:379-385)
-  int jj = k;
-  for (int i = 1; i < k; ++i) {
-    double m = 0;
-    for (int a = 0; a < i; ++a)
-      for (int b = 0; b < i; ++b) m = std::max(m, std::fabs(H[a + (size_t)(k + 1) * b]));
-    if (std::fabs(H[i + (size_t)(k + 1) * (i - 1)]) <= 1e-8 * std::max(1.0, m)) {
-      jj = i;
-      break;
+  lmin.assign(ns, NAN);
+  lmax.assign(ns, NAN);
+  for (int s = 0; s < ns; ++s) {
+    const double* H = Hall.data() + (size_t)hs * s;
+    // breakdown truncation (src/preconditioners.jl:379-385)
+    int jj = k;
+    for (int i = 1; i < k; ++i) {
+      double m = 0;
+      for (int a = 0; a < i; ++a)
+        for (int b = 0; b < i; ++b) m = std::max(m, std::fabs(H[a + (size_t)ld * b]));
+      if (std::fabs(H[i + (size_t)ld * (i - 1)]) <= 1e-8 * std::max(1.0, m)) {
+        jj = i;
+        break;
+      }
     }
+    std::vector<double> Hs((size_t)jj * jj);
+    for (int a = 0; a < jj; ++a)
+      for (int b = 0; b < jj; ++b) Hs[a + (size_t)jj * b] = H[a + (size_t)ld * b];
+    std::vector<double> re(jj), im(jj);
+    if (!hessenberg_eigvals(jj, Hs, re.data(), im.data())) continue;
+    lmin[s] = *std::min_element(re.begin(), re.end());
+    lmax[s] = *std::max_element(re.begin(), re.end());
   }
-  std::vector<double> Hs((size_t)jj * jj);
-  for (int a = 0; a < jj; ++a)
-    for (int b = 0; b < jj; ++b) Hs[a + (size_t)jj * b] = H[a + (size_t)(k + 1) * b];
-  std::vector<double> re(jj), im(jj);
-  if (!hessenberg_eigvals(jj, Hs, re.data(), im.data())) {
-    *lmin = *lmax = NAN;
-    return;
-  }
-  *lmin = *std::min_element(re.begin(), re.end());
-  *lmax = *std::max_element(re.begin(), re.end());
 }
 
-void chebyshev_start_vector(int64_t n, std::vector<double>& v) {
-  v.resize(n);
-  double s = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    const double ii = (double)(i + 1);
-    v[i] = std::sin(1.0 + 0.7 * ii) + 0.3 * std::cos(2.3 * ii);
-    s += v[i] * v[i];
+// The fixed start vector of the eigenvalue estimate (src/smoothers.jl:68-71); with segments, each
+// segment gets the vector of its own size (so that it sees the start of a problem solved alone).
+void chebyshev_start_vector(const hfk_problem* p, std::vector<double>& v) {
+  v.resize(p->nfree);
+  const int ns = p->seg_off.empty() ? 1 : p->nseg;
+  for (int sg = 0; sg < ns; ++sg) {
+    const int64_t a = p->seg_off.empty() ? 0 : p->seg_off[sg], e = p->seg_off.empty() ? p->nfree : p->seg_off[sg + 1];
+    double s = 0;
+    for (int64_t i = a; i < e; ++i) {
+      const double ii = (double)(i - a + 1);
+      v[i] = std::sin(1.0 + 0.7 * ii) + 0.3 * std::cos(2.3 * ii);
+      s += v[i] * v[i];
+    }
+    s = std::sqrt(s);
+    for (int64_t i = a; i < e; ++i) v[i] /= s;
   }
-  s = std::sqrt(s);
-  for (auto& x : v) x /= s;
 }
 
 // ---- GPU sparsity pattern (sparsity, src/assembly.jl:773-818; cell_positions!, :864-880) -----------
@@ -1123,10 +1196,14 @@ struct hfk_pmg {
   int since = 0, nupdate = 0, nbuild = 0;
   std::vector<std::unique_ptr<LevelWork<double>>> w64;
   std::vector<std::unique_ptr<LevelWork<float>>> w32;
-  // coarse: dense Cholesky factor (lower) of the assembled coarse tangent
+  // coarse: dense Cholesky factor (lower) of the assembled coarse tangent, or (HFK_COARSE_CG) a
+  // fixed number of block-Jacobi CG steps per segment on the matrix-free coarse level
+  int coarse_mode = HFK_COARSE_CHOLESKY, coarse_iters = 20;
   DBuf<double> Lc, cb, cx;
+  DBuf<double> ccg_r, ccg_z, ccg_p, ccg_q, ccg_sc;
   bool coarse_ok = false;
   std::vector<std::unique_ptr<EigWork>> ew;          // per level (no reallocation between levels)
+  std::vector<std::vector<double>> seg_lmin, seg_lmax;  // per level, per segment
   std::vector<std::unique_ptr<DBuf<double>>> start;  // per level: the fixed Arnoldi start vector
   DBuf<double> potrf_work;
   DBuf<int> potrf_info;
@@ -1137,8 +1214,8 @@ struct hfk_pmg {
   double t_potrf = 0;
   // learned correction after each cycle (null = plain cycle) and its work buffers
   hfk_mlp* mlp = nullptr;
-  DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_u, ml_scal;
-  DBuf<float> ml_feats, ml_out;
+  DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_u, ml_scal;  // ml_scal: 8 per segment
+  DBuf<float> ml_feats, ml_out, ml_loglm;                    // ml_loglm: log lambda, log mu per segment
   DBuf<int> ml_accepted;
   int64_t ml_tried = 0;
   // Chebyshev coefficients per level on the device (rewritten at every update)
@@ -1207,6 +1284,23 @@ void coarse_factor(hfk_pmg* m) {
   if (m->coarse_ok) m->nbuild++;
 }
 
+// the inexact coarse solve's set-up: the coarse level's blocks and work vectors
+void coarse_cg_update(hfk_pmg* m) {
+  hfk_problem* c = m->lv[m->L - 1];
+  const int64_t n = c->nfree;
+  int bok = 0;
+  blocks_update_dev(c, &bok);
+  ensure_seg_items(c);
+  m->ccg_r.resize(n);
+  m->ccg_z.resize(n);
+  m->ccg_p.resize(n);
+  m->ccg_q.resize(n);
+  m->ccg_sc.resize((size_t)SEG_NS * c->nseg);
+  m->ccg_sc.zero(c->stream);
+  m->coarse_ok = bok != 0;
+  if (m->coarse_ok) m->nbuild++;
+}
+
 // x = A^-1 b with the Cholesky factor: L y = b, L^T x = y (cuBLAS triangular solves, FP64)
 void coarse_solve(hfk_pmg* m, const double* b, double* x) {
   hfk_problem* c = m->lv[m->L - 1];
@@ -1226,6 +1320,41 @@ void coarse_solve(hfk_pmg* m, const double* b, double* x) {
       cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
                   m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS)
     throw Error{HFK_ERR_CUDA, "HyperFEMKernels: triangular solve of the coarse level failed"};
+}
+
+// x ~= A^-1 b on the coarse level by coarse_iters steps of block-Jacobi preconditioned CG per
+// segment from x = 0, with every scalar on the device (capturable in the cycle's graph). The
+// approximation varies with b, which the flexible outer CG tolerates. Used where a dense factor of
+// the coarse level does not fit (many problems, or more coarse dofs than the dense solve takes).
+void coarse_cg(hfk_pmg* m, const double* b, double* x) {
+  hfk_problem* c = m->lv[m->L - 1];
+  const int64_t n = c->nfree;
+  const int ns = c->nseg;
+  const int32_t* seg = seg_dof_map(c);
+  const int sg = std::max(1, (ns + 255) / 256);
+  double* sc = m->ccg_sc.p;
+  double *r = m->ccg_r.p, *z = m->ccg_z.p, *pp = m->ccg_p.p, *q = m->ccg_q.p;
+  cudaStream_t st = c->stream;
+  HFK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
+  HFK_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  blocks_apply_dev<double>(c, r, z);
+  HFK_CUDA(cudaMemcpyAsync(pp, z, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  seg_dots<double>(c, 1, sc + S_RZ, SEG_NS, r, z);
+  for (int it = 0; it < m->coarse_iters; ++it) {
+    mf_apply_dev(c, pp, q);
+    seg_dots<double>(c, 1, sc + S_PQ, SEG_NS, pp, q);
+    seg_ratio_kernel<<<sg, 256, 0, st>>>(ns, sc, S_RZ, S_PQ, S_ALPHA, 0);
+    check_launch(c);
+    seg_cg_update_kernel<<<vec_grid(n), 256, 0, st>>>(n, seg, sc, pp, q, x, r, nullptr);
+    check_launch(c);
+    if (it + 1 == m->coarse_iters) break;
+    blocks_apply_dev<double>(c, r, z);
+    seg_dots<double>(c, 1, sc + S_ZR, SEG_NS, z, r);
+    seg_ratio_kernel<<<sg, 256, 0, st>>>(ns, sc, S_ZR, S_RZ, S_BETA, 1);
+    check_launch(c);
+    seg_xpby_kernel<<<vec_grid(n), 256, 0, st>>>(n, seg, sc, S_BETA, z, pp);
+    check_launch(c);
+  }
 }
 
 template <typename R>
@@ -1258,7 +1387,8 @@ void vcycle_dev(hfk_pmg* m, int l) {
       check_launch(p);
       bc = m->cb.p;
     }
-    coarse_solve(m, bc, m->cx.p);
+    if (m->coarse_mode == HFK_COARSE_CG) coarse_cg(m, bc, m->cx.p);
+    else coarse_solve(m, bc, m->cx.p);
     convert_kernel<double, R><<<vec_grid(c->nfree), 256, 0, p->stream>>>(c->nfree, m->cx.p, wc.x.p);
     check_launch(p);
   } else {
@@ -1318,51 +1448,36 @@ void pmg_cycle_on_buffers(hfk_pmg* m) {
   m->cycles_since_update++;
 }
 
-// sum of squares of x into *out (device), sync-free
-void sumsq_to(hfk_problem* p, Reducer& red, int64_t n, const double* x, double* out) {
-  red.partial.resize((size_t)3 * RED_BLOCKS);
-  dots_kernel<double><<<RED_BLOCKS, RED_THREADS, 0, p->stream>>>(n, 1, x, x, nullptr, nullptr, nullptr, nullptr,
-                                                                  red.partial.p);
-  check_launch(p);
-  finish_sums_kernel<<<1, 1024, 0, p->stream>>>(RED_BLOCKS, 1, red.partial.p, out);
-  check_launch(p);
-}
-
-__global__ void rms_kernel(int k, double* v, double inv_n) {
-  if (blockIdx.x == 0 && threadIdx.x < k) v[threadIdx.x] = sqrt(v[threadIdx.x] * inv_n);
-}
-
-// Features of the fine level for the residual r and the cycle output y: s = r - A y, scales
-// [rms s, rms Binv s, rms r, rms y], |s|^2 kept in ml_scal[4]. Returns the block count.
+// Features of the fine level for the residual r and the cycle output y: s = r - A y and, per
+// segment at ml_scal + 8 seg, the scales [rms s, rms Binv s, rms r, rms y] and |s|^2 (slot 4).
+// Returns the block count.
 int mlp_prepare_features(hfk_pmg* m, const double* r, const double* y) {
   hfk_problem* p = m->lv[0];
   const int64_t n = p->nfree;
   const int nb = p->nblocks;
+  const int ns = p->nseg;
   m->ml_s.resize(n);
   m->ml_t.resize(n);
   m->ml_q.resize(n);
-  m->ml_scal.resize(8);
+  m->ml_scal.resize((size_t)8 * ns);
   m->ml_feats.resize((size_t)nb * MLP_IN);
-  Reducer& red = m->ew[0]->red;
   mf_apply_dev(p, y, m->ml_q.p);
   axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0, r, -1.0, m->ml_q.p, m->ml_s.p);
   check_launch(p);
   blocks_apply_dev<double>(p, m->ml_s.p, m->ml_t.p);
-  sumsq_to(p, red, n, m->ml_s.p, m->ml_scal.p + 0);
-  sumsq_to(p, red, n, m->ml_t.p, m->ml_scal.p + 1);
-  sumsq_to(p, red, n, r, m->ml_scal.p + 2);
-  sumsq_to(p, red, n, y, m->ml_scal.p + 3);
-  HFK_CUDA(cudaMemcpyAsync(m->ml_scal.p + 4, m->ml_scal.p, sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
-  rms_kernel<<<1, 32, 0, p->stream>>>(4, m->ml_scal.p, 1.0 / (double)std::max<int64_t>(n, 1));
+  seg_dots<double>(p, 3, m->ml_scal.p, 8, m->ml_s.p, m->ml_s.p, m->ml_t.p, m->ml_t.p, r, r);
+  seg_dots<double>(p, 2, m->ml_scal.p + 3, 8, y, y, m->ml_s.p, m->ml_s.p);
+  ensure_seg_items(p);
+  seg_rms_kernel<<<std::max(1, (ns + 255) / 256), 256, 0, p->stream>>>(ns, m->ml_scal.p, 8, 4, p->seg_off_d.p);
   check_launch(p);
-  const float ll = (float)std::log(std::max(p->params[0], 1e-300)), lm = (float)std::log(std::max(p->params[1], 1e-300));
-  mlp_features_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, p->Binv.p, m->ml_s.p, r, y, m->ml_scal.p,
-                                                            ll, lm, m->ml_feats.p);
+  mlp_features_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, seg_block_map(p), p->Binv.p, m->ml_s.p, r,
+                                                            y, m->ml_scal.p, 8, m->ml_loglm.p, m->ml_feats.p);
   check_launch(p);
   return nb;
 }
 
-// y += delta = MLP(features) if that reduces the residual |r - A y| (the acceptance rule)
+// y += delta = MLP(features) in every segment where that reduces the residual |r - A y| (the
+// acceptance rule, applied per segment)
 void mlp_correct(hfk_pmg* m, const double* r, double* y) {
   hfk_problem* p = m->lv[0];
   const int64_t n = p->nfree;
@@ -1380,16 +1495,19 @@ void mlp_correct(hfk_pmg* m, const double* r, double* y) {
                                                                                        m->ml_out.p);
   check_launch(p);
   HFK_CUDA(cudaMemsetAsync(m->ml_delta.p, 0, n * sizeof(double), p->stream));
-  mlp_scatter_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, m->ml_out.p, m->ml_scal.p, m->ml_delta.p);
+  mlp_scatter_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, seg_block_map(p), m->ml_out.p, m->ml_scal.p,
+                                                           8, m->ml_delta.p);
   check_launch(p);
   mf_apply_dev(p, m->ml_delta.p, m->ml_q.p);
   axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0, m->ml_s.p, -1.0, m->ml_q.p, m->ml_u.p);
   check_launch(p);
-  sumsq_to(p, m->ew[0]->red, n, m->ml_u.p, m->ml_scal.p + 5);
+  seg_dots<double>(p, 1, m->ml_scal.p + 5, 8, m->ml_u.p, m->ml_u.p);
   m->ml_accepted.resize(1);
-  mlp_accept_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, m->ml_scal.p + 4, m->ml_delta.p, y, m->ml_accepted.p);
+  mlp_accept_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg_dof_map(p), m->ml_scal.p + 4, 8, m->ml_delta.p, y);
   check_launch(p);
-  m->ml_tried++;
+  mlp_accept_count_kernel<<<1, 256, 0, p->stream>>>(p->nseg, m->ml_scal.p + 4, 8, m->ml_accepted.p);
+  check_launch(p);
+  m->ml_tried += p->nseg;
 }
 
 // ldiv!(y, PMultigridState, r) on device vectors
@@ -1737,12 +1855,18 @@ int hfk_eigenvalue_bounds(hfk_problem* p, int k, const double* start, double* lm
   HFK_REQUIRE(p->nblocks > 0 || p->blocks_ok, HFK_ERR_STATE, "blocks not built (call hfk_blocks_update)");
   std::vector<double> v;
   if (!start) {
-    chebyshev_start_vector(p->nfree, v);
+    chebyshev_start_vector(p, v);
     start = v.data();
   }
   const double* d = dev_in(start, p->nfree, p->stage_in2, p->stream);
   EigWork ew;
-  eig_bounds_dev(p, ew, k, d, lmin, lmax);
+  std::vector<double> lo, hi;
+  eig_bounds_dev(p, ew, k, d, lo, hi);
+  // a problem with several segments reports the extreme bounds over its segments
+  *lmin = *std::min_element(lo.begin(), lo.end());
+  *lmax = *std::max_element(hi.begin(), hi.end());
+  for (size_t s = 0; s < lo.size(); ++s)
+    if (!std::isfinite(lo[s]) || !std::isfinite(hi[s])) *lmin = *lmax = NAN;
   HFK_API_END
 }
 
@@ -1881,6 +2005,9 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
     HFK_REQUIRE(levels[l], HFK_ERR_ARG, "null level");
     m->lv.push_back(levels[l]);
   }
+  for (int l = 1; l < nlevels; ++l)
+    HFK_REQUIRE(levels[l]->nseg == levels[0]->nseg && levels[l]->seg_cells == levels[0]->seg_cells, HFK_ERR_ARG,
+                "the levels hold different segments (set the same segments on every level before the hierarchy)");
   for (int l = 0; l < nlevels - 1; ++l) {
     HFK_REQUIRE(transfers[l] && transfers[l]->fine == levels[l] && transfers[l]->coarse == levels[l + 1], HFK_ERR_ARG,
                 "transfers[l] must go from level l+1 to level l");
@@ -1901,6 +2028,8 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
   m->a.assign(nlevels, 0);
   m->b.assign(nlevels, 0);
   m->lmin.assign(nlevels, 0);
+  m->seg_lmin.assign(nlevels, {});
+  m->seg_lmax.assign(nlevels, {});
   m->lmax.assign(nlevels, 0);
   m->lok.assign(nlevels, 0);
   for (int l = 0; l < nlevels; ++l) {
@@ -1923,15 +2052,13 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
   }
   for (int l = 0; l < nlevels; ++l) {
     m->coef.push_back(std::make_unique<DBuf<double>>());
-    m->coef.back()->resize(1 + 2 * (size_t)degree);
+    m->coef.back()->resize((1 + 2 * (size_t)degree) * levels[l]->nseg);
     m->ew.push_back(std::make_unique<EigWork>());
     m->start.push_back(std::make_unique<DBuf<double>>());
   }
   const int64_t nc = levels[nlevels - 1]->nfree;
   m->cb.resize(nc);
   m->cx.resize(nc);
-  std::vector<double> v;
-  chebyshev_start_vector(levels[0]->nfree, v);
   *out = m.release();
   HFK_API_END
 }
@@ -1982,7 +2109,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     c->x.resize(c->nfree);
     c->dvals.resize(std::max<int64_t>(c->ndir, 1));
     inject_dev(m->tr[l], f->x.p, f->dvals.p, c->x.p, c->dvals.p);
-    if (l + 1 < m->L - 1) {
+    if (l + 1 < m->L - 1 || m->coarse_mode == HFK_COARSE_CG) {
       prepare_F(c);
     } else {
       c->prepared = true;  // the coarse level is assembled
@@ -2004,29 +2131,56 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     }
     if (m->start[l]->n != (size_t)p->nfree) {
       std::vector<double> v;
-      chebyshev_start_vector(p->nfree, v);
+      chebyshev_start_vector(p, v);
       m->start[l]->upload(v.data(), v.size(), p->stream);
     }
-    double lmin = 0, lmax = 0;
     auto te = std::chrono::steady_clock::now();
-    eig_bounds_dev(p, *m->ew[l], m->eig_iters, m->start[l]->p, &lmin, &lmax);
+    std::vector<double>&lo = m->seg_lmin[l], &hi = m->seg_lmax[l];
+    eig_bounds_dev(p, *m->ew[l], m->eig_iters, m->start[l]->p, lo, hi);
     m->t_eig += ms_since(te);
-    m->lmin[l] = lmin;
-    m->lmax[l] = lmax;
-    const bool lok = std::isfinite(lmax) && lmax > 0 && lmin > 0;
+    // per segment: interval [b / range, b] with b = inflate * lmax (smoother_update!,
+    // src/smoothers.jl:86-107) and its coefficients at coef + s * (1 + 2 degree)
+    const int ns = p->nseg;
+    std::vector<double> coefs;
+    coefs.reserve((size_t)ns * (1 + 2 * m->degree));
+    bool lok = true;
+    m->lmin[l] = INFINITY;
+    m->lmax[l] = -INFINITY;
+    for (int sgi = 0; sgi < ns; ++sgi) {
+      const bool ok_s = std::isfinite(hi[sgi]) && hi[sgi] > 0 && lo[sgi] > 0;
+      lok &= ok_s;
+      const double bs = ok_s ? m->inflate * hi[sgi] : 1.0;
+      const std::vector<double> c = chebyshev_coefficients(bs / m->range, bs, m->degree);
+      coefs.insert(coefs.end(), c.begin(), c.end());
+      m->lmin[l] = std::min(m->lmin[l], lo[sgi]);
+      m->lmax[l] = std::max(m->lmax[l], hi[sgi]);
+    }
+    if (!lok) m->lmin[l] = m->lmax[l] = NAN;
     m->lok[l] = lok;
     all_ok &= lok;
-    m->b[l] = m->inflate * lmax;
+    m->b[l] = m->inflate * m->lmax[l];
     m->a[l] = m->b[l] / m->range;
-    const std::vector<double> c = chebyshev_coefficients(m->a[l], m->b[l], m->degree);
-    m->coef[l]->upload(c.data(), c.size(), p->stream);
+    if (m->coef[l]->n != coefs.size()) pmg_drop_graph(m);  // the captured cycle holds the buffer's address
+    m->coef[l]->upload(coefs.data(), coefs.size(), p->stream);
     if (f32) ensure_F32(p);
+  }
+  {
+    // the network's material features: log lambda, log mu per segment of the working level
+    std::vector<float> lg((size_t)2 * p0->nseg);
+    for (int sgi = 0; sgi < p0->nseg; ++sgi) {
+      const double la = p0->seg_lm.empty() ? p0->params[0] : p0->seg_lm[2 * (size_t)sgi];
+      const double mu = p0->seg_lm.empty() ? p0->params[1] : p0->seg_lm[2 * (size_t)sgi + 1];
+      lg[2 * sgi] = (float)std::log(std::max(la, 1e-300));
+      lg[2 * sgi + 1] = (float)std::log(std::max(mu, 1e-300));
+    }
+    m->ml_loglm.upload(lg.data(), lg.size(), p0->stream);
   }
   // coarse level (every coarse_every updates)
   m->since++;
   if (!m->built || m->since >= m->coarse_every) {
     auto tc = std::chrono::steady_clock::now();
-    coarse_factor(m);
+    if (m->coarse_mode == HFK_COARSE_CG) coarse_cg_update(m);
+    else coarse_factor(m);
     HFK_CUDA(cudaStreamSynchronize(p0->stream));
     m->t_coarse += ms_since(tc);
     m->since = 0;
@@ -2189,6 +2343,126 @@ void solve_cg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, do
   *converged = conv;
   if (indefinite) *indefinite = indef;
 }
+// MatrixFreeSolver.solve! (src/solvers.jl:111-159) on every segment of op at once: one FP64
+// (flexible) CG per segment with its own alpha, beta, tolerance atol + rtol ||b_s|| and stopping
+// test; every product and preconditioner application covers all segments in one launch sequence.
+// The scalars stay on the device; one flag count is read per iteration. A segment stops when it
+// converges or meets non-positive curvature (indefinite); its iterate is then left unchanged.
+void solve_cg_seg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                      int flexible, int* iters, int* converged, int* indefinite, double* relres, int* sweeps) {
+  HFK_REQUIRE(op && b && x && iters && converged, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(rtol >= 0 && rtol < 1, HFK_ERR_ARG, "the relative tolerance must be in [0, 1)");
+  HFK_REQUIRE(atol >= 0 && maxiter > 0, HFK_ERR_ARG, "atol must be >= 0 and maxiter > 0");
+  HFK_REQUIRE(op->prepared, HFK_ERR_STATE, "the operator has not been prepared");
+  const int64_t n = op->nfree;
+  const int ns = op->nseg;
+  if (prec) {
+    HFK_REQUIRE(prec->lv[0] == op, HFK_ERR_ARG, "the preconditioner's working level is not this operator");
+    pmg_bind_stream(prec);
+  }
+  cudaStream_t s = op->stream;
+  for (int i = 0; i < ns; ++i) {
+    iters[i] = 0;
+    converged[i] = 0;
+    if (indefinite) indefinite[i] = 0;
+    if (relres) relres[i] = NAN;
+  }
+  if (sweeps) *sweeps = 0;
+  if (prec && !prec->ok) {  // src/solvers.jl:114-121: no iteration, a failed solve
+    if (is_device_ptr(x)) HFK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    else std::fill(x, x + n, 0.0);
+    HFK_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
+  ensure_seg_items(op);
+  hfk::CGWork& cw = op->cg;
+  DBuf<double>&db = cw.b, &dx = cw.x, &r = cw.r, &z = cw.z, &pp = cw.p, &q = cw.q, &rold = cw.rold;
+  const double* bd = dev_in(b, n, db, s);
+  double* xd = x;
+  if (!is_device_ptr(x)) {
+    dx.resize(n);
+    HFK_CUDA(cudaMemcpyAsync(dx.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    xd = dx.p;
+  }
+  r.resize(n);
+  z.resize(n);
+  pp.resize(n);
+  q.resize(n);
+  if (flexible) rold.resize(n);
+  cw.sc.resize((size_t)SEG_NS * ns);
+  cw.fl.resize((size_t)SEG_NF * ns);
+  cw.cnt.resize(1);
+  double* sc = cw.sc.p;
+  int* fl = cw.fl.p;
+  const int32_t* seg = seg_dof_map(op);
+  const int sg = std::max(1, (ns + 255) / 256);
+  auto active_count = [&]() {
+    int c = 0;
+    HFK_CUDA(cudaMemcpyAsync(&c, cw.cnt.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HFK_CUDA(cudaStreamSynchronize(s));
+    return c;
+  };
+  // r = b - A x
+  mf_apply_dev(op, xd, q.p);
+  axpbyz_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, bd, -1.0, q.p, r.p);
+  check_launch(op);
+  seg_dots<double>(op, 2, sc + S_BB, SEG_NS, bd, bd, r.p, r.p);
+  seg_cg_init_kernel<<<1, 256, 0, s>>>(ns, sc, fl, rtol, atol, cw.cnt.p);
+  check_launch(op);
+  int nact = active_count();
+  int it = 0;
+  auto apply_prec = [&](const double* in, double* outp) {
+    if (prec) pmg_apply_dev(prec, in, outp);
+    else HFK_CUDA(cudaMemcpyAsync(outp, in, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  };
+  if (nact > 0) {
+    apply_prec(r.p, z.p);
+    HFK_CUDA(cudaMemcpyAsync(pp.p, z.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    seg_dots<double>(op, 1, sc + S_RZ, SEG_NS, r.p, z.p);
+    while (it < maxiter) {
+      ++it;
+      mf_apply_dev(op, pp.p, q.p);
+      seg_dots<double>(op, 1, sc + S_PQ, SEG_NS, pp.p, q.p);
+      seg_cg_alpha_kernel<<<sg, 256, 0, s>>>(ns, sc, fl);
+      check_launch(op);
+      seg_cg_update_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, pp.p, q.p, xd, r.p, flexible ? rold.p : nullptr);
+      check_launch(op);
+      seg_dots<double>(op, 1, sc + S_RR, SEG_NS, r.p, r.p);
+      seg_cg_check_kernel<<<1, 256, 0, s>>>(ns, sc, fl, cw.cnt.p);
+      check_launch(op);
+      if (active_count() == 0) break;
+      apply_prec(r.p, z.p);
+      if (flexible) seg_dots<double>(op, 2, sc + S_ZR, SEG_NS, z.p, r.p, z.p, rold.p);
+      else seg_dots<double>(op, 1, sc + S_ZR, SEG_NS, z.p, r.p);
+      seg_cg_beta_kernel<<<sg, 256, 0, s>>>(ns, sc, fl, flexible);
+      check_launch(op);
+      seg_xpby_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, S_BETA, z.p, pp.p);
+      check_launch(op);
+    }
+  }
+  // true residual check per segment (src/solvers.jl:150-157)
+  mf_apply_dev(op, xd, q.p);
+  axpbyz_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, bd, -1.0, q.p, r.p);
+  check_launch(op);
+  seg_dots<double>(op, 1, sc + S_RR, SEG_NS, r.p, r.p);
+  std::vector<double> hs((size_t)SEG_NS * ns);
+  std::vector<int> hf((size_t)SEG_NF * ns);
+  HFK_CUDA(cudaMemcpyAsync(hs.data(), sc, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  HFK_CUDA(cudaMemcpyAsync(hf.data(), fl, hf.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  finish_out(x, xd, n, s);
+  HFK_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < ns; ++i) {
+    const double* c = hs.data() + (size_t)SEG_NS * i;
+    const int* f = hf.data() + (size_t)SEG_NF * i;
+    const double tr = std::sqrt(c[S_RR]), nb = std::sqrt(c[S_BB]);
+    if (relres) relres[i] = nb > 0 ? tr / nb : tr;
+    // the recursive residual decides; a solve stopped without it is judged on the true residual
+    converged[i] = !f[F_INDEF] && (f[F_CONV] || tr <= c[S_TOL]);
+    iters[i] = f[F_ITERS];
+    if (indefinite) indefinite[i] = f[F_INDEF];
+  }
+  if (sweeps) *sweeps = it;
+}
 }  // namespace
 
 extern "C" {
@@ -2196,6 +2470,150 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
                  int flexible, int* iters, int* converged, int* indefinite, double* relres) {
   HFK_API_BEGIN
   solve_cg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres);
+  HFK_API_END
+}
+
+int hfk_solve_cg_batched(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol,
+                         int maxiter, int flexible, int* iters, int* converged, int* indefinite, double* relres,
+                         int* sweeps) {
+  HFK_API_BEGIN
+  solve_cg_seg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres, sweeps);
+  HFK_API_END
+}
+
+int hfk_problem_set_segments(hfk_problem* p, int nseg, const int64_t* dof_off, const int32_t* cell_off,
+                             const double* params) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && dof_off && nseg >= 1, HFK_ERR_ARG, "segments: null argument or nseg < 1");
+  HFK_REQUIRE(dof_off[0] == 0 && dof_off[nseg] == p->nfree, HFK_ERR_ARG,
+              "segments: dof offsets must start at 0 and end at the number of free dofs");
+  for (int s = 0; s < nseg; ++s)
+    HFK_REQUIRE(dof_off[s] <= dof_off[s + 1], HFK_ERR_ARG, "segments: dof offsets must be non-decreasing");
+  HFK_REQUIRE(!params || cell_off, HFK_ERR_ARG, "segments: per-segment parameters need the cell ranges");
+  if (cell_off) {
+    HFK_REQUIRE(cell_off[0] == 0 && cell_off[nseg] == p->ncells, HFK_ERR_ARG,
+                "segments: cell offsets must start at 0 and end at the number of cells");
+    for (int s = 0; s < nseg; ++s) {
+      HFK_REQUIRE(cell_off[s] <= cell_off[s + 1], HFK_ERR_ARG, "segments: cell offsets must be non-decreasing");
+      // independence: the free dofs of a segment's cells lie in the segment's dof range
+      for (int32_t c = cell_off[s]; c < cell_off[s + 1]; ++c)
+        for (int j = 0; j < p->ndl; ++j) {
+          const int32_t id = p->h_ids[(size_t)c * p->ndl + j];
+          HFK_REQUIRE(id <= 0 || (id - 1 >= dof_off[s] && id - 1 < dof_off[s + 1]), HFK_ERR_ARG,
+                      "segments: a cell of one segment holds a free dof of another (segments must be independent)");
+        }
+    }
+  }
+  if (params)
+    for (int s = 0; s < 2 * nseg; ++s)
+      HFK_REQUIRE(std::isfinite(params[s]), HFK_ERR_ARG, "segments: non-finite law parameter");
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  p->nseg = nseg;
+  p->seg_off.assign(dof_off, dof_off + nseg + 1);
+  if (cell_off) p->seg_cells.assign(cell_off, cell_off + nseg + 1);
+  else p->seg_cells.clear();
+  if (nseg > 1) {
+    std::vector<int32_t> sd(std::max<int64_t>(p->nfree, 1), 0);
+    for (int s = 0; s < nseg; ++s)
+      for (int64_t i = dof_off[s]; i < dof_off[s + 1]; ++i) sd[i] = s;
+    p->seg_of_dof.upload(sd.data(), sd.size(), p->stream);
+    if (p->nblocks > 0) {
+      std::vector<int32_t> dofs((size_t)3 * p->nblocks);
+      HFK_CUDA(cudaMemcpy(dofs.data(), p->bdofs.p, dofs.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      build_seg_of_block(p, dofs);
+    }
+  } else {
+    p->seg_of_dof.release();
+    p->seg_of_block.release();
+  }
+  if (params) {
+    p->seg_lm.assign(params, params + 2 * (size_t)nseg);
+    std::vector<double> lm((size_t)2 * std::max(p->ncells, 1), 0.0);
+    for (int s = 0; s < nseg; ++s)
+      for (int32_t c = cell_off[s]; c < cell_off[s + 1]; ++c) {
+        lm[2 * (size_t)c] = params[2 * s];
+        lm[2 * (size_t)c + 1] = params[2 * s + 1];
+      }
+    p->cell_lm.upload(lm.data(), lm.size(), p->stream);
+  } else {
+    p->seg_lm.clear();
+  }
+  p->items_built = false;
+  ensure_seg_items(p);
+  HFK_API_END
+}
+
+int hfk_problem_segments(hfk_problem* p, int* nseg) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && nseg, HFK_ERR_ARG, "null argument");
+  *nseg = p->nseg;
+  HFK_API_END
+}
+
+int hfk_problem_set_cell_params(hfk_problem* p, const double* lm) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p, HFK_ERR_ARG, "null handle");
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  if (!lm) {
+    p->cell_lm.release();
+  } else {
+    HFK_REQUIRE(!is_device_ptr(lm), HFK_ERR_ARG, "per-cell parameters are read from host memory");
+    for (size_t i = 0; i < 2 * (size_t)p->ncells; ++i)
+      HFK_REQUIRE(std::isfinite(lm[i]), HFK_ERR_ARG, "non-finite per-cell law parameter");
+    p->cell_lm.upload(lm, 2 * (size_t)p->ncells, p->stream);
+    HFK_CUDA(cudaStreamSynchronize(p->stream));
+  }
+  HFK_API_END
+}
+
+int hfk_segment_dots(hfk_problem* p, const double* a, const double* b, double* out) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && a && b && out, HFK_ERR_ARG, "null argument");
+  const double* da = dev_in(a, p->nfree, p->stage_in, p->stream);
+  const double* db = dev_in(b, p->nfree, p->stage_in2, p->stream);
+  DBuf<double> o;
+  o.resize(p->nseg);
+  seg_dots<double>(p, 1, o.p, 1, da, db);
+  HFK_CUDA(cudaMemcpyAsync(out, o.p, p->nseg * sizeof(double), cudaMemcpyDefault, p->stream));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  HFK_API_END
+}
+
+int hfk_segment_scale(hfk_problem* p, double* x, const double* f) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && x && f, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(is_device_ptr(x), HFK_ERR_ARG, "hfk_segment_scale scales a device vector");
+  DBuf<double> d;
+  d.upload(f, p->nseg, p->stream);
+  seg_mul_kernel<<<vec_grid(p->nfree), 256, 0, p->stream>>>(p->nfree, seg_dof_map(p), d.p, x);
+  check_launch(p);
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  HFK_API_END
+}
+
+int hfk_pmg_segment_bounds(hfk_pmg* m, int level, double* lmin, double* lmax) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && level >= 0 && level < m->L && lmin && lmax, HFK_ERR_ARG, "invalid argument");
+  const std::vector<double>&lo = m->seg_lmin[level], &hi = m->seg_lmax[level];
+  for (int s = 0; s < m->lv[level]->nseg; ++s) {
+    lmin[s] = s < (int)lo.size() ? lo[s] : NAN;
+    lmax[s] = s < (int)hi.size() ? hi[s] : NAN;
+  }
+  HFK_API_END
+}
+
+int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && (mode == HFK_COARSE_CHOLESKY || mode == HFK_COARSE_CG), HFK_ERR_ARG,
+              "coarse mode must be HFK_COARSE_CHOLESKY or HFK_COARSE_CG");
+  HFK_REQUIRE(mode != HFK_COARSE_CG || iters >= 1, HFK_ERR_ARG, "the coarse CG needs at least one iteration");
+  HFK_CUDA(cudaStreamSynchronize(m->lv[0]->stream));
+  m->coarse_mode = mode;
+  if (mode == HFK_COARSE_CG) m->coarse_iters = iters;
+  pmg_drop_graph(m);
+  // the hierarchy is rebuilt by the next update
+  m->built = false;
+  m->ok = false;
   HFK_API_END
 }
 
@@ -2483,11 +2901,18 @@ int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets
     const int nb = mlp_prepare_features(m, r, y.p);
     // the remaining error e = A^-1 s, by an accurate solve preconditioned by the plain cycle
     HFK_CUDA(cudaMemsetAsync(e.p, 0, n * sizeof(double), p->stream));
-    int its = 0, conv = 0, ind = 0;
-    double rel = 0;
-    solve_cg_dev(p, m, m->ml_s.p, e.p, rtol, 0.0, 500, 1, &its, &conv, &ind, &rel);
-    HFK_REQUIRE(conv, HFK_ERR_NUMERIC, "the target solve of a training sample did not converge");
-    mlp_targets_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, e.p, m->ml_scal.p, targets);
+    if (p->nseg > 1) {
+      std::vector<int> its(p->nseg), conv(p->nseg);
+      solve_cg_seg_dev(p, m, m->ml_s.p, e.p, rtol, 0.0, 500, 1, its.data(), conv.data(), nullptr, nullptr, nullptr);
+      for (int c : conv) HFK_REQUIRE(c, HFK_ERR_NUMERIC, "the target solve of a training sample did not converge");
+    } else {
+      int its = 0, conv = 0, ind = 0;
+      double rel = 0;
+      solve_cg_dev(p, m, m->ml_s.p, e.p, rtol, 0.0, 500, 1, &its, &conv, &ind, &rel);
+      HFK_REQUIRE(conv, HFK_ERR_NUMERIC, "the target solve of a training sample did not converge");
+    }
+    mlp_targets_kernel<<<vec_grid(nb), 256, 0, p->stream>>>(nb, p->bdofs.p, seg_block_map(p), e.p, m->ml_scal.p, 8,
+                                                             targets);
     check_launch(p);
     HFK_CUDA(cudaMemcpyAsync(feats, m->ml_feats.p, (size_t)nb * MLP_IN * sizeof(float), cudaMemcpyDeviceToDevice,
                              p->stream));

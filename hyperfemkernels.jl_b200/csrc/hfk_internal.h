@@ -82,6 +82,9 @@ struct CellData {
   const double* w;        // (np) tensor point order
   int law;                // HFK_LAW_*
   double lam, mu, body[3];
+  const double* cell_lm;  // optional (2, ncells): lambda, mu per cell (batched problems), else lam, mu
+  __host__ __device__ double lam_of(int cell) const { return cell_lm ? cell_lm[2 * (size_t)cell] : lam; }
+  __host__ __device__ double mu_of(int cell) const { return cell_lm ? cell_lm[2 * (size_t)cell + 1] : mu; }
 };
 
 // Work of the two-stage reductions (partial sums and the result)
@@ -94,6 +97,8 @@ struct Reducer {
 struct CGWork {
   DBuf<double> b, x, r, z, p, q, rold;
   Reducer red;
+  DBuf<double> sc;  // per-segment scalars of the batched solve
+  DBuf<int> fl, cnt;
 };
 
 // State of a matrix-free level in a precision
@@ -123,6 +128,22 @@ struct hfk_problem {
   hfk::DBuf<int32_t> ids;                 // (ndl, ncells)
   hfk::DBuf<double> geo, coords, dMt, w, Nt, dNt;  // Nt (nn, np), dNt (nn, 3, np) tensor order
   hfk::DBuf<uint8_t> affine;
+  hfk::DBuf<double> cell_lm;              // per-cell lambda, mu (empty: the problem's parameters)
+  // segments: independent problems held in one handle. Segment s owns the free dofs
+  // [seg_off[s], seg_off[s+1]) and the cells [seg_cells[s], seg_cells[s+1]); reductions, Krylov
+  // scalars, Chebyshev intervals and convergence are per segment. One segment by default.
+  int nseg = 1;
+  std::vector<int64_t> seg_off;           // nseg + 1
+  std::vector<int32_t> seg_cells;         // nseg + 1 (empty: not given)
+  std::vector<double> seg_lm;             // (2, nseg) lambda, mu per segment (empty: the problem's)
+  hfk::DBuf<int32_t> seg_of_dof;          // per free dof (empty when nseg == 1)
+  hfk::DBuf<int32_t> seg_of_block;        // per nodal block (empty when nseg == 1)
+  hfk::DBuf<int64_t> item_lo, item_hi;    // segmented reductions: chunks of one segment's dofs
+  hfk::DBuf<int32_t> item_first;          // nseg + 1: the first chunk of each segment
+  hfk::DBuf<int64_t> seg_off_d;           // device copy of seg_off
+  hfk::DBuf<double> seg_partial;          // per-chunk partial sums (3 per chunk)
+  int nitems = 0;
+  bool items_built = false;
   // colours
   int ncolors = 0;
   std::vector<int32_t> h_color_of;        // per cell, 1-based

@@ -63,7 +63,7 @@ __device__ void asm_point_phase(const CellData& cd, const AsmIO& io, int cell, c
   for (int e = threadIdx.x; e < np * 9; e += blockDim.x) {
     const int q = e / 9, ck = e % 9, c = ck / 3, k = ck % 3;
     double T[81];
-    law_tangent(cd.law, cd.lam, cd.mu, Hs + q * 9, T);
+    law_tangent(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, T);
     const double* iJ = iJs + q * 9;
     const double dV = dVs[q];
     // X[J][K'] = sum_L T[(c,J),(k,L)] iJ[L + 3K']

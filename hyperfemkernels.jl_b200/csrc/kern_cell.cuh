@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
   const int list_index = (blockIdx.x * nwarps + warp) * CPW + (active ? slot : 0);
   const bool has_cell = active && list_index < cd.ncells_list;
   const int cell = has_cell ? (cd.cells ? cd.cells[list_index] : list_index) : 0;
+  const R lam_c = (R)cd.lam_of(cell), mu_c = (R)cd.mu_of(cell);
 
   // ---- gather (gather_cell!, src/assembly.jl:1060-1070; increments are zero at Dirichlet dofs) ----
   if (has_cell) {
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
       R outv[3] = {0, 0, 0};
       if (MODE == MODE_RESIDUAL) {
         R Pm[9];
-        law_stress<R>(cd.law, (R)cd.lam, (R)cd.mu, H, Pm);
+        law_stress<R>(cd.law, lam_c, mu_c, H, Pm);
         pull_back<R>(iJ, Pm, dV, out);
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) outv[cc] = -dV * (R)cd.body[cc];
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
 #pragma unroll
           for (int i = 0; i < 9; ++i) Fm[i] = (i % 4) == 0 ? R(1) : R(0);
         }
-        law_dstress_F<R>(cd.law, (R)cd.lam, (R)cd.mu, Fm, H, dP);
+        law_dstress_F<R>(cd.law, lam_c, mu_c, Fm, H, dP);
         pull_back<R>(iJ, dP, dV, out);
       } else {
         // stored tangent: sv = dV T su (apply_cells!, src/matrixfree.jl:367-375)

@@ -195,13 +195,18 @@ __global__ void mlp_to_bf16_kernel(int np, const float* w, __nv_bfloat16* wb) {
 
 // ---- features and the correction on the free dofs, per nodal block ----------------------------
 // feats[b] = [s/ss, (Binv s)/sm, r/sr, y/sy, log lam, log mu, 0, 0]; the dofs of block b = bdofs[3b..]
-__global__ void mlp_features_kernel(int nb, const int32_t* dofs, const double* Binv, const double* s, const double* r,
-                                    const double* y, const double* scales, float loglam, float logmu, float* feats) {
-  const float is = scales[0] > 0 ? 1.f / (float)scales[0] : 0.f;
-  const float im = scales[1] > 0 ? 1.f / (float)scales[1] : 0.f;
-  const float ir = scales[2] > 0 ? 1.f / (float)scales[2] : 0.f;
-  const float iy = scales[3] > 0 ? 1.f / (float)scales[3] : 0.f;
+// Per-segment scales: scales[seg * sstride + j], j = 0..3 the root mean squares of s, Binv s, r, y;
+// loglm[2 seg], loglm[2 seg + 1] = log lambda, log mu of the segment (one segment: segb null).
+__global__ void mlp_features_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* Binv,
+                                    const double* s, const double* r, const double* y, const double* scales,
+                                    int sstride, const float* loglm, float* feats) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const int sg = segb ? segb[b] : 0;
+    const double* sc = scales + (size_t)sg * sstride;
+    const float is = sc[0] > 0 ? 1.f / (float)sc[0] : 0.f;
+    const float im = sc[1] > 0 ? 1.f / (float)sc[1] : 0.f;
+    const float ir = sc[2] > 0 ? 1.f / (float)sc[2] : 0.f;
+    const float iy = sc[3] > 0 ? 1.f / (float)sc[3] : 0.f;
     const int d0 = dofs[3 * b], d1 = dofs[3 * b + 1], d2 = dofs[3 * b + 2];
     const double sv[3] = {d0 ? s[d0 - 1] : 0.0, d1 ? s[d1 - 1] : 0.0, d2 ? s[d2 - 1] : 0.0};
     const double* M = Binv + 9 * (size_t)b;
@@ -214,40 +219,52 @@ __global__ void mlp_features_kernel(int nb, const int32_t* dofs, const double* B
       f[6 + i] = dd[i] ? (float)r[dd[i] - 1] * ir : 0.f;
       f[9 + i] = dd[i] ? (float)y[dd[i] - 1] * iy : 0.f;
     }
-    f[12] = loglam;
-    f[13] = logmu;
+    f[12] = loglm[2 * sg];
+    f[13] = loglm[2 * sg + 1];
     f[14] = 0.f;
     f[15] = 0.f;
   }
 }
-
-// delta[dofs of b] = out[b] * scale (the network predicts the error in units of the Binv s scale)
-__global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const float* out, const double* scales, double* delta) {
-  const double sc = scales[1];
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+__global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* segb, const float* out,
+                                   const double* scales, int sstride, double* delta) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const double sc = scales[(size_t)(segb ? segb[b] : 0) * sstride + 1];
     for (int i = 0; i < 3; ++i) {
       const int d = dofs[3 * b + i];
       if (d) delta[d - 1] = (double)out[(size_t)b * MLP_OUT + i] * sc;
     }
+  }
 }
-
-// targets[b] = e[dofs of b] / scale
-__global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const double* e, const double* scales, float* t) {
-  const double sc = scales[1] > 0 ? 1.0 / scales[1] : 0.0;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+__global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* e,
+                                   const double* scales, int sstride, float* t) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const double s1 = scales[(size_t)(segb ? segb[b] : 0) * sstride + 1];
+    const double sc = s1 > 0 ? 1.0 / s1 : 0.0;
     for (int i = 0; i < 3; ++i) {
       const int d = dofs[3 * b + i];
       t[(size_t)b * MLP_OUT + i] = d ? (float)(e[d - 1] * sc) : 0.f;
     }
+  }
 }
-
-// the acceptance rule: y += delta only if |s - A delta| < |s| (norms squared in nrm[0], nrm[1])
-__global__ void mlp_accept_kernel(int64_t n, const double* nrm, const double* delta, double* y, int* accepted) {
-  const bool ok = nrm[1] < nrm[0];
-  if (blockIdx.x == 0 && threadIdx.x == 0 && ok) atomicAdd(accepted, 1);
-  if (!ok) return;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] += delta[i];
+// y += delta in the segments where the corrected residual is smaller: nrm[seg * stride] = |s|^2,
+// nrm[seg * stride + 1] = |s - A delta|^2
+__global__ void mlp_accept_kernel(int64_t n, const int32_t* seg, const double* nrm, int stride, const double* delta,
+                                  double* y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* c = nrm + (size_t)(seg ? seg[i] : 0) * stride;
+    if (c[1] < c[0]) y[i] += delta[i];
+  }
+}
+// one CTA: *accepted += the number of segments whose correction was kept
+__global__ void mlp_accept_count_kernel(int nseg, const double* nrm, int stride, int* accepted) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) mine += nrm[(size_t)s * stride + 1] < nrm[(size_t)s * stride];
+  atomicAdd(&cnt, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) *accepted += cnt;
 }
 
 }  // namespace hfk

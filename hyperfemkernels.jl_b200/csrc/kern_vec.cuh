@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
   for (int e = threadIdx.x; e < np * 9; e += blockDim.x) {
     const int q = e / 9, ck = e % 9, c = ck / 3, k = ck % 3;
     double T[81];
-    law_tangent(cd.law, cd.lam, cd.mu, Hs + q * 9, T);
+    law_tangent(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, T);
     const double* iJ = iJs + q * 9;
     double X[3][3];
     for (int J = 0; J < 3; ++J)
@@ -274,12 +274,13 @@ __global__ void cheb_step_kernel(int nb, const int32_t* dofs, const R* Binv, con
 
 // The same two steps with the coefficients read from device memory (coef = [1/theta, c1_1, c2_1,
 // c1_2, c2_2, ...], written by the host at every update), so that a V-cycle captured once in a CUDA
-// graph stays valid when the smoothing interval changes.
+// graph stays valid when the smoothing interval changes. With segments (segb non-null) block b
+// reads the coefficients of its segment, coef + segb[b] * cstride.
 template <typename R>
 __global__ void cheb_start_dev_kernel(int nb, const int32_t* dofs, const R* Binv, const R* rhs, const R* Ax, R* r,
-                                      R* d, R* x, const double* coef, int zero_guess) {
-  const R inv_theta = (R)coef[0];
+                                      R* d, R* x, const double* coef, const int32_t* segb, int cstride, int zero_guess) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const R inv_theta = (R)coef[(segb ? (size_t)segb[b] * cstride : 0)];
     int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
     R rr[3];
     for (int i = 0; i < 3; ++i) {
@@ -302,9 +303,10 @@ __global__ void cheb_start_dev_kernel(int nb, const int32_t* dofs, const R* Binv
 }
 template <typename R>
 __global__ void cheb_step_dev_kernel(int nb, const int32_t* dofs, const R* Binv, const R* z, R* r, R* d, R* x,
-                                     const double* coef, int step, int update_d) {
-  const R c1 = update_d ? (R)coef[2 * step - 1] : R(0), c2 = update_d ? (R)coef[2 * step] : R(0);
+                                     const double* coef, const int32_t* segb, int cstride, int step, int update_d) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const double* cb = coef + (segb ? (size_t)segb[b] * cstride : 0);
+    const R c1 = update_d ? (R)cb[2 * step - 1] : R(0), c2 = update_d ? (R)cb[2 * step] : R(0);
     int dd[3] = {dofs[3 * b], dofs[3 * b + 1], dofs[3 * b + 2]};
     R rr[3];
     for (int i = 0; i < 3; ++i) {
@@ -328,22 +330,8 @@ __global__ void cheb_step_dev_kernel(int nb, const int32_t* dofs, const R* Binv,
 
 // ---- Arnoldi without host synchronisation: scalars stay on the device -----------------------
 // y += sign * (*alpha) * x
-__global__ void axpy_dev_kernel(int64_t n, const double* alpha, double sign, const double* x, double* y) {
-  const double a = sign * *alpha;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] += a * x[i];
-}
 // *s = sqrt(*s)
-__global__ void sqrt_dev_kernel(double* s) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) *s = sqrt(*s);
-}
 // y = x / *s (0 when *s is 0: the breakdown is decided on the host from the Hessenberg matrix)
-__global__ void scale_dev_kernel(int64_t n, const double* s, const double* x, double* y) {
-  const double v = *s;
-  const double inv = v != 0.0 ? 1.0 / v : 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = x[i] * inv;
-}
 
 // ---- transfers (src/transfers.jl) ------------------------------------------------------------
 struct XferData {

@@ -24,6 +24,8 @@ FP32 = 1
 SCATTER_AUTO = 0
 SCATTER_COLOURED = 1
 SCATTER_ATOMIC = 2
+COARSE_CHOLESKY = 0
+COARSE_CG = 1
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -82,6 +84,14 @@ SIGNATURES = {
     "hfk_pmg_set_mlp": [_vp, _vp],
     "hfk_pmg_mlp_stats": [_vp, _pi64, _pi64],
     "hfk_pmg_mlp_sample": [_vp, _vp, _vp, _vp, _pi, _d],
+    "hfk_pmg_set_coarse": [_vp, _i, _i],
+    "hfk_pmg_segment_bounds": [_vp, _i, _vp, _vp],
+    "hfk_problem_set_segments": [_vp, _i, _vp, _vp, _vp],
+    "hfk_problem_segments": [_vp, _pi],
+    "hfk_problem_set_cell_params": [_vp, _vp],
+    "hfk_segment_dots": [_vp, _vp, _vp, _vp],
+    "hfk_segment_scale": [_vp, _vp, _vp],
+    "hfk_solve_cg_batched": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp, _pi],
 }
 
 _LIB = None

@@ -34,6 +34,12 @@ class Problem:
         self.h = h
         self.nfree, self.ndir = space.nfree, space.ndir
         self.form = form
+        self.nseg = 1
+        if getattr(space, "segments", None) is not None:
+            from .batch import apply_segments  # a union of independent problems
+
+            apply_segments(self, space)
+            self.nseg = space.nseg
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -148,12 +148,21 @@ class PMultigrid:
     """``PMultigrid(spaces; smoother = Chebyshev(), coarse = LUSolver(), coarse_every = 1)`` (src/pmultigrid.jl:256-267).
 
     ``spaces`` lists the trial spaces of the levels, finest first (same mesh, same closed Dirichlet
-    boundary, nested orders). The coarsest level is assembled and factorised on the GPU (dense
-    Cholesky, FP64). ``precision`` "fp64" or "fp32" (smoothers and products of the levels above
-    the coarse one; the eigenvalue estimate and the coarse solve stay FP64).
+    boundary, nested orders). ``coarse`` "cholesky": the coarsest level is assembled and factorised
+    on the GPU (dense Cholesky, FP64); "cg": ``coarse_iters`` block-Jacobi CG steps per problem on
+    the matrix-free coarsest level (for batches and coarse levels too large for a dense factor; a
+    variable preconditioner, use ``krylov="fcg"``). ``precision`` "fp64" or "fp32" (smoothers and
+    products of the levels above the coarse one; the eigenvalue estimate and the coarse solve stay
+    FP64).
     """
 
-    def __init__(self, spaces, smoother: Chebyshev = Chebyshev(), coarse_every: int = 1, precision: str = "fp64"):
+    def __init__(self, spaces, smoother: Chebyshev = Chebyshev(), coarse_every: int = 1, precision: str = "fp64",
+                 coarse: str = "cholesky", coarse_iters: int = 20):
+        if coarse not in ("cholesky", "cg"):
+            raise ValueError("HyperFEMKernels: PMultigrid: coarse must be 'cholesky' or 'cg'")
+        if coarse == "cg" and coarse_iters < 1:
+            raise ValueError("HyperFEMKernels: PMultigrid: coarse_iters must be ≥ 1")
+        self.coarse, self.coarse_iters = coarse, int(coarse_iters)
         if len(spaces) < 2:
             raise ValueError("HyperFEMKernels: PMultigrid needs at least two levels")
         if coarse_every < 1:
@@ -184,6 +193,8 @@ class PMultigridState:
         call("hfk_pmg_create", ctypes.byref(h), L, lv, tr, c.degree, c.range, c.inflate, c.eig_iters, prec.coarse_every,
              _lib.FP32 if prec.precision == "fp32" else _lib.FP64)
         self.h = h
+        if prec.coarse == "cg":
+            call("hfk_pmg_set_coarse", h, _lib.COARSE_CG, prec.coarse_iters)
         self.ncycle = 0
         self.nbuild = 0
         self.update(mf)
@@ -221,6 +232,13 @@ class PMultigridState:
         keys = ("updates", "coarse_builds", "cycles", "t_update_ms", "t_coarse_ms", "t_blocks_ms", "t_eig_ms",
                 "t_cycle_ms", "t_potrf_ms")
         return dict(zip(keys, out.tolist()))
+
+    def segment_bounds(self, level: int):
+        """(lmin, lmax) of the level's eigenvalue estimate per problem of a batch."""
+        k = self.problems[level].nseg
+        lo, hi = np.zeros(k), np.zeros(k)
+        call("hfk_pmg_segment_bounds", self.h, level, ptr(lo), ptr(hi))
+        return lo, hi
 
     def level_info(self, level: int):
         a, b, lo, hi = (ctypes.c_double() for _ in range(4))
@@ -295,6 +313,11 @@ def numerical_setup_update(ns: MatrixFreeSolverNS, mf: MatrixFreeJacobian) -> Ma
 
 def solve(x, ns: MatrixFreeSolverNS, b):
     """``solve!(x, ns, b)`` (src/solvers.jl:111-159); x is the initial guess on input."""
+    if ns.mf.op.problem.nseg > 1:  # a batch: one solve per problem (hfk.batch)
+        from .batch import solve_batched
+
+        solve_batched(x, ns, b)
+        return x
     s = ns.solver
     it, conv, ind, rel = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
     prec = ns.prec.h if ns.prec is not None else None

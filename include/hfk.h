@@ -188,8 +188,21 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y);
  * V-cycles, in the Cholesky factorisation alone. The
  * V-cycle is replayed from a CUDA graph captured on the second cycle after each update. */
 int hfk_pmg_stats(hfk_pmg* m, double* out);
-/* Interval and Ritz values of a level's smoother. */
+/* Interval and Ritz values of a level's smoother (with segments: the extreme Ritz values over the
+ * segments and the interval of the largest). */
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
+/* Coarse solve of the hierarchy: HFK_COARSE_CHOLESKY (default; the assembled coarse level, dense
+ * Cholesky, in place of the reference's LUSolver, src/pmultigrid.jl:212-219) or HFK_COARSE_CG:
+ * `iters` steps of block-Jacobi CG per segment on the matrix-free coarse level from zero (scalars on
+ * the device, inside the captured cycle; a variable preconditioner, so use the flexible CG). The
+ * second serves hierarchies whose coarse level is too large for a dense factor (many batched
+ * problems); it has no counterpart in the reference. Takes effect at the next hfk_pmg_update. */
+/* Ritz values (extremes) of a level's eigenvalue estimate per segment (nseg entries each; NaN
+ * for a level without a smoother or before the first update). */
+int hfk_pmg_segment_bounds(hfk_pmg* m, int level, double* lmin, double* lmax);
+#define HFK_COARSE_CHOLESKY 0
+#define HFK_COARSE_CG 1
+int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters);
 
 /* ---- learned correction (no counterpart in the reference) ------------------------------------
  * A per-node MLP (16 -> 64 -> 64 -> 3, tanh, BF16 weights read by the forward pass, FP32 master
@@ -228,6 +241,33 @@ int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets
  * converged = 0 and indefinite = 1; an unusable preconditioner returns at once, iters = 0. */
 int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
                  int flexible, int* iters, int* converged, int* indefinite, double* relres);
+
+/* ---- batched problems (no counterpart in the reference: many independent solves at once) -------
+ * A problem handle may hold several independent problems ("segments") as one disjoint union of
+ * meshes: segment s owns the free dofs [dof_off[s], dof_off[s+1]) and the cells
+ * [cell_off[s], cell_off[s+1]) (cell_off may be NULL when params is NULL; with it, the call checks
+ * that no cell of a segment touches another segment's free dofs). params (2, nseg): lambda, mu per
+ * segment (NULL keeps the problem's parameters for every cell). Every kernel launch covers all
+ * segments; reductions, Chebyshev intervals (eigenvalue_bounds per segment,
+ * src/preconditioners.jl:374-389) and the Krylov scalars are per segment. Set the same segments on
+ * every level before building a hierarchy. */
+int hfk_problem_set_segments(hfk_problem* p, int nseg, const int64_t* dof_off, const int32_t* cell_off,
+                             const double* params);
+int hfk_problem_segments(hfk_problem* p, int* nseg);
+/* Per-cell law parameters lm (2, ncells) host array (lambda, mu of each cell); NULL returns to the
+ * problem's parameters. */
+int hfk_problem_set_cell_params(hfk_problem* p, const double* lm);
+/* out[s] = a . b over segment s (host or device pointers; out has nseg entries). */
+int hfk_segment_dots(hfk_problem* p, const double* a, const double* b, double* out);
+/* x[i] *= f[segment of i] (x a device vector; f host, nseg entries). */
+int hfk_segment_scale(hfk_problem* p, double* x, const double* f);
+/* MatrixFreeSolver.solve! (src/solvers.jl:111-159) on every segment at once: one (flexible) CG per
+ * segment with its own tolerance atol + rtol ||b_s||, stopping test and curvature check, all
+ * segments advancing in the same launches. iters, converged, indefinite, relres: nseg entries
+ * (host); sweeps: the number of iterations of the common loop. */
+int hfk_solve_cg_batched(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol,
+                         int maxiter, int flexible, int* iters, int* converged, int* indefinite, double* relres,
+                         int* sweeps);
 
 #ifdef __cplusplus
 }

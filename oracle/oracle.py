@@ -358,11 +358,13 @@ class OraclePMG:
     operators are captured from the Newton's forms, src/pmultigrid.jl:244-247).
     """
 
-    def __init__(self, spaces, quad, law=LAW_SVK, params=(2.0, 1.0), degree=2, rng=20.0, inflate=1.1, eig_iters=10):
+    def __init__(self, spaces, quad, law=LAW_SVK, params=(2.0, 1.0), degree=2, rng=20.0, inflate=1.1, eig_iters=10,
+                 coarse="direct", coarse_iters=20):
         self.spaces = spaces
         self.levels = [OracleProblem(s, quad, law, params) for s in spaces]
         self.P = [OracleTransfer(spaces[l], spaces[l + 1]) for l in range(len(spaces) - 1)]
         self.cheb_cfg = (degree, rng, inflate, eig_iters)
+        self.coarse, self.coarse_iters = coarse, coarse_iters
         self.smoothers = None
         self.xs = None
 
@@ -378,15 +380,45 @@ class OraclePMG:
         for l, p in enumerate(self.levels[:-1]):
             p.mf_prepare(xs[l], ds[l])
         c = self.levels[-1]
-        A = c.jacobian(xs[-1], ds[-1])
-        self.coarse_ok = bool(np.all(np.isfinite(A.data)))
-        self.lu = spla.splu(A.tocsc()) if self.coarse_ok else None
+        if self.coarse == "cg":
+            # the engine's inexact coarse solve (HFK_COARSE_CG): matrix-free coarse level, blocks
+            c.mf_prepare(xs[-1], ds[-1])
+            _, _, Binv = c.blocks()
+            self.coarse_ok = bool(np.all(np.isfinite(Binv)))
+        else:
+            A = c.jacobian(xs[-1], ds[-1])
+            self.coarse_ok = bool(np.all(np.isfinite(A.data)))
+            self.lu = spla.splu(A.tocsc()) if self.coarse_ok else None
         self.smoothers = [OracleChebyshev(p, *self.cheb_cfg) for p in self.levels[:-1]]
         self.ok = self.coarse_ok and all(s.ok for s in self.smoothers)
 
+    def coarse_cg(self, b):
+        """``coarse_iters`` block-Jacobi CG steps from zero (the engine's HFK_COARSE_CG): alpha and
+        beta are 0 where their denominator is not positive."""
+        c = self.levels[-1]
+        x = np.zeros_like(b)
+        r = b.copy()
+        z = c.blocks_apply(r)
+        p = z.copy()
+        rz = r @ z
+        for it in range(self.coarse_iters):
+            q = c.mf_apply(p)
+            pq = p @ q
+            a = rz / pq if pq > 0 else 0.0
+            x = x + a * p
+            r = r - a * q
+            if it + 1 == self.coarse_iters:
+                break
+            z = c.blocks_apply(r)
+            zr = z @ r
+            beta = zr / rz if rz > 0 else 0.0
+            rz = zr
+            p = z + beta * p
+        return x
+
     def vcycle(self, b, level=0):
         if level == len(self.levels) - 1:
-            return self.lu.solve(b)
+            return self.coarse_cg(b) if self.coarse == "cg" else self.lu.solve(b)
         S, P = self.smoothers[level], self.P[level]
         x, r = S.smooth(None, b, zero_guess=True, want_residual=True)
         bc = P.restrict(r)
