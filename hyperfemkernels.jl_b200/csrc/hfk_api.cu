@@ -865,7 +865,7 @@ bool hessenberg_eigvals(int n, std::vector<double> H /* column-major n x n */, d
 }
 
 struct EigWork {
-  DBuf<double> V, t, w, Hd;
+  DBuf<double> V, Z, t, w, pw, Hd;
 };
 
 // eigenvalue_bounds (src/preconditioners.jl:374-389) of every segment at once: k Arnoldi steps
@@ -873,8 +873,13 @@ struct EigWork {
 // each segment builds its own Hessenberg matrix (a block-diagonal operator keeps the segments'
 // Krylov spaces apart); breakdown truncation and Ritz values per segment on the host. One copy
 // of the Hessenberg matrices to the host, no other synchronisation.
+// pinner: orthogonalise in the P^-1 inner product <u, v> = u . P^-1 v instead of the Euclidean one
+// (an option of this engine): J P^-1 is self-adjoint in it, so H is symmetric and its Ritz values
+// lie inside the spectrum; the Euclidean process (the reference's) can give Ritz values outside the
+// spectrum of a strongly non-normal J P^-1. Z = P^-1 V is kept beside V, so each step costs one
+// more block application and one more update per basis vector.
 void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev, std::vector<double>& lmin,
-                    std::vector<double>& lmax) {
+                    std::vector<double>& lmax, bool pinner = false) {
   const int64_t n = p->nfree;
   const int ns = p->nseg;
   k = (int)std::max<int64_t>(1, std::min<int64_t>(k, n));
@@ -889,27 +894,52 @@ void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev,
   const int32_t* seg = seg_dof_map(p);
   const int sg = std::max(1, (ns + 255) / 256);
   double* nrm = Hd + (size_t)ld * k;  // scratch scalar past each Hessenberg matrix
-  seg_dots<double>(p, 1, nrm, hs, start_dev, start_dev);
+  auto V = [&](int i) { return ew.V.p + (size_t)i * n; };
+  auto Z = [&](int i) { return ew.Z.p + (size_t)i * n; };
+  if (pinner) {
+    ew.Z.resize((size_t)(k + 1) * n);
+    ew.pw.resize(n);
+    blocks_apply_dev<double>(p, start_dev, ew.t.p);
+    seg_dots<double>(p, 1, nrm, hs, start_dev, ew.t.p);
+  } else {
+    seg_dots<double>(p, 1, nrm, hs, start_dev, start_dev);
+  }
   seg_sqrt_kernel<<<sg, 256, 0, p->stream>>>(ns, nrm, hs);
   check_launch(p);
-  seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, nrm, hs, start_dev, ew.V.p);
+  seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, nrm, hs, start_dev, V(0));
   check_launch(p);
+  if (pinner) {
+    seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, nrm, hs, ew.t.p, Z(0));
+    check_launch(p);
+  }
   for (int j = 0; j < k; ++j) {
-    double* vj = ew.V.p + (size_t)j * n;
-    blocks_apply_dev<double>(p, vj, ew.t.p);
-    mf_apply_dev(p, ew.t.p, ew.w.p);
+    if (pinner) {
+      mf_apply_dev(p, Z(j), ew.w.p);
+      blocks_apply_dev<double>(p, ew.w.p, ew.pw.p);
+    } else {
+      blocks_apply_dev<double>(p, V(j), ew.t.p);
+      mf_apply_dev(p, ew.t.p, ew.w.p);
+    }
     for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, coefficients written into H on the device
       double* hij = Hd + i + (size_t)ld * j;
-      seg_dots<double>(p, 1, hij, hs, ew.V.p + (size_t)i * n, ew.w.p);
-      seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, ew.V.p + (size_t)i * n, ew.w.p);
+      seg_dots<double>(p, 1, hij, hs, pinner ? Z(i) : V(i), ew.w.p);
+      seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, V(i), ew.w.p);
       check_launch(p);
+      if (pinner) {
+        seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, Z(i), ew.pw.p);
+        check_launch(p);
+      }
     }
     double* hn = Hd + (j + 1) + (size_t)ld * j;
-    seg_dots<double>(p, 1, hn, hs, ew.w.p, ew.w.p);
+    seg_dots<double>(p, 1, hn, hs, ew.w.p, pinner ? ew.pw.p : ew.w.p);
     seg_sqrt_kernel<<<sg, 256, 0, p->stream>>>(ns, hn, hs);
     check_launch(p);
-    seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hn, hs, ew.w.p, ew.V.p + (size_t)(j + 1) * n);
+    seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hn, hs, ew.w.p, V(j + 1));
     check_launch(p);
+    if (pinner) {
+      seg_scale_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hn, hs, ew.pw.p, Z(j + 1));
+      check_launch(p);
+    }
   }
   std::vector<double> Hall((size_t)hs * ns);
   HFK_CUDA(cudaMemcpyAsync(Hall.data(), Hd, sizeof(double) * Hall.size(), cudaMemcpyDeviceToHost, p->stream));
@@ -1199,6 +1229,7 @@ struct hfk_pmg {
   // coarse: dense Cholesky factor (lower) of the assembled coarse tangent, or (HFK_COARSE_CG) a
   // fixed number of block-Jacobi CG steps per segment on the matrix-free coarse level
   int coarse_mode = HFK_COARSE_CHOLESKY, coarse_iters = 20;
+  int eig_inner = HFK_EIG_EUCLIDEAN;  // inner product of the eigenvalue estimate
   DBuf<double> Lc, cb, cx;
   DBuf<double> ccg_r, ccg_z, ccg_p, ccg_q, ccg_sc;
   bool coarse_ok = false;
@@ -2136,7 +2167,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     }
     auto te = std::chrono::steady_clock::now();
     std::vector<double>&lo = m->seg_lmin[l], &hi = m->seg_lmax[l];
-    eig_bounds_dev(p, *m->ew[l], m->eig_iters, m->start[l]->p, lo, hi);
+    eig_bounds_dev(p, *m->ew[l], m->eig_iters, m->start[l]->p, lo, hi, m->eig_inner == HFK_EIG_PRECONDITIONED);
     m->t_eig += ms_since(te);
     // per segment: interval [b / range, b] with b = inflate * lmax (smoother_update!,
     // src/smoothers.jl:86-107) and its coefficients at coef + s * (1 + 2 degree)
@@ -2599,6 +2630,14 @@ int hfk_pmg_segment_bounds(hfk_pmg* m, int level, double* lmin, double* lmax) {
     lmin[s] = s < (int)lo.size() ? lo[s] : NAN;
     lmax[s] = s < (int)hi.size() ? hi[s] : NAN;
   }
+  HFK_API_END
+}
+
+int hfk_pmg_set_eig_inner(hfk_pmg* m, int mode) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && (mode == HFK_EIG_EUCLIDEAN || mode == HFK_EIG_PRECONDITIONED), HFK_ERR_ARG,
+              "eigenvalue estimate: mode must be HFK_EIG_EUCLIDEAN or HFK_EIG_PRECONDITIONED");
+  m->eig_inner = mode;
   HFK_API_END
 }
 

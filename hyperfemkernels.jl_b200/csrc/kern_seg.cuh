@@ -71,10 +71,11 @@ __global__ void seg_scale_kernel(int64_t n, const int32_t* seg, const double* s,
   }
 }
 
-// s[j * stride] = sqrt(s[j * stride]) for every segment j
+// s[j * stride] = sqrt(max(s[j * stride], 0)) for every segment j (a rounding-negative square of a
+// vanished vector, possible in the P^-1 inner product, is a breakdown, not a NaN)
 __global__ void seg_sqrt_kernel(int nseg, double* s, int stride) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nseg; j += gridDim.x * blockDim.x)
-    s[(size_t)j * stride] = sqrt(s[(size_t)j * stride]);
+    s[(size_t)j * stride] = sqrt(fmax(s[(size_t)j * stride], 0.0));
 }
 
 // sc[out] = sc[den] > 0 ? sc[num] / sc[den] : 0 per segment; then sc[den] = sc[num] when `shift`

@@ -26,6 +26,8 @@ SCATTER_COLOURED = 1
 SCATTER_ATOMIC = 2
 COARSE_CHOLESKY = 0
 COARSE_CG = 1
+EIG_EUCLIDEAN = 0
+EIG_PRECONDITIONED = 1
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -86,6 +88,7 @@ SIGNATURES = {
     "hfk_pmg_mlp_sample": [_vp, _vp, _vp, _vp, _pi, _d],
     "hfk_pmg_set_coarse": [_vp, _i, _i],
     "hfk_pmg_segment_bounds": [_vp, _i, _vp, _vp],
+    "hfk_pmg_set_eig_inner": [_vp, _i],
     "hfk_problem_set_segments": [_vp, _i, _vp, _vp, _vp],
     "hfk_problem_segments": [_vp, _pi],
     "hfk_problem_set_cell_params": [_vp, _vp],

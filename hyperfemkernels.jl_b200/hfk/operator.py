@@ -213,6 +213,7 @@ class MatrixFreeJacobian:
         self.op = op
         self.mode = mode
         self.x = np.zeros(0)
+        self.dvals = None
         self.prepared = False
 
     @property
@@ -236,6 +237,8 @@ class MatrixFreeJacobian:
         mode = _lib.MF_STORED if self.mode == "stored" else _lib.MF_RECOMPUTE
         call("hfk_mf_prepare", self.op.problem.h, ptr(x), ptr(d), mode)
         self.x = x.copy() if isinstance(x, np.ndarray) else x.clone()
+        # the Dirichlet values of the prepared state (the p-multigrid levels follow this state)
+        self.dvals = d.copy() if isinstance(d, np.ndarray) else d.clone()
         self.prepared = True
         return self
 

@@ -21,12 +21,18 @@ from .operator import KernelOperator, MatrixFreeJacobian, Problem
 
 @dataclasses.dataclass(frozen=True)
 class Chebyshev:
-    """``Chebyshev(; degree = 2, range = 20.0, inflate = 1.1, eig_iters = 10)`` (src/smoothers.jl:21-33)."""
+    """``Chebyshev(; degree = 2, range = 20.0, inflate = 1.1, eig_iters = 10)`` (src/smoothers.jl:21-33).
+
+    ``eig_inner`` (an option of this engine): "euclidean" is the reference's Arnoldi estimate;
+    "preconditioner" runs it in the P^-1 inner product, where J P^-1 is self-adjoint and the Ritz
+    values stay inside the spectrum (a Lanczos estimate).
+    """
 
     degree: int = 2
     range: float = 20.0
     inflate: float = 1.1
     eig_iters: int = 10
+    eig_inner: str = "euclidean"
 
     def __post_init__(self):
         if self.degree < 1:
@@ -37,6 +43,8 @@ class Chebyshev:
             raise ValueError("HyperFEMKernels: Chebyshev: inflate must be ≥ 1")
         if self.eig_iters < 2:
             raise ValueError("HyperFEMKernels: Chebyshev: eig_iters must be ≥ 2")
+        if self.eig_inner not in ("euclidean", "preconditioner"):
+            raise ValueError("HyperFEMKernels: Chebyshev: eig_inner must be 'euclidean' or 'preconditioner'")
 
 
 def chebyshev_damping(c: Chebyshev) -> float:
@@ -195,6 +203,8 @@ class PMultigridState:
         self.h = h
         if prec.coarse == "cg":
             call("hfk_pmg_set_coarse", h, _lib.COARSE_CG, prec.coarse_iters)
+        if c.eig_inner == "preconditioner":
+            call("hfk_pmg_set_eig_inner", h, _lib.EIG_PRECONDITIONED)
         self.ncycle = 0
         self.nbuild = 0
         self.update(mf)
@@ -214,7 +224,9 @@ class PMultigridState:
             p.set_params(mf.op.res)
         ok = ctypes.c_int()
         x = mf.x
-        call("hfk_pmg_update", self.h, ptr(x), ptr(mf.op.dirichlet_values()), ctypes.byref(ok))
+        # the levels follow the state the Jacobian was prepared at (its Dirichlet values included)
+        d = mf.dvals if mf.dvals is not None else mf.op.dirichlet_values()
+        call("hfk_pmg_update", self.h, ptr(x), ptr(d), ctypes.byref(ok))
         self.ok = bool(ok.value)
         self.nbuild += 1
         return self

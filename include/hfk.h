@@ -200,6 +200,14 @@ int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double
 /* Ritz values (extremes) of a level's eigenvalue estimate per segment (nseg entries each; NaN
  * for a level without a smoother or before the first update). */
 int hfk_pmg_segment_bounds(hfk_pmg* m, int level, double* lmin, double* lmax);
+/* Inner product of the smoothers' eigenvalue estimate: HFK_EIG_EUCLIDEAN (default; the reference's
+ * Arnoldi, src/preconditioners.jl:374-389) or HFK_EIG_PRECONDITIONED: the same Arnoldi in the
+ * P^-1 inner product, in which J P^-1 is self-adjoint, so that H is symmetric and the Ritz values
+ * lie inside the spectrum (a Lanczos estimate). An option of this engine. Takes effect at the next
+ * hfk_pmg_update. */
+#define HFK_EIG_EUCLIDEAN 0
+#define HFK_EIG_PRECONDITIONED 1
+int hfk_pmg_set_eig_inner(hfk_pmg* m, int mode);
 #define HFK_COARSE_CHOLESKY 0
 #define HFK_COARSE_CG 1
 int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters);

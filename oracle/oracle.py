@@ -272,26 +272,46 @@ def chebyshev_damping(degree, rng):
     return 1.0 / np.cosh(degree * np.arccosh(th / de))
 
 
-def arnoldi_bounds(apply_op, apply_prec, b, k):
+def arnoldi_bounds(apply_op, apply_prec, b, k, inner="euclidean"):
     """Ritz bounds of J P^-1 after k Arnoldi steps from b (``eigenvalue_bounds``, src/preconditioners.jl:374-389).
 
     Modified Gram-Schmidt Arnoldi; a (near) breakdown at step j (|H[j+1,j]| <= 1e-8 max(1, max|H[1:j,1:j]|))
     truncates the Hessenberg matrix; returns (min, max) of the real parts of its eigenvalues.
+    ``inner="preconditioner"`` is the engine's option that orthogonalises in the P^-1 inner product
+    <u, v> = u . P^-1 v, in which J P^-1 is self-adjoint: H is then symmetric and its Ritz values lie
+    inside the spectrum (a Lanczos estimate).
     """
     n = len(b)
     k = min(k, n)
     V = np.zeros((n, k + 1))
     H = np.zeros((k + 1, k))
-    V[:, 0] = b / np.linalg.norm(b)
-    for j in range(k):
-        w = apply_op(apply_prec(V[:, j]))
-        for i in range(j + 1):
-            H[i, j] = V[:, i] @ w
-            w = w - H[i, j] * V[:, i]
-        H[j + 1, j] = np.linalg.norm(w)
-        if H[j + 1, j] == 0:
-            break
-        V[:, j + 1] = w / H[j + 1, j]
+    if inner == "preconditioner":
+        Z = np.zeros((n, k + 1))  # Z = P^-1 V
+        z = apply_prec(b)
+        nb = np.sqrt(max(b @ z, 0.0))
+        V[:, 0], Z[:, 0] = b / nb, z / nb
+        for j in range(k):
+            w = apply_op(Z[:, j])
+            pw = apply_prec(w)
+            for i in range(j + 1):
+                H[i, j] = Z[:, i] @ w
+                w = w - H[i, j] * V[:, i]
+                pw = pw - H[i, j] * Z[:, i]
+            H[j + 1, j] = np.sqrt(max(w @ pw, 0.0))
+            if H[j + 1, j] == 0:
+                break
+            V[:, j + 1], Z[:, j + 1] = w / H[j + 1, j], pw / H[j + 1, j]
+    else:
+        V[:, 0] = b / np.linalg.norm(b)
+        for j in range(k):
+            w = apply_op(apply_prec(V[:, j]))
+            for i in range(j + 1):
+                H[i, j] = V[:, i] @ w
+                w = w - H[i, j] * V[:, i]
+            H[j + 1, j] = np.linalg.norm(w)
+            if H[j + 1, j] == 0:
+                break
+            V[:, j + 1] = w / H[j + 1, j]
     jj = k
     for i in range(1, k):
         if abs(H[i, i - 1]) <= 1e-8 * max(1.0, np.max(np.abs(H[:i, :i]))):
@@ -304,8 +324,9 @@ def arnoldi_bounds(apply_op, apply_prec, b, k):
 class OracleChebyshev:
     """``ChebyshevState`` (src/smoothers.jl:42-146) on an oracle problem prepared at its state."""
 
-    def __init__(self, prob: OracleProblem, degree=2, rng=20.0, inflate=1.1, eig_iters=10):
+    def __init__(self, prob: OracleProblem, degree=2, rng=20.0, inflate=1.1, eig_iters=10, eig_inner="euclidean"):
         self.prob, self.degree, self.range, self.inflate, self.eig_iters = prob, degree, rng, inflate, eig_iters
+        self.eig_inner = eig_inner
         self.update()
 
     def update(self):
@@ -315,7 +336,8 @@ class OracleChebyshev:
         if not self.blocks_ok:
             self.ok = False
             return
-        lmin, lmax, _ = arnoldi_bounds(p.mf_apply, p.blocks_apply, chebyshev_start(p.nfree), self.eig_iters)
+        lmin, lmax, _ = arnoldi_bounds(p.mf_apply, p.blocks_apply, chebyshev_start(p.nfree), self.eig_iters,
+                                       self.eig_inner)
         self.lmin, self.lmax = lmin, lmax
         self.ok = bool(np.isfinite(lmax) and lmax > 0 and lmin > 0)
         self.b = self.inflate * lmax
@@ -359,11 +381,11 @@ class OraclePMG:
     """
 
     def __init__(self, spaces, quad, law=LAW_SVK, params=(2.0, 1.0), degree=2, rng=20.0, inflate=1.1, eig_iters=10,
-                 coarse="direct", coarse_iters=20):
+                 coarse="direct", coarse_iters=20, eig_inner="euclidean"):
         self.spaces = spaces
         self.levels = [OracleProblem(s, quad, law, params) for s in spaces]
         self.P = [OracleTransfer(spaces[l], spaces[l + 1]) for l in range(len(spaces) - 1)]
-        self.cheb_cfg = (degree, rng, inflate, eig_iters)
+        self.cheb_cfg = (degree, rng, inflate, eig_iters, eig_inner)
         self.coarse, self.coarse_iters = coarse, coarse_iters
         self.smoothers = None
         self.xs = None

@@ -219,6 +219,40 @@ def test_vcycle_parity_with_oracle(precision):
     assert reldiff(y, mg.ldiv(r)) < tol
 
 
+def test_vcycle_parity_with_preconditioned_eigenvalue_estimate():
+    # the P^-1 inner-product Arnoldi option of the smoothers' estimate, against the oracle
+    Vs, res, jac = _pmg_case(3, (2, 1), "svk")
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = svk_state(Vs[0], amp=0.0, disp=0.0)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=2, eig_inner="preconditioner")), mf)
+    assert st.ok
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_SVK, (2.0, 1.0, 0.3, -0.2, 0.5), degree=2,
+                     eig_inner="preconditioner")
+    mg.update(x, Vs[0].dirichlet_values)
+    info = st.level_info(0)
+    assert abs(info["lmax"] - mg.smoothers[0].lmax) < 1e-9 * mg.smoothers[0].lmax
+    assert abs(info["lmin"] - mg.smoothers[0].lmin) < 1e-8 * mg.smoothers[0].lmax
+    r = np.random.default_rng(2).standard_normal(Vs[0].nfree)
+    assert reldiff(st.ldiv(np.zeros(Vs[0].nfree), r), mg.ldiv(r)) < 1e-9
+
+
+def test_pmg_follows_the_prepared_dirichlet_values():
+    # the hierarchy is built at the state the Jacobian was prepared at, not at the space's values
+    Vs, res, jac = _pmg_case(3, (2, 1), "svk")
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = np.zeros(Vs[0].nfree)
+    d = 0.1 * Vs[0].dirichlet_values
+    mf = op.allocate_jacobian(x)
+    mf.prepare(x, d)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=2)), mf)
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_SVK, (2.0, 1.0, 0.3, -0.2, 0.5), degree=2)
+    mg.update(x, d)
+    r = np.random.default_rng(3).standard_normal(Vs[0].nfree)
+    assert reldiff(st.ldiv(np.zeros(Vs[0].nfree), r), mg.ldiv(r)) < 1e-9
+
+
 @pytest.mark.parametrize("orders", [(2, 1), (3, 1), (4, 2, 1)])
 def test_pmg_solve_matches_direct_and_iterations_bounded(orders):
     # test/solvers/test_pmultigrid.jl:37-51

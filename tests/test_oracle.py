@@ -212,6 +212,32 @@ def test_chebyshev_damps_every_eigencomponent():
         assert np.linalg.norm(e - y) <= damp * np.linalg.norm(e) * (1 + 1e-6) + 1e-12
 
 
+def test_preconditioned_arnoldi_is_symmetric_and_inside_the_spectrum():
+    # the engine's HFK_EIG_PRECONDITIONED option: Arnoldi in the P^-1 inner product gives a
+    # symmetric (tridiagonal) H whose Ritz values lie inside the spectrum of P^-1 J
+    V = svk_space(n=(2, 2, 2), order=2)
+    p = O.OracleProblem(V, Quadrature.gauss(4), O.LAW_SVK, (15.0, 0.3))
+    x = svk_state(V)
+    d = V.dirichlet_values
+    A = p.jacobian(x, d).toarray()
+    p.mf_prepare(x, d)
+    dofs, B, Binv = p.blocks()
+    Minv = np.zeros_like(A)
+    for k in range(len(dofs)):
+        ix = dofs[k] - 1
+        Minv[np.ix_(ix, ix)] = Binv[k]
+    lam = np.sort(np.linalg.eigvals(Minv @ A).real)
+    b = O.chebyshev_start(V.nfree)
+    lo, hi, H = O.arnoldi_bounds(p.mf_apply, p.blocks_apply, b, 10, "preconditioner")
+    Hs = H[:10, :10]
+    assert np.allclose(Hs, Hs.T, atol=1e-10 * np.abs(Hs).max())
+    assert np.allclose(np.triu(Hs, 2), 0, atol=1e-10 * np.abs(Hs).max())
+    assert lam[0] * (1 - 1e-10) <= lo <= hi <= lam[-1] * (1 + 1e-10)
+    # the Euclidean estimate of the same operator (the reference's) has nearly the same top value
+    _, hi_e, _ = O.arnoldi_bounds(p.mf_apply, p.blocks_apply, b, 10)
+    assert abs(hi_e - hi) < 0.05 * hi
+
+
 def test_transfers_transpose_partition_of_unity_injection():
     # test/solvers/test_transfers.jl:60-122
     for qf, qc in ((2, 1), (3, 1), (3, 2), (4, 2)):
