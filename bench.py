@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--n", type=int, default=N_CELLS, help="cells per direction")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--batch", action="store_true",
+                    help="the batched workload instead: 256 SVK Q2 Newton solves (plain p-MG vs learned correction)")
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
     return ap.parse_args()
 
 
@@ -402,9 +406,162 @@ def reference(args):
     print(json.dumps(line))
 
 
+BATCH_LOADS = (0.1, 0.325, 0.55, 0.775, 1.0)
+
+
+def _batch_setup(count, seed=4):
+    from hfk import batch as B
+
+    problems = B.draw_batch(256, seed=seed)[:count]
+    (U2, U1), g = B.cube_batch(problems)
+    return problems, U2, U1, g, B.cube_lifting(U2)
+
+
+def _batch_solver(U2, U1, precision):
+    from hfk import solvers as S
+
+    return S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, maxiter=400,
+                              preconditioner=S.PMultigrid([U2, U1], S.Chebyshev(degree=4), precision=precision,
+                                                          coarse="cg", coarse_iters=20))
+
+
+def batch_cpu_sample(problems, budget_s=20.0):
+    """The same per-problem Newton (lifting predictor, 5 load steps, FCG + p-MG Q2 -> Q1 with the
+    20-step coarse CG, all to 1e-8) by the oracle on the host cores, on the smallest problems of
+    the batch until ``budget_s`` is spent; returns seconds per free dof (to extrapolate)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hfk import batch as B
+    from hfk.fespace import Quadrature
+
+    q = Quadrature.gauss(4)
+    done, dofs, t_all = [], 0, 0.0
+    for k in np.argsort([p.n for p in problems]):
+        pb = problems[k]
+        (U2, U1), g = B.cube_batch([pb])
+        V2, V1 = U2.spaces[0], U1.spaces[0]
+        lift = B.cube_lifting(U2)
+        orc = O.OracleProblem(V2, q, O.LAW_SVK, (pb.lam, pb.mu))
+        mg = O.OraclePMG([V2, V1], q, O.LAW_SVK, (pb.lam, pb.mu), degree=4, coarse="cg", coarse_iters=20)
+        x = np.zeros(V2.nfree)
+        t0 = time.perf_counter()
+        prev = 0.0
+        for lam in BATCH_LOADS:
+            d = lam * g
+            x = x + (lam - prev) * lift
+            prev = lam
+            r0 = None
+            for _ in range(20):
+                r = orc.residual(x, d)
+                rn = np.linalg.norm(r)
+                r0 = rn if r0 is None else r0
+                if rn <= max(1e-8 * r0, 1e-12):
+                    break
+                orc.mf_prepare(x, d)
+                mg.update(x, d)
+                dx, _, ok, _ = O.pcg(orc.mf_apply, -r, mg.ldiv, rtol=1e-8, maxiter=400)
+                x = x + dx
+        t_all += time.perf_counter() - t0
+        dofs += V2.nfree
+        done.append(int(pb.n))
+        if t_all > budget_s:
+            break
+    return {"seconds_per_free_dof": t_all / dofs, "sample": f"{len(done)} problems n={done} ({dofs} free dofs), "
+            f"{t_all:.1f} s", "cores": O.lib().o_max_threads(), "kind": "port"}
+
+
+def batch_main(args):
+    """Batched workload: ``--batch-count`` independent SVK Q2 Newton solves (n ~ U{8..24} cells per
+    direction, lambda, mu log-uniform in [0.5, 20] x [0.2, 5], seed 4), x = 0 clamped, x = 1 moved
+    0.05 along x in 5 load steps, every Newton and linear solve to 1e-8, all problems advanced by the
+    same launches (one handle, per-problem scalars). First with the plain p-multigrid (Q2 -> Q1,
+    Chebyshev 4, 20-step coarse CG), then with the learned correction trained on pairs from the
+    plain cycle at seeded states of the converged solution."""
+    import torch
+
+    from hfk import batch as B
+    from hfk import forms, learned
+    from hfk.operator import KernelOperator
+
+    t0 = time.perf_counter()
+    problems, U2, U1, g, lift = _batch_setup(args.batch_count)
+    res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
+    op = KernelOperator(res, jac, U2, jacobian="matrixfree")
+    t_setup = time.perf_counter() - t0
+    # warm-up (kernel attributes, handles, first-touch allocations) on a two-problem batch
+    p0, W2, W1, gw, lw = _batch_setup(2)
+    opw = KernelOperator(res, jac, W2, jacobian="matrixfree")
+    B.newton_solve_batched(opw, _batch_solver(W2, W1, args.batch_precision), gw, BATCH_LOADS[:1], lift=lw)
+    del opw
+    clocks = ClockSampler(0)
+    with clocks:
+        x, st = B.newton_solve_batched(op, _batch_solver(U2, U1, args.batch_precision), g, BATCH_LOADS, lift=lift)
+    plain = {"seconds": st.seconds, "newton_sweeps": st.newton_sweeps, "krylov_sweeps": int(sum(st.krylov_sweeps)),
+             "newton_iters_mean": float(st.newton_iters.mean()), "krylov_iters_mean": float(st.krylov_iters.mean()),
+             "krylov_iters_max": int(st.krylov_iters.max()), "converged": int(st.converged.sum()), "pmg": st.pmg}
+    # training pairs from the plain cycle at the converged state: right-hand sides of the next load
+    # increment (the residual at load 1.1 from the lifted predictor) and a seeded N(0, 1) vector
+    t1 = time.perf_counter()
+    mf = op.allocate_jacobian(x)
+    ls = _batch_solver(U2, U1, args.batch_precision)
+    from hfk import solvers as S
+
+    dv = torch.as_tensor(g, device="cuda")
+    mf.prepare(x, dv)
+    ns = S.numerical_setup(ls, mf)
+    r = torch.zeros_like(x)
+    op.residual(r, x + 0.1 * torch.as_tensor(lift, device="cuda"), 1.1 * dv)
+    rhs = [-r, torch.as_tensor(np.random.default_rng(11).standard_normal(U2.nfree), device="cuda")]
+    feats, targets = [], []
+    for b in rhs:
+        f, t = learned.collect_samples(ns.prec, mf, b, cycles=2)
+        feats.append(f)
+        targets.append(t)
+    del ns
+    feats, targets = torch.cat(feats), torch.cat(targets)
+    net = learned.MLP(seed=4)
+    loss = net.train(feats, targets, steps=3000, batch=8192, lr=1e-3)
+    t_train = time.perf_counter() - t1
+    del feats, targets
+    holder = {}
+
+    def attach(ns):
+        learned.attach(ns.prec, net)
+        holder["prec"] = ns.prec
+
+    x2, st2 = B.newton_solve_batched(op, _batch_solver(U2, U1, args.batch_precision), g, BATCH_LOADS, lift=lift,
+                                     on_setup=attach)
+    acc = learned.stats(holder["prec"]) if "prec" in holder else {}
+    lrn = {"seconds": st2.seconds, "newton_sweeps": st2.newton_sweeps, "krylov_sweeps": int(sum(st2.krylov_sweeps)),
+           "newton_iters_mean": float(st2.newton_iters.mean()), "krylov_iters_mean": float(st2.krylov_iters.mean()),
+           "krylov_iters_max": int(st2.krylov_iters.max()), "converged": int(st2.converged.sum()),
+           "corrections": acc, "train_seconds": t_train, "train_loss": loss,
+           "solution_rel_diff_vs_plain": float(torch.linalg.norm(x2 - x) / torch.linalg.norm(x))}
+    cpu = None if args.no_cpu else batch_cpu_sample(problems)
+    line = {"metric": f"seconds to 1e-8 for {args.batch_count} batched SVK Q2 Newton solves (plain p-MG)",
+            "value": plain["seconds"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": plain["seconds"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "f64 outer / f32 cycle",
+            "data": "synthetic",
+            "config": {"workload": "batched Newton, SVK Q2 cubes n ~ U{8..24}, (lambda, mu) log-uniform, seed 4",
+                       "problems": args.batch_count, "free_dofs": U2.nfree, "coarse_free_dofs": U1.nfree,
+                       "cells": U2.mesh.ncells, "loads": list(BATCH_LOADS), "setup_seconds": t_setup,
+                       "levels": "Q2 -> Q1 (Chebyshev 4; coarse: 20 block-Jacobi CG steps per problem)",
+                       "precision": args.batch_precision},
+            "clocks": clocks.summary(), "plain": plain, "learned": lrn,
+            "gain_learned_vs_plain": plain["seconds"] / lrn["seconds"]}
+    if cpu is not None:
+        est = cpu["seconds_per_free_dof"] * U2.nfree
+        line["cpu_baseline"] = {"value": est, "unit": "s (extrapolated by free dofs)", "cores": cpu["cores"],
+                                "kind": cpu["kind"], "sample": cpu["sample"]}
+    print(json.dumps(line))
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         reference(a)
+    elif a.batch:
+        batch_main(a)
     else:
         engine(a)

@@ -1245,7 +1245,7 @@ struct hfk_pmg {
   double t_potrf = 0;
   // learned correction after each cycle (null = plain cycle) and its work buffers
   hfk_mlp* mlp = nullptr;
-  DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_u, ml_scal;  // ml_scal: 8 per segment
+  DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_scal;  // ml_scal: 8 per segment
   DBuf<float> ml_feats, ml_out, ml_loglm;                    // ml_loglm: log lambda, log mu per segment
   DBuf<int> ml_accepted;
   int64_t ml_tried = 0;
@@ -1507,15 +1507,14 @@ int mlp_prepare_features(hfk_pmg* m, const double* r, const double* y) {
   return nb;
 }
 
-// y += delta = MLP(features) in every segment where that reduces the residual |r - A y| (the
-// acceptance rule, applied per segment)
+// y += omega delta, delta = MLP(features), with the per-segment step omega that minimises the energy
+// error of y along delta (omega = 0, the plain cycle, where delta is not a descent direction)
 void mlp_correct(hfk_pmg* m, const double* r, double* y) {
   hfk_problem* p = m->lv[0];
   const int64_t n = p->nfree;
   const int nb = mlp_prepare_features(m, r, y);
   m->ml_out.resize((size_t)nb * MLP_OUT);
   m->ml_delta.resize(n);
-  m->ml_u.resize(n);
   static bool attr = false;
   if (!attr) {
     HFK_CUDA(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1530,13 +1529,11 @@ void mlp_correct(hfk_pmg* m, const double* r, double* y) {
                                                            8, m->ml_delta.p);
   check_launch(p);
   mf_apply_dev(p, m->ml_delta.p, m->ml_q.p);
-  axpbyz_kernel<double><<<vec_grid(n), 256, 0, p->stream>>>(n, 1.0, m->ml_s.p, -1.0, m->ml_q.p, m->ml_u.p);
-  check_launch(p);
-  seg_dots<double>(p, 1, m->ml_scal.p + 5, 8, m->ml_u.p, m->ml_u.p);
+  seg_dots<double>(p, 2, m->ml_scal.p + 5, 8, m->ml_delta.p, m->ml_s.p, m->ml_delta.p, m->ml_q.p);
   m->ml_accepted.resize(1);
-  mlp_accept_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg_dof_map(p), m->ml_scal.p + 4, 8, m->ml_delta.p, y);
+  mlp_accept_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg_dof_map(p), m->ml_scal.p + 5, 8, m->ml_delta.p, y);
   check_launch(p);
-  mlp_accept_count_kernel<<<1, 256, 0, p->stream>>>(p->nseg, m->ml_scal.p + 4, 8, m->ml_accepted.p);
+  mlp_accept_count_kernel<<<1, 256, 0, p->stream>>>(p->nseg, m->ml_scal.p + 5, 8, m->ml_accepted.p);
   check_launch(p);
   m->ml_tried += p->nseg;
 }

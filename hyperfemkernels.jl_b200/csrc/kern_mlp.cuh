@@ -6,7 +6,8 @@
 // block-Jacobi preconditioned value (B_n^-1 s)_n (3), the residual entering the V-cycle r_n (3), the
 // V-cycle output y_n (3), log lambda, log mu; each vector group scaled by its RMS over the nodes
 // (scales passed in, so the network sees O(1) inputs). Target: the remaining error e_n = (A^-1 s)_n
-// in the same scale as (B^-1 s).
+// in the scale of the cycle's output y (what the cycle left undone, relative to what it did: for the
+// smooth modes that the coarse solve reduces only in part, e is close to a local multiple of y).
 #pragma once
 #include <cuda_bf16.h>
 
@@ -228,7 +229,7 @@ __global__ void mlp_features_kernel(int nb, const int32_t* dofs, const int32_t* 
 __global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* segb, const float* out,
                                    const double* scales, int sstride, double* delta) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-    const double sc = scales[(size_t)(segb ? segb[b] : 0) * sstride + 1];
+    const double sc = scales[(size_t)(segb ? segb[b] : 0) * sstride + 3];
     for (int i = 0; i < 3; ++i) {
       const int d = dofs[3 * b + i];
       if (d) delta[d - 1] = (double)out[(size_t)b * MLP_OUT + i] * sc;
@@ -238,7 +239,7 @@ __global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* s
 __global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* e,
                                    const double* scales, int sstride, float* t) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-    const double s1 = scales[(size_t)(segb ? segb[b] : 0) * sstride + 1];
+    const double s1 = scales[(size_t)(segb ? segb[b] : 0) * sstride + 3];
     const double sc = s1 > 0 ? 1.0 / s1 : 0.0;
     for (int i = 0; i < 3; ++i) {
       const int d = dofs[3 * b + i];
@@ -246,22 +247,25 @@ __global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* s
     }
   }
 }
-// y += delta in the segments where the corrected residual is smaller: nrm[seg * stride] = |s|^2,
-// nrm[seg * stride + 1] = |s - A delta|^2
+// y += omega delta per segment, omega = (delta . s) / (delta . A delta) when both are positive, else 0:
+// the step along delta that minimises the energy (A-norm) error of y, the norm the outer CG
+// minimises (a residual-norm test would reject any prediction with small high-frequency noise).
+// c = nrm + seg * stride: c[0] = delta . s, c[1] = delta . A delta.
+__device__ __forceinline__ double mlp_step(const double* c) { return (c[0] > 0 && c[1] > 0) ? c[0] / c[1] : 0.0; }
 __global__ void mlp_accept_kernel(int64_t n, const int32_t* seg, const double* nrm, int stride, const double* delta,
                                   double* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double* c = nrm + (size_t)(seg ? seg[i] : 0) * stride;
-    if (c[1] < c[0]) y[i] += delta[i];
+    const double w = mlp_step(nrm + (size_t)(seg ? seg[i] : 0) * stride);
+    if (w > 0) y[i] += w * delta[i];
   }
 }
-// one CTA: *accepted += the number of segments whose correction was kept
+// one CTA: *accepted += the number of segments with a positive step
 __global__ void mlp_accept_count_kernel(int nseg, const double* nrm, int stride, int* accepted) {
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
   int mine = 0;
-  for (int s = threadIdx.x; s < nseg; s += blockDim.x) mine += nrm[(size_t)s * stride + 1] < nrm[(size_t)s * stride];
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) mine += mlp_step(nrm + (size_t)s * stride) > 0;
   atomicAdd(&cnt, mine);
   __syncthreads();
   if (threadIdx.x == 0) *accepted += cnt;

@@ -147,13 +147,17 @@ class BatchedNewtonStats:
 
 
 def newton_solve_batched(op, solver: S.MatrixFreeSolver, g_full: np.ndarray, loads, x0=None, *, rtol_newton=1e-8,
-                         atol_newton=1e-12, max_newton=20):
+                         atol_newton=1e-12, max_newton=20, lift=None, on_setup=None):
     """Newton with load stepping on every problem of a batched operator at once.
 
     The per-problem algorithm is the one of ``newton_solve`` (the reference's Newton loop,
     ``test/solvers/test_pmultigrid.jl:86-115``): per problem, Newton stops when
     ||R_s|| <= max(rtol_newton ||R_s,0||, atol_newton). Problems that have converged get a zero
     right-hand side (their Krylov solve stops at once) while the others continue.
+    ``lift`` (free dofs, at load factor 1): a field that carries the Dirichlet data into the
+    interior; each load step starts from x + (load increment) * lift instead of x, which keeps the
+    first iterate of a step free of a strain jump at the loaded boundary (``newton_solve``'s
+    ``lift``). ``on_setup(ns)`` is called once the solver's numerical set-up exists.
     """
     import torch
 
@@ -169,10 +173,15 @@ def newton_solve_batched(op, solver: S.MatrixFreeSolver, g_full: np.ndarray, loa
     ns = None
     st = BatchedNewtonStats(newton_iters=np.zeros(k, dtype=np.int64), krylov_iters=np.zeros(k, dtype=np.int64),
                             converged=np.ones(k, dtype=bool))
+    lift_d = None if lift is None else torch.as_tensor(np.ascontiguousarray(lift, dtype=float), device=dev)
+    prev = 0.0
     t0 = time.perf_counter()
     for lam in loads:
         U.dirichlet_values = np.ascontiguousarray(lam * g_full)
         dv = torch.as_tensor(U.dirichlet_values, device=dev)
+        if lift_d is not None:
+            x += (lam - prev) * lift_d
+        prev = lam
         st.load_steps += 1
         r0 = None
         for it in range(max_newton):
@@ -187,6 +196,8 @@ def newton_solve_batched(op, solver: S.MatrixFreeSolver, g_full: np.ndarray, loa
             mf.prepare(x, dv)
             if ns is None:
                 ns = S.numerical_setup(S.symbolic_setup(solver, mf), mf)
+                if on_setup is not None:
+                    on_setup(ns)
             else:
                 S.numerical_setup_update(ns, mf)
             dx.zero_()
@@ -227,6 +238,13 @@ def draw_batch(count=256, nmin=8, nmax=24, lam_range=(0.5, 20.0), mu_range=(0.2,
     lam = np.exp(rng.uniform(np.log(lam_range[0]), np.log(lam_range[1]), size=count))
     mu = np.exp(rng.uniform(np.log(mu_range[0]), np.log(mu_range[1]), size=count))
     return [BatchProblem(int(a), float(b), float(c)) for a, b, c in zip(ns, lam, mu)]
+
+
+def cube_lifting(union, displacement=0.05):
+    """Free-dof values of u = displacement * x e_x on every problem of ``union`` (the affine field
+    that matches ``cube_batch``'s Dirichlet data at load factor 1)."""
+    f = lambda X: np.column_stack([displacement * X[:, 0], 0 * X[:, 1], 0 * X[:, 2]])
+    return np.concatenate([V.interpolate(f)[0] for V in union.spaces])
 
 
 def cube_batch(problems, orders=(2, 1), displacement=0.05):

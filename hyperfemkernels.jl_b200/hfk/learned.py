@@ -2,8 +2,9 @@
 
 A per-node MLP (16 -> 64 -> 64 -> 3, BF16 weights, FP32 accumulation; ``libhfk`` kernels for the
 forward pass, the gradient and Adam) predicts the error left by the plain V-cycle from local
-features of the residual. Inside the cycle the prediction is added only if it lowers the FP64
-residual, so the plain cycle remains the fallback (``hfk_pmg_set_mlp``). Training pairs come from
+features of the residual. Inside the cycle the prediction delta is added with the per-problem step
+that minimises the energy error along it (zero when delta is not a descent direction), so the plain
+cycle remains the fallback (``hfk_pmg_set_mlp``). Training pairs come from
 the plain cycle on seeded states (``hfk_pmg_mlp_sample``: target = the exact remaining error).
 """
 from __future__ import annotations

@@ -30,11 +30,14 @@ class NewtonStats:
 
 
 def newton_solve(op: KernelOperator, solver: S.MatrixFreeSolver, g_full: np.ndarray, loads, x0=None, *,
-                 rtol_newton=1e-8, atol_newton=1e-12, max_newton=20, device=True):
+                 rtol_newton=1e-8, atol_newton=1e-12, max_newton=20, device=True, lift=None):
     """Solve R(x; load * g_full) = 0 for each load factor in ``loads`` (continuation from the previous one).
 
     ``g_full`` are the Dirichlet values at load factor 1. Returns (x, NewtonStats). Newton stops when
     ||R|| <= max(rtol_newton * ||R_0||, atol_newton), R_0 the residual at the first iterate of the step.
+    ``lift`` (free dofs, at load factor 1): a field that carries the Dirichlet data into the interior;
+    each load step then starts from x + (load increment) * lift (no strain jump at the loaded
+    boundary in the step's first tangent). None keeps x, as the reference's loop does.
     """
     import torch
 
@@ -47,10 +50,15 @@ def newton_solve(op: KernelOperator, solver: S.MatrixFreeSolver, g_full: np.ndar
     mf = op.allocate_jacobian(x)
     ns = None
     st = NewtonStats()
+    lift_d = None if lift is None else torch.as_tensor(np.ascontiguousarray(lift, dtype=float), device=dev)
+    prev = 0.0
     t0 = time.perf_counter()
     for lam in loads:
         U.dirichlet_values = np.ascontiguousarray(lam * g_full)
         dv = torch.as_tensor(U.dirichlet_values, device=dev)
+        if lift_d is not None:
+            x += (lam - prev) * lift_d
+        prev = lam
         st.load_steps += 1
         r0 = None
         for it in range(max_newton):

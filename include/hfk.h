@@ -214,8 +214,10 @@ int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters);
 
 /* ---- learned correction (no counterpart in the reference) ------------------------------------
  * A per-node MLP (16 -> 64 -> 64 -> 3, tanh, BF16 weights read by the forward pass, FP32 master
- * weights, FP32 accumulation) whose output, scaled, is added to the V-cycle's result after each cycle
- * only if it reduces the FP64 residual |r - A y| (the plain cycle stays the fallback). Features per
+ * weights, FP32 accumulation) whose output delta, scaled, is added to the V-cycle's result y after
+ * each cycle with the step omega = (delta . s) / (delta . A delta) per segment (s = r - A y), the
+ * step that minimises the energy error of y along delta; omega = 0 (the plain cycle) when delta is
+ * not a descent direction. Features per
  * node: residual after the cycle s, its block-Jacobi value, the cycle's input r and output y (each
  * group scaled by its RMS), log lambda, log mu. Training pairs (features, remaining error A^-1 s)
  * come from the plain cycle (hfk_pmg_mlp_sample); training is Adam on the GPU (hfk_mlp_train). */
