@@ -281,12 +281,10 @@ void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R
 // GPU, then one launch over all cells with atomicAdd (an order-dependent last bit). A colour needs
 // about 4 warps per SM to hide the gather latency.
 bool use_atomic_scatter(const hfk_problem* p) {
-  if (p->scatter == HFK_SCATTER_COLOURED) return false;
-  if (p->scatter == HFK_SCATTER_ATOMIC) return true;
-  const int m = std::max(p->Q, p->P);
-  const int cpw = m > 0 ? std::max(1, 32 / (m * m)) : 1;
-  const int64_t per_colour = p->ncolors ? p->ncells / p->ncolors : p->ncells;
-  return per_colour < (int64_t)sm_count() * 4 * cpw;
+  // AUTO scatters with atomics: one launch instead of one per colour (no wave tails, no launch
+  // gaps), and a fire-and-forget reduction in L2 instead of a dependent read of y before the
+  // write (measured on B200, Q2 64^3 J*v: 0.55 ms against 0.75 ms by colour)
+  return p->scatter != HFK_SCATTER_COLOURED;
 }
 
 template <int MODE, typename R>

@@ -66,11 +66,11 @@ __host__ __device__ constexpr size_t cell_region_bytes() {
   return raw;
 }
 
-// resident CTAs per SM the register allocation of a mode targets (measured on B200: the stored
-// formulation prefers fewer, larger register files; the recompute product more warps)
+// resident CTAs per SM the register allocation of a mode targets (measured on B200 with the atomic
+// scatter: the stored formulation prefers 2, the recompute product 3 (no spills) over 4)
 template <int MODE>
 constexpr int cell_min_blocks() {
-  return MODE == MODE_JV_STORED ? 2 : (MODE == MODE_JV ? 4 : 3);
+  return MODE == MODE_JV_STORED ? 2 : 3;
 }
 
 template <typename R>

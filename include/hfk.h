@@ -77,8 +77,9 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
 /* Scatter of the sum-factorised kernels (residual, products): colour by colour with plain
  * read-modify-writes (deterministic, the reference's race-free colouring, src/coloring.jl:1-3), or
  * one launch over all cells with FP64 atomics (the summation order, hence the last bit, varies
- * between runs). AUTO (default) colours unless the colours are too small to fill the GPU. The
- * assembled Jacobian and the nodal blocks always scatter by colour. */
+ * between runs). AUTO (default) is the atomic scatter (faster on B200: one launch, no read of the
+ * output before the write); COLOURED gives bit-reproducible results. The assembled Jacobian and the
+ * nodal blocks always scatter by colour. */
 #define HFK_SCATTER_AUTO 0
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2
