@@ -115,11 +115,12 @@ class ClockSampler:
 
 
 def jv_flops_per_cell(Q, P):
-    """FP64 flops of one recompute J*v cell: 6 interpolations, 3 contractions, pointwise law."""
+    """FP64 flops of one recompute J*v cell: 3 interpolations (the components of dx), 3
+    contractions, the pointwise law (F is stored, not interpolated)."""
     interp = 2 * (2 * P * Q**3 + 3 * P**2 * Q**2 + 3 * P**3 * Q)  # x, y, z sweeps (FMA = 2)
     contract = 2 * (3 * P**3 * Q + 3 * P**2 * Q**2 + 2 * P * Q**3)
     pointwise = P**3 * (2 * (27 + 27 + 18 + 27 + 27 + 27 + 27) + 60)  # grads, F'F, F'Hd, Hd S, F W, pull-back
-    return 6 * interp + 3 * contract + pointwise
+    return 3 * interp + 3 * contract + pointwise
 
 
 def engine(args):
@@ -234,6 +235,7 @@ def engine(args):
         err32 = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
         extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
         extra.update(assembly_case(torch, dev, stream, timed))
+        extra.update(jv_sizes_case(torch, dev, stream, timed))
         extra.update(newton_case())
 
     cpu = cpu_baseline_sample() if rank == 0 and not args.no_cpu else None
@@ -253,6 +255,42 @@ def engine(args):
         dist.destroy_process_group()
 
 
+def jv_sizes_case(torch, dev, stream, timed, cases=((2, 48), (4, 48), (4, 64))):
+    """Secondary: the other C1 sizes (Q2 48^3, Q4 48^3 and 64^3; Q4 with Gauss 5^3), FP64 and FP32
+    recompute J*v, same law, state and increment as the headline."""
+    from hfk import _lib, forms
+    from hfk.operator import KernelOperator, MatrixFreeJacobian
+
+    out = {}
+    for order, n in cases:
+        V, x, dx = build_case(n, order)
+        deg = 2 * order
+        op = KernelOperator(forms.svk_residual(2.0, 1.0, deg), forms.svk_jacobian(2.0, 1.0, deg), V,
+                            jacobian="matrixfree")
+        op.problem.set_stream(stream.cuda_stream)
+        xd = torch.from_numpy(x).to(dev)
+        dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+        dxd = torch.from_numpy(dx).to(dev)
+        yd = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
+        mf = MatrixFreeJacobian(op, "recompute")
+        mf.prepare(xd, dd)
+        h = op.problem.h
+        steps = 20 if order == 4 else 50
+        ms64 = timed(lambda: _lib.call("hfk_mf_apply", h, _lib.ptr(dxd), _lib.ptr(yd)), steps, 3) / steps
+        dx32, y32 = dxd.float(), torch.zeros(V.nfree, dtype=torch.float32, device=dev)
+        ms32 = timed(lambda: _lib.call("hfk_mf_apply_f32", h, _lib.ptr(dx32, np.float32), _lib.ptr(y32, np.float32)),
+                     steps, 3) / steps
+        err = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
+        Q, P = order + 1, order + 1
+        flops = jv_flops_per_cell(Q, P) * V.mesh.ncells
+        out[f"jv_q{order}_{n}"] = {"free_dofs": V.nfree, "fp64_ms": ms64, "fp64_gdofs": V.nfree / (ms64 * 1e-3) / 1e9,
+                                   "fp64_tflops": flops / (ms64 * 1e-3) / 1e12, "fp32_ms": ms32,
+                                   "fp32_gdofs": V.nfree / (ms32 * 1e-3) / 1e9, "fp32_rel_err": err}
+        del op, mf, xd, dxd, yd, dx32, y32
+        torch.cuda.empty_cache()
+    return out
+
+
 def assembly_case(torch, dev, stream, timed):
     """Secondary: Q2 SVK 20x10x10 residual + CSC Jacobian (the reference's CPU-runnable case)."""
     from hfk import _lib, forms
@@ -261,7 +299,7 @@ def assembly_case(torch, dev, stream, timed):
 
     m = CartesianMesh((20, 10, 10))
     g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
-    V = VectorLagrangeSpace(m, 2, ("x0", "x1"), g=g)
+    V = VectorLagrangeSpace(m, 2, ("x0", "x1"), g=g, open_faces=True)  # Gridap face tags: 52 077 free dofs
     rng = np.random.default_rng(0)
     x, _ = V.interpolate(lambda p: np.stack([0.05 * p[:, 0], 0 * p[:, 0], 0 * p[:, 0]], axis=1))
     x = x + rng.uniform(-1e-3, 1e-3, V.nfree)

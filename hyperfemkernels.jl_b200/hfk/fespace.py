@@ -203,12 +203,14 @@ class VectorLagrangeSpace:
     ``dirichlet`` lists the closed faces ("x0", "x1", ...; "boundary" = all six) on which every
     component is fixed; a face includes its edges and vertices (the closed Dirichlet set that
     the p-multigrid transfers need, HyperFEMKernels ``src/transfers.jl:188-207``).
+    ``open_faces=True`` fixes only the faces' interiors, as Gridap's face tags do (the assembly
+    benchmark's setting, ``test/solvers/test_transfers.jl:10-12``).
     ``g`` gives the Dirichlet values: a callable x (m x 3) -> (m x 3), or one callable per face
     in ``dirichlet`` order (later faces win on shared edges).
     """
 
     def __init__(self, mesh: CartesianMesh, order: int, dirichlet: Sequence[str] = ("x0", "x1"),
-                 g=None):
+                 g=None, open_faces: bool = False):
         self.mesh = mesh
         self.order = p = int(order)
         self.Q = p + 1
@@ -229,6 +231,12 @@ class VectorLagrangeSpace:
         face_of = np.full(nnodes, -1)
         sel = {"x0": gi == 0, "x1": gi == self.NX - 1, "y0": gj == 0, "y1": gj == self.NY - 1,
                "z0": gk == 0, "z1": gk == self.NZ - 1}
+        if open_faces:
+            # Gridap's face tags: the interior of the face, without its edges and vertices
+            inner = {"x": (gj > 0) & (gj < self.NY - 1) & (gk > 0) & (gk < self.NZ - 1),
+                     "y": (gi > 0) & (gi < self.NX - 1) & (gk > 0) & (gk < self.NZ - 1),
+                     "z": (gi > 0) & (gi < self.NX - 1) & (gj > 0) & (gj < self.NY - 1)}
+            sel = {f: m & inner[f[0]] for f, m in sel.items()}
         for f_idx, f in enumerate(self.dirichlet_faces):
             if f not in sel:
                 raise ValueError(f"HyperFEMKernels: unknown face {f!r}")

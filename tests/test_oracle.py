@@ -316,3 +316,12 @@ def test_oracle_mlp_gradient_matches_finite_differences():
         fd = (loss(w + e) - loss(w - e)) / 2e-6
         assert abs(g[i] - fd) <= 1e-6 * max(1.0, abs(fd))
     assert np.array_equal(O.bf16_round(np.float32([1.0, 1.00390625, -2.5])), np.float32([1.0, 1.0, -2.5]))
+
+
+def test_open_face_dirichlet_counts_of_the_assembly_case():
+    # Gridap's face tags fix the face interiors only: Q2 20x10x10 with x0/x1 has 41*21*21 nodes,
+    # 2*19*19 fixed nodes, 52 077 free dofs (the assembly benchmark's setting)
+    V = VectorLagrangeSpace(CartesianMesh((20, 10, 10)), 2, ("x0", "x1"), open_faces=True)
+    assert (V.nfree, V.ndir) == (52077, 2166)
+    Vc = VectorLagrangeSpace(CartesianMesh((20, 10, 10)), 2, ("x0", "x1"))
+    assert Vc.ndir == 2 * 21 * 21 * 3
