@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -229,6 +230,9 @@ CellData cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) 
   cd.lam = p->params[0];
   cd.mu = p->params[1];
   cd.cell_lm = p->cell_lm.p;
+  const bool masked = p->seg_active && p->cell_seg.p;
+  cd.cell_seg = masked ? p->cell_seg.p : nullptr;
+  cd.seg_active = masked ? p->seg_active : nullptr;
   for (int c = 0; c < 3; ++c) cd.body[c] = p->params[2 + c];
   return cd;
 }
@@ -621,18 +625,24 @@ void blocks_update_dev(hfk_problem* p, int* ok) {
     return;
   }
   p->B.zero(p->stream);
-  BlockIO io{p->x.p, p->dvals.p, p->dNt.p, p->block_of.p, p->B.p, p->np, p->nn};
+  BlockIO io{p->x.p, p->dvals.p, p->dNt.p, p->block_of.p, p->B.p, p->np, p->nn, 0};
   const size_t smem = ((size_t)3 * p->nn + 9 * p->np + 9 * p->np + p->np + 81 * p->np) * sizeof(double);
   static size_t attr = 0;
   if (smem > attr) {
     HFK_CUDA(cudaFuncSetAttribute(blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = smem;
   }
-  for (int c = 0; c < p->ncolors; ++c) {
-    const int n = p->color_start[c + 1] - p->color_start[c];
-    if (!n) continue;
-    blocks_kernel<<<n, 256, smem, p->stream>>>(cell_data(p, p->cells_by_color.p + p->color_start[c], n), io);
+  if (use_atomic_scatter(p)) {  // one launch over all cells, atomic accumulation of the blocks
+    io.atomic = 1;
+    blocks_kernel<<<p->ncells, 256, smem, p->stream>>>(cell_data(p, nullptr, p->ncells), io);
     check_launch(p);
+  } else {
+    for (int c = 0; c < p->ncolors; ++c) {
+      const int n = p->color_start[c + 1] - p->color_start[c];
+      if (!n) continue;
+      blocks_kernel<<<n, 256, smem, p->stream>>>(cell_data(p, p->cells_by_color.p + p->color_start[c], n), io);
+      check_launch(p);
+    }
   }
   p->flag.resize(1);
   p->flag.zero(p->stream);
@@ -2040,10 +2050,12 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
     m->tr.push_back(transfers[l]);
     require_tp(levels[l]);
   }
-  // one stream for the whole hierarchy: the V-cycle moves data between levels
+  // one stream for the whole hierarchy: the V-cycle moves data between levels; with batched
+  // problems the levels also read the working level's segment flags
   for (int l = 1; l < nlevels; ++l) {
     HFK_CUDA(cudaStreamSynchronize(levels[l]->stream));
     levels[l]->stream = levels[0]->stream;
+    if (levels[l]->seg_active && levels[0]->seg_active) levels[l]->seg_active = levels[0]->seg_active;
   }
   m->degree = degree;
   m->range = range;
@@ -2093,8 +2105,11 @@ int hfk_pmg_destroy(hfk_pmg* m) {
   HFK_API_BEGIN
   if (m) {
     cudaStreamSynchronize(m->lv[0]->stream);
-    // the coarser levels go back to their own streams (levels must outlive their hierarchy)
-    for (int l = 1; l < m->L; ++l) m->lv[l]->stream = m->lv[l]->own_stream;
+    // the coarser levels go back to their own streams and flags (levels must outlive their hierarchy)
+    for (int l = 1; l < m->L; ++l) {
+      m->lv[l]->stream = m->lv[l]->own_stream;
+      if (m->lv[l]->seg_active) m->lv[l]->seg_active = m->lv[l]->seg_active_own.p;
+    }
     if (m->solver) cusolverDnDestroy(m->solver);
     if (m->blas) cublasDestroy(m->blas);
     pmg_drop_graph(m);
@@ -2435,6 +2450,19 @@ void solve_cg_seg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x
   seg_dots<double>(op, 2, sc + S_BB, SEG_NS, bd, bd, r.p, r.p);
   seg_cg_init_kernel<<<1, 256, 0, s>>>(ns, sc, fl, rtol, atol, cw.cnt.p);
   check_launch(op);
+  // the cell kernels of every level skip the problems that are not active (the flags are shared
+  // with the hierarchy's levels); every flag is set back to 1 when the solve ends
+  int32_t* mask = op->seg_active;
+  auto set_mask = [&](int value) {
+    if (mask) seg_mask_kernel<<<sg, 256, 0, s>>>(ns, fl, mask, value);
+  };
+  struct MaskReset {
+    std::function<void()> f;
+    ~MaskReset() { f(); }
+  } mask_reset{[&]() {
+    if (mask) seg_mask_kernel<<<sg, 256, 0, s>>>(ns, fl, mask, 1);
+  }};
+  set_mask(-1);
   int nact = active_count();
   int it = 0;
   auto apply_prec = [&](const double* in, double* outp) {
@@ -2456,6 +2484,7 @@ void solve_cg_seg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x
       seg_dots<double>(op, 1, sc + S_RR, SEG_NS, r.p, r.p);
       seg_cg_check_kernel<<<1, 256, 0, s>>>(ns, sc, fl, cw.cnt.p);
       check_launch(op);
+      set_mask(-1);
       if (active_count() == 0) break;
       apply_prec(r.p, z.p);
       if (flexible) seg_dots<double>(op, 2, sc + S_ZR, SEG_NS, z.p, r.p, z.p, rold.p);
@@ -2466,7 +2495,8 @@ void solve_cg_seg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x
       check_launch(op);
     }
   }
-  // true residual check per segment (src/solvers.jl:150-157)
+  // true residual check per segment (src/solvers.jl:150-157), on every problem
+  set_mask(1);
   mf_apply_dev(op, xd, q.p);
   axpbyz_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, bd, -1.0, q.p, r.p);
   check_launch(op);
@@ -2551,6 +2581,19 @@ int hfk_problem_set_segments(hfk_problem* p, int nseg, const int64_t* dof_off, c
   } else {
     p->seg_of_dof.release();
     p->seg_of_block.release();
+  }
+  if (nseg > 1 && cell_off) {
+    std::vector<int32_t> cs(std::max(p->ncells, 1), 0);
+    for (int s = 0; s < nseg; ++s)
+      for (int32_t c = cell_off[s]; c < cell_off[s + 1]; ++c) cs[c] = s;
+    p->cell_seg.upload(cs.data(), cs.size(), p->stream);
+    std::vector<int32_t> ones(nseg, 1);
+    p->seg_active_own.upload(ones.data(), ones.size(), p->stream);
+    p->seg_active = p->seg_active_own.p;
+  } else {
+    p->cell_seg.release();
+    p->seg_active_own.release();
+    p->seg_active = nullptr;
   }
   if (params) {
     p->seg_lm.assign(params, params + 2 * (size_t)nseg);

@@ -83,8 +83,13 @@ struct CellData {
   int law;                // HFK_LAW_*
   double lam, mu, body[3];
   const double* cell_lm;  // optional (2, ncells): lambda, mu per cell (batched problems), else lam, mu
+  // batched problems: the cell kernels skip the cells of segments whose flag is 0 (problems that
+  // have converged inside a batched solve; all flags are 1 outside one). nullptr: no masking.
+  const int32_t* cell_seg;    // per cell its segment
+  const int32_t* seg_active;  // per segment 1 = compute, 0 = skip
   __host__ __device__ double lam_of(int cell) const { return cell_lm ? cell_lm[2 * (size_t)cell] : lam; }
   __host__ __device__ double mu_of(int cell) const { return cell_lm ? cell_lm[2 * (size_t)cell + 1] : mu; }
+  __host__ __device__ bool skipped(int cell) const { return seg_active && !seg_active[cell_seg[cell]]; }
 };
 
 // Work of the two-stage reductions (partial sums and the result)
@@ -142,6 +147,9 @@ struct hfk_problem {
   hfk::DBuf<int32_t> item_first;          // nseg + 1: the first chunk of each segment
   hfk::DBuf<int64_t> seg_off_d;           // device copy of seg_off
   hfk::DBuf<double> seg_partial;          // per-chunk partial sums (3 per chunk)
+  hfk::DBuf<int32_t> cell_seg;            // per cell its segment (nseg > 1 with cell ranges)
+  hfk::DBuf<int32_t> seg_active_own;      // per segment: 1 = the cell kernels compute its cells
+  int32_t* seg_active = nullptr;          // the flags the kernels read: own, or the working level's
   int nitems = 0;
   bool items_built = false;
   // colours

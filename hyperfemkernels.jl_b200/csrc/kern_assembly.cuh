@@ -62,8 +62,8 @@ __device__ void asm_point_phase(const CellData& cd, const AsmIO& io, int cell, c
   // per (point, c, k): the 3x3 block of Dh
   for (int e = threadIdx.x; e < np * 9; e += blockDim.x) {
     const int q = e / 9, ck = e % 9, c = ck / 3, k = ck % 3;
-    double T[81];
-    law_tangent(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, T);
+    double Tb[9];  // T[(c,J),(k,L)] at Tb[J + 3 L]
+    law_tangent_block(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, c, k, Tb);
     const double* iJ = iJs + q * 9;
     const double dV = dVs[q];
     // X[J][K'] = sum_L T[(c,J),(k,L)] iJ[L + 3K']
@@ -71,7 +71,7 @@ __device__ void asm_point_phase(const CellData& cd, const AsmIO& io, int cell, c
     for (int J = 0; J < 3; ++J)
       for (int Kp = 0; Kp < 3; ++Kp) {
         double s = 0;
-        for (int L = 0; L < 3; ++L) s += T[(c * 3 + J) + 9 * (k * 3 + L)] * iJ[L + 3 * Kp];
+        for (int L = 0; L < 3; ++L) s += Tb[J + 3 * L] * iJ[L + 3 * Kp];
         X[J][Kp] = s;
       }
     for (int K = 0; K < 3; ++K)

@@ -109,8 +109,9 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
   int32_t* sid = reinterpret_cast<int32_t*>(yr + L::VALS);
 
   const int list_index = (blockIdx.x * nwarps + warp) * CPW + (active ? slot : 0);
-  const bool has_cell = active && list_index < cd.ncells_list;
-  const int cell = has_cell ? (cd.cells ? cd.cells[list_index] : list_index) : 0;
+  const int cell = active && list_index < cd.ncells_list ? (cd.cells ? cd.cells[list_index] : list_index) : 0;
+  const bool has_cell = active && list_index < cd.ncells_list && !cd.skipped(cell);
+  if (__all_sync(0xffffffffu, !has_cell)) return;  // a warp without work (only __syncwarp below)
   const R lam_c = (R)cd.lam_of(cell), mu_c = (R)cd.mu_of(cell);
 
   // ---- gather (gather_cell!, src/assembly.jl:1060-1070; increments are zero at Dirichlet dofs) ----

@@ -181,6 +181,12 @@ __global__ void seg_xpby_kernel(int64_t n, const int32_t* seg, const double* sc,
     p[i] = z[i] + sc[(size_t)seg_at(seg, i) * SEG_NS + slot] * p[i];
 }
 
+// the cell kernels' segment flags from a batched solve's flags (value = -1: set every flag to 1)
+__global__ void seg_mask_kernel(int nseg, const int* fl, int32_t* mask, int value) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+    mask[s] = value < 0 ? fl[(size_t)s * SEG_NF + F_ACTIVE] : value;
+}
+
 // x[i] *= f[seg(i)]
 __global__ void seg_mul_kernel(int64_t n, const int32_t* seg, const double* f, double* x) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

@@ -96,6 +96,7 @@ struct BlockIO {
   const int32_t* block_of; // (nn, ncells)
   double* B;               // (9, nblocks)
   int np, nn;
+  int atomic;              // 1: atomicAdd into B (all cells in one launch)
 };
 
 __global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
@@ -145,14 +146,14 @@ __global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
   __syncthreads();
   for (int e = threadIdx.x; e < np * 9; e += blockDim.x) {
     const int q = e / 9, ck = e % 9, c = ck / 3, k = ck % 3;
-    double T[81];
-    law_tangent(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, T);
+    double Tb[9];  // T[(c,J),(k,L)] at Tb[J + 3 L]
+    law_tangent_block(cd.law, cd.lam_of(cell), cd.mu_of(cell), Hs + q * 9, c, k, Tb);
     const double* iJ = iJs + q * 9;
     double X[3][3];
     for (int J = 0; J < 3; ++J)
       for (int Kp = 0; Kp < 3; ++Kp) {
         double s = 0;
-        for (int L = 0; L < 3; ++L) s += T[(c * 3 + J) + 9 * (k * 3 + L)] * iJ[L + 3 * Kp];
+        for (int L = 0; L < 3; ++L) s += Tb[J + 3 * L] * iJ[L + 3 * Kp];
         X[J][Kp] = s;
       }
     for (int K = 0; K < 3; ++K)
@@ -174,7 +175,8 @@ __global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
       s += a0 * (D[0] * a0 + D[9] * a1 + D[18] * a2) + a1 * (D[1] * a0 + D[10] * a1 + D[19] * a2) +
            a2 * (D[2] * a0 + D[11] * a1 + D[20] * a2);
     }
-    io.B[(size_t)(blk - 1) * 9 + ci + 3 * cj] += s;
+    if (io.atomic) atomicAdd(&io.B[(size_t)(blk - 1) * 9 + ci + 3 * cj], s);
+    else io.B[(size_t)(blk - 1) * 9 + ci + 3 * cj] += s;
   }
 }
 

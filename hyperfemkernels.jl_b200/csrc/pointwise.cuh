@@ -136,6 +136,42 @@ __device__ __forceinline__ void law_dstress_F(int law, R lam, R mu, const R* F, 
 
 // Full tangent T[(c*3+J) + 9*(k*3+L)] = dP[c,J]/dF[k,L] (point_tangent, src/factorforms.jl:316-322)
 // SVK: delta_ck S[L,J] + lam F[c,J] F[k,L] + mu F[c,L] F[k,J] + mu (F F')[c,k] delta_JL
+// One 3x3 block of the tangent: Tb[J + 3 L] = T[(c,J),(k,L)] (the same closed forms as
+// law_tangent, for callers that need the (c, k) block only: no 81-entry array per thread)
+__device__ inline void law_tangent_block(int law, double lam, double mu, const double* H, int c, int k, double* Tb) {
+  if (law == HFK_LAW_LINEAR_ELASTIC) {
+#pragma unroll
+    for (int J = 0; J < 3; ++J)
+#pragma unroll
+      for (int L = 0; L < 3; ++L)
+        Tb[J + 3 * L] = lam * (c == J) * (k == L) + mu * ((c == k) * (J == L) + (c == L) * (J == k));
+    return;
+  }
+  double F[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) F[i] = H[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+  double Fc[3], Fk[3];  // rows c and k of F
+#pragma unroll
+  for (int J = 0; J < 3; ++J) {
+    Fc[J] = c == 0 ? F[3 * J] : (c == 1 ? F[1 + 3 * J] : F[2 + 3 * J]);
+    Fk[J] = k == 0 ? F[3 * J] : (k == 1 ? F[1 + 3 * J] : F[2 + 3 * J]);
+  }
+  double C[9];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = 0; J < 3; ++J) C[I + 3 * J] = F[3 * I] * F[3 * J] + F[1 + 3 * I] * F[1 + 3 * J] + F[2 + 3 * I] * F[2 + 3 * J];
+  const double trE = 0.5 * (C[0] + C[4] + C[8] - 3.0);
+  const double ffck = Fc[0] * Fk[0] + Fc[1] * Fk[1] + Fc[2] * Fk[2];
+#pragma unroll
+  for (int J = 0; J < 3; ++J)
+#pragma unroll
+    for (int L = 0; L < 3; ++L) {
+      const double S = mu * C[L + 3 * J] + (L == J ? lam * trE - mu : 0.0);
+      Tb[J + 3 * L] = (c == k ? S : 0.0) + lam * Fc[J] * Fk[L] + mu * Fc[L] * Fk[J] + (J == L ? mu * ffck : 0.0);
+    }
+}
+
 __device__ inline void law_tangent(int law, double lam, double mu, const double* H, double* T) {
   if (law == HFK_LAW_LINEAR_ELASTIC) {
     for (int c = 0; c < 3; ++c)

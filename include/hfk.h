@@ -78,8 +78,8 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
  * read-modify-writes (deterministic, the reference's race-free colouring, src/coloring.jl:1-3), or
  * one launch over all cells with FP64 atomics (the summation order, hence the last bit, varies
  * between runs). AUTO (default) is the atomic scatter (faster on B200: one launch, no read of the
- * output before the write); COLOURED gives bit-reproducible results. The assembled Jacobian and the
- * nodal blocks always scatter by colour. */
+ * output before the write); COLOURED gives bit-reproducible results. The nodal blocks follow the
+ * same setting; the assembled Jacobian always scatters by colour. */
 #define HFK_SCATTER_AUTO 0
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2

@@ -179,10 +179,15 @@ def test_batched_solve_matches_each_problem_solved_alone():
     pm = dict(smoother=S.Chebyshev(degree=3), coarse="cg", coarse_iters=12)
     ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-10, preconditioner=S.PMultigrid([U2, U1], **pm))
     ns = S.numerical_setup(ls, mf)
+    v = np.random.default_rng(7).standard_normal(U2.nfree)
+    y_before = mf.mul(np.zeros(U2.nfree), v)
     dx = S.solve(np.zeros(U2.nfree), ns, b)
     res = ns.batched
     assert res.converged.all() and S.linear_converged(ns)
     assert res.sweeps == res.iters.max()
+    assert len(set(res.iters.tolist())) > 1  # problems converge at different sweeps (skipped once done)
+    # the skip flags are all reset after the solve: the product covers every problem again
+    assert reldiff(mf.mul(np.zeros(U2.nfree), v), y_before) < 1e-14
     for k in range(U2.nseg):
         V2, V1 = U2.spaces[k], U1.spaces[k]
         f = (forms.svk_residual(PROBLEMS[k].lam, PROBLEMS[k].mu, 4), forms.svk_jacobian(PROBLEMS[k].lam, PROBLEMS[k].mu, 4))
