@@ -1,0 +1,267 @@
+// Oseen–BDF step on Taylor–Hood P2–P1 affine tetrahedra: fused element matrix / load vector with
+// the scatter into the CSC nonzeros (Jacobian) or into the residual a(x, ·) - l(·).
+//
+// Volume terms of the reference's Oseen problem (test/common.jl:200-216): with velocity test
+// v = φ_a e_i, trial u = φ_b e_j and pressures ψ,
+//   K[(i,a),(j,b)] = δ_ij M_ab + Σ_q dV (μ ∂_jφ_a ∂_iφ_b + τl ∂_iφ_a ∂_jφ_b)
+//   M_ab = Σ_q dV (ρ c0 φ_a φ_b + μ ∇φ_a·∇φ_b + ρ (w·∇φ_b) φ_a + τs (w·∇φ_a)(ρ c0 φ_b + ρ w·∇φ_b))
+//   K[(i,a), p_b] = Σ_q dV (-ψ_b ∂_iφ_a + τs (w·∇φ_a) ∂_iψ_b)
+//   K[q_a, (j,b)] = Σ_q dV (-ψ_a ∂_jφ_b - τp ∂_jψ_a (ρ c0 φ_b + ρ w·∇φ_b))
+//   K[q_a, p_b]   = -Σ_q dV τp ∇ψ_a·∇ψ_b
+//   F[(i,a)] = Σ_q dV (ρ f_i φ_a + τs (w·∇φ_a) rk_i),  F[q_a] = -Σ_q dV τp ∇ψ_a·rk,  rk = ρ f + μ Δuⁿ
+// (2μ ε(u):ε(v) expands to μ δ_ij ∇φ_a·∇φ_b + μ ∂_jφ_a ∂_iφ_b), the τ of test/common.jl:196-198
+// at uⁿ and h = (6√2 |K|)^(1/3), w = 2uⁿ - uⁿ⁻¹ and f = c1 uⁿ - c2 uⁿ⁻¹ under BDF2 (:183-187),
+// Δuⁿ exact per cell (P2 on an affine cell). One CTA per cell: the point data are built once in
+// shared memory (one thread per point), then each thread forms whole entries of K.
+#pragma once
+#include "hfk_internal.h"
+#include "pointwise.cuh"
+
+namespace hfk {
+
+constexpr int OS_NV = 10, OS_NP = 4, OS_NDL = 34, OS_MAXQ = 64, OS_THREADS = 128;
+
+struct OseenData {
+  const int32_t* ids;     // (34, ncells)
+  const int32_t* cells;   // list (one colour) or nullptr
+  int ncells_list;
+  const double* coords;   // (3, 4, ncells)
+  const double* w;        // (nq)
+  const double* N2;       // (10, nq)
+  const double* dN2;      // (10, 3, nq)
+  const double* H2;       // (10, 3, 3) reference Hessians
+  const double* N1;       // (4, nq)
+  const double* dN1;      // (4, 3, nq)
+  const double* un;       // history, free values (trial space numbering)
+  const double* und;      // history, Dirichlet values
+  const double* unm1;
+  const double* unm1d;
+  int nq;
+  double rho, mu, c0, c1, c2;
+  int bdf2;
+};
+
+struct OseenIO {
+  int mode;               // 0: residual into b, 1: Jacobian into nzval
+  int atomic;
+  const double* x;        // residual: free values
+  const double* dvals;    // residual: Dirichlet values
+  double* b;
+  const int32_t* nzpos;   // (34*34, ncells) 1-based
+  double* nzval;
+};
+
+// shared layout (doubles) for nq points
+struct OseenSmem {
+  int nq;
+  __host__ __device__ int phi() const { return 0; }                   // [q][10]
+  __host__ __device__ int gphi() const { return phi() + 10 * nq; }    // [q][10][3]
+  __host__ __device__ int psi() const { return gphi() + 30 * nq; }    // [q][4]
+  __host__ __device__ int wg() const { return psi() + 4 * nq; }       // [q][10]  w·∇φ
+  __host__ __device__ int sup() const { return wg() + 10 * nq; }      // [q][10]  ρ c0 φ + ρ w·∇φ
+  __host__ __device__ int rk() const { return sup() + 10 * nq; }      // [q][3]
+  __host__ __device__ int f() const { return rk() + 3 * nq; }         // [q][3]
+  __host__ __device__ int sc() const { return f() + 3 * nq; }         // [q][4]  dV, τs, τp, τl
+  __host__ __device__ int cellv() const { return sc() + 4 * nq; }     // iJ 9, det, h, gpsi 12, lapn 3 (26)
+  __host__ __device__ int loc() const { return cellv() + 32; }        // xl 34, unl 30, uml 30
+  __host__ __device__ int M() const { return loc() + 96; }            // 100
+  __host__ __device__ int K() const { return M() + 100; }             // 34 * 34 + 34 (residual mode)
+  __host__ __device__ int total() const { return K() + OS_NDL * OS_NDL + OS_NDL; }
+};
+
+__global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO io) {
+  extern __shared__ __align__(16) double osm[];
+  __shared__ int32_t sid[OS_NDL];
+  const OseenSmem L{d.nq};
+  const int t = threadIdx.x;
+  const int li = blockIdx.x;
+  if (li >= d.ncells_list) return;
+  const int cell = d.cells ? d.cells[li] : li;
+  const int nq = d.nq;
+  double* cv = osm + L.cellv();
+  double* xl = osm + L.loc();
+  double* unl = xl + OS_NDL;
+  double* uml = unl + 30;
+  // ---- gathers ----------------------------------------------------------------------------
+  if (t < OS_NDL) {
+    const int32_t id = d.ids[(size_t)cell * OS_NDL + t];
+    sid[t] = id;
+    if (io.mode == 0) xl[t] = id > 0 ? io.x[id - 1] : (id < 0 ? io.dvals[-id - 1] : 0.0);
+    if (t < 30) {
+      unl[t] = id > 0 ? d.un[id - 1] : (id < 0 ? d.und[-id - 1] : 0.0);
+      uml[t] = id > 0 ? d.unm1[id - 1] : (id < 0 ? d.unm1d[-id - 1] : 0.0);
+    }
+  }
+  // ---- cell geometry (affine): J[c + 3K] = x_{K+1,c} - x_{0,c}, its inverse, h -----------------
+  if (t == 0) {
+    const double* X = d.coords + (size_t)cell * 12;
+    double J[9], iJ[9];
+    for (int K = 0; K < 3; ++K)
+      for (int c = 0; c < 3; ++c) J[c + 3 * K] = X[c + 3 * (K + 1)] - X[c];
+    const double det = det3(J);
+    inv3(J, det, iJ);  // iJ[K + 3c] = (J^-1)[K][c]
+    for (int i = 0; i < 9; ++i) cv[i] = iJ[i];
+    cv[9] = fabs(det);
+    cv[10] = cbrt(6.0 * sqrt(2.0) * fabs(det) / 6.0);
+  }
+  __syncthreads();
+  if (t < 12) {  // ∇ψ_a (constant): gpsi[a][c] = Σ_K dN1[a,K] (J^-1)[K][c]
+    const int a = t / 3, c = t % 3;
+    double s = 0;
+    for (int K = 0; K < 3; ++K) s += cv[K + 3 * c] * d.dN1[a + OS_NP * (K + 0)];
+    cv[11 + t] = s;
+  } else if (t >= 32 && t < 35) {  // Δuⁿ_c = Σ_a uⁿ_{c,a} Σ_{K,K'} Ĥ_a[K,K'] (J^-1 J^-T)[K,K']
+    const int c = t - 32;
+    double G[9];
+    for (int K = 0; K < 3; ++K)
+      for (int Kp = 0; Kp < 3; ++Kp) G[K + 3 * Kp] = cv[K] * cv[Kp] + cv[K + 3] * cv[Kp + 3] + cv[K + 6] * cv[Kp + 6];
+    double s = 0;
+    for (int a = 0; a < OS_NV; ++a) {
+      double la = 0;
+      for (int e = 0; e < 9; ++e) la += d.H2[a + OS_NV * e] * G[e];
+      s += la * unl[c * OS_NV + a];
+    }
+    cv[23 + c] = s;
+  }
+  __syncthreads();
+  // ---- point data -------------------------------------------------------------------------
+  for (int q = t; q < nq; q += blockDim.x) {
+    double* phi = osm + L.phi() + 10 * q;
+    double* gphi = osm + L.gphi() + 30 * q;
+    double* psi = osm + L.psi() + 4 * q;
+    for (int a = 0; a < OS_NV; ++a) {
+      phi[a] = d.N2[a + OS_NV * q];
+      for (int c = 0; c < 3; ++c) {
+        double s = 0;
+        for (int K = 0; K < 3; ++K) s += cv[K + 3 * c] * d.dN2[a + OS_NV * (K + 3 * q)];
+        gphi[a * 3 + c] = s;
+      }
+    }
+    for (int a = 0; a < OS_NP; ++a) psi[a] = d.N1[a + OS_NP * q];
+    double w[3], f[3], nrm = 0;
+    for (int c = 0; c < 3; ++c) {
+      double u0 = 0, u1 = 0;
+      for (int a = 0; a < OS_NV; ++a) {
+        u0 += phi[a] * unl[c * OS_NV + a];
+        u1 += phi[a] * uml[c * OS_NV + a];
+      }
+      w[c] = d.bdf2 ? 2.0 * u0 - u1 : u0;
+      f[c] = d.c1 * u0 - d.c2 * u1;
+      nrm += u0 * u0;
+    }
+    nrm = sqrt(nrm);
+    const double h = cv[10];
+    const double a1 = 2.0 * nrm / h, a2 = 4.0 * d.mu / (d.rho * h * h);
+    const double taus = 1.0 / sqrt(a1 * a1 + 9.0 * a2 * a2);
+    double* sc = osm + L.sc() + 4 * q;
+    sc[0] = d.w[q] * cv[9];
+    sc[1] = taus;
+    sc[2] = taus / d.rho;
+    sc[3] = d.rho * nrm * h * 0.5;
+    double* wg = osm + L.wg() + 10 * q;
+    double* sup = osm + L.sup() + 10 * q;
+    for (int a = 0; a < OS_NV; ++a) {
+      wg[a] = w[0] * gphi[a * 3] + w[1] * gphi[a * 3 + 1] + w[2] * gphi[a * 3 + 2];
+      sup[a] = d.rho * d.c0 * phi[a] + d.rho * wg[a];
+    }
+    for (int c = 0; c < 3; ++c) {
+      osm[L.f() + 3 * q + c] = f[c];
+      osm[L.rk() + 3 * q + c] = d.rho * f[c] + d.mu * cv[23 + c];
+    }
+  }
+  __syncthreads();
+  // ---- the velocity mass/viscous/advection/SUPG scalar block M_ab ----------------------------
+  if (t < OS_NV * OS_NV) {
+    const int a = t % OS_NV, b = t / OS_NV;
+    double s = 0;
+    for (int q = 0; q < nq; ++q) {
+      const double* phi = osm + L.phi() + 10 * q;
+      const double* g = osm + L.gphi() + 30 * q;
+      const double* sc = osm + L.sc() + 4 * q;
+      const double gg = g[a * 3] * g[b * 3] + g[a * 3 + 1] * g[b * 3 + 1] + g[a * 3 + 2] * g[b * 3 + 2];
+      s += sc[0] * (d.rho * d.c0 * phi[a] * phi[b] + d.mu * gg + d.rho * osm[L.wg() + 10 * q + b] * phi[a] +
+                    sc[1] * osm[L.wg() + 10 * q + a] * osm[L.sup() + 10 * q + b]);
+    }
+    osm[L.M() + a + OS_NV * b] = s;
+  }
+  __syncthreads();
+  // ---- entries of K (test te, trial tr) and of F --------------------------------------------
+  const double* gpsi = cv + 11;
+  double* Ks = osm + L.K();
+  const int32_t* pos = io.nzpos ? io.nzpos + (size_t)OS_NDL * OS_NDL * cell : nullptr;
+  for (int e = t; e < OS_NDL * OS_NDL + OS_NDL; e += blockDim.x) {
+    double val = 0;
+    if (e < OS_NDL * OS_NDL) {
+      const int te = e % OS_NDL, tr = e / OS_NDL;
+      if (te < 30 && tr < 30) {
+        const int i = te / OS_NV, a = te % OS_NV, j = tr / OS_NV, b = tr % OS_NV;
+        for (int q = 0; q < nq; ++q) {
+          const double* g = osm + L.gphi() + 30 * q;
+          const double* sc = osm + L.sc() + 4 * q;
+          val += sc[0] * (d.mu * g[a * 3 + j] * g[b * 3 + i] + sc[3] * g[a * 3 + i] * g[b * 3 + j]);
+        }
+        if (i == j) val += osm[L.M() + a + OS_NV * b];
+      } else if (te < 30) {
+        const int i = te / OS_NV, a = te % OS_NV, b = tr - 30;
+        for (int q = 0; q < nq; ++q) {
+          const double* sc = osm + L.sc() + 4 * q;
+          val += sc[0] * (-osm[L.psi() + 4 * q + b] * osm[L.gphi() + 30 * q + a * 3 + i] +
+                          sc[1] * osm[L.wg() + 10 * q + a] * gpsi[b * 3 + i]);
+        }
+      } else if (tr < 30) {
+        const int a = te - 30, j = tr / OS_NV, b = tr % OS_NV;
+        for (int q = 0; q < nq; ++q) {
+          const double* sc = osm + L.sc() + 4 * q;
+          val += sc[0] * (-osm[L.psi() + 4 * q + a] * osm[L.gphi() + 30 * q + b * 3 + j] -
+                          sc[2] * gpsi[a * 3 + j] * osm[L.sup() + 10 * q + b]);
+        }
+      } else {
+        const int a = te - 30, b = tr - 30;
+        double s = 0;
+        for (int q = 0; q < nq; ++q) s += osm[L.sc() + 4 * q] * osm[L.sc() + 4 * q + 2];
+        val = -s * (gpsi[a * 3] * gpsi[b * 3] + gpsi[a * 3 + 1] * gpsi[b * 3 + 1] + gpsi[a * 3 + 2] * gpsi[b * 3 + 2]);
+      }
+      if (io.mode == 1) {
+        const int32_t ps = pos[e];
+        if (ps > 0) {
+          if (io.atomic) atomicAdd(&io.nzval[ps - 1], val);
+          else io.nzval[ps - 1] += val;
+        }
+      } else {
+        Ks[e] = val;
+      }
+    } else if (io.mode == 0) {
+      const int te = e - OS_NDL * OS_NDL;
+      if (te < 30) {
+        const int i = te / OS_NV, a = te % OS_NV;
+        for (int q = 0; q < nq; ++q) {
+          const double* sc = osm + L.sc() + 4 * q;
+          val += sc[0] * (d.rho * osm[L.f() + 3 * q + i] * osm[L.phi() + 10 * q + a] +
+                          sc[1] * osm[L.wg() + 10 * q + a] * osm[L.rk() + 3 * q + i]);
+        }
+      } else {
+        const int a = te - 30;
+        for (int q = 0; q < nq; ++q) {
+          const double* sc = osm + L.sc() + 4 * q;
+          const double* rk = osm + L.rk() + 3 * q;
+          val -= sc[0] * sc[2] * (gpsi[a * 3] * rk[0] + gpsi[a * 3 + 1] * rk[1] + gpsi[a * 3 + 2] * rk[2]);
+        }
+      }
+      Ks[OS_NDL * OS_NDL + te] = val;
+    }
+  }
+  if (io.mode == 1) return;
+  __syncthreads();
+  // ---- residual r = K x - F at the free test rows ---------------------------------------------
+  if (t < OS_NDL) {
+    const int32_t id = sid[t];
+    if (id > 0) {
+      double r = -Ks[OS_NDL * OS_NDL + t];
+      for (int j = 0; j < OS_NDL; ++j) r += Ks[t + OS_NDL * j] * xl[j];
+      if (io.atomic) atomicAdd(&io.b[id - 1], r);
+      else io.b[id - 1] += r;
+    }
+  }
+}
+
+}  // namespace hfk

@@ -89,6 +89,16 @@ SIGNATURES = {
     "hfk_pmg_set_coarse": [_vp, _i, _i],
     "hfk_pmg_segment_bounds": [_vp, _i, _vp, _vp],
     "hfk_pmg_set_eig_inner": [_vp, _i],
+    "hfk_oseen_create": [ctypes.POINTER(_vp), _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _i],
+    "hfk_oseen_destroy": [_vp],
+    "hfk_oseen_set_params": [_vp, _vp, _i],
+    "hfk_oseen_set_scatter": [_vp, _i],
+    "hfk_oseen_set_history": [_vp, _vp, _vp, _vp, _vp],
+    "hfk_oseen_pattern": [_vp, _pi64],
+    "hfk_oseen_pattern_get": [_vp, _vp, _vp],
+    "hfk_oseen_residual": [_vp, _vp, _vp, _vp],
+    "hfk_oseen_jacobian": [_vp, _vp],
+    "hfk_oseen_launch_count": [_vp, _pi64],
     "hfk_problem_set_segments": [_vp, _i, _vp, _vp, _vp],
     "hfk_problem_segments": [_vp, _pi],
     "hfk_problem_set_cell_params": [_vp, _vp],

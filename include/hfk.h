@@ -280,6 +280,34 @@ int hfk_solve_cg_batched(hfk_problem* op, hfk_pmg* prec, const double* b, double
                          int maxiter, int flexible, int* iters, int* converged, int* indefinite, double* relres,
                          int* sweeps);
 
+/* ---- Oseen–BDF step, Taylor–Hood P2–P1 on affine tetrahedra (test/common.jl:164-228) ----------
+ * The volume terms of the reference's Oseen problem: a((u,p),(v,q)) with SUPG/PSPG/LSIC
+ * stabilisation and l((v,q)) with the BDF history and the elementwise Laplacian of uⁿ, assembled
+ * as the reference's residual!/jacobian! do (src/assembly.jl:909-927): residual = a(x, .) - l(.)
+ * at the free dofs, Jacobian = the CSC nonzeros of a (the form is linear in x). Inputs:
+ *   nq points, w (nq); P2 tables N2 (10, nq), dN2 (10, 3, nq), reference Hessians H2 (10, 3, 3);
+ *   P1 tables N1 (4, nq), dN1 (4, 3, nq); coords (3, 4, ncells) vertices; cell_dof_ids
+ *   (34, ncells): velocity c*10 + n (P2 node n: 4 vertices then the edges 01 02 03 12 13 23),
+ *   pressure 30 + n; params = rho, mu, dt, bdf2 (1: BDF2 coefficients, 0: backward Euler).
+ * The history uⁿ, uⁿ⁻¹ (free and Dirichlet values, trial-space numbering, pressure entries
+ * ignored) gives w = 2uⁿ - uⁿ⁻¹ (BDF2), the history term f and the τ of test/common.jl:196-198. */
+typedef struct hfk_oseen hfk_oseen;
+int hfk_oseen_create(hfk_oseen** out, int ncells, int nq, const double* w, const double* N2, const double* dN2,
+                     const double* H2, const double* N1, const double* dN1, const double* coords,
+                     const int32_t* cell_dof_ids, int64_t nfree, int64_t ndir, const double* params, int nparams);
+int hfk_oseen_destroy(hfk_oseen* o);
+/* update(op, res, jac) for the step (src/assembly.jl:693-744): new rho, mu, dt, bdf2; tables,
+ * pattern and colours kept. */
+int hfk_oseen_set_params(hfk_oseen* o, const double* params, int nparams);
+int hfk_oseen_set_scatter(hfk_oseen* o, int mode);
+int hfk_oseen_set_history(hfk_oseen* o, const double* un, const double* und, const double* unm1, const double* unm1d);
+/* sparsity (src/assembly.jl:773-818): nnz, then colptr (nfree + 1) and rowval, Int64 1-based. */
+int hfk_oseen_pattern(hfk_oseen* o, int64_t* nnz);
+int hfk_oseen_pattern_get(hfk_oseen* o, int64_t* colptr, int64_t* rowval);
+int hfk_oseen_residual(hfk_oseen* o, const double* x, const double* dvals, double* b);
+int hfk_oseen_jacobian(hfk_oseen* o, double* nzval);
+int hfk_oseen_launch_count(hfk_oseen* o, int64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

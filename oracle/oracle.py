@@ -68,6 +68,17 @@ def lib():
         L.o_prolongate.argtypes = [ctypes.c_void_p, c_dp, c_dp]
         L.o_restrict.argtypes = [ctypes.c_void_p, c_dp, c_dp]
         L.o_inject.argtypes = [ctypes.c_void_p, c_dp, c_dp, c_dp, c_dp]
+        L.o_oseen_create.restype = ctypes.c_void_p
+        L.o_oseen_create.argtypes = [ctypes.c_int, ctypes.c_int] + [c_dp] * 7 + [c_ip, ctypes.c_int64, ctypes.c_int64,
+                                                                                  c_dp]
+        L.o_oseen_free.argtypes = [ctypes.c_void_p]
+        L.o_oseen_set_history.argtypes = [ctypes.c_void_p, c_dp, c_dp, c_dp, c_dp]
+        L.o_oseen_element.argtypes = [ctypes.c_void_p, ctypes.c_int, c_dp, c_dp]
+        L.o_oseen_pattern.restype = ctypes.c_int64
+        L.o_oseen_pattern.argtypes = [ctypes.c_void_p]
+        L.o_oseen_pattern_get.argtypes = [ctypes.c_void_p, c_lp, c_lp, c_ip]
+        L.o_oseen_residual.argtypes = [ctypes.c_void_p, c_dp, c_dp, c_dp, ctypes.c_int]
+        L.o_oseen_jacobian.argtypes = [ctypes.c_void_p, c_dp, ctypes.c_int]
         _LIB = L
     return _LIB
 
@@ -546,3 +557,68 @@ def mlp_grad(w, X, T):
     gb1 = d1.sum(0)
     g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
     return g, loss
+
+
+# ---------------------------------------------------------------------------------------------
+# Oseen–BDF step on Taylor–Hood P2–P1 tetrahedra (oseen_oracle.cpp)
+
+
+class OracleOseen:
+    """The volume terms of the reference's Oseen step (test/common.jl:164-228) on a
+    ``hfk.oseen.TaylorHoodSpace``, evaluated literally per (test, trial) pair."""
+
+    def __init__(self, space, params, un, und, unm1=None, unm1d=None, quad_m=3):
+        from hfk import oseen as OS  # host module (pure numpy)
+
+        self.space = space
+        pts, w = OS.tet_quadrature(quad_m)
+        N2, dN2, N1, dN1, H2 = OS.tables(pts)
+        self._keep = (w, N2, dN2, N1, dN1, H2)
+        prm = np.ascontiguousarray(params.array())
+        self.ids = space.cell_dof_ids
+        self.h = lib().o_oseen_create(space.mesh.ncells, len(w), _d(w), _d(N2), _d(dN2), _d(H2), _d(N1), _d(dN1),
+                                      _d(space.mesh.coords), _i(self.ids), space.nfree, space.ndir, _d(prm))
+        if not self.h:
+            raise RuntimeError("oracle: more than 128 colours")
+        unm1 = un if unm1 is None else unm1
+        unm1d = und if unm1d is None else unm1d
+        self._hist = [np.ascontiguousarray(a, dtype=float) for a in (un, und, unm1, unm1d)]
+        lib().o_oseen_set_history(self.h, *[_d(a) for a in self._hist])
+        self.nnz = None
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().o_oseen_free(self.h)
+            self.h = None
+
+    def element(self, cell):
+        Ke = np.zeros((34, 34), order="F")
+        Fe = np.zeros(34)
+        lib().o_oseen_element(self.h, cell, _d(Ke), _d(Fe))
+        return Ke, Fe
+
+    def pattern(self):
+        if self.nnz is None:
+            self.nnz = int(lib().o_oseen_pattern(self.h))
+            n = self.space.nfree
+            self.colptr = np.zeros(n + 1, dtype=np.int64)
+            self.rowval = np.zeros(self.nnz, dtype=np.int64)
+            lib().o_oseen_pattern_get(self.h, _l(self.colptr), _l(self.rowval), None)
+        return self.colptr, self.rowval
+
+    def residual(self, x, dvals, nthreads=0):
+        b = np.zeros(self.space.nfree)
+        lib().o_oseen_residual(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)),
+                               _d(b), nthreads)
+        return b
+
+    def jacobian_values(self, nthreads=0):
+        self.pattern()
+        nz = np.zeros(self.nnz)
+        lib().o_oseen_jacobian(self.h, _d(nz), nthreads)
+        return nz
+
+    def jacobian(self, nthreads=0):
+        nz = self.jacobian_values(nthreads)
+        n = self.space.nfree
+        return sp.csc_matrix((nz, self.rowval - 1, self.colptr - 1), shape=(n, n))
