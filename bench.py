@@ -236,6 +236,7 @@ def engine(args):
         extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
         extra.update(assembly_case(torch, dev, stream, timed))
         extra.update(jv_sizes_case(torch, dev, stream, timed))
+        extra.update(oseen_case(torch, dev, stream, timed))
         extra.update(newton_case())
 
     cpu = cpu_baseline_sample() if rank == 0 and not args.no_cpu else None
@@ -289,6 +290,54 @@ def jv_sizes_case(torch, dev, stream, timed, cases=((2, 48), (4, 48), (4, 64))):
         del op, mf, xd, dxd, yd, dx32, y32
         torch.cuda.empty_cache()
     return out
+
+
+def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
+    """Secondary (config 2): one FP64 residual and one CSC Jacobian of the Oseen-BDF2 step, Taylor-Hood
+    P2-P1 on the 32^3 cube split into 196 608 tetrahedra (859 812 dofs), rho = 1, mu = 1e-3, dt = 1e-3,
+    advection from a seeded sum of 8 divergence-free Fourier modes of amplitude 1 (u^n = u^(n-1));
+    the CPU restatement (literal weak form, all host cores) timed on a 12^3 sample."""
+    from hfk import _lib
+    from hfk import oseen as OS
+
+    m = OS.TetMesh(n)
+    V = OS.TaylorHoodSpace(m)
+    un, und = V.interpolate_velocity(OS.fourier_field(2))
+    params = OS.OseenParams(rho=1.0, mu=1e-3, dt=1e-3, bdf2=True)
+    op = OS.OseenOperator(V, params, un, und)
+    x = np.random.default_rng(0).standard_normal(V.nfree)
+    A = op.sparsity_pattern()
+    xd = torch.from_numpy(x).to(dev)
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+    bd = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
+    nz = torch.zeros(A.nnz, dtype=torch.float64, device=dev)
+    h = op.h
+    ms_j = timed(lambda: _lib.call("hfk_oseen_jacobian", h, _lib.ptr(nz)), 10, 3) / 10
+    ms_r = timed(lambda: _lib.call("hfk_oseen_residual", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(bd)), 10, 3) / 10
+    # CPU restatement on a sample
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    ms_ = OS.TetMesh(cpu_n)
+    Vs = OS.TaylorHoodSpace(ms_)
+    uns, unds = Vs.interpolate_velocity(OS.fourier_field(2))
+    orc = O.OracleOseen(Vs, params, uns, unds)
+    orc.pattern()
+    xs = np.random.default_rng(0).standard_normal(Vs.nfree)
+    t0 = time.perf_counter()
+    orc.jacobian_values()
+    tj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.residual(xs, Vs.dirichlet_values)
+    tr = time.perf_counter() - t0
+    scale = m.ncells / ms_.ncells
+    return {"oseen_p2p1_tet_32": {"cells": m.ncells, "dofs": V.ndof_total, "free_dofs": V.nfree, "nnz": int(A.nnz),
+                                  "jacobian_ms": ms_j, "residual_ms": ms_r,
+                                  "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
+                                  "cpu_sample": f"oracle on {cpu_n}^3 ({ms_.ncells} cells), {O.lib().o_max_threads()} threads",
+                                  "cpu_jacobian_ms_extrapolated": 1e3 * tj * scale,
+                                  "cpu_residual_ms_extrapolated": 1e3 * tr * scale,
+                                  "speedup_jacobian_vs_cpu": 1e3 * tj * scale / ms_j}}
 
 
 def assembly_case(torch, dev, stream, timed):

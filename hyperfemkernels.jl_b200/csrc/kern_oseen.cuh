@@ -12,7 +12,11 @@
 // (2μ ε(u):ε(v) expands to μ δ_ij ∇φ_a·∇φ_b + μ ∂_jφ_a ∂_iφ_b), the τ of test/common.jl:196-198
 // at uⁿ and h = (6√2 |K|)^(1/3), w = 2uⁿ - uⁿ⁻¹ and f = c1 uⁿ - c2 uⁿ⁻¹ under BDF2 (:183-187),
 // Δuⁿ exact per cell (P2 on an affine cell). One CTA per cell: the point data are built once in
-// shared memory (one thread per point), then each thread forms whole entries of K.
+// shared memory (one thread per point). The Jacobian: one thread per basis pair, which forms every
+// component entry of that pair in one pass over the points (the 9 entries of a velocity pair share
+// their loads). The residual a(x, ·) - l(·) is formed matrix-free: the point values of u, ∇u, p,
+// ∇p from x give per point the coefficients of φ_a, ∇φ_a and w·∇φ_a in each test row, then one
+// thread per test function contracts them over the points (no element matrix).
 #pragma once
 #include "hfk_internal.h"
 #include "pointwise.cuh"
@@ -64,9 +68,8 @@ struct OseenSmem {
   __host__ __device__ int sc() const { return f() + 3 * nq; }         // [q][4]  dV, τs, τp, τl
   __host__ __device__ int cellv() const { return sc() + 4 * nq; }     // iJ 9, det, h, gpsi 12, lapn 3 (26)
   __host__ __device__ int loc() const { return cellv() + 32; }        // xl 34, unl 30, uml 30
-  __host__ __device__ int M() const { return loc() + 96; }            // 100
-  __host__ __device__ int K() const { return M() + 100; }             // 34 * 34 + 34 (residual mode)
-  __host__ __device__ int total() const { return K() + OS_NDL * OS_NDL + OS_NDL; }
+  __host__ __device__ int rc() const { return loc() + 96; }           // [q][20] residual point coefficients
+  __host__ __device__ int total() const { return rc() + 20 * nq; }
 };
 
 __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO io) {
@@ -168,98 +171,131 @@ __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO 
       osm[L.f() + 3 * q + c] = f[c];
       osm[L.rk() + 3 * q + c] = d.rho * f[c] + d.mu * cv[23 + c];
     }
-  }
-  __syncthreads();
-  // ---- the velocity mass/viscous/advection/SUPG scalar block M_ab ----------------------------
-  if (t < OS_NV * OS_NV) {
-    const int a = t % OS_NV, b = t / OS_NV;
-    double s = 0;
-    for (int q = 0; q < nq; ++q) {
-      const double* phi = osm + L.phi() + 10 * q;
-      const double* g = osm + L.gphi() + 30 * q;
-      const double* sc = osm + L.sc() + 4 * q;
-      const double gg = g[a * 3] * g[b * 3] + g[a * 3 + 1] * g[b * 3 + 1] + g[a * 3 + 2] * g[b * 3 + 2];
-      s += sc[0] * (d.rho * d.c0 * phi[a] * phi[b] + d.mu * gg + d.rho * osm[L.wg() + 10 * q + b] * phi[a] +
-                    sc[1] * osm[L.wg() + 10 * q + a] * osm[L.sup() + 10 * q + b]);
+    if (io.mode == 0) {
+      // point values of x: u_i, G[k][i] = ∂_k u_i, p, ∇p (constant)
+      double u[3], G[3][3], p = 0, gp[3] = {0, 0, 0};
+      for (int i = 0; i < 3; ++i) {
+        u[i] = 0;
+        for (int k = 0; k < 3; ++k) G[k][i] = 0;
+        for (int a = 0; a < OS_NV; ++a) {
+          const double xa = xl[i * OS_NV + a];
+          u[i] += phi[a] * xa;
+          for (int k = 0; k < 3; ++k) G[k][i] += gphi[a * 3 + k] * xa;
+        }
+      }
+      for (int a = 0; a < OS_NP; ++a) {
+        const double xa = xl[30 + a];
+        p += psi[a] * xa;
+        for (int k = 0; k < 3; ++k) gp[k] += cv[11 + a * 3 + k] * xa;
+      }
+      const double divu = G[0][0] + G[1][1] + G[2][2];
+      const double dV = sc[0];
+      double* R = osm + L.rc() + 20 * q;
+      // velocity row (i, a): Σ_q [φ_a R[i] + Σ_k ∂_kφ_a R[3 + 3i + k] + (w·∇φ_a) R[12 + i]]
+      // pressure row a:     Σ_q [ψ_a R[15]] + ∇ψ_a · Σ_q R[16..18]
+      for (int i = 0; i < 3; ++i) {
+        const double conv = w[0] * G[0][i] + w[1] * G[1][i] + w[2] * G[2][i];  // ((∇u')·w)_i
+        const double Ru = d.rho * d.c0 * u[i] + d.rho * conv;
+        const double rk = osm[L.rk() + 3 * q + i];
+        R[i] = dV * (d.rho * d.c0 * u[i] + d.rho * conv - d.rho * f[i]);
+        for (int k = 0; k < 3; ++k)
+          R[3 + 3 * i + k] = dV * (d.mu * (G[k][i] + G[i][k]) + (k == i ? sc[3] * divu - p : 0.0));
+        R[12 + i] = dV * taus * (Ru + gp[i] - rk);
+        R[16 + i] = -dV * sc[2] * (Ru + gp[i] - rk);
+      }
+      R[15] = -dV * divu;
     }
-    osm[L.M() + a + OS_NV * b] = s;
   }
   __syncthreads();
-  // ---- entries of K (test te, trial tr) and of F --------------------------------------------
+  if (io.mode == 0) {
+    // ---- residual rows, scattered at the free test dofs ----------------------------------------
+    if (t < OS_NDL) {
+      const int32_t id = sid[t];
+      double r = 0;
+      if (t < 30) {
+        const int i = t / OS_NV, a = t % OS_NV;
+        for (int q = 0; q < nq; ++q) {
+          const double* R = osm + L.rc() + 20 * q;
+          const double* g = osm + L.gphi() + 30 * q + a * 3;
+          r += osm[L.phi() + 10 * q + a] * R[i] + g[0] * R[3 + 3 * i] + g[1] * R[4 + 3 * i] + g[2] * R[5 + 3 * i] +
+               osm[L.wg() + 10 * q + a] * R[12 + i];
+        }
+      } else {
+        const int a = t - 30;
+        double v0 = 0, v1 = 0, v2 = 0;
+        for (int q = 0; q < nq; ++q) {
+          const double* R = osm + L.rc() + 20 * q;
+          r += osm[L.psi() + 4 * q + a] * R[15];
+          v0 += R[16];
+          v1 += R[17];
+          v2 += R[18];
+        }
+        r += cv[11 + a * 3] * v0 + cv[12 + a * 3] * v1 + cv[13 + a * 3] * v2;
+      }
+      if (id > 0) {
+        if (io.atomic) atomicAdd(&io.b[id - 1], r);
+        else io.b[id - 1] += r;
+      }
+    }
+    return;
+  }
+  // ---- Jacobian: one thread per basis pair --------------------------------------------------
   const double* gpsi = cv + 11;
-  double* Ks = osm + L.K();
-  const int32_t* pos = io.nzpos ? io.nzpos + (size_t)OS_NDL * OS_NDL * cell : nullptr;
-  for (int e = t; e < OS_NDL * OS_NDL + OS_NDL; e += blockDim.x) {
-    double val = 0;
-    if (e < OS_NDL * OS_NDL) {
-      const int te = e % OS_NDL, tr = e / OS_NDL;
-      if (te < 30 && tr < 30) {
-        const int i = te / OS_NV, a = te % OS_NV, j = tr / OS_NV, b = tr % OS_NV;
-        for (int q = 0; q < nq; ++q) {
-          const double* g = osm + L.gphi() + 30 * q;
-          const double* sc = osm + L.sc() + 4 * q;
-          val += sc[0] * (d.mu * g[a * 3 + j] * g[b * 3 + i] + sc[3] * g[a * 3 + i] * g[b * 3 + j]);
-        }
-        if (i == j) val += osm[L.M() + a + OS_NV * b];
-      } else if (te < 30) {
-        const int i = te / OS_NV, a = te % OS_NV, b = tr - 30;
-        for (int q = 0; q < nq; ++q) {
-          const double* sc = osm + L.sc() + 4 * q;
-          val += sc[0] * (-osm[L.psi() + 4 * q + b] * osm[L.gphi() + 30 * q + a * 3 + i] +
-                          sc[1] * osm[L.wg() + 10 * q + a] * gpsi[b * 3 + i]);
-        }
-      } else if (tr < 30) {
-        const int a = te - 30, j = tr / OS_NV, b = tr % OS_NV;
-        for (int q = 0; q < nq; ++q) {
-          const double* sc = osm + L.sc() + 4 * q;
-          val += sc[0] * (-osm[L.psi() + 4 * q + a] * osm[L.gphi() + 30 * q + b * 3 + j] -
-                          sc[2] * gpsi[a * 3 + j] * osm[L.sup() + 10 * q + b]);
-        }
-      } else {
-        const int a = te - 30, b = tr - 30;
-        double s = 0;
-        for (int q = 0; q < nq; ++q) s += osm[L.sc() + 4 * q] * osm[L.sc() + 4 * q + 2];
-        val = -s * (gpsi[a * 3] * gpsi[b * 3] + gpsi[a * 3 + 1] * gpsi[b * 3 + 1] + gpsi[a * 3 + 2] * gpsi[b * 3 + 2]);
-      }
-      if (io.mode == 1) {
-        const int32_t ps = pos[e];
-        if (ps > 0) {
-          if (io.atomic) atomicAdd(&io.nzval[ps - 1], val);
-          else io.nzval[ps - 1] += val;
-        }
-      } else {
-        Ks[e] = val;
-      }
-    } else if (io.mode == 0) {
-      const int te = e - OS_NDL * OS_NDL;
-      if (te < 30) {
-        const int i = te / OS_NV, a = te % OS_NV;
-        for (int q = 0; q < nq; ++q) {
-          const double* sc = osm + L.sc() + 4 * q;
-          val += sc[0] * (d.rho * osm[L.f() + 3 * q + i] * osm[L.phi() + 10 * q + a] +
-                          sc[1] * osm[L.wg() + 10 * q + a] * osm[L.rk() + 3 * q + i]);
-        }
-      } else {
-        const int a = te - 30;
-        for (int q = 0; q < nq; ++q) {
-          const double* sc = osm + L.sc() + 4 * q;
-          const double* rk = osm + L.rk() + 3 * q;
-          val -= sc[0] * sc[2] * (gpsi[a * 3] * rk[0] + gpsi[a * 3 + 1] * rk[1] + gpsi[a * 3 + 2] * rk[2]);
-        }
-      }
-      Ks[OS_NDL * OS_NDL + te] = val;
+  const int32_t* pos = io.nzpos + (size_t)OS_NDL * OS_NDL * cell;
+  auto put = [&](int te, int tr, double v) {
+    const int32_t ps = pos[te + OS_NDL * tr];
+    if (ps > 0) {
+      if (io.atomic) atomicAdd(&io.nzval[ps - 1], v);
+      else io.nzval[ps - 1] += v;
     }
-  }
-  if (io.mode == 1) return;
-  __syncthreads();
-  // ---- residual r = K x - F at the free test rows ---------------------------------------------
-  if (t < OS_NDL) {
-    const int32_t id = sid[t];
-    if (id > 0) {
-      double r = -Ks[OS_NDL * OS_NDL + t];
-      for (int j = 0; j < OS_NDL; ++j) r += Ks[t + OS_NDL * j] * xl[j];
-      if (io.atomic) atomicAdd(&io.b[id - 1], r);
-      else io.b[id - 1] += r;
+  };
+  for (int item = t; item < 196; item += blockDim.x) {
+    if (item < 100) {  // velocity pair (a, b): M_ab and the 9 component entries
+      const int a = item % OS_NV, b = item / OS_NV;
+      double M = 0, X[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int q = 0; q < nq; ++q) {
+        const double* phi = osm + L.phi() + 10 * q;
+        const double* ga = osm + L.gphi() + 30 * q + a * 3;
+        const double* gb = osm + L.gphi() + 30 * q + b * 3;
+        const double* sc = osm + L.sc() + 4 * q;
+        const double dV = sc[0], mdv = d.mu * dV, ldv = sc[3] * dV;
+        const double wga = osm[L.wg() + 10 * q + a], wgb = osm[L.wg() + 10 * q + b];
+        const double gg = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+        M += dV * (d.rho * d.c0 * phi[a] * phi[b] + d.mu * gg + d.rho * wgb * phi[a] +
+                   sc[1] * wga * osm[L.sup() + 10 * q + b]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) X[i][j] += mdv * ga[j] * gb[i] + ldv * ga[i] * gb[j];
+      }
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) put(i * OS_NV + a, j * OS_NV + b, X[i][j] + (i == j ? M : 0.0));
+    } else if (item < 140) {  // velocity test (., a), pressure trial b
+      const int a = (item - 100) % OS_NV, b = (item - 100) / OS_NV;
+      double V[3] = {0, 0, 0};
+      for (int q = 0; q < nq; ++q) {
+        const double* ga = osm + L.gphi() + 30 * q + a * 3;
+        const double* sc = osm + L.sc() + 4 * q;
+        const double psib = osm[L.psi() + 4 * q + b], wga = osm[L.wg() + 10 * q + a];
+        for (int i = 0; i < 3; ++i) V[i] += sc[0] * (-psib * ga[i] + sc[1] * wga * gpsi[b * 3 + i]);
+      }
+      for (int i = 0; i < 3; ++i) put(i * OS_NV + a, 30 + b, V[i]);
+    } else if (item < 180) {  // pressure test a, velocity trial (., b)
+      const int b = (item - 140) % OS_NV, a = (item - 140) / OS_NV;
+      double V[3] = {0, 0, 0};
+      for (int q = 0; q < nq; ++q) {
+        const double* gb = osm + L.gphi() + 30 * q + b * 3;
+        const double* sc = osm + L.sc() + 4 * q;
+        const double psia = osm[L.psi() + 4 * q + a], supb = osm[L.sup() + 10 * q + b];
+        for (int j = 0; j < 3; ++j) V[j] += sc[0] * (-psia * gb[j] - sc[2] * gpsi[a * 3 + j] * supb);
+      }
+      for (int j = 0; j < 3; ++j) put(30 + a, j * OS_NV + b, V[j]);
+    } else {  // pressure pair
+      const int a = (item - 180) % OS_NP, b = (item - 180) / OS_NP;
+      double s = 0;
+      for (int q = 0; q < nq; ++q) s += osm[L.sc() + 4 * q] * osm[L.sc() + 4 * q + 2];
+      put(30 + a, 30 + b,
+          -s * (gpsi[a * 3] * gpsi[b * 3] + gpsi[a * 3 + 1] * gpsi[b * 3 + 1] + gpsi[a * 3 + 2] * gpsi[b * 3 + 2]));
     }
   }
 }
