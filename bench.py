@@ -45,6 +45,8 @@ def parse():
                     help="the batched workload instead: 256 SVK Q2 Newton solves (plain p-MG vs learned correction)")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--oseen", type=int, default=0, metavar="N",
+                    help="only the Oseen P2-P1 assembly on the N^3 tetrahedral cube (the secondary case; 0 = off)")
     return ap.parse_args()
 
 
@@ -331,13 +333,35 @@ def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
     orc.residual(xs, Vs.dirichlet_values)
     tr = time.perf_counter() - t0
     scale = m.ncells / ms_.ncells
-    return {"oseen_p2p1_tet_32": {"cells": m.ncells, "dofs": V.ndof_total, "free_dofs": V.nfree, "nnz": int(A.nnz),
+    return {f"oseen_p2p1_tet_{n}": {"cells": m.ncells, "dofs": V.ndof_total, "free_dofs": V.nfree, "nnz": int(A.nnz),
                                   "jacobian_ms": ms_j, "residual_ms": ms_r,
                                   "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
                                   "cpu_sample": f"oracle on {cpu_n}^3 ({ms_.ncells} cells), {O.lib().o_max_threads()} threads",
                                   "cpu_jacobian_ms_extrapolated": 1e3 * tj * scale,
                                   "cpu_residual_ms_extrapolated": 1e3 * tr * scale,
                                   "speedup_jacobian_vs_cpu": 1e3 * tj * scale / ms_j}}
+
+
+def oseen_main(args):
+    """The Oseen assembly alone (``--oseen N``), one JSON line: the case for profiling its kernel."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = oseen_case(torch, torch.device("cuda"), stream, timed, n=args.oseen, cpu_n=min(args.oseen, 8))
+    print(json.dumps(out))
 
 
 def assembly_case(torch, dev, stream, timed):
@@ -650,5 +674,7 @@ if __name__ == "__main__":
         reference(a)
     elif a.batch:
         batch_main(a)
+    elif a.oseen:
+        oseen_main(a)
     else:
         engine(a)
