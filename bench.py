@@ -520,10 +520,12 @@ def reference(args):
 BATCH_LOADS = (0.1, 0.325, 0.55, 0.775, 1.0)
 
 
-def _batch_setup(count, seed=4):
+def _batch_setup(count, seed=4, rank=0, world=1):
     from hfk import batch as B
 
     problems = B.draw_batch(256, seed=seed)[:count]
+    if world > 1:  # shard by problem: every rank solves its own subset, no data exchange
+        problems = [problems[k] for k in B.shard_problems(problems, rank, world)]
     (U2, U1), g = B.cube_batch(problems)
     return problems, U2, U1, g, B.cube_lifting(U2)
 
@@ -594,8 +596,25 @@ def batch_main(args):
     from hfk import forms, learned
     from hfk.operator import KernelOperator
 
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     t0 = time.perf_counter()
-    problems, U2, U1, g, lift = _batch_setup(args.batch_count)
+    problems, U2, U1, g, lift = _batch_setup(args.batch_count, rank=rank, world=world)
     res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
     op = KernelOperator(res, jac, U2, jacobian="matrixfree")
     t_setup = time.perf_counter() - t0
@@ -604,9 +623,13 @@ def batch_main(args):
     opw = KernelOperator(res, jac, W2, jacobian="matrixfree")
     B.newton_solve_batched(opw, _batch_solver(W2, W1, args.batch_precision), gw, BATCH_LOADS[:1], lift=lw)
     del opw
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        torch.cuda.synchronize()
+        dist.barrier()
     with clocks:
         x, st = B.newton_solve_batched(op, _batch_solver(U2, U1, args.batch_precision), g, BATCH_LOADS, lift=lift)
+    st.seconds = max_over_ranks(st.seconds)
     plain = {"seconds": st.seconds, "newton_sweeps": st.newton_sweeps, "krylov_sweeps": int(sum(st.krylov_sweeps)),
              "newton_iters_mean": float(st.newton_iters.mean()), "krylov_iters_mean": float(st.krylov_iters.mean()),
              "krylov_iters_max": int(st.krylov_iters.max()), "converged": int(st.converged.sum()), "pmg": st.pmg}
@@ -640,29 +663,40 @@ def batch_main(args):
         learned.attach(ns.prec, net)
         holder["prec"] = ns.prec
 
+    if world > 1:
+        torch.cuda.synchronize()
+        dist.barrier()
     x2, st2 = B.newton_solve_batched(op, _batch_solver(U2, U1, args.batch_precision), g, BATCH_LOADS, lift=lift,
                                      on_setup=attach)
+    st2.seconds = max_over_ranks(st2.seconds)
     acc = learned.stats(holder["prec"]) if "prec" in holder else {}
     lrn = {"seconds": st2.seconds, "newton_sweeps": st2.newton_sweeps, "krylov_sweeps": int(sum(st2.krylov_sweeps)),
            "newton_iters_mean": float(st2.newton_iters.mean()), "krylov_iters_mean": float(st2.krylov_iters.mean()),
            "krylov_iters_max": int(st2.krylov_iters.max()), "converged": int(st2.converged.sum()),
            "corrections": acc, "train_seconds": t_train, "train_loss": loss,
            "solution_rel_diff_vs_plain": float(torch.linalg.norm(x2 - x) / torch.linalg.norm(x))}
-    cpu = None if args.no_cpu else batch_cpu_sample(problems)
+    cpu = None if (args.no_cpu or rank != 0) else batch_cpu_sample(problems)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     line = {"metric": f"seconds to 1e-8 for {args.batch_count} batched SVK Q2 Newton solves (plain p-MG)",
-            "value": plain["seconds"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
-            "ms_per_step": plain["seconds"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "value": plain["seconds"], "unit": "s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": plain["seconds"] * 1e3, "higher_is_better": False, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64" if args.batch_precision == "fp64" else "f64 outer / f32 cycle",
             "data": "synthetic",
             "config": {"workload": "batched Newton, SVK Q2 cubes n ~ U{8..24}, (lambda, mu) log-uniform, seed 4",
-                       "problems": args.batch_count, "free_dofs": U2.nfree, "coarse_free_dofs": U1.nfree,
+                       "problems": args.batch_count, "parallelism": f"problems sharded over {world} GPU(s)",
+                       "free_dofs_rank0": U2.nfree, "coarse_free_dofs": U1.nfree,
                        "cells": U2.mesh.ncells, "loads": list(BATCH_LOADS), "setup_seconds": t_setup,
                        "levels": "Q2 -> Q1 (Chebyshev 4; coarse: 20 block-Jacobi CG steps per problem)",
                        "precision": args.batch_precision},
             "clocks": clocks.summary(), "plain": plain, "learned": lrn,
             "gain_learned_vs_plain": plain["seconds"] / lrn["seconds"]}
     if cpu is not None:
-        est = cpu["seconds_per_free_dof"] * U2.nfree
+        all_free = sum(3 * (2 * q.n - 1) * (2 * q.n + 1) ** 2 for q in B.draw_batch(256, seed=4)[:args.batch_count])
+        est = cpu["seconds_per_free_dof"] * all_free
         line["cpu_baseline"] = {"value": est, "unit": "s (extrapolated by free dofs)", "cores": cpu["cores"],
                                 "kind": cpu["kind"], "sample": cpu["sample"]}
     print(json.dumps(line))

@@ -224,6 +224,20 @@ def newton_solve_batched(op, solver: S.MatrixFreeSolver, g_full: np.ndarray, loa
     return x, st
 
 
+def shard_problems(problems, rank: int, world: int):
+    """Indices of the problems rank ``rank`` of ``world`` solves: independent problems shard with no
+    exchange; greedy balance of the free-dof counts (largest first onto the least loaded rank),
+    deterministic, so every rank computes the same partition without communicating."""
+    cost = [3 * (2 * q.n + 1) ** 3 for q in problems]
+    load = [0] * world
+    owner = [0] * len(problems)
+    for k in sorted(range(len(problems)), key=lambda k: (-cost[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        owner[k] = r
+        load[r] += cost[k]
+    return [k for k in range(len(problems)) if owner[k] == rank]
+
+
 @dataclasses.dataclass(frozen=True)
 class BatchProblem:
     n: int          # cells per direction
