@@ -1233,6 +1233,7 @@ struct hfk_pmg {
   std::vector<char> lok;
   bool ok = false, built = false;
   int since = 0, nupdate = 0, nbuild = 0;
+  int band = -1;  // lower bandwidth of the coarse level's pattern (computed once)
   std::vector<std::unique_ptr<LevelWork<double>>> w64;
   std::vector<std::unique_ptr<LevelWork<float>>> w32;
   // coarse: dense Cholesky factor (lower) of the assembled coarse tangent, or (HFK_COARSE_CG) a
@@ -1280,6 +1281,30 @@ void pmg_bind_stream(hfk_pmg* m) {
   for (int l = 1; l < m->L; ++l) m->lv[l]->stream = m->lv[0]->stream;
 }
 
+__global__ void lower_bandwidth_kernel(int64_t n, const int64_t* colptr, const int64_t* rowval, int* band) {
+  int mine = 0;
+  for (int64_t c = blockIdx.x; c < n; c += gridDim.x)
+    for (int64_t k = colptr[c] - 1 + threadIdx.x; k < colptr[c + 1] - 1; k += blockDim.x)
+      mine = max(mine, (int)(rowval[k] - 1 - c));
+  atomicMax(band, mine);
+}
+
+void ensure_blas(hfk_pmg* m) {
+  if (m->blas) return;
+  if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
+  // a fixed workspace, so that the captured cycle never asks cuBLAS to allocate
+  m->blas_ws.resize(32u << 20);
+  if (cublasSetWorkspace(m->blas, m->blas_ws.p, m->blas_ws.n) != CUBLAS_STATUS_SUCCESS)
+    throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasSetWorkspace failed"};
+}
+
+// Cholesky factor of the assembled coarse level (in place of the reference's LU, the matrix being
+// symmetric positive definite). The coarse matrix is banded in the node-major numbering
+// (bandwidth b ~ 3 (n_x n_y + n_x + 1) dofs), and a Cholesky factor keeps the band, so the
+// factorisation runs over the band only: per block column of T = 256, a dense potrf of the
+// diagonal block, a triangular solve of the b rows below it and a symmetric rank-T update of the
+// b x b window that follows: O(n b^2) work instead of O(n^3). A matrix whose band is wide
+// (b >= n / 3) takes the dense potrf.
 void coarse_factor(hfk_pmg* m) {
   hfk_problem* c = m->lv[m->L - 1];
   pattern_build_dev(c);
@@ -1296,22 +1321,56 @@ void coarse_factor(hfk_pmg* m) {
       throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cusolverDnCreate failed"};
   }
   cusolverDnSetStream(m->solver, c->stream);
+  if (m->band < 0) {  // the pattern's lower bandwidth, once
+    DBuf<int> bd;
+    bd.resize(1);
+    bd.zero(c->stream);
+    lower_bandwidth_kernel<<<(int)std::min<int64_t>(n, 4096), 128, 0, c->stream>>>(n, c->colptr.p, c->rowval.p, bd.p);
+    check_launch(c);
+    HFK_CUDA(cudaMemcpyAsync(&m->band, bd.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HFK_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  constexpr int T = 256;
+  const bool banded = (int64_t)m->band * 3 < n;
+  const int nt = banded ? (int)((n + T - 1) / T) : 1;
   int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Lc.p, (int)n, &lwork) !=
+  if (cusolverDnDpotrf_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, banded ? T : (int)n, m->Lc.p, (int)n, &lwork) !=
       CUSOLVER_STATUS_SUCCESS)
     throw Error{HFK_ERR_CUDA, "HyperFEMKernels: potrf_bufferSize failed"};
   if (m->potrf_work.n < (size_t)lwork + 1) m->potrf_work.resize((size_t)lwork + 1);
-  m->potrf_info.resize(1);
-  DBuf<double>& work = m->potrf_work;
-  DBuf<int>& info = m->potrf_info;
+  if (m->potrf_info.n < (size_t)nt) m->potrf_info.resize(nt);
+  m->potrf_info.zero(c->stream);
+  double* A = m->Lc.p;
+  int* info = m->potrf_info.p;
   cudaEvent_t e0, e1;
   HFK_CUDA(cudaEventCreate(&e0));
   HFK_CUDA(cudaEventCreate(&e1));
   HFK_CUDA(cudaEventRecord(e0, c->stream));
-  cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, m->Lc.p, (int)n, work.p, lwork, info.p);
+  if (!banded) {
+    cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, A, (int)n, m->potrf_work.p, lwork, info);
+  } else {
+    ensure_blas(m);
+    cublasSetStream(m->blas, c->stream);
+    const double one = 1.0, minus = -1.0;
+    for (int k = 0; k < nt; ++k) {
+      const int64_t k0 = (int64_t)k * T;
+      const int kk = (int)std::min<int64_t>(T, n - k0);
+      double* Akk = A + k0 + n * k0;
+      cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, kk, Akk, (int)n, m->potrf_work.p, lwork, info + k);
+      const int64_t r0 = k0 + kk, r1 = std::min<int64_t>(n, k0 + kk + m->band);
+      const int nr = (int)(r1 - r0);
+      if (nr <= 0) continue;
+      double* Aik = A + r0 + n * k0;
+      if (cublasDtrsm(m->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nr, kk,
+                      &one, Akk, (int)n, Aik, (int)n) != CUBLAS_STATUS_SUCCESS ||
+          cublasDsyrk(m->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, nr, kk, &minus, Aik, (int)n, &one, A + r0 + n * r0,
+                      (int)n) != CUBLAS_STATUS_SUCCESS)
+        throw Error{HFK_ERR_CUDA, "HyperFEMKernels: banded Cholesky update of the coarse level failed"};
+    }
+  }
   HFK_CUDA(cudaEventRecord(e1, c->stream));
-  int h_info = 0;
-  HFK_CUDA(cudaMemcpyAsync(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<int> h_info(nt, 0);
+  HFK_CUDA(cudaMemcpyAsync(h_info.data(), info, nt * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HFK_CUDA(cudaStreamSynchronize(c->stream));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
@@ -1320,7 +1379,7 @@ void coarse_factor(hfk_pmg* m) {
   cudaEventDestroy(e1);
   // the lower triangle now holds the Cholesky factor L (A = L L^T); the cycle applies A^-1 by two
   // triangular solves
-  m->coarse_ok = h_info == 0;
+  m->coarse_ok = std::all_of(h_info.begin(), h_info.end(), [](int v) { return v == 0; });
   if (m->coarse_ok) m->nbuild++;
 }
 
@@ -1345,16 +1404,12 @@ void coarse_cg_update(hfk_pmg* m) {
 void coarse_solve(hfk_pmg* m, const double* b, double* x) {
   hfk_problem* c = m->lv[m->L - 1];
   const int64_t n = c->nfree;
-  if (!m->blas) {
-    if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
-    // a fixed workspace, so that the captured cycle never asks cuBLAS to allocate
-    m->blas_ws.resize(32u << 20);
-    if (cublasSetWorkspace(m->blas, m->blas_ws.p, m->blas_ws.n) != CUBLAS_STATUS_SUCCESS)
-      throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasSetWorkspace failed"};
-  }
+  ensure_blas(m);
   cublasSetStream(m->blas, c->stream);
   HFK_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   const double one = 1.0;
+  // dense triangular solves (zeros outside the band): measured faster here than block-column
+  // trsv/gemv calls over the band
   if (cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
                   m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS ||
       cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,

@@ -238,6 +238,25 @@ def test_vcycle_parity_with_preconditioned_eigenvalue_estimate():
     assert reldiff(st.ldiv(np.zeros(Vs[0].nfree), r), mg.ldiv(r)) < 1e-9
 
 
+def test_banded_coarse_factor_matches_the_oracle_vcycle():
+    # an elongated mesh: the coarse level's band is narrow against its size, so the Cholesky factor
+    # is computed block column by block column over the band (several 256-row blocks)
+    m = CartesianMesh((3, 3, 40), domain=(0.0, 1.0, 0.0, 1.0, 0.0, 10.0))
+    g = lambda x: np.stack([0.01 * x[:, 2], 0 * x[:, 0], 0 * x[:, 0]], axis=1)
+    Vs = [VectorLagrangeSpace(m, o, ("z0", "z1"), g=g if o == 2 else None) for o in (2, 1)]
+    res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = svk_state(Vs[0], amp=1e-3, disp=0.0)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=2)), mf)
+    assert st.ok and Vs[1].nfree > 3 * 256
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_SVK, (2.0, 1.0), degree=2)
+    mg.update(x, Vs[0].dirichlet_values)
+    r = np.random.default_rng(4).standard_normal(Vs[0].nfree)
+    assert reldiff(st.ldiv(np.zeros(Vs[0].nfree), r), mg.ldiv(r)) < 1e-9
+
+
 def test_pmg_follows_the_prepared_dirichlet_values():
     # the hierarchy is built at the state the Jacobian was prepared at, not at the space's values
     Vs, res, jac = _pmg_case(3, (2, 1), "svk")
