@@ -236,6 +236,7 @@ def engine(args):
         torch.cuda.synchronize()
         err32 = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
         extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
+        extra["autotuned_launch_shape"] = {k: op.problem.tuning(*k.split("_")) for k in ("jv_fp64", "jv_fp32")}
         extra.update(assembly_case(torch, dev, stream, timed))
         extra.update(jv_sizes_case(torch, dev, stream, timed))
         extra.update(oseen_case(torch, dev, stream, timed))

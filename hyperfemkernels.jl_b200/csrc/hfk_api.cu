@@ -240,29 +240,28 @@ CellData cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) 
 
 // ---- cell-kernel dispatch over (Q, P) ----------------------------------------------------------
 template <int Q, int P, int MODE, typename R>
-void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
-  constexpr int WARPS = 4;
+void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int warps) {
   using S = TPShape<Q, P>;
-  const size_t smem = cell_smem_bytes<Q, P, R>(WARPS);
-  static bool attr = false;
-  if (!attr) {
+  const size_t smem = cell_smem_bytes<Q, P, R>(warps);
+  static size_t attr = 0;
+  if (smem > attr) {
     HFK_CUDA(cudaFuncSetAttribute(cell_kernel<Q, P, MODE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
+    attr = smem;
   }
-  const int per_cta = WARPS * S::CPW;
+  const int per_cta = warps * S::CPW;
   const int grid = (ncl + per_cta - 1) / per_cta;
   if (grid == 0) return;
-  cell_kernel<Q, P, MODE, R><<<grid, WARPS * 32, smem, p->stream>>>(cell_data(p, cells, ncl), make_tab<R>(p), io);
+  cell_kernel<Q, P, MODE, R><<<grid, warps * 32, smem, p->stream>>>(cell_data(p, cells, ncl), make_tab<R>(p), io);
   check_launch(p);
 }
 
 template <int MODE, typename R>
-void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
+void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int warps = 4) {
   const int key = p->Q * 10 + p->P;
   switch (key) {
 #define HFK_CASE(Qv, Pv) \
   case Qv * 10 + Pv:     \
-    launch_cell<Qv, Pv, MODE, R>(p, cells, ncl, io); \
+    launch_cell<Qv, Pv, MODE, R>(p, cells, ncl, io, warps); \
     return;
     HFK_CASE(2, 2)
     HFK_CASE(2, 3)
@@ -293,17 +292,68 @@ bool use_atomic_scatter(const hfk_problem* p) {
 }
 
 template <int MODE, typename R>
-void run_cells(hfk_problem* p, CellIO<R> io) {
-  if (use_atomic_scatter(p)) {
+void run_cells_as(hfk_problem* p, CellIO<R> io, bool atomic, int warps) {
+  if (atomic) {
     io.atomic = 1;
-    dispatch_cell<MODE, R>(p, nullptr, p->ncells, io);
+    dispatch_cell<MODE, R>(p, nullptr, p->ncells, io, warps);
     return;
   }
   io.atomic = 0;
   for (int c = 0; c < p->ncolors; ++c) {
     const int n = p->color_start[c + 1] - p->color_start[c];
-    dispatch_cell<MODE, R>(p, p->cells_by_color.p + p->color_start[c], n, io);
+    dispatch_cell<MODE, R>(p, p->cells_by_color.p + p->color_start[c], n, io, warps);
   }
+}
+
+// Launch-shape autotuner (per problem, per kernel mode and precision, so per degree): on the first
+// AUTO call the kernel runs with each candidate (atomic or colour-by-colour scatter, 2 or 4 warps
+// per CTA), timed with CUDA events, and the fastest is kept. Outputs are zeroed before each
+// candidate and once more before the real run. No tuning while the stream is being captured (the
+// V-cycle is captured from its second application, when every kernel of it has run once).
+template <int MODE, typename R>
+void run_cells(hfk_problem* p, CellIO<R> io) {
+  if (p->scatter != HFK_SCATTER_AUTO) {
+    run_cells_as<MODE, R>(p, io, p->scatter == HFK_SCATTER_ATOMIC, 4);
+    return;
+  }
+  const int key = MODE * 2 + (sizeof(R) == sizeof(float) ? 1 : 0);
+  auto it = p->tuned.find(key);
+  if (it == p->tuned.end()) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    HFK_CUDA(cudaStreamIsCapturing(p->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone || !io.y) {
+      run_cells_as<MODE, R>(p, io, true, 4);
+      return;
+    }
+    const int cand[4][2] = {{1, 4}, {1, 2}, {0, 4}, {0, 2}};
+    cudaEvent_t e0, e1;
+    HFK_CUDA(cudaEventCreate(&e0));
+    HFK_CUDA(cudaEventCreate(&e1));
+    float best = 0;
+    int pick = 0;
+    for (int c = 0; c < 4; ++c) {
+      float t = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        HFK_CUDA(cudaMemsetAsync(io.y, 0, p->nfree * sizeof(R), p->stream));
+        HFK_CUDA(cudaEventRecord(e0, p->stream));
+        run_cells_as<MODE, R>(p, io, cand[c][0] != 0, cand[c][1]);
+        HFK_CUDA(cudaEventRecord(e1, p->stream));
+        HFK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        HFK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t = std::min(t, ms);
+      }
+      if (c == 0 || t < best) {
+        best = t;
+        pick = c;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    it = p->tuned.emplace(key, std::make_pair(cand[pick][0] != 0, cand[pick][1])).first;
+    HFK_CUDA(cudaMemsetAsync(io.y, 0, p->nfree * sizeof(R), p->stream));
+  }
+  run_cells_as<MODE, R>(p, io, it->second.first, it->second.second);
 }
 
 // ---- colouring (color_cells, src/coloring.jl:4-28) --------------------------------------------
@@ -1749,6 +1799,16 @@ int hfk_problem_set_stream(hfk_problem* p, void* stream) {
   HFK_REQUIRE(p, HFK_ERR_ARG, "null handle");
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+  HFK_API_END
+}
+
+int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* warps) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && atomic && warps && (precision == HFK_FP64 || precision == HFK_FP32), HFK_ERR_ARG, "invalid argument");
+  const int internal = mode == 0 ? MODE_JV : (mode == 1 ? MODE_RESIDUAL : MODE_JV_STORED);
+  auto it = p->tuned.find(internal * 2 + (precision == HFK_FP32 ? 1 : 0));
+  *atomic = it == p->tuned.end() ? -1 : (int)it->second.first;
+  *warps = it == p->tuned.end() ? 0 : it->second.second;
   HFK_API_END
 }
 

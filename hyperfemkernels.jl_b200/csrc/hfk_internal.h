@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "../../include/hfk.h"
@@ -190,5 +191,6 @@ struct hfk_problem {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int launches = 0;
   int scatter = HFK_SCATTER_AUTO;
+  std::map<int, std::pair<bool, int>> tuned;  // autotuned (atomic scatter, warps per CTA) per kernel mode
   hfk::CGWork cg;
 };

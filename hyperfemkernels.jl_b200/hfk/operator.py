@@ -70,6 +70,13 @@ class Problem:
         m = {"auto": _lib.SCATTER_AUTO, "coloured": _lib.SCATTER_COLOURED, "atomic": _lib.SCATTER_ATOMIC}[mode]
         call("hfk_problem_set_scatter", self.h, m)
 
+    def tuning(self, kernel: str = "jv", precision: str = "fp64"):
+        """The launch-shape autotuner's choice: {"atomic": bool, "warps": int} or None (not run yet)."""
+        a, w = ctypes.c_int(), ctypes.c_int()
+        call("hfk_problem_tuning", self.h, {"jv": 0, "residual": 1, "jv_stored": 2}[kernel],
+             _lib.FP32 if precision == "fp32" else _lib.FP64, ctypes.byref(a), ctypes.byref(w))
+        return None if a.value < 0 else {"atomic": bool(a.value), "warps": w.value}
+
     def launches(self) -> int:
         c = ctypes.c_int64()
         call("hfk_launch_count", self.h, ctypes.byref(c))

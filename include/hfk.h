@@ -77,13 +77,19 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
 /* Scatter of the sum-factorised kernels (residual, products): colour by colour with plain
  * read-modify-writes (deterministic, the reference's race-free colouring, src/coloring.jl:1-3), or
  * one launch over all cells with FP64 atomics (the summation order, hence the last bit, varies
- * between runs). AUTO (default) is the atomic scatter (faster on B200: one launch, no read of the
- * output before the write); COLOURED gives bit-reproducible results. The nodal blocks follow the
- * same setting; the assembled Jacobian always scatters by colour. */
+ * between runs). AUTO (default) is autotuned per kernel mode and precision on the first call (the
+ * atomic or the colour-by-colour scatter, 2 or 4 warps per CTA, timed with CUDA events; on B200
+ * the atomic scatter usually wins: one launch, no read of the output before the write); COLOURED
+ * gives bit-reproducible results. The nodal blocks scatter atomically unless COLOURED is set; the
+ * assembled Jacobian always scatters by colour. */
 #define HFK_SCATTER_AUTO 0
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2
 int hfk_problem_set_scatter(hfk_problem* p, int mode);
+/* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
+ * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), warps per CTA; atomic = -1 if
+ * that kernel has not run under AUTO yet. No counterpart in the reference. */
+int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* warps);
 /* Number of kernels this handle launched so far (launch accounting for benchmarks). */
 int hfk_launch_count(hfk_problem* p, int64_t* count);
 

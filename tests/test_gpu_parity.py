@@ -115,6 +115,20 @@ def test_device_pointers_and_host_pointers_agree():
     assert np.array_equal(bd.cpu().numpy(), b_host)
 
 
+def test_autotuned_launch_shape_gives_the_same_product():
+    V, op, orc = make(2, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    assert op.problem.tuning("jv") is None
+    dx = np.random.default_rng(5).standard_normal(V.nfree)
+    y1 = mf.mul(np.zeros(V.nfree), dx)  # first AUTO call: candidates timed, the fastest kept
+    t = op.problem.tuning("jv")
+    assert t is not None and t["warps"] in (2, 4)
+    y2 = mf.mul(np.zeros(V.nfree), dx)
+    assert reldiff(y1, y2) < 1e-14 and reldiff(y1, orc.jacobian(x, V.dirichlet_values) @ dx) < TOL64
+
+
 @pytest.mark.parametrize("order", [2, 4])
 def test_atomic_and_coloured_scatter_agree(order):
     V, op, orc = make(order, jac="matrixfree")
