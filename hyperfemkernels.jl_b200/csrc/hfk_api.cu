@@ -1199,6 +1199,54 @@ void residual_dev(hfk_problem* p, const double* u, const double* dvals, double* 
 
 }  // namespace
 
+// ---- functionals (KernelFunctional, src/functionals.jl:10-27) ----------------------------------
+__global__ void functional_finish_kernel(int64_t nw, const double* red, double* out) {
+  double s = 0, mn = INFINITY;
+  for (int64_t i = threadIdx.x; i < nw; i += blockDim.x) {
+    s += red[2 * i];
+    mn = fmin(mn, red[2 * i + 1]);
+  }
+  __shared__ double ss[32], sm[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    ss[w] = s;
+    sm[w] = mn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = INFINITY;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      a += ss[i];
+      b = fmin(b, sm[i]);
+    }
+    out[0] = a;
+    out[1] = b;
+  }
+}
+
+// out[0] = Σ_cells Σ_q Ψ(F) dV, out[1] = min_q det F (device), at the state (u, dvals)
+void functional_dev(hfk_problem* p, const double* u, const double* dvals, double* out) {
+  require_tp(p);
+  constexpr int WARPS = 4;
+  const int m = std::max(p->Q, p->P);
+  const int cpw = std::max(1, 32 / (m * m));
+  const int64_t grid = ((int64_t)p->ncells + WARPS * cpw - 1) / (WARPS * cpw);
+  const int64_t nw = grid * WARPS;
+  p->func_red.resize((size_t)2 * nw);
+  CellIO<double> io{};
+  io.u = u;
+  io.dvals = dvals;
+  io.red = p->func_red.p;
+  dispatch_cell<MODE_ENERGY, double>(p, nullptr, p->ncells, io, WARPS);
+  functional_finish_kernel<<<1, 1024, 0, p->stream>>>(nw, p->func_red.p, out);
+  check_launch(p);
+}
+
 // ---- transfers and p-multigrid handles ---------------------------------------------------------
 struct hfk_transfer {
   hfk_problem* fine = nullptr;
@@ -1799,6 +1847,23 @@ int hfk_problem_set_stream(hfk_problem* p, void* stream) {
   HFK_REQUIRE(p, HFK_ERR_ARG, "null handle");
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+  HFK_API_END
+}
+
+int hfk_functional(hfk_problem* p, const double* x, const double* dvals, int kind, double* out) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && x && out && (dvals || p->ndir == 0), HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(kind == HFK_FUNCTIONAL_ENERGY || kind == HFK_FUNCTIONAL_MIN_DETF, HFK_ERR_ARG,
+              "functional kind must be HFK_FUNCTIONAL_ENERGY or HFK_FUNCTIONAL_MIN_DETF");
+  const double* dx = dev_in(x, p->nfree, p->stage_in, p->stream);
+  const double* dd = dvals ? dev_in(dvals, p->ndir, p->stage_in2, p->stream) : nullptr;
+  DBuf<double> o;
+  o.resize(2);
+  functional_dev(p, dx, dd, o.p);
+  double h[2];
+  HFK_CUDA(cudaMemcpyAsync(h, o.p, sizeof h, cudaMemcpyDeviceToHost, p->stream));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  *out = kind == HFK_FUNCTIONAL_ENERGY ? h[0] : h[1];
   HFK_API_END
 }
 

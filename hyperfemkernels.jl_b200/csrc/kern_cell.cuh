@@ -1,6 +1,7 @@
 // Sum-factorised cell kernels for a 3-component Lagrangian field on hexahedra:
 //   MODE_RESIDUAL  residual of the law at the state u (gathers u)
 //   MODE_PREP_F    deformation gradient F = I + grad u at every point, stored (gathers u)
+//   MODE_ENERGY    the stored energy Σ Ψ(F) dV and min det F of the cells (gathers u; per-warp partials)
 //   MODE_JV        J(u) dx with the tangent re-evaluated from the stored F (gathers dx)
 //   MODE_JV_STORED J(u) dx with the reference's stored per-point tangents T, inv(Jt), dV
 //
@@ -21,7 +22,7 @@
 
 namespace hfk {
 
-enum CellMode { MODE_RESIDUAL = 0, MODE_JV = 1, MODE_JV_STORED = 2, MODE_PREP_F = 3 };
+enum CellMode { MODE_RESIDUAL = 0, MODE_JV = 1, MODE_JV_STORED = 2, MODE_PREP_F = 3, MODE_ENERGY = 4 };
 
 template <int Q, int P>
 struct TPShape {
@@ -85,6 +86,7 @@ struct CellIO {
   const double* iJtq;
   const double* dVq;
   int atomic;       // 1: atomicAdd scatter (all cells in one launch)
+  double* red;      // MODE_ENERGY: per warp of the grid, (Σ Ψ dV, min det F)
 };
 
 template <int Q, int P, int MODE, typename R>
@@ -111,7 +113,13 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
   const int list_index = (blockIdx.x * nwarps + warp) * CPW + (active ? slot : 0);
   const int cell = active && list_index < cd.ncells_list ? (cd.cells ? cd.cells[list_index] : list_index) : 0;
   const bool has_cell = active && list_index < cd.ncells_list && !cd.skipped(cell);
-  if (__all_sync(0xffffffffu, !has_cell)) return;  // a warp without work (only __syncwarp below)
+  if (__all_sync(0xffffffffu, !has_cell)) {  // a warp without work (only __syncwarp below)
+    if (MODE == MODE_ENERGY && lane == 0) {
+      io.red[2 * ((size_t)blockIdx.x * nwarps + warp)] = 0.0;
+      io.red[2 * ((size_t)blockIdx.x * nwarps + warp) + 1] = INFINITY;
+    }
+    return;
+  }
   const R lam_c = (R)cd.lam_of(cell), mu_c = (R)cd.mu_of(cell);
 
   // ---- gather (gather_cell!, src/assembly.jl:1060-1070; increments are zero at Dirichlet dofs) ----
@@ -121,7 +129,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
     for (int j = t; j < NDL; j += TPC) {
       const int32_t id = gid[j];
       sid[j] = id;
-      if (MODE == MODE_RESIDUAL || MODE == MODE_PREP_F)
+      if (MODE == MODE_RESIDUAL || MODE == MODE_PREP_F || MODE == MODE_ENERGY)
         xl[j] = id > 0 ? io.u[id - 1] : (id < 0 ? io.dvals[-id - 1] : R(0));
       else
         xl[j] = id > 0 ? io.dx[id - 1] : R(0);
@@ -189,6 +197,7 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
   }
 
   // ---- pointwise phase: lane (a, b) owns the points (a, b, c) --------------------------------
+  double esum = 0.0, dmin = INFINITY;  // MODE_ENERGY
   if (t < PP) {
     const int ab = t;
     R yc[3][3][Q];  // this lane's column of the y-sweep: [field][kind][k]
@@ -248,6 +257,19 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
         }
         continue;
       }
+      if (MODE == MODE_ENERGY) {
+        if (has_cell) {
+          double Hd[9], Fd[9];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) {
+            Hd[i] = (double)H[i];
+            Fd[i] = Hd[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+          }
+          esum += (double)dV * law_energy(cd.law, (double)lam_c, (double)mu_c, Hd);
+          dmin = fmin(dmin, det3(Fd));
+        }
+        continue;
+      }
       R out[3][3];
       R outv[3] = {0, 0, 0};
       if (MODE == MODE_RESIDUAL) {
@@ -292,6 +314,18 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(Cell
     }
   }
   if (MODE == MODE_PREP_F) return;
+  if (MODE == MODE_ENERGY) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      esum += __shfl_down_sync(0xffffffffu, esum, o);
+      dmin = fmin(dmin, __shfl_down_sync(0xffffffffu, dmin, o));
+    }
+    if (lane == 0) {
+      io.red[2 * ((size_t)blockIdx.x * nwarps + warp)] = esum;
+      io.red[2 * ((size_t)blockIdx.x * nwarps + warp) + 1] = dmin;
+    }
+    return;
+  }
   __syncwarp();
 
   // ---- contraction (tp_contract! 3D): z (in place, per lane column), y, x -------------------

@@ -136,6 +136,25 @@ __device__ __forceinline__ void law_dstress_F(int law, R lam, R mu, const R* F, 
 
 // Full tangent T[(c*3+J) + 9*(k*3+L)] = dP[c,J]/dF[k,L] (point_tangent, src/factorforms.jl:316-322)
 // SVK: delta_ck S[L,J] + lam F[c,J] F[k,L] + mu F[c,L] F[k,J] + mu (F F')[c,k] delta_JL
+// Stored energy density of a law at H = grad u (H[c + 3J] = d u_c / d x_J): SVK
+// Ψ = μ E:E + λ/2 (tr E)², E = (FᵀF - I)/2; linear elasticity the same with E = sym(H)
+__device__ inline double law_energy(int law, double lam, double mu, const double* H) {
+  double E[9];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = 0; J < 3; ++J) {
+      double e = 0.5 * (H[I + 3 * J] + H[J + 3 * I]);
+      if (law != HFK_LAW_LINEAR_ELASTIC) e += 0.5 * (H[3 * I] * H[3 * J] + H[1 + 3 * I] * H[1 + 3 * J] + H[2 + 3 * I] * H[2 + 3 * J]);
+      E[I + 3 * J] = e;
+    }
+  double ee = 0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) ee += E[i] * E[i];
+  const double tr = E[0] + E[4] + E[8];
+  return mu * ee + 0.5 * lam * tr * tr;
+}
+
 // One 3x3 block of the tangent: Tb[J + 3 L] = T[(c,J),(k,L)] (the same closed forms as
 // law_tangent, for callers that need the (c, k) block only: no 81-entry array per thread)
 __device__ inline void law_tangent_block(int law, double lam, double mu, const double* H, int c, int k, double* Tb) {

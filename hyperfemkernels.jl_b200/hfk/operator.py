@@ -164,6 +164,14 @@ class KernelOperator:
     def dirichlet_values(self):
         return np.ascontiguousarray(self.U.dirichlet_values, dtype=np.float64)
 
+    def functional(self, x, dvals=None, kind: str = "energy") -> float:
+        """``KernelFunctional`` of the operator's law (src/functionals.jl:10-27): "energy" (the
+        stored energy Σ Ψ dV, reduce = :sum) or "min_detF" (min over the points, reduce = :min)."""
+        d = self.dirichlet_values() if dvals is None else dvals
+        out = ctypes.c_double()
+        call("hfk_functional", self.problem.h, ptr(x), ptr(d), {"energy": 0, "min_detF": 1}[kind], ctypes.byref(out))
+        return out.value
+
     def residual(self, b, x, dvals=None):
         """``residual!(b, op, x)`` (src/assembly.jl:909-916); Dirichlet values re-read from ``U``."""
         d = self.dirichlet_values() if dvals is None else dvals

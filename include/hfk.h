@@ -90,6 +90,16 @@ int hfk_problem_set_scatter(hfk_problem* p, int mode);
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), warps per CTA; atomic = -1 if
  * that kernel has not run under AUTO yet. No counterpart in the reference. */
 int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* warps);
+
+/* KernelFunctional (src/functionals.jl:10-27) for the recognised laws at the state (x, dvals):
+ * HFK_FUNCTIONAL_ENERGY = Σ_cells Σ_q Ψ(F) dV, the stored energy (reduce = :sum; SVK
+ * Ψ = μ E:E + λ/2 (tr E)², linear elasticity the same with E = sym ∇u; body-force work excluded:
+ * it is the linear term of the load vector), HFK_FUNCTIONAL_MIN_DETF = min over the quadrature
+ * points of det F (reduce = :min, unweighted: the injectivity check of a line search). One launch
+ * of the sum-factorised cell kernel and a deterministic reduction. */
+#define HFK_FUNCTIONAL_ENERGY 0
+#define HFK_FUNCTIONAL_MIN_DETF 1
+int hfk_functional(hfk_problem* p, const double* x, const double* dvals, int kind, double* out);
 /* Number of kernels this handle launched so far (launch accounting for benchmarks). */
 int hfk_launch_count(hfk_problem* p, int64_t* count);
 

@@ -1001,6 +1001,45 @@ void o_inject(void* h, const double* xf, const double* df, double* xc, double* d
   }
 }
 
+// KernelFunctional (src/functionals.jl:10-27) for the recognised laws: kind 0 = the stored energy
+// Σ_cells Σ_q Ψ(F) dV (reduce = :sum; SVK Ψ = μ E:E + λ/2 (tr E)², linear elasticity
+// Ψ = μ ε:ε + λ/2 (tr ε)²), kind 1 = min over the points of det F (reduce = :min, unweighted)
+double o_functional(void* h, const double* x, const double* dvals, int kind) {
+  auto& p = *(Problem*)h;
+  double total = kind == 0 ? 0.0 : INFINITY;
+  std::vector<double> xl(p.ndl);
+  for (int cell = 0; cell < p.ncells; ++cell) {
+    gather_cell(p, x, dvals, cell, xl.data());
+    for (int q = 0; q < p.np; ++q) {
+      double dV, iJt[9], F[9];
+      point_geometry(p, q, cell, dV, iJt);
+      point_F(p, xl.data(), q, iJt, F);
+      if (kind == 1) {
+        const double d = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) +
+                         F[6] * (F[1] * F[5] - F[4] * F[2]);
+        total = std::min(total, d);
+        continue;
+      }
+      double E[9];
+      for (int I = 0; I < 3; ++I)
+        for (int J = 0; J < 3; ++J) {
+          if (p.law == 2) {
+            E[I + 3 * J] = 0.5 * (F[I + 3 * J] + F[J + 3 * I]) - (I == J ? 1.0 : 0.0);
+          } else {
+            double s = 0;
+            for (int a = 0; a < 3; ++a) s += F[a + 3 * I] * F[a + 3 * J];
+            E[I + 3 * J] = 0.5 * (s - (I == J ? 1.0 : 0.0));
+          }
+        }
+      double ee = 0;
+      for (int i = 0; i < 9; ++i) ee += E[i] * E[i];
+      const double tr = E[0] + E[4] + E[8];
+      total += dV * (p.mu * ee + 0.5 * p.lam * tr * tr);
+    }
+  }
+  return total;
+}
+
 int o_max_threads() { return nthreads_or(0); }
 
 }  // extern "C"

@@ -68,6 +68,8 @@ def lib():
         L.o_prolongate.argtypes = [ctypes.c_void_p, c_dp, c_dp]
         L.o_restrict.argtypes = [ctypes.c_void_p, c_dp, c_dp]
         L.o_inject.argtypes = [ctypes.c_void_p, c_dp, c_dp, c_dp, c_dp]
+        L.o_functional.restype = ctypes.c_double
+        L.o_functional.argtypes = [ctypes.c_void_p, c_dp, c_dp, ctypes.c_int]
         L.o_oseen_create.restype = ctypes.c_void_p
         L.o_oseen_create.argtypes = [ctypes.c_int, ctypes.c_int] + [c_dp] * 7 + [c_ip, ctypes.c_int64, ctypes.c_int64,
                                                                                   c_dp]
@@ -194,6 +196,11 @@ class OracleProblem:
         lib().o_element_jacobian(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)),
                                  cell, point_block, _d(KeT))
         return KeT
+
+    def functional(self, x, dvals, kind="energy"):
+        """KernelFunctional restatement: "energy" (Σ Ψ dV) or "min_detF" (min over the points)."""
+        return float(lib().o_functional(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)),
+                                        {"energy": 0, "min_detF": 1}[kind]))
 
     def mf_prepare(self, x, dvals, nthreads=0):
         lib().o_mf_prepare(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)), nthreads)

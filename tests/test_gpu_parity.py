@@ -115,6 +115,24 @@ def test_device_pointers_and_host_pointers_agree():
     assert np.array_equal(bd.cpu().numpy(), b_host)
 
 
+@pytest.mark.parametrize("order,perturb,law", [(2, 0.0, "svk"), (2, 0.2, "svk"), (3, 0.0, "linear"), (4, 0.0, "svk")])
+def test_functionals_match_the_oracle_and_the_residual(order, perturb, law):
+    # KernelFunctional (src/functionals.jl:10-27): the energy's directional derivative is the residual
+    V, op, orc = make(order, perturb=perturb, law=law, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    d = V.dirichlet_values
+    e = op.functional(x, d, "energy")
+    assert abs(e - orc.functional(x, d, "energy")) < 1e-12 * abs(e)
+    dm = op.functional(x, d, "min_detF")
+    assert abs(dm - orc.functional(x, d, "min_detF")) < 1e-13
+    v = np.random.default_rng(3).standard_normal(V.nfree)
+    E = lambda t: op.functional(x + t * v, d)  # a polynomial of degree 4 in t: the 5-point rule is exact
+    h = 1e-3
+    de = (E(-2 * h) - 8 * E(-h) + 8 * E(h) - E(2 * h)) / (12 * h)
+    r = op.residual(np.zeros(V.nfree), x, d)
+    assert abs(de - r @ v) < 1e-9 * abs(r @ v)
+
+
 def test_autotuned_launch_shape_gives_the_same_product():
     V, op, orc = make(2, jac="matrixfree")
     x = svk_state(V, amp=1e-2)

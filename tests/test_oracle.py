@@ -325,3 +325,20 @@ def test_open_face_dirichlet_counts_of_the_assembly_case():
     assert (V.nfree, V.ndir) == (52077, 2166)
     Vc = VectorLagrangeSpace(CartesianMesh((20, 10, 10)), 2, ("x0", "x1"))
     assert Vc.ndir == 2 * 21 * 21 * 3
+
+
+@pytest.mark.parametrize("law", [O.LAW_SVK, O.LAW_LINEAR])
+def test_oracle_energy_derivative_is_the_residual(law):
+    # the KernelFunctional restatement: d/dε E(x + ε v) = R(x)·v (no body force)
+    V = svk_space(n=(2, 2, 2), order=2, perturb=0.2)
+    p = O.OracleProblem(V, Quadrature.gauss(4), law, (2.0, 1.0))
+    x = svk_state(V, amp=1e-2)
+    d = V.dirichlet_values
+    v = np.random.default_rng(4).standard_normal(V.nfree)
+    # the energy is a polynomial of degree 4 in the step: the 5-point derivative is exact for it
+    E = lambda t: p.functional(x + t * v, d)
+    h = 1e-3
+    de = (E(-2 * h) - 8 * E(-h) + 8 * E(h) - E(2 * h)) / (12 * h)
+    rv = p.residual(x, d) @ v
+    assert abs(de - rv) < 1e-9 * abs(rv)
+    assert 0.5 < p.functional(x, d, "min_detF") < 1.5
