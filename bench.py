@@ -296,8 +296,9 @@ def jv_sizes_case(torch, dev, stream, timed, cases=((2, 48), (4, 48), (4, 64))):
 
 
 def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
-    """Secondary (config 2): one FP64 residual and one CSC Jacobian of the Oseen-BDF2 step, Taylor-Hood
-    P2-P1 on the 32^3 cube split into 196 608 tetrahedra (859 812 dofs), rho = 1, mu = 1e-3, dt = 1e-3,
+    """Secondary (config 2): one FP64 residual and one CSC Jacobian of the Oseen-BDF2 step (volume terms
+    and the outlet boundary group), Taylor-Hood P2-P1 on the 32^3 cube split into 196 608 tetrahedra
+    (859 812 dofs), rho = 1, mu = 1e-3, dt = 1e-3,
     advection from a seeded sum of 8 divergence-free Fourier modes of amplitude 1 (u^n = u^(n-1));
     the CPU restatement (literal weak form, all host cores) timed on a 12^3 sample."""
     from hfk import _lib
@@ -308,6 +309,7 @@ def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
     un, und = V.interpolate_velocity(OS.fourier_field(2))
     params = OS.OseenParams(rho=1.0, mu=1e-3, dt=1e-3, bdf2=True)
     op = OS.OseenOperator(V, params, un, und)
+    op.set_outlet(OS.OutletFacets(m))  # the outlet boundary group (backflow, Robin, Windkessel)
     x = np.random.default_rng(0).standard_normal(V.nfree)
     A = op.sparsity_pattern()
     xd = torch.from_numpy(x).to(dev)
@@ -325,6 +327,7 @@ def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
     Vs = OS.TaylorHoodSpace(ms_)
     uns, unds = Vs.interpolate_velocity(OS.fourier_field(2))
     orc = O.OracleOseen(Vs, params, uns, unds)
+    orc.set_outlet(OS.OutletFacets(ms_))
     orc.pattern()
     xs = np.random.default_rng(0).standard_normal(Vs.nfree)
     t0 = time.perf_counter()

@@ -3196,6 +3196,11 @@ struct hfk_oseen {
   DBuf<double> w, N2, dN2, H2, N1, dN1, un, und, unm1, unm1d;
   double rho = 1, mu = 1e-3, dt = 1e-3;
   int bdf2 = 1;
+  // outlet boundary group (0 facets: none)
+  int nf = 0, nqf = 0;
+  DBuf<int32_t> fcell, fface;
+  DBuf<double> farea, fnormal, fw, fN;
+  double Pc = 0.7, ZA = 2.3;
 };
 
 namespace {
@@ -3246,6 +3251,15 @@ void oseen_run(hfk_oseen* o, OseenIO io) {
     oseen_kernel<<<n, OS_THREADS, smem, p->stream>>>(oseen_data(o, p->cells_by_color.p + p->color_start[c], n), io);
     check_launch(p);
   }
+}
+
+// the outlet boundary group after the volume terms (atomic scatter: its facets are few)
+void oseen_run_outlet(hfk_oseen* o, OseenIO io) {
+  if (!o->nf) return;
+  hfk_problem* p = &o->base;
+  OutletData fd{o->nf, o->nqf, o->fcell.p, o->fface.p, o->farea.p, o->fnormal.p, o->fw.p, o->fN.p, o->Pc, o->ZA};
+  oseen_outlet_kernel<<<o->nf, 128, 0, p->stream>>>(oseen_data(o, nullptr, p->ncells), fd, io);
+  check_launch(p);
 }
 
 void oseen_set_params(hfk_oseen* o, const double* params, int nparams) {
@@ -3391,6 +3405,7 @@ int hfk_oseen_residual(hfk_oseen* o, const double* x, const double* dvals, doubl
   io.b = dev_out(b, p->nfree, p->stage_out);
   HFK_CUDA(cudaMemsetAsync(io.b, 0, p->nfree * sizeof(double), p->stream));
   oseen_run(o, io);
+  oseen_run_outlet(o, io);
   finish_out(b, io.b, p->nfree, p->stream);
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   HFK_API_END
@@ -3407,7 +3422,34 @@ int hfk_oseen_jacobian(hfk_oseen* o, double* nzval) {
   io.nzval = is_device_ptr(nzval) ? nzval : p->nzval.p;
   HFK_CUDA(cudaMemsetAsync(io.nzval, 0, p->nnz * sizeof(double), p->stream));
   oseen_run(o, io);
+  oseen_run_outlet(o, io);
   finish_out(nzval, io.nzval, p->nnz, p->stream);
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  HFK_API_END
+}
+
+int hfk_oseen_set_outlet(hfk_oseen* o, int nfacets, const int32_t* cells, const int32_t* faces, const double* areas,
+                         const double* normals, int nq, const double* w, const double* N, double Pc, double ZA) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(o && nfacets >= 0, HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(nfacets == 0 || (cells && faces && areas && normals && w && N && nq > 0 && nq <= OS_MAXQF), HFK_ERR_ARG,
+              "outlet facets: null array or 0 < nq <= 32 violated");
+  hfk_problem* p = &o->base;
+  for (int f = 0; f < nfacets; ++f)
+    HFK_REQUIRE(cells[f] >= 0 && cells[f] < p->ncells && faces[f] >= 0 && faces[f] < 4, HFK_ERR_ARG,
+                "outlet facet: cell or local face out of range");
+  o->nf = nfacets;
+  o->nqf = nq;
+  o->Pc = Pc;
+  o->ZA = ZA;
+  if (nfacets) {
+    o->fcell.upload(cells, nfacets, p->stream);
+    o->fface.upload(faces, nfacets, p->stream);
+    o->farea.upload(areas, nfacets, p->stream);
+    o->fnormal.upload(normals, 3 * (size_t)nfacets, p->stream);
+    o->fw.upload(w, nq, p->stream);
+    o->fN.upload(N, (size_t)OS_NV * nq * 4, p->stream);
+  }
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   HFK_API_END
 }

@@ -300,4 +300,88 @@ __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO 
   }
 }
 
+// ---- the outlet boundary group (test/common.jl:194-210) ----------------------------------------
+// -∫ ρ negpart(w·n)(u·v) dΓ + ∫ ZA (u·n)(v·n) dΓ in a, -∫ Pc (v·n) dΓ in l, negpart(s) = (s - |s|)/2,
+// on the facets of one boundary part, each with its cell, local face, area and outward unit normal.
+constexpr int OS_MAXQF = 32;
+
+struct OutletData {
+  int nf, nqf;
+  const int32_t* cell;
+  const int32_t* face;
+  const double* area;
+  const double* normal;  // (3, nf)
+  const double* w;       // (nqf), sum 1
+  const double* N;       // (10, nqf, 4): the cell's P2 values at the points of each local face
+  double Pc, ZA;
+};
+
+__global__ void __launch_bounds__(128) oseen_outlet_kernel(OseenData d, OutletData fd, OseenIO io) {
+  __shared__ double phi[OS_MAXQF][OS_NV], c1[OS_MAXQF], c2[OS_MAXQF], dS[OS_MAXQF], uq[OS_MAXQF][3];
+  __shared__ double unl[30], uml[30], xl[30];
+  __shared__ int32_t sid[OS_NDL];
+  const int f = blockIdx.x, t = threadIdx.x;
+  if (f >= fd.nf) return;
+  const int cell = fd.cell[f], lf = fd.face[f];
+  const double n0 = fd.normal[3 * (size_t)f], n1 = fd.normal[3 * (size_t)f + 1], n2 = fd.normal[3 * (size_t)f + 2];
+  if (t < OS_NDL) sid[t] = d.ids[(size_t)cell * OS_NDL + t];
+  __syncthreads();
+  if (t < 30) {
+    const int32_t id = sid[t];
+    unl[t] = id > 0 ? d.un[id - 1] : (id < 0 ? d.und[-id - 1] : 0.0);
+    uml[t] = id > 0 ? d.unm1[id - 1] : (id < 0 ? d.unm1d[-id - 1] : 0.0);
+    if (io.mode == 0) xl[t] = id > 0 ? io.x[id - 1] : (id < 0 ? io.dvals[-id - 1] : 0.0);
+  }
+  __syncthreads();
+  for (int q = t; q < fd.nqf; q += blockDim.x) {
+    double w[3], u[3];
+    for (int a = 0; a < OS_NV; ++a) phi[q][a] = fd.N[a + OS_NV * (q + fd.nqf * lf)];
+    for (int c = 0; c < 3; ++c) {
+      double u0 = 0, u1 = 0, ux = 0;
+      for (int a = 0; a < OS_NV; ++a) {
+        u0 += phi[q][a] * unl[c * OS_NV + a];
+        u1 += phi[q][a] * uml[c * OS_NV + a];
+        if (io.mode == 0) ux += phi[q][a] * xl[c * OS_NV + a];
+      }
+      w[c] = d.bdf2 ? 2.0 * u0 - u1 : u0;
+      u[c] = ux;
+    }
+    const double wn = w[0] * n0 + w[1] * n1 + w[2] * n2;
+    dS[q] = fd.w[q] * fd.area[f];
+    c1[q] = -d.rho * 0.5 * (wn - fabs(wn)) * dS[q];
+    c2[q] = fd.ZA * dS[q];
+    for (int c = 0; c < 3; ++c) uq[q][c] = u[c];
+  }
+  __syncthreads();
+  const double nv[3] = {n0, n1, n2};
+  if (io.mode == 0) {  // residual rows of the velocity test functions (i, a)
+    if (t < 30) {
+      const int i = t / OS_NV, a = t % OS_NV;
+      double r = 0;
+      for (int q = 0; q < fd.nqf; ++q) {
+        const double un = uq[q][0] * n0 + uq[q][1] * n1 + uq[q][2] * n2;
+        r += phi[q][a] * (c1[q] * uq[q][i] + c2[q] * un * nv[i] + dS[q] * fd.Pc * nv[i]);
+      }
+      const int32_t id = sid[t];
+      if (id > 0) atomicAdd(&io.b[id - 1], r);
+    }
+    return;
+  }
+  if (t < OS_NV * OS_NV) {  // Jacobian: velocity pair (a, b), its 9 component entries
+    const int a = t % OS_NV, b = t / OS_NV;
+    double m1 = 0, m2 = 0;
+    for (int q = 0; q < fd.nqf; ++q) {
+      const double pp = phi[q][a] * phi[q][b];
+      m1 += c1[q] * pp;
+      m2 += c2[q] * pp;
+    }
+    const int32_t* pos = io.nzpos + (size_t)OS_NDL * OS_NDL * cell;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const int32_t ps = pos[(i * OS_NV + a) + OS_NDL * (j * OS_NV + b)];
+        if (ps > 0) atomicAdd(&io.nzval[ps - 1], (i == j ? m1 : 0.0) + nv[i] * nv[j] * m2);
+      }
+  }
+}
+
 }  // namespace hfk

@@ -101,6 +101,7 @@ SIGNATURES = {
     "hfk_oseen_residual": [_vp, _vp, _vp, _vp],
     "hfk_oseen_jacobian": [_vp, _vp],
     "hfk_oseen_launch_count": [_vp, _pi64],
+    "hfk_oseen_set_outlet": [_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _d, _d],
     "hfk_problem_set_segments": [_vp, _i, _vp, _vp, _vp],
     "hfk_problem_segments": [_vp, _pi],
     "hfk_problem_set_cell_params": [_vp, _vp],

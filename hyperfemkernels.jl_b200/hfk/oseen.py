@@ -56,6 +56,67 @@ class TetMesh:
         self.coords = np.asfortranarray(self.vertices[self.tets].transpose(2, 1, 0))
 
 
+# local faces of a tetrahedron: face f is opposite local vertex f
+FACES = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))
+# reference vertices
+REF_V = np.array([[0.0, 0, 0], [1.0, 0, 0], [0.0, 1, 0], [0.0, 0, 1]])
+
+
+def tri_quadrature(m: int = 3):
+    """Conical-product rule on the reference triangle (barycentric (s, t) in the unit simplex) with m²
+    points, exact for degree 2m - 1 (m = 3: degree 5, the backflow term's measure); weights sum to 1
+    (multiplied by the facet area)."""
+    from scipy.special import roots_jacobi
+
+    a, wa = roots_jacobi(m, 1, 0)
+    b, wb = roots_jacobi(m, 0, 0)
+    a, b = (a + 1) / 2, (b + 1) / 2
+    wa, wb = wa / 4, wb / 2
+    pts, ws = [], []
+    for i in range(m):
+        for j in range(m):
+            pts.append((a[i], b[j] * (1 - a[i])))
+            ws.append(wa[i] * wb[j] * 2)  # × 2: weights of the unit-area normalisation
+    return np.array(pts), np.array(ws)
+
+
+class OutletFacets:
+    """The boundary facets of the outlet x = 1: per facet its cell, the local face, the area and the
+    outward unit normal; and the P2 tables of the cell at the facet points for each local face."""
+
+    def __init__(self, mesh: TetMesh, quad_m: int = 3):
+        tets, X = mesh.tets, mesh.vertices
+        on = np.isclose(X[:, 0], 1.0)
+        cells, faces, areas, normals = [], [], [], []
+        for f_id, (i, j, k) in enumerate(FACES):
+            sel = np.nonzero(on[tets[:, i]] & on[tets[:, j]] & on[tets[:, k]])[0]
+            for c in sel:
+                P = X[tets[c, [i, j, k]]]
+                nrm = np.cross(P[1] - P[0], P[2] - P[0])
+                opp = X[tets[c, f_id]]
+                if nrm @ (P[0] - opp) < 0:
+                    nrm = -nrm
+                cells.append(c)
+                faces.append(f_id)
+                areas.append(np.linalg.norm(nrm) / 2)
+                normals.append(nrm / np.linalg.norm(nrm))
+        order = np.argsort(cells, kind="stable")
+        self.cells = np.array(cells, dtype=np.int32)[order]
+        self.faces = np.array(faces, dtype=np.int32)[order]
+        self.areas = np.array(areas)[order]
+        self.normals = np.ascontiguousarray(np.array(normals)[order].T)  # (3, nfacets)
+        self.nfacets = len(self.cells)
+        st, self.w = tri_quadrature(quad_m)
+        self.nq = len(self.w)
+        # P2 values of the cell at the facet points, per local face: (10, nq, 4)
+        N = np.zeros((NV, self.nq, 4))
+        for f_id, vs in enumerate(FACES):
+            V0, V1, V2 = REF_V[list(vs)]
+            for q, (s_, t_) in enumerate(st):
+                N[:, q, f_id] = p2_basis(V0 + s_ * (V1 - V0) + t_ * (V2 - V0))[0]
+        self.N = np.asfortranarray(N)
+
+
 def p2_basis(xi):
     """P2 basis values (10,) and reference gradients (10, 3) at xi (3,): vertices λ(2λ-1), edges 4λiλj."""
     lam = np.array([1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]])
@@ -256,6 +317,16 @@ class OseenOperator:
             except Exception:
                 pass
             self.h = None
+
+    def set_outlet(self, facets: "OutletFacets | None", Pc: float = 0.7, ZA: float = 2.3):
+        """The outlet boundary group (backflow, Robin, Windkessel pressure; the reference's Pc and ZA)."""
+        if facets is None:
+            call("hfk_oseen_set_outlet", self.h, 0, None, None, None, None, 0, None, None, Pc, ZA)
+            return
+        self._outlet = facets
+        call("hfk_oseen_set_outlet", self.h, facets.nfacets, ptr(facets.cells, np.int32), ptr(facets.faces, np.int32),
+             ptr(np.ascontiguousarray(facets.areas)), ptr(np.asfortranarray(facets.normals)), facets.nq,
+             ptr(np.ascontiguousarray(facets.w)), ptr(facets.N), Pc, ZA)
 
     def set_history(self, un, und, unm1, unm1d):
         """uⁿ and uⁿ⁻¹ (free and Dirichlet values of the trial space; pressure entries ignored)."""

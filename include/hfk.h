@@ -323,6 +323,14 @@ int hfk_oseen_pattern_get(hfk_oseen* o, int64_t* colptr, int64_t* rowval);
 int hfk_oseen_residual(hfk_oseen* o, const double* x, const double* dvals, double* b);
 int hfk_oseen_jacobian(hfk_oseen* o, double* nzval);
 int hfk_oseen_launch_count(hfk_oseen* o, int64_t* count);
+/* The outlet boundary group of the reference's Oseen problem (test/common.jl:194-210):
+ * -∫ ρ negpart(w·n)(u·v) dΓ (backflow) + ∫ ZA (u·n)(v·n) dΓ (Robin) in a, -∫ Pc (v·n) dΓ
+ * (Windkessel pressure) in l, added to the residual and the Jacobian. Per facet: its cell, the
+ * local face (opposite local vertex f), the area and the outward unit normal (3, nfacets); nq facet
+ * points with weights w summing to 1 and the cell's P2 values at them for each local face,
+ * N (10, nq, 4). nfacets = 0 removes the group. */
+int hfk_oseen_set_outlet(hfk_oseen* o, int nfacets, const int32_t* cells, const int32_t* faces, const double* areas,
+                         const double* normals, int nq, const double* w, const double* N, double Pc, double ZA);
 
 #ifdef __cplusplus
 }

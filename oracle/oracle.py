@@ -81,6 +81,8 @@ def lib():
         L.o_oseen_pattern_get.argtypes = [ctypes.c_void_p, c_lp, c_lp, c_ip]
         L.o_oseen_residual.argtypes = [ctypes.c_void_p, c_dp, c_dp, c_dp, ctypes.c_int]
         L.o_oseen_jacobian.argtypes = [ctypes.c_void_p, c_dp, ctypes.c_int]
+        L.o_oseen_set_outlet.argtypes = [ctypes.c_void_p, ctypes.c_int, c_ip, c_ip, c_dp, c_dp, ctypes.c_int, c_dp, c_dp,
+                                         ctypes.c_double, ctypes.c_double]
         _LIB = L
     return _LIB
 
@@ -597,6 +599,14 @@ class OracleOseen:
         if getattr(self, "h", None):
             lib().o_oseen_free(self.h)
             self.h = None
+
+    def set_outlet(self, facets, Pc=0.7, ZA=2.3):
+        """The outlet boundary group (a ``hfk.oseen.OutletFacets``), the reference's Pc and ZA."""
+        self._outlet = (facets.cells, facets.faces, np.ascontiguousarray(facets.areas), facets.normals,
+                        np.ascontiguousarray(facets.w), facets.N)
+        c, fa, ar, nr, w, N = self._outlet
+        lib().o_oseen_set_outlet(self.h, facets.nfacets, _i(c), _i(fa), _d(ar), _d(np.asfortranarray(nr)), facets.nq,
+                                 _d(w), _d(N), Pc, ZA)
 
     def element(self, cell):
         Ke = np.zeros((34, 34), order="F")

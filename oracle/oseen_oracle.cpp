@@ -32,6 +32,11 @@ struct Oseen {
   std::vector<std::vector<int32_t>> colors;
   std::vector<int64_t> colptr, rowval;
   std::vector<int32_t> nzpos;  // (34*34, ncells) 1-based, 0 = none
+  // outlet boundary group (test/common.jl:194-210): facets, their cell, local face, area, normal
+  int nf = 0, nqf = 0;
+  std::vector<int32_t> fcell, fface;
+  std::vector<double> farea, fnormal, fw, fN;  // fN (10, nqf, 4)
+  double Pc = 0.7, ZA = 2.3;
 };
 
 double det3(const double* A) {  // column-major
@@ -219,9 +224,62 @@ void element(const Oseen& o, int cell, double* Ke, double* Fe) {
   }
 }
 
+// outlet facet f: Kf[test + 34 trial] and Ff over the velocity dofs of its cell (test/common.jl:
+// -∫ρ negpart(w·n)(u·v) dΓ + ∫ ZA (u·n)(v·n) dΓ in a, -∫ Pc (v·n) dΓ in l; negpart(s) = (s - |s|)/2)
+void facet_element(const Oseen& o, int f, double* Kf, double* Ff) {
+  std::fill(Kf, Kf + NDL * NDL, 0.0);
+  std::fill(Ff, Ff + NDL, 0.0);
+  const int cell = o.fcell[f], lf = o.fface[f];
+  const int32_t* id = &o.ids[(size_t)cell * NDL];
+  const double* n = &o.fnormal[3 * (size_t)f];
+  for (int q = 0; q < o.nqf; ++q) {
+    const double* phi = &o.fN[NV * (q + o.nqf * lf)];
+    double w[3];
+    for (int c = 0; c < 3; ++c) {
+      double u0 = 0, u1 = 0;
+      for (int a = 0; a < NV; ++a) {
+        u0 += phi[a] * local_value(o, o.un, o.und, id[c * NV + a]);
+        u1 += phi[a] * local_value(o, o.unm1, o.unm1d, id[c * NV + a]);
+      }
+      w[c] = o.bdf2 ? 2.0 * u0 - u1 : u0;
+    }
+    const double wn = w[0] * n[0] + w[1] * n[1] + w[2] * n[2];
+    const double neg = 0.5 * (wn - std::fabs(wn));
+    const double dS = o.fw[q] * o.farea[f];
+    for (int te = 0; te < 30; ++te) {
+      double v[3] = {0, 0, 0};
+      v[te / NV] = phi[te % NV];
+      const double vn = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+      Ff[te] += dS * (-o.Pc * vn);
+      for (int tr = 0; tr < 30; ++tr) {
+        double u[3] = {0, 0, 0};
+        u[tr / NV] = phi[tr % NV];
+        const double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+        const double uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+        Kf[te + NDL * tr] += dS * (-o.rho * neg * uv + o.ZA * un * vn);
+      }
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+void o_oseen_set_outlet(void* h, int nf, const int32_t* cells, const int32_t* faces, const double* areas,
+                        const double* normals, int nqf, const double* w, const double* N, double Pc, double ZA) {
+  auto& o = *(Oseen*)h;
+  o.nf = nf;
+  o.nqf = nqf;
+  o.fcell.assign(cells, cells + nf);
+  o.fface.assign(faces, faces + nf);
+  o.farea.assign(areas, areas + nf);
+  o.fnormal.assign(normals, normals + 3 * (size_t)nf);
+  o.fw.assign(w, w + nqf);
+  o.fN.assign(N, N + (size_t)NV * nqf * 4);
+  o.Pc = Pc;
+  o.ZA = ZA;
+}
 
 void* o_oseen_create(int ncells, int nq, const double* w, const double* N2, const double* dN2, const double* H2,
                      const double* N1, const double* dN1, const double* coords, const int32_t* ids, int64_t nfree,
@@ -352,6 +410,19 @@ void o_oseen_residual(void* h, const double* x, const double* dvals, double* b, 
       }
     }
   }
+  std::vector<double> Kf(NDL * NDL), Ff(NDL);
+  for (int f = 0; f < o.nf; ++f) {  // outlet boundary group, serial (few facets)
+    facet_element(o, f, Kf.data(), Ff.data());
+    const int32_t* id = &o.ids[(size_t)o.fcell[f] * NDL];
+    double xl[NDL];
+    for (int j = 0; j < NDL; ++j) xl[j] = id[j] > 0 ? x[id[j] - 1] : (id[j] < 0 ? dvals[-id[j] - 1] : 0.0);
+    for (int i = 0; i < NDL; ++i) {
+      if (id[i] <= 0) continue;
+      double s = -Ff[i];
+      for (int j = 0; j < NDL; ++j) s += Kf[i + NDL * j] * xl[j];
+      b[id[i] - 1] += s;
+    }
+  }
 }
 
 void o_oseen_jacobian(void* h, double* nzval, int nthreads) {
@@ -372,6 +443,13 @@ void o_oseen_jacobian(void* h, double* nzval, int nthreads) {
           if (pos[e] > 0) nzval[pos[e] - 1] += Ke[e];
       }
     }
+  }
+  std::vector<double> Kf(NDL * NDL), Ff(NDL);
+  for (int f = 0; f < o.nf; ++f) {
+    facet_element(o, f, Kf.data(), Ff.data());
+    const int32_t* pos = &o.nzpos[(size_t)o.fcell[f] * NDL * NDL];
+    for (int e = 0; e < NDL * NDL; ++e)
+      if (pos[e] > 0) nzval[pos[e] - 1] += Kf[e];
   }
 }
 

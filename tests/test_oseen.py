@@ -126,6 +126,30 @@ def test_oracle_residual_is_affine_with_the_jacobian():
     assert np.abs(A0 - A0.T).max() < 1e-12 * np.abs(A0).max()
 
 
+def test_oracle_outlet_group_is_symmetric_and_affine():
+    # the outlet terms (test/common.jl:194-210): backflow and Robin parts are symmetric in (u, v);
+    # the Windkessel term is a load, so r(x) - r(0) = J x still holds with the group added
+    m, V, hist, x = _case(2)
+    params = OS.OseenParams()
+    plain = O.OracleOseen(V, params, *hist)
+    orc = O.OracleOseen(V, params, *hist)
+    F = OS.OutletFacets(m)
+    assert F.nfacets == 2 * m.n**2 and abs(F.areas.sum() - 1) < 1e-14
+    orc.set_outlet(F)
+    B = (orc.jacobian() - plain.jacobian()).toarray()
+    assert np.abs(B).max() > 0 and np.abs(B - B.T).max() < 1e-14 * np.abs(B).max()
+    d = V.dirichlet_values
+    r0, r1 = orc.residual(np.zeros(V.nfree), d), orc.residual(x, d)
+    assert reldiff(r1 - r0, orc.jacobian() @ x) < 1e-12
+    # at w = 0 (no history) the backflow part vanishes and the group is ZA ∫ (u·n)(v·n)
+    z = (np.zeros(V.nfree), np.zeros(V.ndir), np.zeros(V.nfree), np.zeros(V.ndir))
+    a, b = O.OracleOseen(V, params, *z), O.OracleOseen(V, params, *z)
+    b.set_outlet(F, ZA=1.0)
+    Bz = (b.jacobian() - a.jacobian()).toarray()
+    nx_rows = [V.gid_u[3 * g] - 1 for g in range(V.nnodes) if V.gid_u[3 * g] > 0]
+    assert np.abs(np.delete(np.delete(Bz, nx_rows, 0), nx_rows, 1)).max() < 1e-15  # only u_x·v_x on x = 1
+
+
 # ---- GPU ------------------------------------------------------------------------------------
 
 
@@ -140,6 +164,21 @@ def test_oseen_residual_and_jacobian_match_the_oracle(scatter):
     A = op.sparsity_pattern()
     cp, rv = orc.pattern()
     assert np.array_equal(A.indptr, cp - 1) and np.array_equal(A.indices, rv - 1)
+    assert reldiff(op.jacobian_values(np.zeros(A.nnz)), orc.jacobian_values()) < 1e-12
+    d = V.dirichlet_values
+    assert reldiff(op.residual(np.zeros(V.nfree), x, d), orc.residual(x, d)) < 1e-12
+
+
+@pytest.mark.gpu
+def test_oseen_outlet_group_matches_the_oracle():
+    m, V, hist, x = _case(3)
+    params = OS.OseenParams()
+    F = OS.OutletFacets(m)
+    op = OS.OseenOperator(V, params, *hist)
+    op.set_outlet(F, Pc=0.7, ZA=2.3)
+    orc = O.OracleOseen(V, params, *hist)
+    orc.set_outlet(F, Pc=0.7, ZA=2.3)
+    A = op.sparsity_pattern()
     assert reldiff(op.jacobian_values(np.zeros(A.nnz)), orc.jacobian_values()) < 1e-12
     d = V.dirichlet_values
     assert reldiff(op.residual(np.zeros(V.nfree), x, d), orc.residual(x, d)) < 1e-12
