@@ -4,7 +4,6 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
-#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -12,7 +11,6 @@
 #include <memory>
 #include <mutex>
 #include <string>
-#include <unordered_map>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -623,42 +621,31 @@ __global__ void store_tangents_kernel(CellData cd, const double* u, const double
 // ---- blocks -----------------------------------------------------------------------------------
 void build_block_structure(hfk_problem* p) {
   // field_blocks (src/preconditioners.jl:151-173): one block per node key (its 3 test ids), numbered
-  // in order of first appearance over cells and the caller's node order
-  struct KeyHash {
-    size_t operator()(const std::array<int32_t, 3>& k) const {
-      uint64_t h = (uint64_t)(uint32_t)k[0] * 0x9E3779B97F4A7C15ull;
-      h ^= (uint64_t)(uint32_t)k[1] + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2);
-      h ^= (uint64_t)(uint32_t)k[2] + 0x85EBCA77C2B2AE63ull + (h << 6) + (h >> 2);
-      return (size_t)h;
-    }
-  };
-  std::unordered_map<std::array<int32_t, 3>, int32_t, KeyHash> keys;
-  keys.reserve((size_t)p->nfree / 3 + 16);
+  // in order of first appearance over cells and the caller's node order. A free dof belongs to one
+  // node, so a node with a free dof is identified by its first free id: a direct-indexed table
+  // (O(1) per node, no hashing) gives the same numbering as a map of the keys.
+  std::vector<int32_t> block_by_first((size_t)p->nfree + 1, 0);
   std::vector<int32_t> dofs;
   std::vector<int32_t> block_of((size_t)p->nn * p->ncells, 0);  // tensor order
   std::vector<int> inv_node(p->nn);
   for (int lin = 0; lin < p->nn; ++lin) inv_node[p->nodeperm[lin]] = lin;
+  int32_t nb = 0;
   for (int cell = 0; cell < p->ncells; ++cell)
     for (int n = 0; n < p->nn; ++n) {
-      std::array<int32_t, 3> key;
-      bool anyfree = false;
+      int32_t key[3], first = 0;
       for (int c = 0; c < 3; ++c) {
         key[c] = p->h_ids[(size_t)cell * p->ndl + c * p->nn + n];
-        anyfree |= key[c] > 0;
+        if (!first && key[c] > 0) first = key[c];
       }
-      if (!anyfree) continue;
-      auto it = keys.find(key);
-      int32_t blk;
-      if (it == keys.end()) {
+      if (!first) continue;
+      int32_t& blk = block_by_first[first];
+      if (!blk) {
         for (int c = 0; c < 3; ++c) dofs.push_back(key[c] > 0 ? key[c] : 0);
-        blk = (int32_t)keys.size() + 1;
-        keys.emplace(key, blk);
-      } else {
-        blk = it->second;
+        blk = ++nb;
       }
       block_of[inv_node[n] + (size_t)p->nn * cell] = blk;
     }
-  p->nblocks = (int)keys.size();
+  p->nblocks = (int)nb;
   p->block_of.upload(block_of.data(), block_of.size(), p->stream);
   p->bdofs.upload(dofs.data(), dofs.size(), p->stream);
   build_seg_of_block(p, dofs);
