@@ -19,6 +19,7 @@
 
 #include "hfk_internal.h"
 #include "kern_assembly.cuh"
+#include "kern_band.cuh"
 #include "kern_cell.cuh"
 #include "kern_mlp.cuh"
 #include "kern_oseen.cuh"
@@ -1242,6 +1243,10 @@ struct hfk_transfer {
   DBuf<double> E, Einj;
   DBuf<int32_t> mult;
   // the transfer's colours: those of the fine level (cells sharing a coarse dof share a fine dof)
+  // tensor-product pair of levels (E = E1 x E1 x E1): the sum-factorised kernels
+  bool tp = false;
+  XferTP tpd;
+  DBuf<double> invmult;
 };
 
 namespace {
@@ -1259,10 +1264,22 @@ XferData xfer_data(hfk_transfer* t, const int32_t* cells, int ncl) {
   return d;
 }
 
+// warps per CTA of the sum-factorised transfer kernels and their dynamic shared memory
+int xfer_tp_warps(const hfk_transfer* t) {
+  return 4 * xfer_tp_slab(t->tpd.nf, t->tpd.nc) * (int)sizeof(double) <= 48 * 1024 ? 4 : 2;
+}
+
 template <typename R>
 void prolongate_dev(hfk_transfer* t, const R* xc, R* yf) {
   hfk_problem* p = t->fine;
   HFK_CUDA(cudaMemsetAsync(yf, 0, p->nfree * sizeof(R), p->stream));
+  if (t->tp) {
+    const int w = xfer_tp_warps(t);
+    prolongate_tp_kernel<R><<<(p->ncells + w - 1) / w, 32 * w, w * xfer_tp_slab(t->tpd.nf, t->tpd.nc) * sizeof(double),
+                              p->stream>>>(xfer_data(t, nullptr, p->ncells), t->tpd, xc, yf);
+    check_launch(p);
+    return;
+  }
   for (int c = 0; c < p->ncolors; ++c) {
     const int n = p->color_start[c + 1] - p->color_start[c];
     if (!n) continue;
@@ -1276,6 +1293,25 @@ template <typename R>
 void restrict_dev(hfk_transfer* t, const R* yf, R* yc) {
   hfk_problem* p = t->fine;
   HFK_CUDA(cudaMemsetAsync(yc, 0, t->coarse->nfree * sizeof(R), p->stream));
+  if (t->tp) {
+    // one atomic launch, or colour by colour (reproducible sums) when the fine level scatters so
+    const int w = xfer_tp_warps(t);
+    const size_t sm = (size_t)w * xfer_tp_slab(t->tpd.nf, t->tpd.nc) * sizeof(double);
+    if (p->scatter != HFK_SCATTER_COLOURED) {
+      restrict_tp_kernel<R><<<(p->ncells + w - 1) / w, 32 * w, sm, p->stream>>>(xfer_data(t, nullptr, p->ncells),
+                                                                                 t->tpd, 1, yf, yc);
+      check_launch(p);
+      return;
+    }
+    for (int c = 0; c < p->ncolors; ++c) {
+      const int n = p->color_start[c + 1] - p->color_start[c];
+      if (!n) continue;
+      restrict_tp_kernel<R><<<(n + w - 1) / w, 32 * w, sm, p->stream>>>(
+          xfer_data(t, p->cells_by_color.p + p->color_start[c], n), t->tpd, 0, yf, yc);
+      check_launch(p);
+    }
+    return;
+  }
   for (int c = 0; c < p->ncolors; ++c) {
     const int n = p->color_start[c + 1] - p->color_start[c];
     if (!n) continue;
@@ -1333,6 +1369,14 @@ struct hfk_pmg {
   std::vector<std::unique_ptr<DBuf<double>>> start;  // per level: the fixed Arnoldi start vector
   DBuf<double> potrf_work;
   DBuf<int> potrf_info;
+  // banded factor: the block tiles of both triangular solves (kern_band.cuh), rebuilt with the
+  // factor; bs_sync holds both directions' flags and tickets, then the error word
+  bool bs_on = false;
+  int bs_nb = 0, bs_wt = 0;
+  DBuf<double> bs_tiles, bs_diag, bs_y;
+  DBuf<int> bs_sync;
+  DBuf<const double*> bs_aptr;
+  DBuf<double*> bs_bptr;
   DBuf<double> top_r, top_y;
   cusolverDnHandle_t solver = nullptr;
   cublasHandle_t blas = nullptr;
@@ -1381,6 +1425,63 @@ void ensure_blas(hfk_pmg* m) {
   m->blas_ws.resize(32u << 20);
   if (cublasSetWorkspace(m->blas, m->blas_ws.p, m->blas_ws.n) != CUBLAS_STATUS_SUCCESS)
     throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasSetWorkspace failed"};
+}
+
+// The tiles of the block triangular solves (kern_band.cuh) from the banded factor in m->Lc: the
+// band of each block row and block column copied into BS_T x BS_T tiles, then one batched
+// triangular solve per direction with the diagonal blocks turns them into D^-1 L tiles (and the
+// identity tile into D^-1).
+void band_prepare(hfk_pmg* m, int64_t n) {
+  hfk_problem* c = m->lv[m->L - 1];
+  const int nb = (int)((n + BS_T - 1) / BS_T);
+  const int wt = std::min(nb - 1, (m->band + BS_T - 1) / BS_T);
+  const size_t tt = (size_t)BS_T * BS_T;
+  const size_t per = (size_t)(wt + 1) * tt;
+  m->bs_tiles.resize((size_t)2 * nb * per);
+  m->bs_diag.resize((size_t)2 * nb * tt);
+  m->bs_y.resize(n);
+  m->bs_sync.resize((size_t)2 * (nb + 1) + 1);
+  if (m->bs_nb != nb || m->bs_wt != wt) {
+    std::vector<const double*> a(2 * nb);
+    std::vector<double*> b(2 * nb);
+    for (int q = 0; q < 2 * nb; ++q) {
+      a[q] = m->bs_diag.p + (size_t)q * tt;
+      b[q] = m->bs_tiles.p + (size_t)q * per;
+    }
+    m->bs_aptr.upload(a.data(), a.size(), c->stream);
+    m->bs_bptr.upload(b.data(), b.size(), c->stream);
+    m->bs_sync.zero(c->stream);
+    m->bs_nb = nb;
+    m->bs_wt = wt;
+  }
+  const int64_t total = (int64_t)2 * nb * (wt + 2) * (int64_t)tt;
+  band_tiles_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 64), 256, 0, c->stream>>>(
+      n, nb, wt, m->Lc.p, m->bs_tiles.p, m->bs_diag.p);
+  check_launch(c);
+  ensure_blas(m);
+  cublasSetStream(m->blas, c->stream);
+  const double one = 1.0;
+  for (int d = 0; d < 2; ++d)
+    if (cublasDtrsmBatched(m->blas, CUBLAS_SIDE_LEFT, d ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                           CUBLAS_DIAG_NON_UNIT, BS_T, (wt + 1) * BS_T, &one, m->bs_aptr.p + (size_t)d * nb, BS_T,
+                           m->bs_bptr.p + (size_t)d * nb, BS_T, nb) != CUBLAS_STATUS_SUCCESS)
+      throw Error{HFK_ERR_CUDA, "HyperFEMKernels: batched triangular solve of the coarse tiles failed"};
+  m->bs_on = true;
+}
+
+// the error word of the block triangular solves: a wait between blocks that ran out (the cycle's
+// coarse correction is then invalid)
+void band_check(hfk_pmg* m) {
+  if (!m->bs_on) return;
+  int e = 0;
+  hfk_problem* c = m->lv[m->L - 1];
+  int* word = m->bs_sync.p + 2 * (m->bs_nb + 1);
+  HFK_CUDA(cudaMemcpyAsync(&e, word, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HFK_CUDA(cudaStreamSynchronize(c->stream));
+  if (e) {
+    HFK_CUDA(cudaMemsetAsync(word, 0, sizeof(int), c->stream));
+    throw Error{HFK_ERR_INTERNAL, "HyperFEMKernels: a block of the coarse triangular solve timed out"};
+  }
 }
 
 // Cholesky factor of the assembled coarse level (in place of the reference's LU, the matrix being
@@ -1465,6 +1566,8 @@ void coarse_factor(hfk_pmg* m) {
   // the lower triangle now holds the Cholesky factor L (A = L L^T); the cycle applies A^-1 by two
   // triangular solves
   m->coarse_ok = std::all_of(h_info.begin(), h_info.end(), [](int v) { return v == 0; });
+  m->bs_on = false;
+  if (m->coarse_ok && banded) band_prepare(m, n);
   if (m->coarse_ok) m->nbuild++;
 }
 
@@ -1485,12 +1588,27 @@ void coarse_cg_update(hfk_pmg* m) {
   if (m->coarse_ok) m->nbuild++;
 }
 
-// x = A^-1 b with the Cholesky factor: L y = b, L^T x = y (cuBLAS triangular solves, FP64)
+// x = A^-1 b with the Cholesky factor: L y = b, L^T x = y, FP64 (the block solves over the band
+// when the factor is banded, else cuBLAS triangular solves)
 void coarse_solve(hfk_pmg* m, const double* b, double* x) {
   hfk_problem* c = m->lv[m->L - 1];
   const int64_t n = c->nfree;
   ensure_blas(m);
   cublasSetStream(m->blas, c->stream);
+  if (m->bs_on) {
+    // banded factor: the block solves of kern_band.cuh, forward into bs_y, backward into x
+    const int nb = m->bs_nb;
+    int* sy = m->bs_sync.p;
+    HFK_CUDA(cudaMemsetAsync(sy, 0, (size_t)2 * (nb + 1) * sizeof(int), c->stream));
+    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 0, m->bs_tiles.p, b, m->bs_y.p, sy,
+                                                        sy + 2 * (nb + 1));
+    check_launch(c);
+    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 1,
+                                                        m->bs_tiles.p + (size_t)nb * (m->bs_wt + 1) * BS_T * BS_T,
+                                                        m->bs_y.p, x, sy + nb + 1, sy + 2 * (nb + 1));
+    check_launch(c);
+    return;
+  }
   HFK_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   const double one = 1.0;
   // dense triangular solves (zeros outside the band): measured faster here than block-column
@@ -2142,6 +2260,40 @@ int hfk_transfer_create(hfk_transfer** out, hfk_problem* fine, hfk_problem* coar
   t->E.upload(Et.data(), Et.size(), fine->stream);
   t->Einj.upload(Eit.data(), Eit.size(), fine->stream);
   t->mult.upload(mult.data(), mult.size(), fine->stream);
+  // a tensor-product pair: E1 from the first row of nodes, then every entry of E checked against
+  // E1 x E1 x E1 (E1[0][0] = cbrt E[0][0])
+  {
+    const int nf = (int)std::lround(std::cbrt((double)t->NF)), nc = (int)std::lround(std::cbrt((double)t->NC));
+    bool tp = nf * nf * nf == t->NF && nc * nc * nc == t->NC && nf <= MAXQ && nc <= MAXQ && Et[0] > 0;
+    if (tp) {
+      const double c0 = std::cbrt(Et[0]);
+      double emax = 0;
+      for (double v : Et) emax = std::max(emax, std::fabs(v));
+      XferTP d;
+      d.nf = nf;
+      d.nc = nc;
+      for (int i = 0; i < nf; ++i)
+        for (int b = 0; b < nc; ++b) d.e1[i * nc + b] = Et[i + (size_t)t->NF * b] / (c0 * c0);
+      for (int f = 0; f < t->NF && tp; ++f)
+        for (int c = 0; c < t->NC; ++c) {
+          const int i1 = f % nf, i2 = (f / nf) % nf, i3 = f / (nf * nf);
+          const int b1 = c % nc, b2 = (c / nc) % nc, b3 = c / (nc * nc);
+          const double k = d.e1[i1 * nc + b1] * d.e1[i2 * nc + b2] * d.e1[i3 * nc + b3];
+          if (std::fabs(k - Et[f + (size_t)t->NF * c]) > 1e-13 * emax) {
+            tp = false;
+            break;
+          }
+        }
+      if (tp) {
+        std::vector<double> im(mult.size());
+        for (size_t q = 0; q < mult.size(); ++q) im[q] = mult[q] > 0 ? 1.0 / mult[q] : 0.0;
+        t->invmult.upload(im.data(), im.size(), fine->stream);
+        d.invmult = t->invmult.p;
+        t->tpd = d;
+        t->tp = true;
+      }
+    }
+  }
   HFK_CUDA(cudaStreamSynchronize(fine->stream));
   *out = t.release();
   HFK_API_END
@@ -2414,6 +2566,7 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y) {
   pmg_apply_dev(m, dr, dy);
   finish_out(y, dy, p0->nfree, p0->stream);
   HFK_CUDA(cudaStreamSynchronize(p0->stream));
+  band_check(m);
   HFK_API_END
 }
 
@@ -2694,6 +2847,7 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
                  int flexible, int* iters, int* converged, int* indefinite, double* relres) {
   HFK_API_BEGIN
   solve_cg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres);
+  if (prec) band_check(prec);
   HFK_API_END
 }
 
@@ -2702,6 +2856,7 @@ int hfk_solve_cg_batched(hfk_problem* op, hfk_pmg* prec, const double* b, double
                          int* sweeps) {
   HFK_API_BEGIN
   solve_cg_seg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres, sweeps);
+  if (prec) band_check(prec);
   HFK_API_END
 }
 

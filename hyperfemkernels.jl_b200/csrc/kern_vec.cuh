@@ -390,6 +390,110 @@ __global__ void restrict_kernel(XferData t, const R* yf, R* yc) {
   }
 }
 
+// Sum-factorised transfers for tensor-product pairs of levels: the cell interpolation matrix is
+// E = E1 (x) E1 (x) E1 (fine node i = i1 + nf (i2 + nf i3), coarse node b likewise), so the cell
+// products of prolongate_cells! / restrict_cells! run as three 1D contractions per component
+// instead of one dense NF x NC product. One warp per cell; the warp's shared-memory slab holds the
+// cell's values and the two intermediate contractions.
+struct XferTP {
+  int nf = 0, nc = 0;            // 1D node counts of the fine and coarse levels
+  double e1[MAXQ * MAXQ] = {};   // e1[i * nc + b] = E1[i][b]
+  const double* invmult = nullptr;  // 1 / multiplicity per fine free dof (exact: 1, 2, 4, 8 cells)
+};
+
+__host__ __device__ inline int xfer_tp_slab(int nf, int nc) {  // doubles of one warp's slab
+  return 3 * (nf * nf * nf + nf * nf * nc + nf * nc * nc);
+}
+
+// restrict_cells! (src/transfers.jl:195-213), sum-factorised: E^T (yf / multiplicity) per cell,
+// added into yc atomically (atomic = 1) or by plain read-modify-write (one colour per launch)
+template <typename R>
+__global__ void restrict_tp_kernel(XferData t, XferTP tp, int atomic, const R* __restrict__ yf, R* yc) {
+  extern __shared__ double xsm[];
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li = blockIdx.x * wpb + warp;
+  if (li >= t.ncells_list) return;
+  const int cell = t.cells ? t.cells[li] : li;
+  const int nf = tp.nf, nc = tp.nc, NF = nf * nf * nf, NC = nc * nc * nc;
+  double* u = xsm + (size_t)warp * xfer_tp_slab(nf, nc);  // [comp][i3][i2][i1]
+  double* a = u + 3 * NF;                                 // [comp][i3][i2][b1]
+  double* b = a + 3 * nf * nf * nc;                       // [comp][i3][b2][b1]
+  const int32_t* iff = t.ids_f + (size_t)cell * 3 * NF;
+  for (int q = lane; q < 3 * NF; q += 32) {
+    const int32_t id = iff[q];
+    u[q] = id > 0 ? (double)yf[id - 1] * tp.invmult[id - 1] : 0.0;
+  }
+  __syncwarp();
+  for (int q = lane; q < 3 * nf * nf * nc; q += 32) {
+    const int b1 = q % nc, r = q / nc;
+    double s = 0;
+    for (int i = 0; i < nf; ++i) s += tp.e1[i * nc + b1] * u[r * nf + i];
+    a[q] = s;
+  }
+  __syncwarp();
+  for (int q = lane; q < 3 * nf * nc * nc; q += 32) {
+    const int b1 = q % nc, b2 = (q / nc) % nc, r = q / (nc * nc);
+    double s = 0;
+    for (int j = 0; j < nf; ++j) s += tp.e1[j * nc + b2] * a[(r * nf + j) * nc + b1];
+    b[q] = s;
+  }
+  __syncwarp();
+  const int32_t* ic = t.ids_c + (size_t)cell * 3 * NC;
+  for (int q = lane; q < 3 * NC; q += 32) {
+    const int32_t idc = ic[q];
+    if (idc <= 0) continue;
+    const int b12 = q % (nc * nc), r = q / (nc * nc), b3 = r % nc, comp = r / nc;
+    double s = 0;
+    for (int k = 0; k < nf; ++k) s += tp.e1[k * nc + b3] * b[(comp * nf + k) * nc * nc + b12];
+    if (atomic) atomicAdd(yc + idc - 1, (R)s);
+    else yc[idc - 1] += (R)s;
+  }
+}
+
+// prolongate_cells! (src/transfers.jl:179-193), sum-factorised: fine values = E x coarse local
+// values, written (cells sharing a fine dof write the same value)
+template <typename R>
+__global__ void prolongate_tp_kernel(XferData t, XferTP tp, const R* __restrict__ xc, R* yf) {
+  extern __shared__ double xsm[];
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li = blockIdx.x * wpb + warp;
+  if (li >= t.ncells_list) return;
+  const int cell = t.cells ? t.cells[li] : li;
+  const int nf = tp.nf, nc = tp.nc, NF = nf * nf * nf, NC = nc * nc * nc;
+  double* v = xsm + (size_t)warp * xfer_tp_slab(nf, nc);  // [comp][b3][b2][b1]
+  double* b = v + 3 * NC;                                 // [comp][i3][b2][b1]
+  double* a = b + 3 * nf * nc * nc;                       // [comp][i3][i2][b1]
+  const int32_t* ic = t.ids_c + (size_t)cell * 3 * NC;
+  for (int q = lane; q < 3 * NC; q += 32) {
+    const int32_t id = ic[q];
+    v[q] = id > 0 ? (double)xc[id - 1] : 0.0;
+  }
+  __syncwarp();
+  for (int q = lane; q < 3 * nf * nc * nc; q += 32) {
+    const int b12 = q % (nc * nc), r = q / (nc * nc), k = r % nf, comp = r / nf;
+    double s = 0;
+    for (int b3 = 0; b3 < nc; ++b3) s += tp.e1[k * nc + b3] * v[(comp * nc + b3) * nc * nc + b12];
+    b[q] = s;
+  }
+  __syncwarp();
+  for (int q = lane; q < 3 * nf * nf * nc; q += 32) {
+    const int b1 = q % nc, j = (q / nc) % nf, r = q / (nc * nf);
+    double s = 0;
+    for (int b2 = 0; b2 < nc; ++b2) s += tp.e1[j * nc + b2] * b[(r * nc + b2) * nc + b1];
+    a[q] = s;
+  }
+  __syncwarp();
+  const int32_t* iff = t.ids_f + (size_t)cell * 3 * NF;
+  for (int q = lane; q < 3 * NF; q += 32) {
+    const int32_t idf = iff[q];
+    if (idf <= 0) continue;
+    const int i = q % nf, r = q / nf;
+    double s = 0;
+    for (int b1 = 0; b1 < nc; ++b1) s += tp.e1[i * nc + b1] * a[r * nc + b1];
+    yf[idf - 1] = (R)s;
+  }
+}
+
 // inject_field! (src/transfers.jl:295-313)
 __global__ void inject_kernel(XferData t, int ncells, const double* xf, const double* df, double* xc, double* dc) {
   const int per = 3 * t.NC;

@@ -66,7 +66,8 @@ class Problem:
         call("hfk_problem_set_stream", self.h, ctypes.c_void_p(stream_handle or 0))
 
     def set_scatter(self, mode: str):
-        """"auto" (default), "coloured" (deterministic) or "atomic" for the sum-factorised kernels."""
+        """"auto" (default), "coloured" (deterministic) or "atomic" for the sum-factorised kernels and
+        the restriction from this level."""
         m = {"auto": _lib.SCATTER_AUTO, "coloured": _lib.SCATTER_COLOURED, "atomic": _lib.SCATTER_ATOMIC}[mode]
         call("hfk_problem_set_scatter", self.h, m)
 

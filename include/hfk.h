@@ -80,8 +80,9 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
  * between runs). AUTO (default) is autotuned per kernel mode and precision on the first call (the
  * atomic or the colour-by-colour scatter, 2 or 4 warps per CTA, timed with CUDA events; on B200
  * the atomic scatter usually wins: one launch, no read of the output before the write); COLOURED
- * gives bit-reproducible results. The nodal blocks scatter atomically unless COLOURED is set; the
- * assembled Jacobian always scatters by colour. */
+ * gives bit-reproducible results. The nodal blocks, and the restriction of a transfer whose fine
+ * level is this problem, scatter atomically unless COLOURED is set; the assembled Jacobian always
+ * scatters by colour. */
 #define HFK_SCATTER_AUTO 0
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2
@@ -171,7 +172,8 @@ int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, int degree,
 
 /* ---- transfers between nested levels on one mesh (src/transfers.jl) --------------------------
  * E (nn_f, nn_c): coarse basis at the fine nodes; Einj (nn_c, nn_f): fine basis at the coarse
- * nodes (TransferField, src/transfers.jl:57-131). */
+ * nodes (TransferField, src/transfers.jl:57-131). When E is a tensor product E1 x E1 x E1 (checked
+ * entry by entry at creation), prolongation and restriction run sum-factorised, one warp per cell. */
 int hfk_transfer_create(hfk_transfer** out, hfk_problem* fine, hfk_problem* coarse, const double* E,
                         const double* Einj);
 int hfk_transfer_destroy(hfk_transfer* t);

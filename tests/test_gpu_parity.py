@@ -199,20 +199,27 @@ def test_eigenvalue_bounds_and_chebyshev_parity():
     assert reldiff(xg, xo) < 1e-11 and reldiff(rg, ro) < 1e-10
 
 
-@pytest.mark.parametrize("qf,qc", [(2, 1), (4, 2), (3, 2)])
-def test_transfers_parity(qf, qc):
+@pytest.mark.parametrize("scatter", ["atomic", "coloured"])
+@pytest.mark.parametrize("qf,qc", [(2, 1), (4, 2), (3, 2), (4, 1)])
+def test_transfers_parity(qf, qc, scatter):
+    # the levels are tensor-product pairs, so the sum-factorised transfer kernels run; the
+    # restriction adds atomically, or colour by colour (bitwise reproducible) with the coloured scatter
     m = CartesianMesh((2, 3, 2))
     Vf = VectorLagrangeSpace(m, qf, ("x0", "x1"))
     Vc = VectorLagrangeSpace(m, qc, ("x0", "x1"))
     q = Quadrature.gauss(2 * qf)
     opf = KernelOperator(forms.svk_residual(degree=2 * qf), forms.svk_jacobian(degree=2 * qf), Vf)
     opc = KernelOperator(forms.svk_residual(degree=2 * qf), forms.svk_jacobian(degree=2 * qf), Vc)
+    opf.problem.set_scatter(scatter)
     P = S.Prolongation(opc.problem, opf.problem)
     T = O.OracleTransfer(Vf, Vc)
     rng = np.random.default_rng(0)
     xc, yf = rng.standard_normal(Vc.nfree), rng.standard_normal(Vf.nfree)
     assert reldiff(P.prolongate(np.zeros(Vf.nfree), xc), T.prolongate(xc)) < 1e-14
-    assert reldiff(P.restrict(np.zeros(Vc.nfree), yf), T.restrict(yf)) < 1e-14
+    rc = P.restrict(np.zeros(Vc.nfree), yf)
+    assert reldiff(rc, T.restrict(yf)) < 1e-14
+    if scatter == "coloured":
+        assert np.array_equal(P.restrict(np.zeros(Vc.nfree), yf), rc)
     df = rng.standard_normal(Vf.ndir)
     xi, di = P.inject(np.zeros(Vc.nfree), np.zeros(Vc.ndir), yf, df)
     oxi, odi = T.inject(yf, df, Vc.nfree, Vc.ndir)
@@ -270,10 +277,13 @@ def test_vcycle_parity_with_preconditioned_eigenvalue_estimate():
     assert reldiff(st.ldiv(np.zeros(Vs[0].nfree), r), mg.ldiv(r)) < 1e-9
 
 
-def test_banded_coarse_factor_matches_the_oracle_vcycle():
+@pytest.mark.parametrize("cross", [3, 6])
+def test_banded_coarse_factor_matches_the_oracle_vcycle(cross):
     # an elongated mesh: the coarse level's band is narrow against its size, so the Cholesky factor
-    # is computed block column by block column over the band (several 256-row blocks)
-    m = CartesianMesh((3, 3, 40), domain=(0.0, 1.0, 0.0, 1.0, 0.0, 10.0))
+    # is computed block column by block column over the band (several 256-row blocks) and the
+    # cycle's triangular solves run block by block (128-row blocks; cross section 3: one band tile
+    # per block, 6: two, with a partial last block in both)
+    m = CartesianMesh((cross, cross, 40), domain=(0.0, 1.0, 0.0, 1.0, 0.0, 10.0))
     g = lambda x: np.stack([0.01 * x[:, 2], 0 * x[:, 0], 0 * x[:, 0]], axis=1)
     Vs = [VectorLagrangeSpace(m, o, ("z0", "z1"), g=g if o == 2 else None) for o in (2, 1)]
     res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
