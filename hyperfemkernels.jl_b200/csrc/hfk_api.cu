@@ -21,6 +21,7 @@
 #include "kern_assembly.cuh"
 #include "kern_band.cuh"
 #include "kern_cell.cuh"
+#include "kern_jvp.cuh"
 #include "kern_mlp.cuh"
 #include "kern_oseen.cuh"
 #include "kern_seg.cuh"
@@ -254,13 +255,40 @@ void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>&
   check_launch(p);
 }
 
+// the point-parallel product (kern_jvp.cuh), NT threads per CTA
+template <int Q, int P, typename R, int NT>
+void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
+  using S = JvpShape<Q, P, NT>;
+  const size_t smem = jvp_smem_bytes<Q, P, R, NT>();
+  static size_t attr = 0;
+  if (smem > attr) {
+    HFK_CUDA(cudaFuncSetAttribute(jvp_kernel<Q, P, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  const int grid = (ncl + S::C - 1) / S::C;
+  if (grid == 0) return;
+  jvp_kernel<Q, P, R, NT><<<grid, NT, smem, p->stream>>>(cell_data(p, cells, ncl), make_tab<R>(p), io);
+  check_launch(p);
+}
+
+// Launch shapes: 2 or 4 = warps per CTA of the line-mapped kernel; SHAPE_PT_NARROW / SHAPE_PT_WIDE =
+// the point-parallel product (matrix-free product only) with one cell per CTA or 256 threads
+constexpr int SHAPE_PT_NARROW = 100, SHAPE_PT_WIDE = 108;
+
+template <int Q, int P, int MODE, typename R>
+void launch_shape(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int shape) {
+  if (MODE == MODE_JV && shape == SHAPE_PT_NARROW) launch_jvp<Q, P, R, jvp_narrow<P>()>(p, cells, ncl, io);
+  else if (MODE == MODE_JV && shape == SHAPE_PT_WIDE) launch_jvp<Q, P, R, JVP_WIDE>(p, cells, ncl, io);
+  else launch_cell<Q, P, MODE, R>(p, cells, ncl, io, shape >= SHAPE_PT_NARROW ? 4 : shape);
+}
+
 template <int MODE, typename R>
 void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int warps = 4) {
   const int key = p->Q * 10 + p->P;
   switch (key) {
 #define HFK_CASE(Qv, Pv) \
   case Qv * 10 + Pv:     \
-    launch_cell<Qv, Pv, MODE, R>(p, cells, ncl, io, warps); \
+    launch_shape<Qv, Pv, MODE, R>(p, cells, ncl, io, warps); \
     return;
     HFK_CASE(2, 2)
     HFK_CASE(2, 3)
@@ -306,13 +334,14 @@ void run_cells_as(hfk_problem* p, CellIO<R> io, bool atomic, int warps) {
 
 // Launch-shape autotuner (per problem, per kernel mode and precision, so per degree): on the first
 // AUTO call the kernel runs with each candidate (atomic or colour-by-colour scatter, 2 or 4 warps
-// per CTA), timed with CUDA events, and the fastest is kept. Outputs are zeroed before each
+// per CTA of the line-mapped kernel and, for the matrix-free product, the point-parallel kernel of
+// 8 warps), timed with CUDA events, and the fastest is kept. Outputs are zeroed before each
 // candidate and once more before the real run. No tuning while the stream is being captured (the
 // V-cycle is captured from its second application, when every kernel of it has run once).
 template <int MODE, typename R>
 void run_cells(hfk_problem* p, CellIO<R> io) {
   if (p->scatter != HFK_SCATTER_AUTO) {
-    run_cells_as<MODE, R>(p, io, p->scatter == HFK_SCATTER_ATOMIC, 4);
+    run_cells_as<MODE, R>(p, io, p->scatter == HFK_SCATTER_ATOMIC, p->shape);
     return;
   }
   const int key = MODE * 2 + (sizeof(R) == sizeof(float) ? 1 : 0);
@@ -324,13 +353,22 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
       run_cells_as<MODE, R>(p, io, true, 4);
       return;
     }
-    const int cand[4][2] = {{1, 4}, {1, 2}, {0, 4}, {0, 2}};
+    // (atomic, warps per CTA); the matrix-free product also tries the point-parallel kernel
+    const int cand[8][2] = {{1, 4},
+                            {1, 2},
+                            {0, 4},
+                            {0, 2},
+                            {1, SHAPE_PT_NARROW},
+                            {1, SHAPE_PT_WIDE},
+                            {0, SHAPE_PT_NARROW},
+                            {0, SHAPE_PT_WIDE}};
+    const int ncand = MODE == MODE_JV ? 8 : 4;
     cudaEvent_t e0, e1;
     HFK_CUDA(cudaEventCreate(&e0));
     HFK_CUDA(cudaEventCreate(&e1));
     float best = 0;
     int pick = 0;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < ncand; ++c) {
       float t = 1e30f;
       for (int rep = 0; rep < 2; ++rep) {
         HFK_CUDA(cudaMemsetAsync(io.y, 0, p->nfree * sizeof(R), p->stream));
@@ -1972,13 +2010,26 @@ int hfk_functional(hfk_problem* p, const double* x, const double* dvals, int kin
   HFK_API_END
 }
 
-int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* warps) {
+int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* kernel, int* warps) {
   HFK_API_BEGIN
-  HFK_REQUIRE(p && atomic && warps && (precision == HFK_FP64 || precision == HFK_FP32), HFK_ERR_ARG, "invalid argument");
+  HFK_REQUIRE(p && atomic && kernel && warps && (precision == HFK_FP64 || precision == HFK_FP32), HFK_ERR_ARG,
+              "invalid argument");
   const int internal = mode == 0 ? MODE_JV : (mode == 1 ? MODE_RESIDUAL : MODE_JV_STORED);
   auto it = p->tuned.find(internal * 2 + (precision == HFK_FP32 ? 1 : 0));
   *atomic = it == p->tuned.end() ? -1 : (int)it->second.first;
-  *warps = it == p->tuned.end() ? 0 : it->second.second;
+  const int shape = it == p->tuned.end() ? 0 : it->second.second;
+  *kernel = shape >= SHAPE_PT_NARROW ? 1 : 0;
+  *warps = shape == SHAPE_PT_NARROW ? (p->P * p->P * p->P + 31) / 32 : (shape == SHAPE_PT_WIDE ? JVP_WIDE / 32 : shape);
+  HFK_API_END
+}
+
+int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && (kernel == 0 || kernel == 1), HFK_ERR_ARG, "kernel must be 0 (line-mapped) or 1 (point-parallel)");
+  HFK_REQUIRE(kernel == 1 || warps == 2 || warps == 4, HFK_ERR_ARG, "the line-mapped kernels take 2 or 4 warps per CTA");
+  HFK_REQUIRE(kernel == 0 || warps == 0 || warps == JVP_WIDE / 32, HFK_ERR_ARG,
+              "the point-parallel product takes 0 (one cell per CTA) or 8 warps per CTA");
+  p->shape = kernel == 0 ? warps : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE);
   HFK_API_END
 }
 

@@ -191,6 +191,7 @@ struct hfk_problem {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int launches = 0;
   int scatter = HFK_SCATTER_AUTO;
+  int shape = 4;  // launch shape under an explicit scatter mode (warps per CTA, or a point-parallel shape)
   hfk::DBuf<double> func_red;             // per-warp partials of the functionals
   std::map<int, std::pair<bool, int>> tuned;  // autotuned (atomic scatter, warps per CTA) per kernel mode
   hfk::CGWork cg;

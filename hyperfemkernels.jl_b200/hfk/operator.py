@@ -71,12 +71,20 @@ class Problem:
         m = {"auto": _lib.SCATTER_AUTO, "coloured": _lib.SCATTER_COLOURED, "atomic": _lib.SCATTER_ATOMIC}[mode]
         call("hfk_problem_set_scatter", self.h, m)
 
+    def set_launch(self, kernel: str = "line", warps: int = 4):
+        """Launch shape under an explicit scatter mode: "line" (the line-mapped kernels, 2 or 4 warps
+        per CTA) or "point" (the point-parallel matrix-free product, warps 0 = one cell per CTA or
+        8)."""
+        call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1}[kernel], int(warps))
+
     def tuning(self, kernel: str = "jv", precision: str = "fp64"):
-        """The launch-shape autotuner's choice: {"atomic": bool, "warps": int} or None (not run yet)."""
-        a, w = ctypes.c_int(), ctypes.c_int()
+        """The launch-shape autotuner's choice: {"atomic": bool, "kernel": "line" | "point",
+        "warps": int} or None (not run yet)."""
+        a, k, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hfk_problem_tuning", self.h, {"jv": 0, "residual": 1, "jv_stored": 2}[kernel],
-             _lib.FP32 if precision == "fp32" else _lib.FP64, ctypes.byref(a), ctypes.byref(w))
-        return None if a.value < 0 else {"atomic": bool(a.value), "warps": w.value}
+             _lib.FP32 if precision == "fp32" else _lib.FP64, ctypes.byref(a), ctypes.byref(k), ctypes.byref(w))
+        return None if a.value < 0 else {"atomic": bool(a.value), "kernel": ("line", "point")[k.value],
+                                         "warps": w.value}
 
     def launches(self) -> int:
         c = ctypes.c_int64()

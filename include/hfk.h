@@ -87,10 +87,17 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2
 int hfk_problem_set_scatter(hfk_problem* p, int mode);
+/* Launch shape under an explicit scatter mode (COLOURED or ATOMIC; AUTO tunes its own): kernel 0,
+ * the line-mapped kernels with 2 or 4 warps per CTA (default 4); kernel 1, the point-parallel
+ * matrix-free product with one cell per CTA (warps = 0) or 8 warps per CTA (the other kernels
+ * then take the line-mapped shape of 4 warps). */
+int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
- * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), warps per CTA; atomic = -1 if
- * that kernel has not run under AUTO yet. No counterpart in the reference. */
-int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* warps);
+ * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
+ * warp's lanes on the tensor lines of a few cells) or 1 (point-parallel product: one thread per
+ * quadrature point), warps per CTA; atomic = -1 if that kernel has not run under AUTO yet. No
+ * counterpart in the reference. */
+int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* kernel, int* warps);
 
 /* KernelFunctional (src/functionals.jl:10-27) for the recognised laws at the state (x, dvals):
  * HFK_FUNCTIONAL_ENERGY = Σ_cells Σ_q Ψ(F) dV, the stored energy (reduce = :sum; SVK

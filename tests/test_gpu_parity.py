@@ -89,6 +89,26 @@ def test_matrix_free_product_parity(order, perturb, mode):
     assert reldiff(y, orc.mf_apply(dx)) < TOL64
 
 
+@pytest.mark.parametrize("order,perturb", CASES)
+@pytest.mark.parametrize("scatter,warps", [("coloured", 8), ("atomic", 8), ("atomic", 0)])
+def test_point_parallel_product_parity(order, perturb, scatter, warps):
+    # the point-parallel kernel (one thread per quadrature point; one cell per CTA, or 8 warps per
+    # CTA) against the oracle, FP64 and FP32, affine and perturbed (trilinear) cells, several CTAs
+    # and a partial one
+    V, op, orc = make(order, perturb=perturb, jac="matrixfree")
+    op.problem.set_scatter(scatter)
+    op.problem.set_launch("point", warps)
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    orc.mf_prepare(x, V.dirichlet_values)
+    dx = np.random.default_rng(1).standard_normal(V.nfree)
+    ref = orc.mf_apply(dx)
+    assert reldiff(mf.mul(np.zeros(V.nfree), dx), ref) < TOL64
+    y32 = mf.mul_f32(np.zeros(V.nfree, dtype=np.float32), dx.astype(np.float32))
+    assert reldiff(y32.astype(np.float64), ref) < 2e-6
+
+
 @pytest.mark.parametrize("order", [2, 4])
 def test_matrix_free_fp32_error_bounded(order):
     V, op, orc = make(order, jac="matrixfree")
@@ -142,7 +162,7 @@ def test_autotuned_launch_shape_gives_the_same_product():
     dx = np.random.default_rng(5).standard_normal(V.nfree)
     y1 = mf.mul(np.zeros(V.nfree), dx)  # first AUTO call: candidates timed, the fastest kept
     t = op.problem.tuning("jv")
-    assert t is not None and t["warps"] in (2, 4)
+    assert t is not None and (t["kernel"], t["warps"]) in {("line", 2), ("line", 4), ("point", 1), ("point", 8)}
     y2 = mf.mul(np.zeros(V.nfree), dx)
     assert reldiff(y1, y2) < 1e-14 and reldiff(y1, orc.jacobian(x, V.dirichlet_values) @ dx) < TOL64
 
