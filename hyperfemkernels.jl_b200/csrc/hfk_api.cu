@@ -1411,6 +1411,12 @@ struct hfk_pmg {
   // factor; bs_sync holds both directions' flags and tickets, then the error word
   bool bs_on = false;
   int bs_nb = 0, bs_wt = 0;
+  // the coarse build runs on a side stream while the smoothers are set up (enqueued by
+  // coarse_factor_launch, collected by coarse_factor_finish)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_c0 = nullptr, ev_c1 = nullptr, ev_p0 = nullptr, ev_p1 = nullptr;
+  bool cf_pending = false, cf_banded = false;
+  int cf_nt = 0;
   DBuf<double> bs_tiles, bs_diag, bs_y;
   DBuf<int> bs_sync;
   DBuf<const double*> bs_aptr;
@@ -1504,7 +1510,6 @@ void band_prepare(hfk_pmg* m, int64_t n) {
                            CUBLAS_DIAG_NON_UNIT, BS_T, (wt + 1) * BS_T, &one, m->bs_aptr.p + (size_t)d * nb, BS_T,
                            m->bs_bptr.p + (size_t)d * nb, BS_T, nb) != CUBLAS_STATUS_SUCCESS)
       throw Error{HFK_ERR_CUDA, "HyperFEMKernels: batched triangular solve of the coarse tiles failed"};
-  m->bs_on = true;
 }
 
 // the error word of the block triangular solves: a wait between blocks that ran out (the cycle's
@@ -1529,8 +1534,9 @@ void band_check(hfk_pmg* m) {
 // diagonal block, a triangular solve of the b rows below it and a symmetric rank-T update of the
 // b x b window that follows: O(n b^2) work instead of O(n^3). A matrix whose band is wide
 // (b >= n / 3) takes the dense potrf.
-void coarse_factor(hfk_pmg* m) {
+void coarse_factor_launch(hfk_pmg* m) {
   hfk_problem* c = m->lv[m->L - 1];
+  HFK_CUDA(cudaEventRecord(m->ev_c0, c->stream));
   pattern_build_dev(c);
   jacobian_dev(c, c->x.p, c->dvals.p, c->nzval.p);
   const int64_t n = c->nfree;
@@ -1566,10 +1572,7 @@ void coarse_factor(hfk_pmg* m) {
   m->potrf_info.zero(c->stream);
   double* A = m->Lc.p;
   int* info = m->potrf_info.p;
-  cudaEvent_t e0, e1;
-  HFK_CUDA(cudaEventCreate(&e0));
-  HFK_CUDA(cudaEventCreate(&e1));
-  HFK_CUDA(cudaEventRecord(e0, c->stream));
+  HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
   if (!banded) {
     cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, A, (int)n, m->potrf_work.p, lwork, info);
   } else {
@@ -1592,22 +1595,66 @@ void coarse_factor(hfk_pmg* m) {
         throw Error{HFK_ERR_CUDA, "HyperFEMKernels: banded Cholesky update of the coarse level failed"};
     }
   }
-  HFK_CUDA(cudaEventRecord(e1, c->stream));
-  std::vector<int> h_info(nt, 0);
-  HFK_CUDA(cudaMemcpyAsync(h_info.data(), info, nt * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HFK_CUDA(cudaEventRecord(m->ev_p1, c->stream));
+  // the block tiles of the cycle's triangular solves (used only if every pivot was positive)
+  if (banded) band_prepare(m, n);
+  HFK_CUDA(cudaEventRecord(m->ev_c1, c->stream));
+  m->cf_banded = banded;
+  m->cf_nt = nt;
+  m->cf_pending = true;
+}
+
+// waits for the coarse build (on the coarse level's stream, the side stream) and reads the pivots'
+// status; the lower triangle of Lc then holds the Cholesky factor L (A = L L^T) and the cycle
+// applies A^-1 by two triangular solves
+void coarse_factor_finish(hfk_pmg* m) {
+  if (!m->cf_pending) return;
+  hfk_problem* c = m->lv[m->L - 1];
+  m->cf_pending = false;
+  std::vector<int> h_info(m->cf_nt, 0);
+  HFK_CUDA(cudaMemcpyAsync(h_info.data(), m->potrf_info.p, m->cf_nt * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HFK_CUDA(cudaStreamSynchronize(c->stream));
   float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
+  HFK_CUDA(cudaEventElapsedTime(&ms, m->ev_p0, m->ev_p1));
   m->t_potrf += ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  // the lower triangle now holds the Cholesky factor L (A = L L^T); the cycle applies A^-1 by two
-  // triangular solves
+  HFK_CUDA(cudaEventElapsedTime(&ms, m->ev_c0, m->ev_c1));
+  m->t_coarse += ms;
   m->coarse_ok = std::all_of(h_info.begin(), h_info.end(), [](int v) { return v == 0; });
-  m->bs_on = false;
-  if (m->coarse_ok && banded) band_prepare(m, n);
+  m->bs_on = m->coarse_ok && m->cf_banded;
   if (m->coarse_ok) m->nbuild++;
 }
+
+// The coarse level's build on the side stream: forked from the level-0 stream once the coarse state
+// is injected, joined (on the host) before the update returns. The guard also joins it when an
+// exception leaves the update early, and gives the coarse level the shared stream back.
+struct CoarseFork {
+  hfk_pmg* m;
+  bool active = false;
+  explicit CoarseFork(hfk_pmg* mm) : m(mm) {}
+  void fork() {
+    hfk_problem* p0 = m->lv[0];
+    if (!m->side) {
+      HFK_CUDA(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+      for (cudaEvent_t* e : {&m->ev_fork, &m->ev_c0, &m->ev_c1, &m->ev_p0, &m->ev_p1}) HFK_CUDA(cudaEventCreate(e));
+    }
+    HFK_CUDA(cudaEventRecord(m->ev_fork, p0->stream));
+    HFK_CUDA(cudaStreamWaitEvent(m->side, m->ev_fork, 0));
+    m->lv[m->L - 1]->stream = m->side;
+    active = true;
+  }
+  void join() {
+    if (!active) return;
+    coarse_factor_finish(m);  // still on the side stream
+    active = false;
+    m->lv[m->L - 1]->stream = m->lv[0]->stream;
+  }
+  ~CoarseFork() {
+    if (!active) return;
+    cudaStreamSynchronize(m->side);
+    m->cf_pending = false;
+    m->lv[m->L - 1]->stream = m->lv[0]->stream;
+  }
+};
 
 // the inexact coarse solve's set-up: the coarse level's blocks and work vectors
 void coarse_cg_update(hfk_pmg* m) {
@@ -2483,6 +2530,11 @@ int hfk_pmg_destroy(hfk_pmg* m) {
     }
     if (m->solver) cusolverDnDestroy(m->solver);
     if (m->blas) cublasDestroy(m->blas);
+    if (m->side) {
+      cudaStreamSynchronize(m->side);
+      cudaStreamDestroy(m->side);
+      for (cudaEvent_t e : {m->ev_fork, m->ev_c0, m->ev_c1, m->ev_p0, m->ev_p1}) cudaEventDestroy(e);
+    }
     pmg_drop_graph(m);
     if (m->ev0) cudaEventDestroy(m->ev0);
     if (m->ev1) cudaEventDestroy(m->ev1);
@@ -2528,6 +2580,15 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     }
   }
   (void)f32;
+  // coarse level (every coarse_every updates): the assembled factorisation starts now on the side
+  // stream and overlaps the smoothers' set-up below
+  m->since++;
+  const bool rebuild = !m->built || m->since >= m->coarse_every;
+  CoarseFork cfork(m);
+  if (rebuild && m->coarse_mode != HFK_COARSE_CG) {
+    cfork.fork();
+    coarse_factor_launch(m);
+  }
   // smoothers: blocks and intervals (smoother_update!, src/smoothers.jl:86-107)
   bool all_ok = true;
   for (int l = 0; l + 1 < m->L; ++l) {
@@ -2587,14 +2648,15 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     }
     m->ml_loglm.upload(lg.data(), lg.size(), p0->stream);
   }
-  // coarse level (every coarse_every updates)
-  m->since++;
-  if (!m->built || m->since >= m->coarse_every) {
-    auto tc = std::chrono::steady_clock::now();
-    if (m->coarse_mode == HFK_COARSE_CG) coarse_cg_update(m);
-    else coarse_factor(m);
-    HFK_CUDA(cudaStreamSynchronize(p0->stream));
-    m->t_coarse += ms_since(tc);
+  if (rebuild) {
+    if (m->coarse_mode == HFK_COARSE_CG) {
+      auto tc = std::chrono::steady_clock::now();
+      coarse_cg_update(m);
+      HFK_CUDA(cudaStreamSynchronize(p0->stream));
+      m->t_coarse += ms_since(tc);
+    } else {
+      cfork.join();
+    }
     m->since = 0;
   }
   all_ok &= m->coarse_ok;

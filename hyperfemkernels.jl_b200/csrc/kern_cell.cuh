@@ -68,10 +68,12 @@ __host__ __device__ constexpr size_t cell_region_bytes() {
 }
 
 // resident CTAs per SM the register allocation of a mode targets (measured on B200 with the atomic
-// scatter: the stored formulation prefers 2, the recompute product 3 (no spills) over 4)
-template <int MODE>
+// scatter: the stored formulation prefers 2, the recompute product 3 (no spills) over 4; the FP32
+// recompute product 6 (80 registers, 24 warps per SM: 0.40 -> 0.30 ms on Q2 64^3), where FP64 at
+// 4 or 5 spills and loses)
+template <int MODE, typename R>
 constexpr int cell_min_blocks() {
-  return MODE == MODE_JV_STORED ? 2 : 3;
+  return MODE == MODE_JV_STORED ? 2 : (MODE == MODE_JV && sizeof(R) == 4 ? 6 : 3);
 }
 
 template <typename R>
@@ -90,7 +92,7 @@ struct CellIO {
 };
 
 template <int Q, int P, int MODE, typename R>
-__global__ void __launch_bounds__(128, cell_min_blocks<MODE>()) cell_kernel(CellData cd, Tab1D<R> tab, CellIO<R> io) {
+__global__ void __launch_bounds__(128, cell_min_blocks<MODE, R>()) cell_kernel(CellData cd, Tab1D<R> tab, CellIO<R> io) {
   using S = TPShape<Q, P>;
   using L = CellSmem<Q, P>;
   constexpr int NN = S::NN, NP = S::NP, TPC = S::TPC, CPW = S::CPW;
