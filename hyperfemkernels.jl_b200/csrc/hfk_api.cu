@@ -2021,6 +2021,13 @@ int hfk_problem_destroy(hfk_problem* p) {
     cudaStreamSynchronize(p->own_stream);
     cudaStreamDestroy(p->own_stream);
   }
+  for (cudaStream_t s : p->many_s)
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  for (cudaEvent_t e : p->many_ev)
+    if (e) cudaEventDestroy(e);
   delete p;
   HFK_API_END
 }
@@ -2218,6 +2225,62 @@ int hfk_mf_apply(hfk_problem* p, const double* dx, double* y) {
   double* dy = dev_out(y, p->nfree, p->stage_out);
   mf_apply_dev(p, d, dy);
   finish_out(y, dy, p->nfree, p->stream);
+  HFK_API_END
+}
+
+// A stream of products: H2D of vector i + 1 and D2H of vector i - 1 overlap the product of vector
+// i (two staging slots per direction, a copy-in and a copy-out stream, the product on the problem's
+// stream). Device pointers skip their copies. Returns when every output is written.
+int hfk_mf_apply_many(hfk_problem* p, int count, const double* const* dx, double* const* y) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && count >= 0 && (count == 0 || (dx && y)), HFK_ERR_ARG, "null argument");
+  for (int i = 0; i < count; ++i) HFK_REQUIRE(dx[i] && y[i], HFK_ERR_ARG, "null vector pointer");
+  if (count == 0) return HFK_OK;
+  const size_t n = p->nfree, bytes = n * sizeof(double);
+  if (!p->many_s[0]) {
+    for (cudaStream_t& s : p->many_s) HFK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : p->many_ev) HFK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  for (int b = 0; b < 2; ++b) {
+    p->many_in[b].resize(std::max<size_t>(p->many_in[b].n, n));
+    p->many_out[b].resize(std::max<size_t>(p->many_out[b].n, n));
+  }
+  cudaStream_t sin = p->many_s[0], sout = p->many_s[1], sc = p->stream;
+  cudaEvent_t* ev = p->many_ev;  // 0 fork, 1+b copied in, 3+b product done, 5+b copied out
+  // the copies start after the work the caller queued on the problem's stream
+  HFK_CUDA(cudaEventRecord(ev[0], sc));
+  HFK_CUDA(cudaStreamWaitEvent(sin, ev[0], 0));
+  HFK_CUDA(cudaStreamWaitEvent(sout, ev[0], 0));
+  for (int i = 0; i < count; ++i) {
+    const int b = i & 1;
+    const bool din = is_device_ptr(dx[i]), dout = is_device_ptr(y[i]);
+    const double* d = dx[i];
+    if (!din) {
+      if (i >= 2) HFK_CUDA(cudaStreamWaitEvent(sin, ev[3 + b], 0));  // slot read by product i - 2
+      HFK_CUDA(cudaMemcpyAsync(p->many_in[b].p, dx[i], bytes, cudaMemcpyHostToDevice, sin));
+      HFK_CUDA(cudaEventRecord(ev[1 + b], sin));
+      HFK_CUDA(cudaStreamWaitEvent(sc, ev[1 + b], 0));
+      d = p->many_in[b].p;
+    }
+    double* o = y[i];
+    if (!dout) {
+      if (i >= 2) HFK_CUDA(cudaStreamWaitEvent(sc, ev[5 + b], 0));  // slot copied out by D2H i - 2
+      o = p->many_out[b].p;
+    }
+    mf_apply_dev(p, d, o);
+    HFK_CUDA(cudaEventRecord(ev[3 + b], sc));
+    if (!dout) {
+      HFK_CUDA(cudaStreamWaitEvent(sout, ev[3 + b], 0));
+      HFK_CUDA(cudaMemcpyAsync(y[i], o, bytes, cudaMemcpyDeviceToHost, sout));
+      HFK_CUDA(cudaEventRecord(ev[5 + b], sout));
+    }
+  }
+  // later work on the problem's stream follows every copy; host outputs are complete on return
+  HFK_CUDA(cudaEventRecord(ev[5], sout));
+  HFK_CUDA(cudaStreamWaitEvent(sc, ev[5], 0));
+  HFK_CUDA(cudaEventRecord(ev[1], sin));
+  HFK_CUDA(cudaStreamWaitEvent(sc, ev[1], 0));
+  HFK_CUDA(cudaStreamSynchronize(sc));
   HFK_API_END
 }
 

@@ -183,6 +183,11 @@ struct hfk_problem {
   bool blocks_ok = false;
   // staging for host pointers
   hfk::DBuf<double> stage_in, stage_in2, stage_out;
+  // hfk_mf_apply_many: two staging slots per direction, the copy-in and copy-out streams and their
+  // events (fork, then per slot: copied in, product done, copied out), created on first use
+  hfk::DBuf<double> many_in[2], many_out[2];
+  cudaStream_t many_s[2] = {nullptr, nullptr};
+  cudaEvent_t many_ev[7] = {};
   hfk::DBuf<int64_t> stage_l;
   hfk::DBuf<float> tmp32a, tmp32b;
   // error flag for numerical checks

@@ -273,6 +273,20 @@ class MatrixFreeJacobian:
         call("hfk_mf_apply", self.op.problem.h, ptr(dx), ptr(y))
         return y
 
+    def mul_many(self, ys, dxs):
+        """``mul!`` over a list of vectors in one call: the host copies of one vector overlap the
+        product of the next (page-locked host buffers), device vectors are used in place."""
+        if not self.prepared:
+            raise RuntimeError("HyperFEMKernels: the MatrixFreeJacobian has not been prepared")
+        if len(ys) != len(dxs):
+            raise ValueError("HyperFEMKernels: as many outputs as inputs")
+        k = len(dxs)
+        pin = (ctypes.c_void_p * max(k, 1))(*[ptr(a).value for a in dxs])
+        pout = (ctypes.c_void_p * max(k, 1))(*[ptr(a).value for a in ys])
+        call("hfk_mf_apply_many", self.op.problem.h, k, ctypes.cast(pin, ctypes.c_void_p),
+             ctypes.cast(pout, ctypes.c_void_p))
+        return ys
+
     def mul_f32(self, y, dx):
         """The same product in FP32 (mixed-precision smoothers)."""
         call("hfk_mf_apply_f32", self.op.problem.h, ptr(dx, np.float32), ptr(y, np.float32))

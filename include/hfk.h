@@ -140,6 +140,14 @@ int hfk_mf_prepare(hfk_problem* p, const double* x, const double* dvals, int mod
 int hfk_mf_apply(hfk_problem* p, const double* dx, double* y);
 /* The same product in FP32 (state, increment and result in FP32; mixed-precision smoothers). */
 int hfk_mf_apply_f32(hfk_problem* p, const float* dx, float* y);
+/* y[i] = J dx[i] for count vectors (the reference's mul! of src/matrixfree.jl:246-260, applied to
+ * a stream of inputs): host vectors are copied in and out on two copy streams of their own, with
+ * two staging slots per direction, so that the copies of vectors i + 1 and i - 1 overlap the
+ * product of vector i (host buffers must be page-locked for the copies to overlap anything).
+ * Device pointers skip their copies. The copies start after the work already queued on the
+ * problem's stream, later work on it follows them, and the call returns when every y[i] is
+ * written. The staging buffers (4 n doubles) are allocated on the first call. */
+int hfk_mf_apply_many(hfk_problem* p, int count, const double* const* dx, double* const* y);
 
 /* BlockJacobi nodal blocks of the prepared tangent (field_blocks/block_diagonal!/invert_blocks!,
  * src/preconditioners.jl:151-327); ok = 0 if a block is not finite. */
