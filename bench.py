@@ -538,6 +538,10 @@ def reference(args):
 
 
 BATCH_LOADS = (0.1, 0.325, 0.55, 0.775, 1.0)
+# block-Jacobi CG steps of the batched coarse solve (measured on the 256 problems, FP64: 5 / 10 / 15
+# / 20 / 40 steps -> 29.8 / 21.7 / 23.2 / 24.1 / 32.8 s; each step costs ~0.85 ms a cycle, and more
+# steps barely lower the Krylov count of the slowest problem)
+BATCH_COARSE_STEPS = 10
 
 
 def _batch_setup(count, seed=4, rank=0, world=1):
@@ -555,12 +559,12 @@ def _batch_solver(U2, U1, precision):
 
     return S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, maxiter=400,
                               preconditioner=S.PMultigrid([U2, U1], S.Chebyshev(degree=4), precision=precision,
-                                                          coarse="cg", coarse_iters=20))
+                                                          coarse="cg", coarse_iters=BATCH_COARSE_STEPS))
 
 
 def batch_cpu_sample(problems, budget_s=20.0):
     """The same per-problem Newton (lifting predictor, 5 load steps, FCG + p-MG Q2 -> Q1 with the
-    20-step coarse CG, all to 1e-8) by the oracle on the host cores, on the smallest problems of
+    10-step coarse CG, all to 1e-8) by the oracle on the host cores, on the smallest problems of
     the batch until ``budget_s`` is spent; returns seconds per free dof (to extrapolate)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -575,7 +579,7 @@ def batch_cpu_sample(problems, budget_s=20.0):
         V2, V1 = U2.spaces[0], U1.spaces[0]
         lift = B.cube_lifting(U2)
         orc = O.OracleProblem(V2, q, O.LAW_SVK, (pb.lam, pb.mu))
-        mg = O.OraclePMG([V2, V1], q, O.LAW_SVK, (pb.lam, pb.mu), degree=4, coarse="cg", coarse_iters=20)
+        mg = O.OraclePMG([V2, V1], q, O.LAW_SVK, (pb.lam, pb.mu), degree=4, coarse="cg", coarse_iters=BATCH_COARSE_STEPS)
         x = np.zeros(V2.nfree)
         t0 = time.perf_counter()
         prev = 0.0
@@ -608,7 +612,7 @@ def batch_main(args):
     direction, lambda, mu log-uniform in [0.5, 20] x [0.2, 5], seed 4), x = 0 clamped, x = 1 moved
     0.05 along x in 5 load steps, every Newton and linear solve to 1e-8, all problems advanced by the
     same launches (one handle, per-problem scalars). First with the plain p-multigrid (Q2 -> Q1,
-    Chebyshev 4, 20-step coarse CG), then with the learned correction trained on pairs from the
+    Chebyshev 4, 10-step coarse CG), then with the learned correction trained on pairs from the
     plain cycle at seeded states of the converged solution."""
     import torch
 
@@ -710,7 +714,7 @@ def batch_main(args):
                        "problems": args.batch_count, "parallelism": f"problems sharded over {world} GPU(s)",
                        "free_dofs_rank0": U2.nfree, "coarse_free_dofs": U1.nfree,
                        "cells": U2.mesh.ncells, "loads": list(BATCH_LOADS), "setup_seconds": t_setup,
-                       "levels": "Q2 -> Q1 (Chebyshev 4; coarse: 20 block-Jacobi CG steps per problem)",
+                       "levels": f"Q2 -> Q1 (Chebyshev 4; coarse: {BATCH_COARSE_STEPS} block-Jacobi CG steps per problem)",
                        "precision": args.batch_precision},
             "clocks": clocks.summary(), "plain": plain, "learned": lrn,
             "gain_learned_vs_plain": plain["seconds"] / lrn["seconds"]}
