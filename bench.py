@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--oseen", type=int, default=0, metavar="N",
                     help="only the Oseen P2-P1 assembly on the N^3 tetrahedral cube (the secondary case; 0 = off)")
+    ap.add_argument("--vcycle", type=int, default=0, metavar="K",
+                    help="only K V-cycles of the Q4 16^3 p-multigrid 4 -> 2 -> 1 (the Newton case's preconditioner)")
     return ap.parse_args()
 
 
@@ -382,6 +384,43 @@ def oseen_main(args):
 
     out = oseen_case(torch, torch.device("cuda"), stream, timed, n=args.oseen, cpu_n=min(args.oseen, 8))
     print(json.dumps(out))
+
+
+def vcycle_main(args, n=16):
+    """The p-multigrid V-cycle alone (``--vcycle K``): the Newton case's hierarchy (SVK Q4 -> Q2 -> Q1
+    on the 16^3 cube, Chebyshev degree 4, assembled Q1 coarse level with its banded Cholesky) built
+    once at a loaded state, then K cycles on a device vector, timed with CUDA events. One JSON line;
+    the case for the cycle's launch list."""
+    import torch
+
+    from hfk import forms
+    from hfk import solvers as S
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.operator import KernelOperator
+
+    m = CartesianMesh((n, n, n))
+    gfun = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
+    Vs = [VectorLagrangeSpace(m, o, ("x0", "x1"), g=gfun if o == 4 else None) for o in (4, 2, 1)]
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 8), forms.svk_jacobian(2.0, 1.0, 8), Vs[0], jacobian="matrixfree")
+    x = np.zeros(Vs[0].nfree)
+    mf = op.allocate_jacobian(x)
+    mf.prepare(x, 0.1 * Vs[0].dirichlet_values)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=4)), mf)
+    r = torch.randn(Vs[0].nfree, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    y = torch.zeros_like(r)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        st.ldiv(y, r)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.vcycle):
+        st.ldiv(y, r)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": f"V-cycle SVK Q4 {n}^3 -> Q2 -> Q1", "free_dofs": Vs[0].nfree,
+                      "coarse_free_dofs": Vs[2].nfree, "cycles": args.vcycle,
+                      "ms_per_cycle": e0.elapsed_time(e1) / args.vcycle}))
 
 
 def assembly_case(torch, dev, stream, timed):
@@ -734,5 +773,7 @@ if __name__ == "__main__":
         batch_main(a)
     elif a.oseen:
         oseen_main(a)
+    elif a.vcycle:
+        vcycle_main(a)
     else:
         engine(a)
