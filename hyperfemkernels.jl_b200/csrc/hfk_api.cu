@@ -1408,7 +1408,7 @@ struct hfk_pmg {
   DBuf<double> potrf_work;
   DBuf<int> potrf_info;
   // banded factor: the block tiles of both triangular solves (kern_band.cuh), rebuilt with the
-  // factor; bs_sync holds both directions' flags and tickets, then the error word
+  // factor; bs_sync holds both directions' tickets, then the error word
   bool bs_on = false;
   int bs_nb = 0, bs_wt = 0;
   // the coarse build runs on a side stream while the smoothers are set up (enqueued by
@@ -1484,7 +1484,7 @@ void band_prepare(hfk_pmg* m, int64_t n) {
   m->bs_tiles.resize((size_t)2 * nb * per);
   m->bs_diag.resize((size_t)2 * nb * tt);
   m->bs_y.resize(n);
-  m->bs_sync.resize((size_t)2 * (nb + 1) + 1);
+  m->bs_sync.resize(3);  // the two directions' tickets, the error word
   if (m->bs_nb != nb || m->bs_wt != wt) {
     std::vector<const double*> a(2 * nb);
     std::vector<double*> b(2 * nb);
@@ -1518,7 +1518,7 @@ void band_check(hfk_pmg* m) {
   if (!m->bs_on) return;
   int e = 0;
   hfk_problem* c = m->lv[m->L - 1];
-  int* word = m->bs_sync.p + 2 * (m->bs_nb + 1);
+  int* word = m->bs_sync.p + 2;
   HFK_CUDA(cudaMemcpyAsync(&e, word, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HFK_CUDA(cudaStreamSynchronize(c->stream));
   if (e) {
@@ -1684,13 +1684,14 @@ void coarse_solve(hfk_pmg* m, const double* b, double* x) {
     // banded factor: the block solves of kern_band.cuh, forward into bs_y, backward into x
     const int nb = m->bs_nb;
     int* sy = m->bs_sync.p;
-    HFK_CUDA(cudaMemsetAsync(sy, 0, (size_t)2 * (nb + 1) * sizeof(int), c->stream));
-    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 0, m->bs_tiles.p, b, m->bs_y.p, sy,
-                                                        sy + 2 * (nb + 1));
+    HFK_CUDA(cudaMemsetAsync(sy, 0, 2 * sizeof(int), c->stream));
+    HFK_CUDA(cudaMemsetAsync(m->bs_y.p, 0xff, n * sizeof(double), c->stream));  // the sentinel
+    HFK_CUDA(cudaMemsetAsync(x, 0xff, n * sizeof(double), c->stream));
+    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 0, m->bs_tiles.p, b, m->bs_y.p, sy, sy + 2);
     check_launch(c);
     band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 1,
                                                         m->bs_tiles.p + (size_t)nb * (m->bs_wt + 1) * BS_T * BS_T,
-                                                        m->bs_y.p, x, sy + nb + 1, sy + 2 * (nb + 1));
+                                                        m->bs_y.p, x, sy + 1, sy + 2);
     check_launch(c);
     return;
   }

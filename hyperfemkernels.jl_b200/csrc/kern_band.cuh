@@ -8,12 +8,15 @@
 //     y_k = D_k^-1 in_k - sum_{j in the band} G_{k,j} y_j
 // so a step reads its dependencies' outputs only through dense BS_T x BS_T tiles and no step
 // carries a triangular substitution. One launch per direction: CTAs take steps in the order they
-// start (a ticket counter), add the tile of a dependency as soon as that dependency's flag is set
-// (a step's last dependency is the only one on the critical path), write their block and set their
-// own flag. A CTA waits only for steps with smaller tickets, which belong to CTAs already running,
-// so the launch progresses whatever the number of resident CTAs. Every wait is bounded: on expiry
-// the CTA records the failure in the error word, skips its remaining tiles and still publishes its
-// flag, so that every CTA of the launch returns; the host reads the error word after the cycle.
+// start (a ticket counter), add the tile of a dependency as soon as that dependency's block is
+// published (a step's last dependency is the only one on the critical path) and publish their own.
+// The output is filled with a sentinel bit pattern before the launch and a block is published by
+// writing its values: a reader polls the very words it needs, so the critical path between two
+// steps is one store and one load through L2 (no fence, no flag). A CTA waits only for steps with
+// smaller tickets, which belong to CTAs already running, so the launch progresses whatever the
+// number of resident CTAs. Every wait is bounded: on expiry the CTA records the failure in the error
+// word, skips its remaining tiles and still publishes its block (zeros), so that every CTA of the
+// launch returns; the host reads the error word after the cycle.
 #pragma once
 #include <cstdint>
 
@@ -75,31 +78,31 @@ __global__ void band_tiles_kernel(int64_t n, int nb, int wt, const double* __res
   }
 }
 
-__device__ __forceinline__ int bs_load_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+// the bit pattern the outputs are filled with before a launch (a negative NaN with every payload
+// bit set; NaNs computed on the GPU are canonical)
+constexpr unsigned long long BS_SENTINEL = 0xffffffffffffffffull;
+
+__device__ __forceinline__ unsigned long long bs_load_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ void bs_store_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void bs_store_relaxed_u64(double* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // One direction of the solve: out_k = tile_wt(s) in_k - sum_t tile_t(s) out_{step s - wt + t}.
-// sync: flags[nb] (one per step), then the ticket; zeroed before the launch. err: set to 1 when a
+// ticket: zeroed before the launch, out: filled with BS_SENTINEL before the launch. err: set to 1 when a
 // wait ran out. Launched with nb CTAs of BS_THREADS threads.
 __global__ void __launch_bounds__(BS_THREADS, 1)
     band_solve_kernel(int64_t n, int nb, int wt, int backward, const double* __restrict__ tiles,
-                      const double* __restrict__ in, double* out, int* sync, int* err) {
-  __shared__ int s_step, s_fail;
+                      const double* __restrict__ in, double* out, int* ticket, int* err) {
+  __shared__ int s_step;
   __shared__ double yb[BS_T];
   __shared__ double part[BS_H][BS_T];
-  int* flags = sync;
   const int tid = threadIdx.x, i = tid % BS_T, h = tid / BS_T;
-  if (tid == 0) {
-    s_step = atomicAdd(sync + nb, 1);
-    s_fail = 0;
-  }
+  if (tid == 0) s_step = atomicAdd(ticket, 1);
   __syncthreads();
   const int s = s_step;
   if (s >= nb) return;  // the grid has nb CTAs: never taken
@@ -122,6 +125,7 @@ __global__ void __launch_bounds__(BS_THREADS, 1)
   // the dependencies in step order; the next tile's values are loaded before its flag is polled
   const int t0 = wt - s > 0 ? wt - s : 0;
   double reg[BS_J];
+  bool failed = false;  // uniform over the CTA
   if (t0 < wt) {
     const double* tp = ts + (int64_t)t0 * tt + i + (int64_t)BS_T * j0;
 #pragma unroll
@@ -130,24 +134,31 @@ __global__ void __launch_bounds__(BS_THREADS, 1)
   for (int t = t0; t < wt; ++t) {
     const int sd = s - wt + t;
     __syncthreads();  // yb is rewritten below
-    if (tid == 0 && !s_fail) {
-      int polls = 0;
-      while (bs_load_acquire(flags + sd) == 0) {
-        if (++polls > BS_SPIN_LIMIT) {
-          atomicExch(err, 1);
-          s_fail = 1;
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __syncthreads();
-    if (s_fail) break;
+    // the dependency's block, each value polled until it is no longer the sentinel
+    int fail = 0;
     if (tid < BS_T) {
       const int64_t r = (int64_t)(backward ? nb - 1 - sd : sd) * BS_T + tid;
-      yb[tid] = r < n ? __ldcg(out + r) : 0.0;
+      double v = 0.0;
+      if (r < n) {
+        int polls = 0;
+        for (;;) {
+          const unsigned long long bits = bs_load_relaxed_u64(out + r);
+          if (bits != BS_SENTINEL) {
+            v = __longlong_as_double((long long)bits);
+            break;
+          }
+          if (++polls > BS_SPIN_LIMIT || ((polls & 1023) == 0 && *((volatile int*)err))) {
+            atomicExch(err, 1);
+            fail = 1;
+            break;
+          }
+          __nanosleep(20);
+        }
+      }
+      yb[tid] = v;
     }
-    __syncthreads();
+    failed = __syncthreads_or(fail) != 0;
+    if (failed) break;
 #pragma unroll
     for (int jj = 0; jj < BS_J; ++jj) acc = fma(-reg[jj], yb[j0 + jj], acc);
     if (t + 1 < wt) {
@@ -163,11 +174,10 @@ __global__ void __launch_bounds__(BS_THREADS, 1)
 #pragma unroll
     for (int q = 1; q < BS_H; ++q) v += part[q][tid];
     const int64_t r = k * BS_T + tid;
-    if (r < n) out[r] = v;
+    // published value by value: a successor polls these very words (a value that reached the
+    // sentinel's bit pattern would have to be a NaN that arithmetic on the GPU never produces)
+    if (r < n) bs_store_relaxed_u64(out + r, (unsigned long long)__double_as_longlong(failed ? 0.0 : v));
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) bs_store_release(flags + s, 1);
 }
 
 }  // namespace hfk
