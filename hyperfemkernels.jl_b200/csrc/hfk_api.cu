@@ -27,6 +27,12 @@
 #include "kern_seg.cuh"
 #include "kern_vec.cuh"
 
+namespace hfk {
+GmresWork::~GmresWork() {
+  if (blas) cublasDestroy((cublasHandle_t)blas);
+}
+}  // namespace hfk
+
 using namespace hfk;
 
 namespace hfk {
@@ -2882,6 +2888,154 @@ void solve_cg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, do
   *converged = conv;
   if (indefinite) *indefinite = indef;
 }
+// MatrixFreeSolver.solve! with krylov = :gmres / :fgmres (src/solvers.jl:128-131): restarted GMRES
+// with right preconditioning (A N^-1 u = b, x = N^-1 u; Krylov.jl's gmres!/fgmres! with restart),
+// every vector on the device. Each iteration: z = N^-1 v_j, w = A z, classical Gram-Schmidt with
+// one reorthogonalisation (two passes of cuBLAS gemv: h = V^T w, w -= V h), v_{j+1} = w / ||w||;
+// the Hessenberg matrix and its Givens rotations live on the host. The cycle ends when the
+// residual estimate |g_{j+1}| meets atol + rtol ||b||, at `restart` iterations or at maxiter; then
+// x += Z y (FGMRES, flexible != 0: the preconditioned basis kept, any preconditioner) or
+// x += N^-1 (V y) (GMRES: one more preconditioner application, a fixed preconditioner), and the
+// true residual decides convergence or a restart. x is the initial guess on input.
+void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                     int restart, int flexible, int* iters, int* converged, double* relres) {
+  HFK_REQUIRE(op && b && x && iters && converged, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(rtol >= 0 && rtol < 1, HFK_ERR_ARG, "the relative tolerance must be in [0, 1)");
+  HFK_REQUIRE(atol >= 0 && maxiter > 0 && restart > 0, HFK_ERR_ARG, "atol must be >= 0, maxiter and restart > 0");
+  HFK_REQUIRE(op->prepared, HFK_ERR_STATE, "the operator has not been prepared");
+  const int64_t n = op->nfree;
+  HFK_REQUIRE(n < ((int64_t)1 << 31), HFK_ERR_UNSUPPORTED, "GMRES supports fewer than 2^31 free dofs");
+  if (prec) {
+    HFK_REQUIRE(prec->lv[0] == op, HFK_ERR_ARG, "the preconditioner's working level is not this operator");
+    pmg_bind_stream(prec);
+  }
+  cudaStream_t s = op->stream;
+  *iters = 0;
+  *converged = 0;
+  if (relres) *relres = NAN;
+  if (prec && !prec->ok) {  // src/solvers.jl:114-121: no iteration, a failed solve
+    if (is_device_ptr(x)) HFK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    else std::fill(x, x + n, 0.0);
+    HFK_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
+  const int m = std::min(restart, maxiter);
+  hfk::CGWork& cw = op->cg;
+  hfk::GmresWork& gw = op->gm;
+  const double* bd = dev_in(b, n, cw.b, s);
+  double* xd = x;
+  if (!is_device_ptr(x)) {
+    cw.x.resize(n);
+    HFK_CUDA(cudaMemcpyAsync(cw.x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    xd = cw.x.p;
+  }
+  gw.V.resize((size_t)(m + 1) * n);
+  gw.Z.resize((size_t)(flexible ? m : 1) * n);
+  gw.w.resize(n);
+  gw.h.resize(m + 1);
+  if (!gw.blas) {
+    cublasHandle_t hb = nullptr;
+    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
+    gw.blas = hb;
+  }
+  cublasHandle_t blas = (cublasHandle_t)gw.blas;
+  cublasSetStream(blas, s);
+  auto blas_ok = [](cublasStatus_t st) {
+    if (st != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cuBLAS call of the GMRES solve failed"};
+  };
+  auto apply_prec = [&](const double* in, double* outp) {
+    if (prec) pmg_apply_dev(prec, in, outp);
+    else HFK_CUDA(cudaMemcpyAsync(outp, in, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  };
+  Reducer& red = cw.red;
+  double res[3];
+  double* V = gw.V.p;
+  // r0 = b - A x into V[:, 0]
+  mf_apply_dev(op, xd, gw.w.p);
+  axpbyz_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, bd, -1.0, gw.w.p, V);
+  check_launch(op);
+  dots<double>(op, red, n, 2, bd, bd, V, V, nullptr, nullptr, res);
+  const double nb = std::sqrt(res[0]);
+  const double tol = atol + rtol * nb;
+  double beta = std::sqrt(res[1]);
+  bool conv = beta <= tol;
+  int it = 0;
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), h1(m + 1), h2(m + 1);
+  const double one = 1.0, zero = 0.0, minus = -1.0;
+  while (!conv && it < maxiter) {
+    scale_kernel<<<vec_grid(n), 256, 0, s>>>(n, 1.0 / beta, V);
+    check_launch(op);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int jend = 0;
+    for (int j = 0; j < m && it < maxiter; ++j) {
+      double* vj = V + (size_t)j * n;
+      double* vn = V + (size_t)(j + 1) * n;
+      double* zj = gw.Z.p + (flexible ? (size_t)j * n : 0);
+      apply_prec(vj, zj);
+      mf_apply_dev(op, zj, vn);
+      // classical Gram-Schmidt, twice
+      for (int pass = 0; pass < 2; ++pass) {
+        blas_ok(cublasDgemv(blas, CUBLAS_OP_T, (int)n, j + 1, &one, V, (int)n, vn, 1, &zero, gw.h.p, 1));
+        blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, j + 1, &minus, V, (int)n, gw.h.p, 1, &one, vn, 1));
+        HFK_CUDA(cudaMemcpyAsync(pass ? h2.data() : h1.data(), gw.h.p, (j + 1) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+      }
+      dots<double>(op, red, n, 1, vn, vn, nullptr, nullptr, nullptr, nullptr, res);  // synchronises
+      const double hn = std::sqrt(res[0]);
+      double* Hj = H.data() + (size_t)j * (m + 1);
+      for (int i = 0; i <= j; ++i) Hj[i] = h1[i] + h2[i];
+      Hj[j + 1] = hn;
+      for (int i = 0; i < j; ++i) {  // the previous rotations
+        const double t = cs[i] * Hj[i] + sn[i] * Hj[i + 1];
+        Hj[i + 1] = -sn[i] * Hj[i] + cs[i] * Hj[i + 1];
+        Hj[i] = t;
+      }
+      const double rr = std::hypot(Hj[j], Hj[j + 1]);
+      cs[j] = rr > 0 ? Hj[j] / rr : 1.0;
+      sn[j] = rr > 0 ? Hj[j + 1] / rr : 0.0;
+      Hj[j] = rr;
+      Hj[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      ++it;
+      jend = j + 1;
+      if (std::fabs(g[j + 1]) <= tol || !(hn > 0) || !std::isfinite(hn)) break;  // estimate met, or breakdown
+      scale_kernel<<<vec_grid(n), 256, 0, s>>>(n, 1.0 / hn, vn);
+      check_launch(op);
+    }
+    // y = R^-1 g, then the update of x
+    for (int i = jend - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int k = i + 1; k < jend; ++k) t -= H[(size_t)k * (m + 1) + i] * y[k];
+      const double d = H[(size_t)i * (m + 1) + i];
+      y[i] = d != 0.0 ? t / d : 0.0;
+    }
+    HFK_CUDA(cudaMemcpyAsync(gw.h.p, y.data(), jend * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (flexible) {
+      blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, jend, &one, gw.Z.p, (int)n, gw.h.p, 1, &one, xd, 1));
+    } else {
+      blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, jend, &one, V, (int)n, gw.h.p, 1, &zero, gw.w.p, 1));
+      apply_prec(gw.w.p, gw.Z.p);
+      axpby_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, gw.Z.p, 1.0, xd);
+      check_launch(op);
+    }
+    // the true residual decides (and starts the next cycle)
+    mf_apply_dev(op, xd, gw.w.p);
+    axpbyz_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, bd, -1.0, gw.w.p, V);
+    check_launch(op);
+    dots<double>(op, red, n, 1, V, V, nullptr, nullptr, nullptr, nullptr, res);
+    beta = std::sqrt(res[0]);
+    conv = beta <= tol;
+    if (!std::isfinite(beta)) break;
+  }
+  if (relres) *relres = nb > 0 ? beta / nb : beta;
+  finish_out(x, xd, n, s);
+  HFK_CUDA(cudaStreamSynchronize(s));
+  *iters = it;
+  *converged = conv;
+}
+
 // MatrixFreeSolver.solve! (src/solvers.jl:111-159) on every segment of op at once: one FP64
 // (flexible) CG per segment with its own alpha, beta, tolerance atol + rtol ||b_s|| and stopping
 // test; every product and preconditioner application covers all segments in one launch sequence.
@@ -3024,6 +3178,14 @@ int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, dou
                  int flexible, int* iters, int* converged, int* indefinite, double* relres) {
   HFK_API_BEGIN
   solve_cg_dev(op, prec, b, x, rtol, atol, maxiter, flexible, iters, converged, indefinite, relres);
+  if (prec) band_check(prec);
+  HFK_API_END
+}
+
+int hfk_solve_gmres(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                    int restart, int flexible, int* iters, int* converged, double* relres) {
+  HFK_API_BEGIN
+  solve_gmres_dev(op, prec, b, x, rtol, atol, maxiter, restart, flexible, iters, converged, relres);
   if (prec) band_check(prec);
   HFK_API_END
 }

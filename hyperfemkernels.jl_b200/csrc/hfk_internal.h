@@ -107,6 +107,14 @@ struct CGWork {
   DBuf<int> fl, cnt;
 };
 
+// Work of the restarted GMRES / FGMRES: the Krylov basis V ((restart + 1) n), the preconditioned
+// basis Z (restart n for FGMRES, one vector for GMRES), a work vector and the projections (device)
+struct GmresWork {
+  DBuf<double> V, Z, w, h;
+  void* blas = nullptr;  // cublasHandle_t, created on first use
+  ~GmresWork();
+};
+
 // State of a matrix-free level in a precision
 template <typename R>
 struct LevelState {
@@ -200,4 +208,5 @@ struct hfk_problem {
   hfk::DBuf<double> func_red;             // per-warp partials of the functionals
   std::map<int, std::pair<bool, int>> tuned;  // autotuned (atomic scatter, warps per CTA) per kernel mode
   hfk::CGWork cg;
+  hfk::GmresWork gm;
 };

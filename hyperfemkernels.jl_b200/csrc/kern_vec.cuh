@@ -70,6 +70,10 @@ __global__ void axpby_kernel(int64_t n, R a, const R* x, R b, R* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
 }
 // z = a x + b y
+// x *= a
+__global__ void scale_kernel(int64_t n, double a, double* x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] *= a;
+}
 template <typename R>
 __global__ void axpbyz_kernel(int64_t n, R a, const R* x, R b, const R* y, R* z) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) z[i] = a * x[i] + b * y[i];

@@ -79,6 +79,7 @@ SIGNATURES = {
     "hfk_pmg_level_info": [_vp, _i, _pd, _pd, _pd, _pd],
     "hfk_pmg_stats": [_vp, _vp],
     "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
+    "hfk_solve_gmres": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _i, _pi, _pi, _pd],
     "hfk_mlp_create": [ctypes.POINTER(_vp), ctypes.c_uint64],
     "hfk_mlp_destroy": [_vp],
     "hfk_mlp_num_params": [],

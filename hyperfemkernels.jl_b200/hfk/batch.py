@@ -116,6 +116,8 @@ class BatchedSolveResult:
 def solve_batched(x, ns: S.MatrixFreeSolverNS, b) -> BatchedSolveResult:
     """``solve!`` on every problem of a batched operator (``hfk_solve_cg_batched``)."""
     s = ns.solver
+    if s.krylov not in ("cg", "fcg"):
+        raise ValueError("HyperFEMKernels: batched solves run CG or FCG (krylov = 'cg' or 'fcg')")
     p = ns.mf.op.problem
     k = p.nseg
     it = np.zeros(k, dtype=np.int32)

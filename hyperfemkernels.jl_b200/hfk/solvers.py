@@ -260,10 +260,12 @@ class PMultigridState:
 
 @dataclasses.dataclass
 class MatrixFreeSolver:
-    """``MatrixFreeSolver(; krylov, rtol, atol, maxiter, preconditioner)`` (src/solvers.jl:33-53).
+    """``MatrixFreeSolver(; krylov, rtol, atol, maxiter, restart, preconditioner)`` (src/solvers.jl:33-53).
 
-    ``krylov`` is "fcg" (flexible CG, for variable preconditioners such as a mixed-precision
-    V-cycle) or "cg".
+    ``krylov`` is "gmres" or "fgmres" (restarted, right-preconditioned, ``restart`` iterations per
+    cycle as the reference's memory; FGMRES keeps the preconditioned basis and accepts a variable
+    preconditioner), "fcg" (flexible CG, for variable preconditioners such as a mixed-precision
+    V-cycle) or "cg". The default stays "fcg": the batched solves of ``hfk.batch`` are CG only.
     """
 
     krylov: str = "fcg"
@@ -271,10 +273,14 @@ class MatrixFreeSolver:
     atol: float = 0.0
     maxiter: int = 500
     preconditioner: object = None
+    restart: int = 50
 
     def __post_init__(self):
-        if self.krylov not in ("fcg", "cg"):
-            raise ValueError(f"HyperFEMKernels: MatrixFreeSolver: krylov must be 'fcg' or 'cg' (got {self.krylov!r})")
+        if self.krylov not in ("fcg", "cg", "gmres", "fgmres"):
+            raise ValueError("HyperFEMKernels: MatrixFreeSolver: krylov must be 'gmres', 'fgmres', 'fcg' or 'cg' "
+                             f"(got {self.krylov!r})")
+        if self.restart <= 0:
+            raise ValueError("HyperFEMKernels: MatrixFreeSolver: restart must be positive")
         if not (0 <= self.rtol < 1):
             raise ValueError(f"HyperFEMKernels: the relative tolerance must be in [0, 1) (got {self.rtol})")
         if self.atol < 0:
@@ -333,8 +339,12 @@ def solve(x, ns: MatrixFreeSolverNS, b):
     s = ns.solver
     it, conv, ind, rel = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
     prec = ns.prec.h if ns.prec is not None else None
-    call("hfk_solve_cg", ns.mf.op.problem.h, prec, ptr(b), ptr(x), ns.rtol, s.atol, s.maxiter,
-         1 if s.krylov == "fcg" else 0, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(ind), ctypes.byref(rel))
+    if s.krylov in ("gmres", "fgmres"):
+        call("hfk_solve_gmres", ns.mf.op.problem.h, prec, ptr(b), ptr(x), ns.rtol, s.atol, s.maxiter, s.restart,
+             1 if s.krylov == "fgmres" else 0, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(rel))
+    else:
+        call("hfk_solve_cg", ns.mf.op.problem.h, prec, ptr(b), ptr(x), ns.rtol, s.atol, s.maxiter,
+             1 if s.krylov == "fcg" else 0, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(ind), ctypes.byref(rel))
     ns.iters, ns.converged, ns.indefinite, ns.rnorm = it.value, bool(conv.value), bool(ind.value), rel.value
     return x
 

@@ -283,6 +283,16 @@ int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets
  * (true residual). flexible != 0 uses the Polak-Ribiere beta (a variable preconditioner, e.g. a
  * mixed-precision V-cycle). x is the initial guess on input. A non-positive curvature stops with
  * converged = 0 and indefinite = 1; an unusable preconditioner returns at once, iters = 0. */
+/* MatrixFreeSolver.solve! with krylov = :gmres or :fgmres (src/solvers.jl:128-131; Krylov.jl's
+ * gmres!/fgmres! with right preconditioning and restart): restarted GMRES on the device, classical
+ * Gram-Schmidt with one reorthogonalisation, Givens rotations on the host; `restart` iterations per
+ * cycle (the reference's memory, default 50). flexible != 0 is FGMRES (the preconditioned basis is
+ * kept: any, also variable, preconditioner); flexible = 0 is GMRES (x += N^-1 (V y) at the end of
+ * a cycle: a fixed preconditioner). Stops when ||b - J x|| <= atol + rtol ||b|| on the true
+ * residual, computed at the end of every cycle. x is the initial guess on input; an unusable
+ * preconditioner returns at once with iters = 0. */
+int hfk_solve_gmres(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
+                    int restart, int flexible, int* iters, int* converged, double* relres);
 int hfk_solve_cg(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, double rtol, double atol, int maxiter,
                  int flexible, int* iters, int* converged, int* indefinite, double* relres);
 

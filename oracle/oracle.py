@@ -512,6 +512,73 @@ def pcg(apply_op, b, prec=None, rtol=1e-8, atol=0.0, maxiter=500, x0=None):
     return x, it, False, np.linalg.norm(r) / nb
 
 
+def gmres(apply_op, b, prec=None, rtol=1e-8, atol=0.0, maxiter=500, restart=50, flexible=True, x0=None):
+    """Restarted GMRES with right preconditioning (A N^-1 u = b, x = N^-1 u), the method of
+    ``MatrixFreeSolver(krylov = :gmres / :fgmres)`` (src/solvers.jl:128-131, Krylov.jl gmres!/fgmres!),
+    restated after Saad's (F)GMRES: Arnoldi by classical Gram-Schmidt with one reorthogonalisation,
+    Givens rotations, a cycle ends when the residual estimate meets atol + rtol ||b|| or after
+    ``restart`` iterations; then x += Z y (flexible: the preconditioned basis) or x += N^-1 V y, and
+    the true residual decides convergence or the next cycle. Returns (x, iters, converged, relres).
+    """
+    M = prec if prec is not None else (lambda v: v.copy())
+    x = np.zeros_like(b) if x0 is None else x0.copy()
+    nb = np.linalg.norm(b)
+    tol = atol + rtol * nb
+    m = min(restart, maxiter)
+    r = b - apply_op(x)
+    beta = np.linalg.norm(r)
+    it = 0
+    while beta > tol and it < maxiter:
+        V = [r / beta]
+        Z = []
+        H = np.zeros((m + 1, m))
+        cs, sn = np.zeros(m), np.zeros(m)
+        g = np.zeros(m + 1)
+        g[0] = beta
+        jend = 0
+        for j in range(m):
+            if it >= maxiter:
+                break
+            z = M(V[j])
+            Z.append(z)
+            w = apply_op(z)
+            Vm = np.array(V).T
+            h = Vm.T @ w
+            w = w - Vm @ h
+            h2 = Vm.T @ w
+            w = w - Vm @ h2
+            h = h + h2
+            hn = np.linalg.norm(w)
+            col = np.zeros(m + 1)
+            col[: j + 1] = h
+            col[j + 1] = hn
+            for i in range(j):
+                t = cs[i] * col[i] + sn[i] * col[i + 1]
+                col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1]
+                col[i] = t
+            rr = np.hypot(col[j], col[j + 1])
+            cs[j], sn[j] = (col[j] / rr, col[j + 1] / rr) if rr > 0 else (1.0, 0.0)
+            col[j], col[j + 1] = rr, 0.0
+            H[:, j] = col
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            it += 1
+            jend = j + 1
+            if abs(g[j + 1]) <= tol or not hn > 0:
+                break
+            V.append(w / hn)
+        y = np.zeros(jend)
+        for i in range(jend - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1:jend] @ y[i + 1:]) / H[i, i] if H[i, i] != 0 else 0.0
+        if flexible:
+            x = x + np.array(Z[:jend]).T @ y
+        else:
+            x = x + M(np.array(V[:jend]).T @ y)
+        r = b - apply_op(x)
+        beta = np.linalg.norm(r)
+    return x, it, beta <= tol, beta / max(nb, 1e-300)
+
+
 # ---------------------------------------------------------------------------------------------
 # MLP of the learned correction (the engine's hfk_mlp_*): numpy forward/backward with the same
 # parameter layout and the BF16 rounding of the weights the GPU forward pass reads.

@@ -382,6 +382,35 @@ def test_pmg_solve_matches_direct_and_iterations_bounded(orders):
     assert its[1] <= 1.4 * its[0] + 2
 
 
+@pytest.mark.parametrize("krylov", ["gmres", "fgmres"])
+def test_gmres_matches_the_oracle(krylov):
+    # MatrixFreeSolver(krylov = :gmres / :fgmres) (src/solvers.jl:128-131): the engine's restarted
+    # right-preconditioned GMRES against the oracle's restatement with the oracle's V-cycle: the same
+    # iteration count (a small restart, so that cycles restart), the same solution, the true
+    # residual at the tolerance; without a preconditioner as well
+    Vs, res, jac = _pmg_case(3, (2, 1))
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x = np.zeros(Vs[0].nfree)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    b = -op.residual(np.zeros(Vs[0].nfree), x)
+    orc = O.OracleProblem(Vs[0], Quadrature.gauss(4), O.LAW_LINEAR, (2.0, 1.0, 0.3, -0.2, 0.5))
+    A = orc.jacobian(x, Vs[0].dirichlet_values)
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_LINEAR, (2.0, 1.0, 0.3, -0.2, 0.5), degree=2)
+    mg.update(x, Vs[0].dirichlet_values)
+    flex = krylov == "fgmres"
+    for prec, restart in ((S.PMultigrid(Vs), 4), (None, 20)):
+        ls = S.MatrixFreeSolver(krylov=krylov, rtol=1e-10, maxiter=400, restart=restart, preconditioner=prec)
+        ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf)
+        dx = S.solve(np.zeros(Vs[0].nfree), ns, b)
+        ox, oit, oconv, orel = O.gmres(lambda v: A @ v, b, mg.ldiv if prec is not None else None, rtol=1e-10,
+                                       maxiter=400, restart=restart, flexible=flex)
+        assert S.linear_converged(ns) and oconv
+        assert abs(S.linear_iterations(ns) - oit) <= 1, (S.linear_iterations(ns), oit)
+        assert reldiff(dx, ox) < 1e-8
+        assert np.linalg.norm(b - A @ dx) <= 1e-10 * np.linalg.norm(b) * (1 + 1e-6)
+
+
 def test_mixed_precision_solve_reaches_fp64_tolerance():
     Vs, res, jac = _pmg_case(4, (2, 1), "svk")
     op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")

@@ -342,3 +342,27 @@ def test_oracle_energy_derivative_is_the_residual(law):
     rv = p.residual(x, d) @ v
     assert abs(de - rv) < 1e-9 * abs(rv)
     assert 0.5 < p.functional(x, d, "min_detF") < 1.5
+
+
+def test_oracle_gmres_restarted_right_preconditioned():
+    # the oracle's (F)GMRES restatement: a nonsymmetric system solved to the tolerance on the true
+    # residual with restarts, GMRES and FGMRES alike for a fixed preconditioner, and one iteration
+    # with the exact inverse as preconditioner
+    import scipy.sparse as sps
+
+    rng = np.random.default_rng(0)
+    n = 200
+    A = sps.random(n, n, density=0.03, random_state=1) + sps.diags(4.0 + rng.random(n))
+    A = A.tocsr()
+    b = rng.standard_normal(n)
+    D = 1.0 / A.diagonal()
+    jac = lambda v: D * v
+    for flexible in (True, False):
+        x, it, conv, rel = O.gmres(lambda v: A @ v, b, jac, rtol=1e-10, restart=5, flexible=flexible)
+        assert conv and np.linalg.norm(b - A @ x) <= 1e-10 * np.linalg.norm(b) * (1 + 1e-9) and it > 5
+    xg, itg, _, _ = O.gmres(lambda v: A @ v, b, jac, rtol=1e-10, restart=8, flexible=False)
+    xf, itf, _, _ = O.gmres(lambda v: A @ v, b, jac, rtol=1e-10, restart=8, flexible=True)
+    assert itg == itf and np.abs(xg - xf).max() < 1e-8 * np.abs(xf).max()
+    Ainv = sps.linalg.splu(A.tocsc())
+    x, it, conv, _ = O.gmres(lambda v: A @ v, b, Ainv.solve, rtol=1e-10)
+    assert conv and it == 1
