@@ -138,16 +138,8 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE, R>()) cell_kernel(C
     }
   }
   // geometry of an affine cell (cell_geometry, src/assembly.jl:1100-1107), loaded early
-  double iJc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, detc = 0;
   bool aff = false;
-  if (has_cell && MODE != MODE_JV_STORED) {
-    aff = cd.affine[cell];
-    if (aff) {
-#pragma unroll
-      for (int i = 0; i < 9; ++i) iJc[i] = cd.geo[(size_t)cell * 10 + i];
-      detc = cd.geo[(size_t)cell * 10 + 9];
-    }
-  }
+  if (has_cell && MODE != MODE_JV_STORED) aff = cd.affine[cell];
   __syncwarp();
 
   // ---- interpolation sweeps (tp_interpolate! 3D, reference gradients only) ------------------
@@ -238,9 +230,11 @@ __global__ void __launch_bounds__(128, cell_min_blocks<MODE, R>()) cell_kernel(C
           for (int i = 0; i < 9; ++i) iJ[i] = 0;
         }
       } else if (aff || !has_cell) {
+        // the cell's inverse Jacobian read per point (an L1 hit shared by the cell's lanes)
+        const double* gc = cd.geo + (size_t)(has_cell ? cell : 0) * 10;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) iJ[i] = (R)iJc[i];
-        dV = (R)(cd.w[q] * detc);
+        for (int i = 0; i < 9; ++i) iJ[i] = has_cell ? (R)__ldg(gc + i) : R(0);
+        dV = has_cell ? (R)(cd.w[q] * __ldg(gc + 9)) : R(0);
       } else {
         double Jt[9], iJd[9];
         point_jacobian_dev(cd, cell, q, Jt);
