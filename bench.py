@@ -510,6 +510,18 @@ def newton_case(n=16, loads=(0.1, 0.325, 0.55, 0.775, 1.0)):
         out[prec] = {"seconds": st.seconds, "newton_iters": st.newton_iters, "krylov_iters": st.krylov_iters,
                      "converged": st.converged, "final_residual": st.residual_norms[-1], "pmg": st.pmg,
                      "residual_norms": [float(f"{r:.3e}") for r in st.residual_norms]}
+    # the reference guide's production setting: the coarse level rebuilt every third update
+    # (PMultigrid(...; coarse_every = 3), docs/guide/README.md:256-261)
+    for prec in ("fp64", "fp32"):
+        op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-8, maxiter=300,
+                                preconditioner=S.PMultigrid(Vs, S.Chebyshev(degree=4), precision=prec, coarse_every=3))
+        newton_solve(op, ls, g_full, loads[:1], rtol_newton=1e-8)
+        x, st = newton_solve(op, ls, g_full, loads, rtol_newton=1e-8)
+        out[f"{prec}_coarse_every3"] = {"seconds": st.seconds, "newton_iters": st.newton_iters,
+                                        "krylov_iters": int(sum(st.krylov_iters)), "converged": st.converged,
+                                        "final_residual": st.residual_norms[-1],
+                                        "coarse_builds": st.pmg["coarse_builds"]}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
     return {"newton_pmg_svk_q4_16": {"free_dofs": Vs[0].nfree, "levels": "Q4 -> Q2 -> Q1 (assembled, banded Cholesky)",
                                      "loads": list(loads), **out}}

@@ -206,7 +206,6 @@ class PMultigridState:
         if c.eig_inner == "preconditioner":
             call("hfk_pmg_set_eig_inner", h, _lib.EIG_PRECONDITIONED)
         self.ncycle = 0
-        self.nbuild = 0
         self.update(mf)
 
     def __del__(self):
@@ -228,8 +227,13 @@ class PMultigridState:
         d = mf.dvals if mf.dvals is not None else mf.op.dirichlet_values()
         call("hfk_pmg_update", self.h, ptr(x), ptr(d), ctypes.byref(ok))
         self.ok = bool(ok.value)
-        self.nbuild += 1
         return self
+
+    @property
+    def nbuild(self) -> int:
+        """Coarse builds (assembly and factorisation), the count the reference's
+        ``preconditioner_builds`` reports for a p-multigrid (src/pmultigrid.jl:56, :105, :340)."""
+        return int(self.stats()["coarse_builds"])
 
     def ldiv(self, y, r):
         """``ldiv!(y, st, r)`` (src/pmultigrid.jl:331-338): one V-cycle (NaN when not ok)."""

@@ -382,6 +382,58 @@ def test_pmg_solve_matches_direct_and_iterations_bounded(orders):
     assert its[1] <= 1.4 * its[0] + 2
 
 
+def test_lagged_coarse_newton_matches_direct_newton():
+    # test/solvers/test_pmultigrid.jl:95-115: Newton with the matrix-free p-MG GMRES, the coarse level
+    # rebuilt every `coarse_every` updates, against Newton with a direct solve of the assembled
+    # tangent: the same number of Newton iterations, histories within half a decade, the same
+    # solution, and one coarse build per `every` Newton iterations
+    import math
+
+    Vs, res, jac = _pmg_case(3, (2, 1), law="svk")
+
+    def newton(op, solve_lin, maxiter=12, tol=1e-10):
+        x = np.zeros(Vs[0].nfree)
+        b = op.residual(np.zeros(Vs[0].nfree), x)
+        r0 = np.linalg.norm(b)
+        hist = []
+        for _ in range(maxiter):
+            x = x - solve_lin(op, x, b)
+            b = op.residual(np.zeros(Vs[0].nfree), x)
+            hist.append(np.linalg.norm(b) / r0)
+            if hist[-1] < tol:
+                break
+        return x, hist
+
+    def direct(op, x, b):
+        A = op.allocate_jacobian(x)
+        op.jacobian(A, x)
+        return sp.linalg.spsolve(A.tocsc(), b)
+
+    x_lu, h_lu = newton(KernelOperator(res, jac, Vs[0]), direct)
+    for every in (1, 3):
+        op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+        ls = S.MatrixFreeSolver(krylov="gmres", rtol=1e-11, maxiter=200,
+                                preconditioner=S.PMultigrid(Vs, coarse_every=every))
+        state = {}
+
+        def mf_solve(op, x, b):
+            mf = state.get("mf") or op.allocate_jacobian(x)
+            op.jacobian(mf, x)
+            state["mf"] = mf
+            ns = state.get("ns")
+            ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf) if ns is None else S.numerical_setup_update(ns, mf)
+            state["ns"] = ns
+            dx = S.solve(np.zeros(Vs[0].nfree), ns, b)
+            assert S.linear_converged(ns)
+            return dx
+
+        x_mf, h_mf = newton(op, mf_solve)
+        assert len(h_mf) == len(h_lu)
+        assert np.all(np.abs(np.log10(h_mf) - np.log10(h_lu)) < 0.5)
+        assert reldiff(x_mf, x_lu) < 1e-8
+        assert S.preconditioner_builds(state["ns"]) == math.ceil(len(h_mf) / every)
+
+
 @pytest.mark.parametrize("krylov", ["gmres", "fgmres"])
 def test_gmres_matches_the_oracle(krylov):
     # MatrixFreeSolver(krylov = :gmres / :fgmres) (src/solvers.jl:128-131): the engine's restarted
