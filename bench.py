@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--oseen", type=int, default=0, metavar="N",
                     help="only the Oseen P2-P1 assembly on the N^3 tetrahedral cube (the secondary case; 0 = off)")
+    ap.add_argument("--launch", default="auto", choices=["auto", "line2", "line4", "point"],
+                    help="launch shape of the J*v (auto: the autotuner's; a fixed one for profiling, where the "
+                         "profiler's overhead would skew the autotuner's timings)")
     ap.add_argument("--vcycle", type=int, default=0, metavar="K",
                     help="only K V-cycles of the Q4 16^3 p-multigrid 4 -> 2 -> 1 (the Newton case's preconditioner)")
     return ap.parse_args()
@@ -153,6 +156,10 @@ def engine(args):
     dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
     dxd = torch.from_numpy(dx).to(dev)
     yd = torch.zeros(n, dtype=torch.float64, device=dev)
+    if args.launch != "auto":
+        op.problem.set_scatter("atomic")
+        op.problem.set_launch("point" if args.launch == "point" else "line",
+                              0 if args.launch == "point" else int(args.launch[-1]))
     mf = MatrixFreeJacobian(op, "recompute")
     mf.prepare(xd, dd)
     h = op.problem.h
@@ -204,7 +211,7 @@ def engine(args):
         _lib.call("hfk_mf_apply_many", h, k_e2e, ctypes.cast(pin, ctypes.c_void_p), ctypes.cast(pout, ctypes.c_void_p))
 
     ms_e2e = timed(step_e2e_many, 1, 1) / k_e2e
-    e2e_err = max(float(torch.linalg.norm(y.to(dev) - yd) / torch.linalg.norm(yd)) for y in yh)
+    e2e_err = max(float(torch.linalg.norm(y.to(dev) - yd) / torch.linalg.norm(yd)) for y in yh[:min(ring, k_e2e)])
 
     def step_e2e():  # one vector per synchronous call: copy in, product, copy out
         _lib.call("hfk_mf_apply", h, _lib.ptr(dxh[0]), _lib.ptr(yh[0]))
@@ -228,8 +235,13 @@ def engine(args):
         hbm, src = 6650.0, "fallback"
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
     flops = jv_flops_per_cell(3, 3) * ncells
+    # DRAM bytes (read + write) of one launch of this kernel and launch shape from an ncu capture of
+    # the 48^3 case (110 592 cells: 302.7 MB + 22.5 MB), scaled by cells; the profile summary gives
+    # the capture's command
+    traffic = (302.712e6 + 22.487e6) * ncells / 110592 if ORDER == 2 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "peak_source": src, "bytes_per_launch": alg_bytes,
+                "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, Q2 48^3 "
+                "launch, scaled by cells", "peak_source": src, "bytes_per_launch": alg_bytes,
                 "fp64_tflops": flops / (ms_step * 1e-3) / 1e12, "fp64_flops_per_launch": flops,
                 "note": "recompute J*v is latency/FP64-issue bound; hbm frac uses the algorithmic bytes"}
 
