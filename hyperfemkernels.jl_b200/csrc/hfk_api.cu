@@ -1387,6 +1387,9 @@ struct LevelWork {
   ChebWork<R> cheb;
 };
 
+// coarse mode of a one-level block-Jacobi slot (not a public value of hfk_pmg_set_coarse)
+constexpr int COARSE_BLOCKS = 2;
+
 struct hfk_pmg {
   int L = 0;
   std::vector<hfk_problem*> lv;
@@ -1403,7 +1406,7 @@ struct hfk_pmg {
   std::vector<std::unique_ptr<LevelWork<float>>> w32;
   // coarse: dense Cholesky factor (lower) of the assembled coarse tangent, or (HFK_COARSE_CG) a
   // fixed number of block-Jacobi CG steps per segment on the matrix-free coarse level
-  int coarse_mode = HFK_COARSE_CHOLESKY, coarse_iters = 20;
+  int coarse_mode = HFK_COARSE_CHOLESKY, coarse_iters = 20;  // or COARSE_BLOCKS (a block-Jacobi slot)
   int eig_inner = HFK_EIG_EUCLIDEAN;  // inner product of the eigenvalue estimate
   DBuf<double> Lc, cb, cx;
   DBuf<double> ccg_r, ccg_z, ccg_p, ccg_q, ccg_sc;
@@ -1542,6 +1545,8 @@ void band_check(hfk_pmg* m) {
 // (b >= n / 3) takes the dense potrf.
 void coarse_factor_launch(hfk_pmg* m) {
   hfk_problem* c = m->lv[m->L - 1];
+  if (!m->ev_c0)
+    for (cudaEvent_t* e : {&m->ev_fork, &m->ev_c0, &m->ev_c1, &m->ev_p0, &m->ev_p1}) HFK_CUDA(cudaEventCreate(e));
   HFK_CUDA(cudaEventRecord(m->ev_c0, c->stream));
   pattern_build_dev(c);
   jacobian_dev(c, c->x.p, c->dvals.p, c->nzval.p);
@@ -1639,10 +1644,9 @@ struct CoarseFork {
   explicit CoarseFork(hfk_pmg* mm) : m(mm) {}
   void fork() {
     hfk_problem* p0 = m->lv[0];
-    if (!m->side) {
-      HFK_CUDA(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+    if (!m->side) HFK_CUDA(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+    if (!m->ev_c0)
       for (cudaEvent_t* e : {&m->ev_fork, &m->ev_c0, &m->ev_c1, &m->ev_p0, &m->ev_p1}) HFK_CUDA(cudaEventCreate(e));
-    }
     HFK_CUDA(cudaEventRecord(m->ev_fork, p0->stream));
     HFK_CUDA(cudaStreamWaitEvent(m->side, m->ev_fork, 0));
     m->lv[m->L - 1]->stream = m->side;
@@ -1763,6 +1767,13 @@ template <typename R>
 void vcycle_dev(hfk_pmg* m, int l) {
   hfk_problem* p = m->lv[l];
   LevelWork<R>& w = level_work<R>(m, l);
+  if (m->L == 1) {  // a one-level slot (hfk_slot_create, FP64): its solve is the whole application
+    if constexpr (sizeof(R) == sizeof(double)) {
+      if (m->coarse_mode == COARSE_BLOCKS) blocks_apply_dev<double>(p, w.b.p, w.x.p);
+      else coarse_solve(m, w.b.p, w.x.p);
+    }
+    return;
+  }
   // pre-smoothing from zero, with the residual for the restriction
   cheb_smooth_coef<R>(p, w.cheb, m->coef[l]->p, m->degree, w.b.p, w.x.p, true, w.r.p);
   if (l + 1 == m->L - 1) {
@@ -2512,11 +2523,11 @@ int hfk_inject(hfk_transfer* t, const double* xf, const double* df, double* xc, 
   HFK_API_END
 }
 
-int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_transfer* const* transfers, int degree,
-                   double range, double inflate, int eig_iters, int coarse_every, int precision) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(out && levels && transfers, HFK_ERR_ARG, "null argument");
-  HFK_REQUIRE(nlevels >= 2, HFK_ERR_ARG, "PMultigrid needs at least two levels");
+}  // extern "C"
+namespace {
+hfk_pmg* pmg_create_impl(int nlevels, hfk_problem* const* levels, hfk_transfer* const* transfers, int degree,
+                         double range, double inflate, int eig_iters, int coarse_every, int precision) {
+  HFK_REQUIRE(levels && (transfers || nlevels == 1), HFK_ERR_ARG, "null argument");
   HFK_REQUIRE(degree >= 1, HFK_ERR_ARG, "Chebyshev: degree must be >= 1");
   HFK_REQUIRE(range > 1, HFK_ERR_ARG, "Chebyshev: range must be > 1");
   HFK_REQUIRE(inflate >= 1, HFK_ERR_ARG, "Chebyshev: inflate must be >= 1");
@@ -2585,7 +2596,30 @@ int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_t
   const int64_t nc = levels[nlevels - 1]->nfree;
   m->cb.resize(nc);
   m->cx.resize(nc);
-  *out = m.release();
+  return m.release();
+}
+}  // namespace
+extern "C" {
+
+int hfk_pmg_create(hfk_pmg** out, int nlevels, hfk_problem* const* levels, hfk_transfer* const* transfers, int degree,
+                   double range, double inflate, int eig_iters, int coarse_every, int precision) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(out && levels && transfers, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(nlevels >= 2, HFK_ERR_ARG, "PMultigrid needs at least two levels");
+  *out = pmg_create_impl(nlevels, levels, transfers, degree, range, inflate, eig_iters, coarse_every, precision);
+  HFK_API_END
+}
+
+int hfk_slot_create(hfk_pmg** out, hfk_problem* op, int kind, int every) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(out && op, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(kind == HFK_SLOT_LAGGED_ASSEMBLED || kind == HFK_SLOT_BLOCK_JACOBI, HFK_ERR_ARG,
+              "slot kind must be HFK_SLOT_LAGGED_ASSEMBLED or HFK_SLOT_BLOCK_JACOBI");
+  HFK_REQUIRE(every >= 1, HFK_ERR_ARG, "LaggedAssembled: every must be >= 1");
+  hfk_problem* lv[1] = {op};
+  hfk_pmg* m = pmg_create_impl(1, lv, nullptr, 1, 20.0, 1.1, 10, kind == HFK_SLOT_BLOCK_JACOBI ? 1 : every, HFK_FP64);
+  m->coarse_mode = kind == HFK_SLOT_BLOCK_JACOBI ? COARSE_BLOCKS : HFK_COARSE_CHOLESKY;
+  *out = m;
   HFK_API_END
 }
 
@@ -2603,8 +2637,9 @@ int hfk_pmg_destroy(hfk_pmg* m) {
     if (m->side) {
       cudaStreamSynchronize(m->side);
       cudaStreamDestroy(m->side);
-      for (cudaEvent_t e : {m->ev_fork, m->ev_c0, m->ev_c1, m->ev_p0, m->ev_p1}) cudaEventDestroy(e);
     }
+    for (cudaEvent_t e : {m->ev_fork, m->ev_c0, m->ev_c1, m->ev_p0, m->ev_p1})
+      if (e) cudaEventDestroy(e);
     pmg_drop_graph(m);
     if (m->ev0) cudaEventDestroy(m->ev0);
     if (m->ev1) cudaEventDestroy(m->ev1);
@@ -2655,8 +2690,8 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   m->since++;
   const bool rebuild = !m->built || m->since >= m->coarse_every;
   CoarseFork cfork(m);
-  if (rebuild && m->coarse_mode != HFK_COARSE_CG) {
-    cfork.fork();
+  if (rebuild && m->coarse_mode == HFK_COARSE_CHOLESKY) {
+    if (m->L > 1) cfork.fork();  // a one-level slot has nothing to overlap with
     coarse_factor_launch(m);
   }
   // smoothers: blocks and intervals (smoother_update!, src/smoothers.jl:86-107)
@@ -2724,8 +2759,17 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
       coarse_cg_update(m);
       HFK_CUDA(cudaStreamSynchronize(p0->stream));
       m->t_coarse += ms_since(tc);
-    } else {
+    } else if (m->coarse_mode == COARSE_BLOCKS) {
+      int bok = 0;
+      auto tb = std::chrono::steady_clock::now();
+      blocks_update_dev(p0, &bok);
+      m->t_blocks += ms_since(tb);
+      m->coarse_ok = bok != 0;
+      if (m->coarse_ok) m->nbuild++;
+    } else if (m->L > 1) {
       cfork.join();
+    } else {
+      coarse_factor_finish(m);
     }
     m->since = 0;
   }

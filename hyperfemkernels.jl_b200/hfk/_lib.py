@@ -28,6 +28,8 @@ COARSE_CHOLESKY = 0
 COARSE_CG = 1
 EIG_EUCLIDEAN = 0
 EIG_PRECONDITIONED = 1
+SLOT_LAGGED_ASSEMBLED = 0
+SLOT_BLOCK_JACOBI = 1
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -80,6 +82,7 @@ SIGNATURES = {
     "hfk_pmg_stats": [_vp, _vp],
     "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
     "hfk_solve_gmres": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _i, _pi, _pi, _pd],
+    "hfk_slot_create": [ctypes.POINTER(_vp), _vp, _i, _i],
     "hfk_mlp_create": [ctypes.POINTER(_vp), ctypes.c_uint64],
     "hfk_mlp_destroy": [_vp],
     "hfk_mlp_num_params": [],

@@ -293,6 +293,65 @@ class MatrixFreeSolver:
             raise ValueError("HyperFEMKernels: MatrixFreeSolver: maxiter must be positive")
 
 
+class LaggedAssembled:
+    """``LaggedAssembled(solver; every = 3)`` (src/preconditioners.jl:41-97): the operator's tangent
+    assembled and factorised at the setup and then every ``every`` updates (a stale factor in
+    between). ``solver`` "cholesky": the GPU Cholesky of the assembled tangent (banded when the
+    numbering is, FP64; at most 40 000 free dofs), in place of the reference's Gridap solver."""
+
+    def __init__(self, solver: str = "cholesky", every: int = 3):
+        if solver != "cholesky":
+            raise ValueError("HyperFEMKernels: LaggedAssembled: solver must be 'cholesky'")
+        if every < 1:
+            raise ValueError("HyperFEMKernels: LaggedAssembled: every must be ≥ 1")
+        self.solver, self.every = solver, int(every)
+
+
+class SlotState:
+    """State of a one-level preconditioner slot (``hfk_slot_create``): ``LaggedAssembled`` or
+    ``BlockJacobi`` inside a ``MatrixFreeSolver`` (``preconditioner_setup``/``update!``/``ldiv!``)."""
+
+    def __init__(self, slot, mf: MatrixFreeJacobian):
+        if not mf.prepared:
+            raise RuntimeError("HyperFEMKernels: the MatrixFreeJacobian has not been prepared")
+        kind = _lib.SLOT_BLOCK_JACOBI if isinstance(slot, BlockJacobi) else _lib.SLOT_LAGGED_ASSEMBLED
+        # the slot's handle refers to the operator's problem: keep it alive until the slot is gone
+        self.problem = mf.op.problem
+        h = ctypes.c_void_p()
+        call("hfk_slot_create", ctypes.byref(h), mf.op.problem.h, kind, getattr(slot, "every", 1))
+        self.h, self.slot = h, slot
+        self.update(mf)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().hfk_pmg_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def update(self, mf: MatrixFreeJacobian):
+        ok = ctypes.c_int()
+        d = mf.dvals if mf.dvals is not None else mf.op.dirichlet_values()
+        call("hfk_pmg_update", self.h, ptr(mf.x), ptr(d), ctypes.byref(ok))
+        self.ok = bool(ok.value)
+        return self
+
+    def ldiv(self, y, r):
+        call("hfk_pmg_vcycle", self.h, ptr(r), ptr(y))
+        return y
+
+    def stats(self):
+        out = np.zeros(9)
+        call("hfk_pmg_stats", self.h, ptr(out))
+        return {"updates": out[0], "builds": out[1]}
+
+    @property
+    def nbuild(self) -> int:
+        return int(self.stats()["builds"])
+
+
 class MatrixFreeSolverNS:
     def __init__(self, solver: MatrixFreeSolver, mf: MatrixFreeJacobian):
         if not mf.prepared:
@@ -304,6 +363,8 @@ class MatrixFreeSolverNS:
             self.prec = None
         elif isinstance(p, PMultigrid):
             self.prec = PMultigridState(p, mf)
+        elif isinstance(p, (LaggedAssembled, BlockJacobi)):
+            self.prec = SlotState(p, mf)
         else:
             raise TypeError("HyperFEMKernels: unsupported preconditioner slot")
         self.rtol = solver.rtol

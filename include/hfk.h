@@ -225,6 +225,17 @@ int hfk_pmg_stats(hfk_pmg* m, double* out);
 /* Interval and Ritz values of a level's smoother (with segments: the extreme Ritz values over the
  * segments and the interval of the largest). */
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
+/* A one-level preconditioner slot on the prepared operator `op`, for hfk_solve_cg / hfk_solve_gmres
+ * (the reference's preconditioner slots, src/preconditioners.jl): HFK_SLOT_LAGGED_ASSEMBLED, the
+ * operator's tangent assembled on the GPU and factorised (banded or dense Cholesky, FP64, at most
+ * 40000 free dofs) at the first update and then every `every` updates (LaggedAssembled(LUSolver();
+ * every), :41-97; a stale factor between builds); HFK_SLOT_BLOCK_JACOBI, the nodal 3x3 block
+ * inverses of the tangent at every update (BlockJacobi, :151-344; `every` ignored). The slot is an
+ * hfk_pmg handle with one level: updated by hfk_pmg_update, applied by the solvers or
+ * hfk_pmg_vcycle, builds counted by hfk_pmg_stats (out[1]), released by hfk_pmg_destroy. */
+#define HFK_SLOT_LAGGED_ASSEMBLED 0
+#define HFK_SLOT_BLOCK_JACOBI 1
+int hfk_slot_create(hfk_pmg** out, hfk_problem* op, int kind, int every);
 /* Coarse solve of the hierarchy: HFK_COARSE_CHOLESKY (default; the assembled coarse level, dense
  * Cholesky, in place of the reference's LUSolver, src/pmultigrid.jl:212-219) or HFK_COARSE_CG:
  * `iters` steps of block-Jacobi CG per segment on the matrix-free coarse level from zero (scalars on

@@ -382,6 +382,59 @@ def test_pmg_solve_matches_direct_and_iterations_bounded(orders):
     assert its[1] <= 1.4 * its[0] + 2
 
 
+def test_solver_slots_reproduce_the_direct_solve():
+    # test/solvers/test_matrixfree_solver.jl:24-52: GMRES, FGMRES and CG without and with the slots
+    # (LaggedAssembled, BlockJacobi) reproduce the direct solve; an up-to-date LaggedAssembled is an
+    # exact preconditioner (at most 2 iterations), and each slot was built once
+    V, op, orc = make(2, jac="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    A = orc.jacobian(x, V.dirichlet_values)
+    b = -op.residual(np.zeros(V.nfree), x)
+    ref = sp.linalg.spsolve(A.tocsc(), b)
+    n = V.nfree
+    configs = [("gmres", None), ("fgmres", None), ("gmres", S.LaggedAssembled()),
+               ("gmres", S.LaggedAssembled(every=2)), ("gmres", S.BlockJacobi()), ("fgmres", S.BlockJacobi()),
+               ("cg", None), ("cg", S.BlockJacobi()), ("cg", S.LaggedAssembled())]
+    for kry, prec in configs:
+        ls = S.MatrixFreeSolver(krylov=kry, rtol=1e-10, maxiter=4000, restart=n, preconditioner=prec)
+        ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf)
+        dx = S.solve(np.zeros(n), ns, b)
+        its = S.linear_iterations(ns)
+        assert S.linear_converged(ns) and reldiff(dx, ref) < 1e-8, (kry, prec)
+        assert 0 < its <= n + 1
+        if isinstance(prec, S.LaggedAssembled):
+            assert its <= 2
+        assert S.preconditioner_builds(ns) == (0 if prec is None else 1)
+
+
+def test_lagged_assembled_rebuilds_every_k_setups():
+    # test/solvers/test_matrixfree_solver.jl:94-112: builds at setups 1 and 4 for every = 3; the
+    # stale factor still converges to each new solution; exact where rebuilt
+    V, op, orc = make(2, jac="matrixfree")
+    n = V.nfree
+    rng = np.random.default_rng(8)
+    states = [svk_state(V, amp=1e-2) + 0.01 * rng.standard_normal(n) for _ in range(5)]
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, states[0])
+    ls = S.MatrixFreeSolver(krylov="gmres", rtol=1e-10, maxiter=4000, restart=n,
+                            preconditioner=S.LaggedAssembled(every=3))
+    ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf)
+    its = []
+    for k, x in enumerate(states, start=1):
+        if k > 1:
+            op.jacobian(mf, x)
+            S.numerical_setup_update(ns, mf)
+        assert S.preconditioner_builds(ns) == 1 + (k - 1) // 3
+        b = op.residual(np.zeros(n), x)
+        dx = S.solve(np.zeros(n), ns, b)
+        A = orc.jacobian(x, V.dirichlet_values)
+        assert S.linear_converged(ns) and reldiff(dx, sp.linalg.spsolve(A.tocsc(), b)) < 1e-8
+        its.append(S.linear_iterations(ns))
+    assert its[0] <= 2 and its[3] <= 2 and all(i > 0 for i in its)
+
+
 def test_lagged_coarse_newton_matches_direct_newton():
     # test/solvers/test_pmultigrid.jl:95-115: Newton with the matrix-free p-MG GMRES, the coarse level
     # rebuilt every `coarse_every` updates, against Newton with a direct solve of the assembled
