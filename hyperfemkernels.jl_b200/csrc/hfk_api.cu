@@ -699,6 +699,68 @@ void build_block_structure(hfk_problem* p) {
   p->Binv32.resize(9 * (size_t)std::max(p->nblocks, 1));
 }
 
+void invert_blocks_and_check(hfk_problem* p, int* ok) {
+  p->flag.resize(1);
+  p->flag.zero(p->stream);
+  invert_blocks_kernel<<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, p->B.p, p->Binv.p,
+                                                                     p->Binv32.p, p->flag.p);
+  check_launch(p);
+  int bad = 0;
+  HFK_CUDA(cudaMemcpyAsync(&bad, p->flag.p, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  p->blocks_ok = !bad;
+  *ok = !bad;
+}
+
+// the sum-factorised block extraction (kern_vec.cuh) for tensor-product cells with Q <= P; false
+// when the problem has no such shape (the dense kernel then runs)
+template <int Q, int P>
+void blocks_tp_launch(hfk_problem* p, BlockIO io) {
+  const size_t smem = blocks_tp_smem<Q, P>();
+  static size_t attr = 0;
+  if (smem > attr) {
+    HFK_CUDA(cudaFuncSetAttribute(blocks_tp_kernel<Q, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  const Tab1D<double> tab = make_tab<double>(p);
+  if (use_atomic_scatter(p)) {
+    io.atomic = 1;
+    blocks_tp_kernel<Q, P><<<p->ncells, 256, smem, p->stream>>>(cell_data(p, nullptr, p->ncells), tab, io);
+    check_launch(p);
+  } else {
+    for (int c = 0; c < p->ncolors; ++c) {
+      const int n = p->color_start[c + 1] - p->color_start[c];
+      if (!n) continue;
+      blocks_tp_kernel<Q, P><<<n, 256, smem, p->stream>>>(cell_data(p, p->cells_by_color.p + p->color_start[c], n), tab,
+                                                          io);
+      check_launch(p);
+    }
+  }
+}
+
+bool blocks_tp_dev(hfk_problem* p, const BlockIO& io) {
+  if (p->Q < 2 || p->P < p->Q || p->nn != p->Q * p->Q * p->Q || p->np != p->P * p->P * p->P) return false;
+  switch (p->Q * 10 + p->P) {
+#define HFK_BCASE(Qv, Pv)             \
+  case Qv * 10 + Pv:                  \
+    blocks_tp_launch<Qv, Pv>(p, io); \
+    return true;
+    HFK_BCASE(2, 2)
+    HFK_BCASE(2, 3)
+    HFK_BCASE(2, 4)
+    HFK_BCASE(2, 5)
+    HFK_BCASE(3, 3)
+    HFK_BCASE(3, 4)
+    HFK_BCASE(3, 5)
+    HFK_BCASE(4, 4)
+    HFK_BCASE(4, 5)
+    HFK_BCASE(5, 5)
+#undef HFK_BCASE
+    default:
+      return false;
+  }
+}
+
 void blocks_update_dev(hfk_problem* p, int* ok) {
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "blocks need a prepared tangent (call hfk_mf_prepare)");
   if (p->bdofs.n == 0 && p->nblocks == 0) build_block_structure(p);
@@ -709,6 +771,10 @@ void blocks_update_dev(hfk_problem* p, int* ok) {
   }
   p->B.zero(p->stream);
   BlockIO io{p->x.p, p->dvals.p, p->dNt.p, p->block_of.p, p->B.p, p->np, p->nn, 0};
+  if (blocks_tp_dev(p, io)) {
+    invert_blocks_and_check(p, ok);
+    return;
+  }
   const size_t smem = ((size_t)3 * p->nn + 9 * p->np + 9 * p->np + p->np + 81 * p->np) * sizeof(double);
   static size_t attr = 0;
   if (smem > attr) {
@@ -727,16 +793,7 @@ void blocks_update_dev(hfk_problem* p, int* ok) {
       check_launch(p);
     }
   }
-  p->flag.resize(1);
-  p->flag.zero(p->stream);
-  invert_blocks_kernel<<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, p->B.p, p->Binv.p,
-                                                                     p->Binv32.p, p->flag.p);
-  check_launch(p);
-  int bad = 0;
-  HFK_CUDA(cudaMemcpyAsync(&bad, p->flag.p, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  p->blocks_ok = !bad;
-  *ok = !bad;
+  invert_blocks_and_check(p, ok);
 }
 
 template <typename R>

@@ -207,8 +207,13 @@ def test_atomic_and_coloured_scatter_agree(order):
     assert reldiff(out["coloured"][0], orc.jacobian(x, V.dirichlet_values) @ dx) < TOL64
 
 
-def test_blocks_parity():
-    V, op, orc = make(2, jac="matrixfree")
+@pytest.mark.parametrize("order,perturb", CASES)
+@pytest.mark.parametrize("scatter", ["atomic", "coloured"])
+def test_blocks_parity(order, perturb, scatter):
+    # the nodal blocks (sum-factorised on tensor-product cells) against the oracle's dense sums,
+    # affine and trilinear cells, atomic and colour-by-colour accumulation
+    V, op, orc = make(order, perturb=perturb, jac="matrixfree")
+    op.problem.set_scatter(scatter)
     x = svk_state(V, amp=1e-2)
     mf = MatrixFreeJacobian(op)
     op.jacobian(mf, x)
