@@ -213,18 +213,11 @@ __global__ void __launch_bounds__(256) blocks_tp_kernel(CellData cd, Tab1D<doubl
   }
   __syncthreads();
   const double* A = io.dNt;
-  for (int q = threadIdx.x; q < NP; q += blockDim.x) {
-    double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int n = 0; n < NN; ++n) {
-      const double a0 = A[n + NN * (3 * q)], a1 = A[n + NN * (1 + 3 * q)], a2 = A[n + NN * (2 + 3 * q)];
-      for (int c = 0; c < 3; ++c) {
-        const double x = xl[c * NN + n];
-        G[c][0] += x * a0;
-        G[c][1] += x * a1;
-        G[c][2] += x * a2;
-      }
-    }
-    double Jt[9], iJ[9], det;
+  // physical gradients H per point: with few points per cell the reference gradients are spread one
+  // (point, component, direction) per thread (measured faster for Q2), else one point per thread
+  constexpr bool SPREAD = 9 * NP <= 512;
+  auto point_geometry = [&](int q, double* iJ, double& det) {
+    double Jt[9];
     if (cd.affine[cell]) {
       for (int i = 0; i < 9; ++i) iJ[i] = cd.geo[(size_t)cell * 10 + i];
       det = cd.geo[(size_t)cell * 10 + 9];
@@ -234,10 +227,49 @@ __global__ void __launch_bounds__(256) blocks_tp_kernel(CellData cd, Tab1D<doubl
       inv3(Jt, det, iJ);
       det = fabs(det);
     }
-    for (int c = 0; c < 3; ++c)
-      for (int J = 0; J < 3; ++J) Hs[q * 9 + c + 3 * J] = iJ[J] * G[c][0] + iJ[J + 3] * G[c][1] + iJ[J + 6] * G[c][2];
-    for (int i = 0; i < 9; ++i) iJs[q * 9 + i] = iJ[i];
-    dVs[q] = cd.w[q] * det;
+  };
+  if constexpr (SPREAD) {
+    double* Gs = F;  // 9 NP, in the field region (free until the tangent phase)
+    for (int e = threadIdx.x; e < NP * 9; e += blockDim.x) {
+      const int q = e / 9, cK = e % 9, c = cK / 3, K = cK % 3;
+      const double* a = A + NN * (K + 3 * q);
+      const double* x = xl + c * NN;
+      double g = 0;
+      for (int n = 0; n < NN; ++n) g += x[n] * a[n];
+      Gs[e] = g;
+    }
+    for (int q = threadIdx.x; q < NP; q += blockDim.x) {
+      double iJ[9], det;
+      point_geometry(q, iJ, det);
+      for (int i = 0; i < 9; ++i) iJs[q * 9 + i] = iJ[i];
+      dVs[q] = cd.w[q] * det;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NP * 9; e += blockDim.x) {  // H[q][c + 3 J] = sum_K iJ[J + 3 K] G[q][c][K]
+      const int q = e / 9, cJ = e % 9, c = cJ % 3, J = cJ / 3;
+      const double* iJ = iJs + q * 9;
+      const double* G = Gs + q * 9 + c * 3;
+      Hs[q * 9 + c + 3 * J] = iJ[J] * G[0] + iJ[J + 3] * G[1] + iJ[J + 6] * G[2];
+    }
+  } else {
+    for (int q = threadIdx.x; q < NP; q += blockDim.x) {
+      double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int n = 0; n < NN; ++n) {
+        const double a0 = A[n + NN * (3 * q)], a1 = A[n + NN * (1 + 3 * q)], a2 = A[n + NN * (2 + 3 * q)];
+        for (int c = 0; c < 3; ++c) {
+          const double x = xl[c * NN + n];
+          G[c][0] += x * a0;
+          G[c][1] += x * a1;
+          G[c][2] += x * a2;
+        }
+      }
+      double iJ[9], det;
+      point_geometry(q, iJ, det);
+      for (int c = 0; c < 3; ++c)
+        for (int J = 0; J < 3; ++J) Hs[q * 9 + c + 3 * J] = iJ[J] * G[c][0] + iJ[J + 3] * G[c][1] + iJ[J + 6] * G[c][2];
+      for (int i = 0; i < 9; ++i) iJs[q * 9 + i] = iJ[i];
+      dVs[q] = cd.w[q] * det;
+    }
   }
   __syncthreads();
   // per point and component pair: D[K][K'] = dV sum_{J,L} iJ[J + 3K] T[(ci,J),(cj,L)] iJ[L + 3K'],
