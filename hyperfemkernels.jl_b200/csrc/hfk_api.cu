@@ -1013,11 +1013,11 @@ bool hessenberg_eigvals(int n, std::vector<double> H /* column-major n x n */, d
 }
 
 struct EigWork {
-  DBuf<double> V, Z, t, w, pw, Hd;
+  DBuf<double> V, Z, t, w, pw, Hd, h2, part;
 };
 
 // eigenvalue_bounds (src/preconditioners.jl:374-389) of every segment at once: k Arnoldi steps
-// (modified Gram-Schmidt) on J P^-1 from the start vector with per-segment inner products, so that
+// (classical Gram-Schmidt with one reorthogonalisation) on J P^-1 from the start vector with per-segment inner products, so that
 // each segment builds its own Hessenberg matrix (a block-diagonal operator keeps the segments'
 // Krylov spaces apart); breakdown truncation and Ritz values per segment on the host. One copy
 // of the Hessenberg matrices to the host, no other synchronisation.
@@ -1038,6 +1038,9 @@ void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev,
   ew.w.resize(n);
   ew.Hd.resize((size_t)hs * ns);
   ew.Hd.zero(p->stream);
+  ew.h2.resize((size_t)hs * ns);
+  ensure_seg_items(p);
+  ew.part.resize((size_t)SEG_MDOTS * std::max(p->nitems, 1));
   double* Hd = ew.Hd.p;
   const int32_t* seg = seg_dof_map(p);
   const int sg = std::max(1, (ns + 255) / 256);
@@ -1068,16 +1071,34 @@ void eig_bounds_dev(hfk_problem* p, EigWork& ew, int k, const double* start_dev,
       blocks_apply_dev<double>(p, V(j), ew.t.p);
       mf_apply_dev(p, ew.t.p, ew.w.p);
     }
-    for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, coefficients written into H on the device
-      double* hij = Hd + i + (size_t)ld * j;
-      seg_dots<double>(p, 1, hij, hs, pinner ? Z(i) : V(i), ew.w.p);
-      seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, V(i), ew.w.p);
-      check_launch(p);
-      if (pinner) {
-        seg_axpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, hij, hs, -1.0, Z(i), ew.pw.p);
+    // classical Gram-Schmidt with one reorthogonalisation: h = B^T w, w -= V h (and pw -= Z h in
+    // the P^-1 inner product, B = Z; else B = V), twice, the second pass's coefficients added to
+    // the first's; one multi-dot and one multi-axpy launch per pass and 16 basis vectors
+    for (int pass = 0; pass < 2; ++pass) {
+      double* hc = pass == 0 ? Hd + (size_t)ld * j : ew.h2.p;  // per segment at stride hs
+      for (int c0 = 0; c0 <= j; c0 += SEG_MDOTS) {
+        const int kc = std::min(SEG_MDOTS, j + 1 - c0);
+        if (p->nitems) {
+          seg_mdots_kernel<<<p->nitems, RED_THREADS, 0, p->stream>>>(kc, p->item_lo.p, p->item_hi.p,
+                                                                    pinner ? Z(c0) : V(c0), n, ew.w.p, ew.part.p);
+          check_launch(p);
+        }
+        seg_mfinish_kernel<<<ns, RED_THREADS, 0, p->stream>>>(kc, p->item_first.p, ew.part.p, hc + c0, hs);
         check_launch(p);
       }
+      for (int c0 = 0; c0 <= j; c0 += SEG_MDOTS) {
+        const int kc = std::min(SEG_MDOTS, j + 1 - c0);
+        seg_maxpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, kc, hc + c0, hs, V(c0), n, ew.w.p);
+        check_launch(p);
+        if (pinner) {
+          seg_maxpy_kernel<<<vec_grid(n), 256, 0, p->stream>>>(n, seg, kc, hc + c0, hs, Z(c0), n, ew.pw.p);
+          check_launch(p);
+        }
+      }
     }
+    seg_add_kernel<<<std::max(1, (ns * (j + 1) + 255) / 256), 256, 0, p->stream>>>(ns, j + 1, ew.h2.p,
+                                                                                 Hd + (size_t)ld * j, hs);
+    check_launch(p);
     double* hn = Hd + (j + 1) + (size_t)ld * j;
     seg_dots<double>(p, 1, hn, hs, ew.w.p, pinner ? ew.pw.p : ew.w.p);
     seg_sqrt_kernel<<<sg, 256, 0, p->stream>>>(ns, hn, hs);

@@ -55,6 +55,60 @@ __global__ void __launch_bounds__(RED_THREADS) seg_finish_kernel(int k, const in
   }
 }
 
+// ---- several inner products at once (classical Gram-Schmidt of the Arnoldi estimate) ---------
+constexpr int SEG_MDOTS = 16;  // vectors per multi-dot launch
+
+// partial[it * SEG_MDOTS + j] = sum over chunk it of V_j[i] w[i], j < k <= SEG_MDOTS (V_j = V + j ldv)
+__global__ void __launch_bounds__(RED_THREADS) seg_mdots_kernel(int k, const int64_t* lo, const int64_t* hi,
+                                                                const double* V, int64_t ldv, const double* w,
+                                                                double* partial) {
+  const int it = blockIdx.x;
+  const int64_t l = lo[it], h = hi[it];
+  double s[SEG_MDOTS];
+#pragma unroll
+  for (int j = 0; j < SEG_MDOTS; ++j) s[j] = 0;
+  for (int64_t i = l + threadIdx.x; i < h; i += blockDim.x) {
+    const double wi = w[i];
+#pragma unroll
+    for (int j = 0; j < SEG_MDOTS; ++j)
+      if (j < k) s[j] += V[(size_t)j * ldv + i] * wi;
+  }
+#pragma unroll
+  for (int j = 0; j < SEG_MDOTS; ++j)
+    if (j < k) block_sum_store(s[j], partial + (size_t)it * SEG_MDOTS + j);
+}
+
+// out[s * stride + j] = sum over the chunks of segment s, j < k (one CTA per segment)
+__global__ void __launch_bounds__(RED_THREADS) seg_mfinish_kernel(int k, const int32_t* first, const double* partial,
+                                                                  double* out, int stride) {
+  const int s = blockIdx.x;
+  const int f = first[s], e = first[s + 1];
+  for (int j = 0; j < k; ++j) {
+    double v = 0;
+    for (int it = f + threadIdx.x; it < e; it += blockDim.x) v += partial[(size_t)it * SEG_MDOTS + j];
+    block_sum_store(v, out + (size_t)s * stride + j);
+  }
+}
+
+// y[i] -= sum_{j<k} c[seg(i) * stride + j] V_j[i]
+__global__ void seg_maxpy_kernel(int64_t n, const int32_t* seg, int k, const double* c, int stride, const double* V,
+                                 int64_t ldv, double* y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* cs = c + (size_t)seg_at(seg, i) * stride;
+    double acc = 0;
+    for (int j = 0; j < k; ++j) acc += cs[j] * V[(size_t)j * ldv + i];
+    y[i] -= acc;
+  }
+}
+
+// dst[s * stride + j] += src[s * stride + j], j < k, every segment s
+__global__ void seg_add_kernel(int ns, int k, const double* src, double* dst, int stride) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ns * k; e += gridDim.x * blockDim.x) {
+    const int s = e / k, j = e - s * k;
+    dst[(size_t)s * stride + j] += src[(size_t)s * stride + j];
+  }
+}
+
 // y[i] += sign * a[seg(i) * stride] x[i]
 __global__ void seg_axpy_kernel(int64_t n, const int32_t* seg, const double* a, int stride, double sign,
                                 const double* x, double* y) {
