@@ -368,7 +368,11 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
                             {1, SHAPE_PT_WIDE},
                             {0, SHAPE_PT_NARROW},
                             {0, SHAPE_PT_WIDE}};
-    const int ncand = MODE == MODE_JV ? 8 : 4;
+    // batched problems keep the line-mapped kernels: the tuning call has every problem active, but
+    // most of a batched solve runs with converged problems masked, where the line-mapped kernels'
+    // per-warp exit measured better (256 SVK Q2 problems: 22.3 s against 23.9 s with the
+    // point-parallel product picked for the Q1 level)
+    const int ncand = MODE == MODE_JV && p->nseg <= 1 ? 8 : 4;
     cudaEvent_t e0, e1;
     HFK_CUDA(cudaEventCreate(&e0));
     HFK_CUDA(cudaEventCreate(&e1));

@@ -106,6 +106,12 @@ __global__ void __launch_bounds__(NT, jvp_min_blocks<NT>()) jvp_kernel(CellData 
     saff[tid] = aff;
   }
   __syncthreads();
+  {
+    // a CTA without an active cell (a batch's converged problems, skipped) returns at once
+    bool none = true;
+    for (int lc = 0; lc < C; ++lc) none = none && scell[lc] < 0;
+    if (none) return;
+  }
 
   // ---- gather (increments are zero at Dirichlet dofs) ------------------------------------------
   for (int e = tid; e < C * NDL; e += NT) {
