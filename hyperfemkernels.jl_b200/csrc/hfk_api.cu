@@ -2412,6 +2412,19 @@ int hfk_blocks_apply(hfk_problem* p, const double* r, double* y) {
   HFK_API_END
 }
 
+int hfk_blocks_set(hfk_problem* p, const double* B, int* ok) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && B && ok, HFK_ERR_ARG, "null argument");
+  HFK_REQUIRE(p->nblocks > 0, HFK_ERR_STATE, "blocks not numbered (call hfk_blocks_update first)");
+  const size_t n = 9 * (size_t)p->nblocks;
+  if (is_device_ptr(B))
+    HFK_CUDA(cudaMemcpyAsync(p->B.p, B, n * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+  else
+    HFK_CUDA(cudaMemcpyAsync(p->B.p, B, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  invert_blocks_and_check(p, ok);
+  HFK_API_END
+}
+
 int hfk_blocks_get(hfk_problem* p, int* nblocks, int32_t* dofs, double* B, double* Binv) {
   HFK_API_BEGIN
   HFK_REQUIRE(p && nblocks, HFK_ERR_ARG, "null argument");

@@ -65,6 +65,7 @@ SIGNATURES = {
     "hfk_blocks_update": [_vp, _pi],
     "hfk_blocks_apply": [_vp, _vp, _vp],
     "hfk_blocks_get": [_vp, _pi, _vp, _vp, _vp],
+    "hfk_blocks_set": [_vp, _vp, _pi],
     "hfk_eigenvalue_bounds": [_vp, _i, _vp, _pd, _pd],
     "hfk_hessenberg_eigvals": [_i, _vp, _vp, _vp],
     "hfk_chebyshev_smooth": [_vp, _d, _d, _i, _vp, _vp, _i, _vp],

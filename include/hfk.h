@@ -154,6 +154,11 @@ int hfk_mf_apply_many(hfk_problem* p, int count, const double* const* dx, double
 int hfk_blocks_update(hfk_problem* p, int* ok);
 /* ldiv!(y, BlockJacobiState, r) (src/preconditioners.jl:329-344). */
 int hfk_blocks_apply(hfk_problem* p, const double* r, double* y);
+/* Replace the nodal blocks B (3, 3, nblocks; the numbering of hfk_blocks_get) and invert them, as
+ * invert_blocks! does (src/preconditioners.jl:284-305); ok = 0 if a block is not finite. A subdomain
+ * of a partitioned mesh passes its blocks summed with the other subdomains' partial blocks of the
+ * nodes they share. Requires hfk_blocks_update once (it numbers the blocks). */
+int hfk_blocks_set(hfk_problem* p, const double* B, int* ok);
 /* Blocks as the reference stores them: dofs (3, nblocks) 1-based (0 = fixed component), B and Binv
  * (3, 3, nblocks). Any output may be NULL; nblocks is always written. */
 int hfk_blocks_get(hfk_problem* p, int* nblocks, int32_t* dofs, double* B, double* Binv);
