@@ -2573,6 +2573,28 @@ int hfk_transfer_create(hfk_transfer** out, hfk_problem* fine, hfk_problem* coar
   HFK_API_END
 }
 
+int hfk_transfer_set_multiplicity(hfk_transfer* t, const int32_t* mult) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(t && mult, HFK_ERR_ARG, "null argument");
+  const int64_t n = t->fine->nfree;
+  std::vector<int32_t> m(mult, mult + n);
+  std::vector<int32_t> own(std::max<int64_t>(n, 1), 0);
+  for (size_t k = 0; k < t->fine->h_ids.size(); ++k)
+    if (t->fine->h_ids[k] > 0) own[t->fine->h_ids[k] - 1] += 1;
+  for (int64_t q = 0; q < n; ++q)
+    HFK_REQUIRE(m[q] >= own[q] && (m[q] > 0) == (own[q] > 0), HFK_ERR_ARG,
+                "a multiplicity is below the number of this level's cells that share the dof");
+  if (n) t->mult.upload(m.data(), m.size(), t->fine->stream);
+  if (t->tp) {
+    std::vector<double> im(std::max<int64_t>(n, 1), 0.0);
+    for (int64_t q = 0; q < n; ++q) im[q] = m[q] > 0 ? 1.0 / m[q] : 0.0;
+    t->invmult.upload(im.data(), im.size(), t->fine->stream);
+    t->tpd.invmult = t->invmult.p;
+  }
+  HFK_CUDA(cudaStreamSynchronize(t->fine->stream));
+  HFK_API_END
+}
+
 int hfk_transfer_destroy(hfk_transfer* t) {
   HFK_API_BEGIN
   delete t;

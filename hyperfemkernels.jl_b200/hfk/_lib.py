@@ -72,6 +72,7 @@ SIGNATURES = {
     "hfk_chebyshev_smooth_noalloc": [_vp, _d, _d, _i, _vp, _vp, _i, _vp],
     "hfk_transfer_create": [ctypes.POINTER(_vp), _vp, _vp, _vp, _vp],
     "hfk_transfer_destroy": [_vp],
+    "hfk_transfer_set_multiplicity": [_vp, _vp],
     "hfk_prolongate": [_vp, _vp, _vp],
     "hfk_restrict": [_vp, _vp, _vp],
     "hfk_inject": [_vp, _vp, _vp, _vp, _vp],

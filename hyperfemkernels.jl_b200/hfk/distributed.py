@@ -28,6 +28,8 @@ import torch
 
 from ._lib import call, ptr
 
+_CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy
+
 
 def slab_partition(mesh, world: int) -> np.ndarray:
     """Rank of every cell when the mesh is cut into ``world`` layers of cells along z (balanced: the
@@ -291,8 +293,12 @@ class DistributedJacobian:
         self.mf = mf
         self._apply = apply
         if mf is not None and torch.cuda.is_available():
-            # order the engine's launches with the exchange's torch and NCCL work
-            mf.op.problem.set_stream(torch.cuda.current_stream().cuda_stream)
+            # the engine's launches on torch's current stream, so that they are ordered with the
+            # exchange's torch and NCCL work and with the other levels' launches; torch's default
+            # stream is the legacy default stream (handle 0), passed as cudaStreamLegacy (handle 1)
+            # because handle 0 selects the problem's own stream
+            s = torch.cuda.current_stream().cuda_stream
+            mf.op.problem.set_stream(s if s else _CUDA_STREAM_LEGACY)
 
     @property
     def nfree(self) -> int:
@@ -430,3 +436,203 @@ class OwnerAssembly:
         nglob = self.sub.space.parent.nfree
         return sp.csr_matrix((coo.data, (coo.row, self.sub.free_global[coo.col])),
                              shape=(rows.shape[0], nglob))
+
+
+def _global_multiplicity(space) -> np.ndarray:
+    """Cells containing every free dof of ``space`` over the whole mesh (``cells_of``,
+    ``src/transfers.jl:124-127``)."""
+    ids = space.cell_dof_ids
+    return np.bincount(ids[ids > 0].astype(np.int64) - 1, minlength=space.nfree).astype(np.int32)
+
+
+class DistributedPMultigrid:
+    """``PMultigrid`` (``src/pmultigrid.jl:256-338``) over a partitioned mesh.
+
+    Every level is partitioned like the finest (the same ``cell_rank``), so a level's subdomain holds
+    the same cells on every level and the transfers stay cell-local: prolongation of a consistent
+    coarse vector is consistent as it is; the restriction divides by the multiplicity over the whole
+    mesh (``hfk_transfer_set_multiplicity``) and its partial coarse sums are completed by the coarse
+    level's halo sum. The smoothers are the reference's Chebyshev–block-Jacobi (``src/smoothers.jl:
+    42-146``) over the halo-summed products and summed nodal blocks, with the Arnoldi estimate's inner
+    products all-reduced and its start vector evaluated at the global dof numbers (the estimate of the
+    single-domain problem). The coarsest level runs ``coarse_iters`` block-Jacobi CG steps (a variable
+    preconditioner: use the flexible ``cg``).
+
+    ``A`` is the finest level's ``DistributedJacobian``; ``spaces`` the global trial spaces of the
+    coarser levels, finest first excluded.
+    """
+
+    def __init__(self, A: DistributedJacobian, spaces, cell_rank, smoother=None, coarse_iters: int = 20):
+        from .operator import KernelOperator, MatrixFreeJacobian
+        from .solvers import Chebyshev, Prolongation
+
+        if A.mf is None:
+            raise ValueError("HyperFEMKernels: the p-multigrid needs the engine's MatrixFreeJacobian")
+        if coarse_iters < 1:
+            raise ValueError("HyperFEMKernels: coarse_iters must be ≥ 1")
+        self.smoother = smoother if smoother is not None else Chebyshev()
+        if self.smoother.eig_inner != "euclidean":
+            raise ValueError("HyperFEMKernels: the partitioned p-multigrid runs the Euclidean Arnoldi estimate")
+        self.coarse_iters = int(coarse_iters)
+        op = A.mf.op
+        self.A = [A]
+        for U in spaces:
+            sub = Subdomain(U, cell_rank, A.sub.rank)
+            lop = KernelOperator(op.res, op.jac, sub.space, jacobian="matrixfree")
+            self.A.append(DistributedJacobian(sub, A.comm, mf=MatrixFreeJacobian(lop)))
+        self.P = []
+        for l in range(len(self.A) - 1):
+            fine, coarse = self.A[l], self.A[l + 1]
+            t = Prolongation(coarse.mf.op.problem, fine.mf.op.problem)
+            glob = fine.sub.space.parent
+            m = np.ascontiguousarray(_global_multiplicity(glob)[fine.sub.free_global])
+            call("hfk_transfer_set_multiplicity", t.h, ptr(m, np.int32))
+            self.P.append(t)
+        self.blocks = [DistributedBlockJacobi(a) for a in self.A]
+        self.bounds = [None] * (len(self.A) - 1)
+        self.ok = False
+
+    @property
+    def levels(self) -> int:
+        return len(self.A)
+
+    def update(self):
+        """``update_levels!`` + the smoothers' updates (``src/pmultigrid.jl:168-221``) at the state the
+        finest level was prepared at."""
+        fine = self.A[0].mf
+        dev = torch.device("cuda", torch.cuda.current_device())
+        x = fine.x if isinstance(fine.x, torch.Tensor) else torch.from_numpy(np.asarray(fine.x)).to(dev)
+        d = fine.dvals if isinstance(fine.dvals, torch.Tensor) else torch.from_numpy(np.asarray(fine.dvals)).to(dev)
+        for l, P in enumerate(self.P):
+            c = self.A[l + 1]
+            xc = torch.zeros(c.sub.nfree, dtype=torch.float64, device=dev)
+            dc = torch.zeros(c.sub.space.ndir, dtype=torch.float64, device=dev)
+            P.inject(xc, dc, x, d)
+            c.prepare(xc, dc)
+            x, d = xc, dc
+        ok = True
+        for b in self.blocks:
+            ok &= b.update().ok
+        for l in range(len(self.A) - 1):
+            lo, hi = self._eig_bounds(l)
+            self.bounds[l] = (lo, hi)
+            ok &= bool(np.isfinite(hi) and hi > 0 and lo > 0)
+        self.ok = ok
+        return self
+
+    def _eig_bounds(self, l: int):
+        """Ritz bounds of J P⁻¹ after ``eig_iters`` Arnoldi steps (``src/preconditioners.jl:350-389``):
+        classical Gram–Schmidt with one reorthogonalisation, each pass one all-reduce."""
+        from .solvers import hessenberg_eigvals
+
+        A, prec = self.A[l], self.blocks[l]
+        k = min(self.smoother.eig_iters, A.sub.space.parent.nfree)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        i = torch.from_numpy(A.sub.free_global.astype(np.float64) + 1.0).to(dev)
+        v0 = torch.sin(1.0 + 0.7 * i) + 0.3 * torch.cos(2.3 * i)
+        v0 /= A.halo.dots([(v0, v0)])[0] ** 0.5
+        V = [v0]
+        H = np.zeros((k + 1, k))
+        z = torch.empty_like(v0)
+        for j in range(k):
+            prec.ldiv(z, V[j])
+            w = torch.empty_like(v0)
+            A.mul(w, z)
+            for _ in range(2):
+                h = A.halo.dots([(V[i], w) for i in range(j + 1)])
+                for i in range(j + 1):
+                    w.add_(V[i], alpha=-h[i])
+                    H[i, j] += h[i]
+            H[j + 1, j] = A.halo.dots([(w, w)])[0] ** 0.5
+            if H[j + 1, j] == 0:
+                break
+            V.append(w / H[j + 1, j])
+        jj = k
+        for i in range(1, k):
+            if abs(H[i, i - 1]) <= 1e-8 * max(1.0, np.max(np.abs(H[:i, :i]))):
+                jj = i
+                break
+        ev = hessenberg_eigvals(np.asfortranarray(H[:jj, :jj])).real
+        return float(ev.min()), float(ev.max())
+
+    def _smooth(self, l: int, x, rhs, zero_guess: bool, want_residual: bool):
+        """``smooth!`` (``src/smoothers.jl:116-146``) on level ``l``."""
+        A, prec, c = self.A[l], self.blocks[l], self.smoother
+        b = c.inflate * self.bounds[l][1]
+        a = b / c.range
+        th, de = (b + a) / 2, (b - a) / 2
+        sg = th / de
+        tmp = torch.empty_like(rhs)
+        if zero_guess:
+            x = torch.zeros_like(rhs)
+            r = rhs.clone()
+        else:
+            A.mul(tmp, x)
+            r = rhs - tmp
+        z = torch.empty_like(rhs)
+        prec.ldiv(z, r)
+        rho = 1 / sg
+        d = z / th
+        for it in range(1, c.degree + 1):
+            x.add_(d)
+            if it == c.degree and not want_residual:
+                break
+            A.mul(tmp, d)
+            r.sub_(tmp)
+            if it == c.degree:
+                break
+            prec.ldiv(z, r)
+            rn = 1 / (2 * sg - rho)
+            d.mul_(rn * rho).add_(z, alpha=2 * rn / de)
+            rho = rn
+        return x, (r if want_residual else None)
+
+    def _coarse(self, b):
+        """``coarse_iters`` block-Jacobi CG steps from zero; α and β are 0 where their denominator is
+        not positive."""
+        A, prec = self.A[-1], self.blocks[-1]
+        x = torch.zeros_like(b)
+        r = b.clone()
+        z = torch.empty_like(b)
+        prec.ldiv(z, r)
+        p = z.clone()
+        q = torch.empty_like(b)
+        rz = A.halo.dots([(r, z)])[0]
+        for it in range(self.coarse_iters):
+            A.mul(q, p)
+            pq = A.halo.dots([(p, q)])[0]
+            a = rz / pq if pq > 0 else 0.0
+            x.add_(p, alpha=a)
+            r.add_(q, alpha=-a)
+            if it + 1 == self.coarse_iters:
+                break
+            prec.ldiv(z, r)
+            zr = A.halo.dots([(z, r)])[0]
+            beta = zr / rz if rz > 0 else 0.0
+            rz = zr
+            p.mul_(beta).add_(z)
+        return x
+
+    def _vcycle(self, b, l: int):
+        if l == len(self.A) - 1:
+            return self._coarse(b)
+        P, coarse = self.P[l], self.A[l + 1]
+        x, r = self._smooth(l, None, b, zero_guess=True, want_residual=True)
+        bc = torch.zeros(coarse.sub.nfree, dtype=b.dtype, device=b.device)
+        P.restrict(bc, r)
+        coarse.halo.sum_(bc)
+        xc = self._vcycle(bc, l + 1)
+        t = torch.empty_like(b)
+        P.prolongate(t, xc)
+        x.add_(t)
+        x, _ = self._smooth(l, x, b, zero_guess=False, want_residual=False)
+        return x
+
+    def ldiv(self, y, r):
+        """``ldiv!(y, PMultigridState, r)``: one V-cycle; NaN when the update failed
+        (``src/pmultigrid.jl:331-335``)."""
+        if not self.ok:
+            y.fill_(float("nan"))
+            return y
+        y.copy_(self._vcycle(r, 0))
+        return y

@@ -197,6 +197,11 @@ int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, int degree,
 int hfk_transfer_create(hfk_transfer** out, hfk_problem* fine, hfk_problem* coarse, const double* E,
                         const double* Einj);
 int hfk_transfer_destroy(hfk_transfer* t);
+/* Replace the multiplicity of every fine free dof (the number of cells containing it, `cells_of`,
+ * src/transfers.jl:27, :124-127) that the restriction divides by. A subdomain of a partitioned mesh
+ * passes the counts over the whole mesh, so that its partial restrictions sum to the global one; each
+ * count must be at least the number of this level's cells that contain the dof. */
+int hfk_transfer_set_multiplicity(hfk_transfer* t, const int32_t* mult);
 /* prolongate!(yf, P, xc) (src/transfers.jl:238-245) */
 int hfk_prolongate(hfk_transfer* t, const double* xc, double* yf);
 /* restrict!(yc, P, yf) (src/transfers.jl:252-259) */

@@ -415,3 +415,62 @@ def test_gpu_owner_assembly_rows_equal_global():
     perm = sp.csr_matrix((np.ones(space.nfree), (order, np.arange(space.nfree))), shape=(space.nfree, space.nfree))
     D = perm @ sp.vstack(blocks).tocsr() - J
     assert abs(D).max() <= 1e-12 * abs(J).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("orders,n", [((2, 1), (3, 3, 6)), ((4, 2, 1), (2, 2, 4))])
+def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n):
+    """The partitioned V-cycle (Chebyshev–block-Jacobi levels, block-Jacobi CG coarse steps) equals the
+    oracle's single-domain V-cycle with the same coarse CG, and preconditions a CG solve to the direct
+    solution."""
+    import torch
+
+    import oracle as O
+    from hfk import forms
+    from hfk.distributed import DistributedJacobian, DistributedPMultigrid, Subdomain, cg, slab_partition
+    from hfk.fespace import CartesianMesh, Quadrature, VectorLagrangeSpace
+    from hfk.operator import KernelOperator, MatrixFreeJacobian
+    from hfk.solvers import Chebyshev
+
+    m = CartesianMesh(n)
+    g = lambda X: np.stack([0.01 * X[:, 0], -0.02 * X[:, 1] * X[:, 2], 0.005 + 0 * X[:, 0]], axis=1)
+    Vs = [VectorLagrangeSpace(m, o, "boundary", g=g if l == 0 else None) for l, o in enumerate(orders)]
+    deg = 2 * orders[0]
+    body = (0.3, -0.2, 0.5)
+    res_f, jac_f = forms.svk_residual(2.0, 1.0, deg, body), forms.svk_jacobian(2.0, 1.0, deg)
+    from conftest import svk_state
+
+    x = svk_state(Vs[0], amp=1e-3, disp=0.0)
+    d = Vs[0].dirichlet_values
+    iters = 8
+    ref = O.OraclePMG(Vs, Quadrature.gauss(deg), O.LAW_SVK, (2.0, 1.0) + body, degree=2, coarse="cg",
+                      coarse_iters=iters)
+    ref.update(x, d)
+    r = np.random.default_rng(2).standard_normal(Vs[0].nfree)
+    yref = ref.ldiv(r)
+    xd = spla.spsolve(ref.levels[0].jacobian(x, d).tocsc(), r)  # any order (the engine assembles Q1/Q2)
+    _, it_ref, conv_ref, _ = O.pcg(ref.levels[0].mf_apply, r, ref.ldiv, rtol=1e-9, maxiter=200)
+    assert conv_ref
+    cr = slab_partition(m, 2)
+
+    def rank_fn(rank, comm):
+        sub = Subdomain(Vs[0], cr, rank)
+        lop = KernelOperator(res_f, jac_f, sub.space, jacobian="matrixfree")
+        A = DistributedJacobian(sub, comm, mf=MatrixFreeJacobian(lop))
+        A.prepare(torch.from_numpy(sub.restrict(x)).cuda(), d)
+        mg = DistributedPMultigrid(A, Vs[1:], cr, Chebyshev(degree=2), coarse_iters=iters).update()
+        rl = torch.from_numpy(sub.restrict(r)).cuda()
+        y = torch.zeros_like(rl)
+        mg.ldiv(y, rl)
+        xs, it, conv, _ = cg(A, rl, mg.ldiv, rtol=1e-9, maxiter=200)
+        torch.cuda.synchronize()
+        return sub.free_global, mg.ok, mg.bounds[0], y.cpu().numpy(), xs.cpu().numpy(), it, conv
+
+    out = _run_threads(2, rank_fn)
+    lmax_ref = ref.smoothers[0].lmax
+    for fg, ok, (lo, hi), y, xs, it, conv in out:
+        assert ok
+        assert abs(hi - lmax_ref) <= 1e-9 * lmax_ref
+        assert np.linalg.norm(y - yref[fg]) <= 1e-9 * np.linalg.norm(yref[fg])
+        assert conv and abs(it - it_ref) <= 2
+        assert np.linalg.norm(xs - xd[fg]) <= 1e-6 * np.linalg.norm(xd[fg])
