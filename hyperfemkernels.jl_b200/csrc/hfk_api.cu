@@ -1906,7 +1906,9 @@ void pmg_collect_cycle_time(hfk_pmg* m) {
 void pmg_cycle_on_buffers(hfk_pmg* m) {
   hfk_problem* p0 = m->lv[0];
   cudaStream_t s = p0->stream;
-  if (!m->graph_exec && m->cycles_since_update >= 1) {
+  // the legacy default stream cannot be captured (a caller that launches its own work there, such
+  // as a partitioned solve ordering the engine with torch, gets the cycle uncaptured)
+  if (!m->graph_exec && m->cycles_since_update >= 1 && s != cudaStreamLegacy) {
     // every buffer exists (the first cycle after the update ran uncaptured): capture the cycle
     HFK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {

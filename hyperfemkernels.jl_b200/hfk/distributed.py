@@ -108,6 +108,14 @@ class Subdomain:
         if (owner == world).any():
             raise ValueError("HyperFEMKernels: a free dof is touched by no cell")
         self.owner_of = owner
+        # Dirichlet dofs: the same rule (lowest rank whose cells reference them), for gathers
+        downer = np.full(space.ndir, world, dtype=np.int32)
+        for s in range(world):
+            g = ids[:, cell_rank == s]
+            t = np.zeros(space.ndir, dtype=bool)
+            t[-g[g < 0].astype(np.int64) - 1] = True
+            downer[t & (downer == world)] = s
+        self.dir_owned = downer == rank
         if ghost:
             mine = owner == rank
             sel = ids > 0
@@ -455,21 +463,27 @@ class DistributedPMultigrid:
     level's halo sum. The smoothers are the reference's Chebyshev–block-Jacobi (``src/smoothers.jl:
     42-146``) over the halo-summed products and summed nodal blocks, with the Arnoldi estimate's inner
     products all-reduced and its start vector evaluated at the global dof numbers (the estimate of the
-    single-domain problem). The coarsest level runs ``coarse_iters`` block-Jacobi CG steps (a variable
-    preconditioner: use the flexible ``cg``).
+    single-domain problem). The coarsest level is solved directly (``coarse="cholesky"``: every rank
+    holds the whole coarse level, assembled and factorised by the engine, and gathers the coarse
+    right-hand side from the owners with one all-reduce) or by ``coarse_iters`` distributed
+    block-Jacobi CG steps (``"cg"``: a variable preconditioner, use the flexible ``cg``).
 
     ``A`` is the finest level's ``DistributedJacobian``; ``spaces`` the global trial spaces of the
     coarser levels, finest first excluded.
     """
 
-    def __init__(self, A: DistributedJacobian, spaces, cell_rank, smoother=None, coarse_iters: int = 20):
+    def __init__(self, A: DistributedJacobian, spaces, cell_rank, smoother=None, coarse: str = "cholesky",
+                 coarse_iters: int = 20):
         from .operator import KernelOperator, MatrixFreeJacobian
         from .solvers import Chebyshev, Prolongation
 
         if A.mf is None:
             raise ValueError("HyperFEMKernels: the p-multigrid needs the engine's MatrixFreeJacobian")
+        if coarse not in ("cholesky", "cg"):
+            raise ValueError("HyperFEMKernels: coarse must be 'cholesky' or 'cg'")
         if coarse_iters < 1:
             raise ValueError("HyperFEMKernels: coarse_iters must be ≥ 1")
+        self.coarse = coarse
         self.smoother = smoother if smoother is not None else Chebyshev()
         if self.smoother.eig_inner != "euclidean":
             raise ValueError("HyperFEMKernels: the partitioned p-multigrid runs the Euclidean Arnoldi estimate")
@@ -482,15 +496,27 @@ class DistributedPMultigrid:
             self.A.append(DistributedJacobian(sub, A.comm, mf=MatrixFreeJacobian(lop)))
         self.P = []
         for l in range(len(self.A) - 1):
-            fine, coarse = self.A[l], self.A[l + 1]
-            t = Prolongation(coarse.mf.op.problem, fine.mf.op.problem)
-            glob = fine.sub.space.parent
-            m = np.ascontiguousarray(_global_multiplicity(glob)[fine.sub.free_global])
+            lf, lc = self.A[l], self.A[l + 1]
+            t = Prolongation(lc.mf.op.problem, lf.mf.op.problem)
+            glob = lf.sub.space.parent
+            m = np.ascontiguousarray(_global_multiplicity(glob)[lf.sub.free_global])
             call("hfk_transfer_set_multiplicity", t.h, ptr(m, np.int32))
             self.P.append(t)
         self.blocks = [DistributedBlockJacobi(a) for a in self.A]
         self.bounds = [None] * (len(self.A) - 1)
         self.ok = False
+        self._gmf = self._slot = None
+        if coarse == "cholesky":
+            # the whole coarse level on every rank: assembled and factorised by the engine's
+            # LaggedAssembled slot (rebuilt at every update, as the reference's LU)
+            gop = KernelOperator(op.res, op.jac, spaces[-1], jacobian="matrixfree")
+            self._gmf = MatrixFreeJacobian(gop)
+            if torch.cuda.is_available():
+                s = torch.cuda.current_stream().cuda_stream
+                gop.problem.set_stream(s if s else _CUDA_STREAM_LEGACY)
+            c = self.A[-1].sub
+            self._own_loc = np.nonzero(c.owned)[0]
+            self._own_glob = c.owned_global()
 
     @property
     def levels(self) -> int:
@@ -511,8 +537,24 @@ class DistributedPMultigrid:
             c.prepare(xc, dc)
             x, d = xc, dc
         ok = True
-        for b in self.blocks:
+        blocks = self.blocks if self.coarse == "cg" else self.blocks[:-1]
+        for b in blocks:
             ok &= b.update().ok
+        if self.coarse == "cholesky":
+            from .solvers import LaggedAssembled, SlotState
+
+            c = self.A[-1]
+            xg = self._gather(x)
+            dg = d * torch.as_tensor(c.sub.dir_owned, device=d.device).to(d.dtype)
+            c.comm.allreduce_(dg, "sum")
+            self._gmf.prepare(xg, dg)
+            if self._slot is None:
+                self._slot = SlotState(LaggedAssembled(every=1), self._gmf)
+            else:
+                self._slot.update(self._gmf)
+            flag = torch.tensor([1.0 if self._slot.ok else 0.0], dtype=torch.float64)
+            c.comm.allreduce_(flag, "min")
+            ok &= bool(flag.item() > 0)
         for l in range(len(self.A) - 1):
             lo, hi = self._eig_bounds(l)
             self.bounds[l] = (lo, hi)
@@ -587,9 +629,29 @@ class DistributedPMultigrid:
             rho = rn
         return x, (r if want_residual else None)
 
+    def _gather(self, v):
+        """The whole coarse-level vector on every rank from the owners' entries (one all-reduce)."""
+        c = self.A[-1]
+        key = str(v.device)
+        if getattr(self, "_gidx", (None,))[0] != key:
+            self._gidx = (key, torch.as_tensor(self._own_loc, device=v.device),
+                          torch.as_tensor(self._own_glob, device=v.device),
+                          torch.as_tensor(c.sub.free_global, device=v.device))
+        _, loc, glob, _ = self._gidx
+        g = torch.zeros(c.sub.space.parent.nfree, dtype=v.dtype, device=v.device)
+        g.index_copy_(0, glob, v.index_select(0, loc))
+        c.comm.allreduce_(g, "sum")
+        return g
+
     def _coarse(self, b):
-        """``coarse_iters`` block-Jacobi CG steps from zero; α and β are 0 where their denominator is
-        not positive."""
+        """The coarse solve: the replicated Cholesky on the gathered right-hand side, or
+        ``coarse_iters`` block-Jacobi CG steps from zero (α and β 0 where their denominator is not
+        positive)."""
+        if self.coarse == "cholesky":
+            bg = self._gather(b)
+            yg = torch.zeros_like(bg)
+            self._slot.ldiv(yg, bg)
+            return yg.index_select(0, self._gidx[3])
         A, prec = self.A[-1], self.blocks[-1]
         x = torch.zeros_like(b)
         r = b.clone()

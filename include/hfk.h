@@ -71,7 +71,9 @@ int hfk_problem_destroy(hfk_problem* p);
 /* Cheap update(op, res, jac) of the same structure: new law parameters, tables/pattern/colours kept
  * (src/assembly.jl:693-744). */
 int hfk_problem_set_params(hfk_problem* p, const double* params, int nparams);
-/* Launch on `stream` (a cudaStream_t) from now on; NULL restores the handle's own stream. */
+/* Launch on `stream` (a cudaStream_t) from now on; NULL restores the handle's own stream. On
+ * cudaStreamLegacy (the legacy default stream, which cannot be captured) a p-multigrid or slot over
+ * this problem runs its cycle uncaptured. */
 int hfk_problem_set_stream(hfk_problem* p, void* stream);
 int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolors, int64_t* nnz);
 /* Scatter of the sum-factorised kernels (residual, products): colour by colour with plain

@@ -418,11 +418,12 @@ def test_gpu_owner_assembly_rows_equal_global():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("coarse", ["cholesky", "cg"])
 @pytest.mark.parametrize("orders,n", [((2, 1), (3, 3, 6)), ((4, 2, 1), (2, 2, 4))])
-def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n):
-    """The partitioned V-cycle (Chebyshev–block-Jacobi levels, block-Jacobi CG coarse steps) equals the
-    oracle's single-domain V-cycle with the same coarse CG, and preconditions a CG solve to the direct
-    solution."""
+def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n, coarse):
+    """The partitioned V-cycle (Chebyshev–block-Jacobi levels; the replicated direct coarse solve or
+    block-Jacobi CG coarse steps) equals the oracle's single-domain V-cycle with the same coarse solve,
+    and preconditions a CG solve to the direct solution."""
     import torch
 
     import oracle as O
@@ -443,8 +444,8 @@ def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n):
     x = svk_state(Vs[0], amp=1e-3, disp=0.0)
     d = Vs[0].dirichlet_values
     iters = 8
-    ref = O.OraclePMG(Vs, Quadrature.gauss(deg), O.LAW_SVK, (2.0, 1.0) + body, degree=2, coarse="cg",
-                      coarse_iters=iters)
+    ref = O.OraclePMG(Vs, Quadrature.gauss(deg), O.LAW_SVK, (2.0, 1.0) + body, degree=2,
+                      coarse="direct" if coarse == "cholesky" else "cg", coarse_iters=iters)
     ref.update(x, d)
     r = np.random.default_rng(2).standard_normal(Vs[0].nfree)
     yref = ref.ldiv(r)
@@ -458,7 +459,7 @@ def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n):
         lop = KernelOperator(res_f, jac_f, sub.space, jacobian="matrixfree")
         A = DistributedJacobian(sub, comm, mf=MatrixFreeJacobian(lop))
         A.prepare(torch.from_numpy(sub.restrict(x)).cuda(), d)
-        mg = DistributedPMultigrid(A, Vs[1:], cr, Chebyshev(degree=2), coarse_iters=iters).update()
+        mg = DistributedPMultigrid(A, Vs[1:], cr, Chebyshev(degree=2), coarse=coarse, coarse_iters=iters).update()
         rl = torch.from_numpy(sub.restrict(r)).cuda()
         y = torch.zeros_like(rl)
         mg.ldiv(y, rl)
