@@ -698,3 +698,67 @@ class DistributedPMultigrid:
             return y
         y.copy_(self._vcycle(r, 0))
         return y
+
+
+def newton_solve(A: DistributedJacobian, prec, g_full, loads, x0=None, *, rtol: float = 1e-8, atol: float = 0.0,
+                 maxiter: int = 500, rtol_newton: float = 1e-8, atol_newton: float = 1e-12, max_newton: int = 20,
+                 lift=None):
+    """The load-stepped Newton loop of ``hfk.newton.newton_solve`` (HyperFEMKernels
+    ``test/solvers/test_pmultigrid.jl:86-115``) over a partitioned problem.
+
+    ``A`` is the finest level's ``DistributedJacobian`` (its ``KernelOperator`` computes the local
+    residuals), ``prec`` a ``DistributedPMultigrid`` over ``A`` (or None). Per Newton iteration: the
+    local residual completed by the halo sum, its norm all-reduced, ``prepare`` at the state, the
+    preconditioner's update, then the flexible ``cg`` to ``atol + rtol ||b||``. ``g_full`` (global
+    Dirichlet values at load factor 1), ``x0`` and ``lift`` are global vectors; the result is the
+    rank's local part of the solution and the ``NewtonStats`` (the same on every rank).
+    """
+    import time
+
+    from .newton import NewtonStats
+
+    sub = A.sub
+    op = A.mf.op
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x = torch.zeros(sub.nfree, dtype=torch.float64, device=dev) if x0 is None else \
+        torch.from_numpy(sub.restrict(np.asarray(x0, dtype=np.float64))).to(dev)
+    b = torch.zeros(sub.nfree, dtype=torch.float64, device=dev)
+    lift_l = None if lift is None else torch.from_numpy(sub.restrict(np.asarray(lift, dtype=np.float64))).to(dev)
+    g_full = np.ascontiguousarray(g_full, dtype=np.float64)
+    st = NewtonStats()
+    prev = 0.0
+    t0 = time.perf_counter()
+    for lam in loads:
+        dv = torch.from_numpy(lam * g_full).to(dev)
+        if lift_l is not None:
+            x.add_(lift_l, alpha=lam - prev)
+        prev = lam
+        st.load_steps += 1
+        r0 = None
+        for _ in range(max_newton):
+            op.residual(b, x, dv)
+            A.halo.sum_(b)
+            rn = A.halo.dots([(b, b)])[0] ** 0.5
+            st.residual_norms.append(rn)
+            if r0 is None:
+                r0 = rn
+            if rn <= max(rtol_newton * r0, atol_newton):
+                break
+            A.prepare(x, dv)
+            if prec is not None:
+                prec.update()
+            dx, its, conv, _ = cg(A, -b, prec.ldiv if prec is not None else None, rtol=rtol, atol=atol,
+                                  maxiter=maxiter)
+            st.krylov_iters.append(its)
+            if not conv:
+                st.converged = False
+                break
+            x.add_(dx)
+            st.newton_iters += 1
+        else:
+            st.converged = False
+        if not st.converged:
+            break
+    torch.cuda.synchronize()
+    st.seconds = time.perf_counter() - t0
+    return x, st

@@ -475,3 +475,44 @@ def test_gpu_two_subdomains_pmultigrid_matches_oracle(orders, n, coarse):
         assert np.linalg.norm(y - yref[fg]) <= 1e-9 * np.linalg.norm(yref[fg])
         assert conv and abs(it - it_ref) <= 2
         assert np.linalg.norm(xs - xd[fg]) <= 1e-6 * np.linalg.norm(xd[fg])
+
+
+@pytest.mark.gpu
+def test_gpu_two_subdomains_newton_matches_single_domain():
+    """The load-stepped Newton over two subdomains (partitioned p-multigrid under the flexible CG)
+    follows the single-domain engine's Newton: the same Newton iterations, the same solution."""
+    import torch
+
+    from hfk import forms
+    from hfk import solvers as S
+    from hfk.distributed import DistributedJacobian, DistributedPMultigrid, Subdomain, newton_solve, slab_partition
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.newton import newton_solve as newton_single
+    from hfk.operator import KernelOperator, MatrixFreeJacobian
+
+    m = CartesianMesh((3, 3, 6))
+    gfun = [lambda X: 0 * X, lambda X: np.tile([0.1, 0.0, 0.0], (len(X), 1))]
+    Vs = [VectorLagrangeSpace(m, o, ("x0", "x1"), g=gfun if o == 2 else None) for o in (2, 1)]
+    g_full = Vs[0].dirichlet_values.copy()
+    res_f, jac_f = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
+    loads = [0.5, 1.0]
+    op = KernelOperator(res_f, jac_f, Vs[0], jacobian="matrixfree")
+    ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-10, preconditioner=S.PMultigrid(Vs, S.Chebyshev(degree=3)))
+    x1, st1 = newton_single(op, ls, g_full, loads, rtol_newton=1e-10)
+    x1 = x1.cpu().numpy()
+    Vs[0].dirichlet_values = g_full.copy()
+    cr = slab_partition(m, 2)
+
+    def rank_fn(rank, comm):
+        sub = Subdomain(Vs[0], cr, rank)
+        lop = KernelOperator(res_f, jac_f, sub.space, jacobian="matrixfree")
+        A = DistributedJacobian(sub, comm, mf=MatrixFreeJacobian(lop))
+        A.prepare(torch.zeros(sub.nfree, dtype=torch.float64, device="cuda"), g_full)
+        mg = DistributedPMultigrid(A, Vs[1:], cr, S.Chebyshev(degree=3))
+        x, st = newton_solve(A, mg, g_full, loads, rtol=1e-10, rtol_newton=1e-10)
+        return sub.free_global, x.cpu().numpy(), st
+
+    out = _run_threads(2, rank_fn)
+    for fg, x, st in out:
+        assert st.converged and st.newton_iters == st1.newton_iters
+        assert np.linalg.norm(x - x1[fg]) <= 1e-8 * np.linalg.norm(x1[fg])
