@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--launch", default="auto", choices=["auto", "line2", "line4", "point"],
                     help="launch shape of the J*v (auto: the autotuner's; a fixed one for profiling, where the "
                          "profiler's overhead would skew the autotuner's timings)")
+    ap.add_argument("--assembly", action="store_true",
+                    help="only the Q2 SVK 20x10x10 residual + CSC Jacobian (the CPU-runnable configuration)")
     ap.add_argument("--vcycle", type=int, default=0, metavar="K",
                     help="only K V-cycles of the Q4 16^3 p-multigrid 4 -> 2 -> 1 (the Newton case's preconditioner)")
     return ap.parse_args()
@@ -377,7 +379,8 @@ def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
 
 
 def oseen_main(args):
-    """The Oseen assembly alone (``--oseen N``), one JSON line: the case for profiling its kernel."""
+    """The Oseen assembly alone (``--oseen N``), or the Q2 SVK 20x10x10 CSC assembly alone
+    (``--assembly``), one JSON line: the cases for profiling their kernels."""
     import torch
 
     stream = torch.cuda.current_stream()
@@ -394,7 +397,10 @@ def oseen_main(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    out = oseen_case(torch, torch.device("cuda"), stream, timed, n=args.oseen, cpu_n=min(args.oseen, 8))
+    if args.assembly:
+        out = assembly_case(torch, torch.device("cuda"), stream, timed)
+    else:
+        out = oseen_case(torch, torch.device("cuda"), stream, timed, n=args.oseen, cpu_n=min(args.oseen, 8))
     print(json.dumps(out))
 
 
@@ -465,6 +471,12 @@ def assembly_case(torch, dev, stream, timed):
 
     ms_j = timed(jac, 10, 3) / 10
     ms_r = timed(res, 10, 3) / 10
+    # the bit-reproducible colour-by-colour scatter (HFK_SCATTER_COLOURED) for comparison
+    op.problem.set_scatter("coloured")
+    ms_jc = timed(jac, 10, 3) / 10
+    nz_c = nz.clone()
+    op.problem.set_scatter("auto")
+    jac()
     # the same assembly by the CPU restatement of the reference algorithm (matrix-product element
     # Jacobian with point blocks of 12, colour loop, OpenMP on all host cores), best of 5
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -487,7 +499,9 @@ def assembly_case(torch, dev, stream, timed):
     got = nz.cpu().numpy()
     err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     cpu_j, cpu_r = 1e3 * min(tj), 1e3 * min(tr)
+    err_c = float(np.linalg.norm(nz_c.cpu().numpy() - ref) / np.linalg.norm(ref))
     return {"assembly_q2_20x10x10": {"free_dofs": V.nfree, "nnz": int(nnz), "jacobian_ms": ms_j, "residual_ms": ms_r,
+                                     "jacobian_coloured_ms": ms_jc, "rel_err_coloured_vs_cpu": err_c,
                                      "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
                                      "jacobian_qps": 27 * V.mesh.ncells / (ms_j * 1e-3),
                                      "cpu_jacobian_ms": cpu_j, "cpu_residual_ms": cpu_r,
@@ -795,7 +809,7 @@ if __name__ == "__main__":
         reference(a)
     elif a.batch:
         batch_main(a)
-    elif a.oseen:
+    elif a.oseen or a.assembly:
         oseen_main(a)
     elif a.vcycle:
         vcycle_main(a)

@@ -1277,27 +1277,37 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   HFK_REQUIRE(p->nn == 27 || p->nn <= 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
   const size_t smem = asm_smem_bytes(p->nn, p->np, g);
   HFK_REQUIRE(smem <= 227 * 1024, HFK_ERR_UNSUPPORTED, "too many quadrature points for the assembly kernel");
+  HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
+  if (g) {
+    static size_t attr = 0;
+    if (smem > attr) {
+      HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_g<27>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = smem;
+    }
+  } else {
+    static size_t attr = 0;
+    if (smem > attr) {
+      HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_direct<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = smem;
+    }
+  }
+  auto launch = [&](const int32_t* cells, int n) {
+    CellData cd = cell_data(p, cells, n);
+    if (g) jacobian_kernel_g<27><<<n, 256, smem, p->stream>>>(cd, io);
+    else jacobian_kernel_direct<8><<<n, 256, smem, p->stream>>>(cd, io);
+    check_launch(p);
+  };
+  // the atomic scatter (the default) assembles every cell in one launch: CTAs of neighbouring cells
+  // may then add to the same nonzero, in an order that can change the last bit from run to run; by
+  // colour (HFK_SCATTER_COLOURED) the adds of one nonzero come one launch after another, in colour
+  // order, and the result is reproducible bit for bit
+  if (use_atomic_scatter(p)) {
+    if (p->ncells) launch(nullptr, p->ncells);
+    return;
+  }
   for (int c = 0; c < p->ncolors; ++c) {
     const int n = p->color_start[c + 1] - p->color_start[c];
-    if (!n) continue;
-    CellData cd = cell_data(p, p->cells_by_color.p + p->color_start[c], n);
-    if (g) {
-      static size_t attr = 0;
-      if (smem > attr) {
-        HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_g<27>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
-      }
-      jacobian_kernel_g<27><<<n, 256, smem, p->stream>>>(cd, io);
-    } else {
-      static size_t attr = 0;
-      if (smem > attr) {
-        HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_direct<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
-      }
-      HFK_REQUIRE(p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
-      jacobian_kernel_direct<8><<<n, 256, smem, p->stream>>>(cd, io);
-    }
-    check_launch(p);
+    if (n) launch(p->cells_by_color.p + p->color_start[c], n);
   }
 }
 

@@ -1,14 +1,13 @@
-// Fused element Jacobian + colour-by-colour scatter into the CSC nonzeros.
+// Fused element Jacobian + scatter into the CSC nonzeros.
 //
-// One CTA per cell of a colour. Per point the tangent is pulled back to the reference gradients
-// once, Dh_q[(c,K),(k,K')] = dV sum_{J,L} iJt[J,K] T[(c,J),(k,L)] iJt[L,K'], so the element matrix
+// One CTA per cell (all cells in one launch, or the cells of one colour per launch). Per point the
+// tangent is pulled back to the reference gradients once, Dh_q[(c,K),(k,K')] = dV sum_{J,L} iJt[J,K] T[(c,J),(k,L)] iJt[L,K'], so the element matrix
 //   K[(n,c),(m,k)] = sum_q sum_{K,K'} dN^[n,K,q] Dh_q[(c,K),(k,K')] dN^[m,K',q]
 // only reads the reference tables (shared by all cells). For 27-node cells it is formed as the
 // reference forms it (element_jacobian_mm!, src/assembly.jl:1316-1342): per test component c,
 // G_c[(q,K),(m,k)] = sum_K' Dh[(c,K),(k,K')] dN^[m,K',q], then K_c = A^T G_c with A = dN^ as an
 // (np*3) x nn matrix, register-tiled. The entries are added at their precomputed positions
-// (scatter_jacobian!, src/assembly.jl:1402-1408): cells of one colour share no free test dof, so
-// no two CTAs of a launch write the same nonzero.
+// (scatter_jacobian!, src/assembly.jl:1402-1408) by reductions.
 #pragma once
 #include "hfk_internal.h"
 #include "pointwise.cuh"
@@ -84,9 +83,14 @@ __device__ void asm_point_phase(const CellData& cd, const AsmIO& io, int cell, c
   __syncthreads();
 }
 
-__device__ __forceinline__ void scatter_entry(const AsmIO& io, const int32_t* pos_cell, int ndl, int ii, int jj, double v) {
-  const int32_t p = pos_cell[ii + ndl * jj];
-  if (p > 0) io.nzval[p - 1] += v;
+// One element-matrix entry added at its precomputed position (scatter_jacobian!,
+// src/assembly.jl:1402-1408). The add is a reduction whose result is not read: the thread does not
+// wait for the nonzero to arrive from memory, as a load-add-store would. Launched colour by colour,
+// no two adds of a launch meet the same nonzero (cells of one colour share no free test dof, the
+// entries of one cell have distinct positions), so the colours add in a fixed order and the sums
+// are deterministic; launched over all cells at once, neighbouring cells' adds meet in L2.
+__device__ __forceinline__ void scatter_add(double* nzval, int32_t p, double v) {
+  if (p > 0) atomicAdd(nzval + (p - 1), v);
 }
 
 // 27-node cells (Q2): G_c in shared memory, 3x3 register tiles of K_c
@@ -128,6 +132,11 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
     constexpr int TN = NN / 3, TM = NDL / 3;
     for (int tile = threadIdx.x; tile < TN * TM; tile += blockDim.x) {
       const int n0 = (tile % TN) * 3, mk0 = (tile / TN) * 3;
+      int32_t pp[3][3];  // positions loaded first: their latency overlaps the products
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) pp[i][j] = __ldg(pos + (c * NN + n0 + i) + NDL * (mk0 + j));
       double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
       for (int r = 0; r < R; ++r) {
         const double a0 = A[n0 + NN * r], a1 = A[n0 + 1 + NN * r], a2 = A[n0 + 2 + NN * r];
@@ -136,8 +145,10 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
         acc[1][0] += a1 * g0; acc[1][1] += a1 * g1; acc[1][2] += a1 * g2;
         acc[2][0] += a2 * g0; acc[2][1] += a2 * g1; acc[2][2] += a2 * g2;
       }
+#pragma unroll
       for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) scatter_entry(io, pos, NDL, c * NN + n0 + i, mk0 + j, acc[i][j]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) scatter_add(io.nzval, pp[i][j], acc[i][j]);
     }
     __syncthreads();
   }
@@ -170,6 +181,7 @@ __global__ void __launch_bounds__(256) jacobian_kernel_direct(CellData cd, AsmIO
   for (int e = threadIdx.x; e < NDL * NDL; e += blockDim.x) {
     const int ii = e % NDL, jj = e / NDL;
     const int c = ii / NN, n = ii % NN, k = jj / NN, m = jj % NN;
+    const int32_t pe = __ldg(pos + ii + NDL * jj);  // loaded first: its latency overlaps the sum
     double acc = 0;
     for (int q = 0; q < np; ++q) {
       const double* D = Dh + q * 81;
@@ -183,7 +195,7 @@ __global__ void __launch_bounds__(256) jacobian_kernel_direct(CellData cd, AsmIO
         acc += an[K] * (Dk[0] * am[0] + Dk[9] * am[1] + Dk[18] * am[2]);
       }
     }
-    scatter_entry(io, pos, NDL, ii, jj, acc);
+    scatter_add(io.nzval, pe, acc);
   }
 }
 

@@ -82,9 +82,9 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
  * between runs). AUTO (default) is autotuned per kernel mode and precision on the first call (the
  * atomic or the colour-by-colour scatter, 2 or 4 warps per CTA, timed with CUDA events; on B200
  * the atomic scatter usually wins: one launch, no read of the output before the write); COLOURED
- * gives bit-reproducible results. The nodal blocks, and the restriction of a transfer whose fine
- * level is this problem, scatter atomically unless COLOURED is set; the assembled Jacobian always
- * scatters by colour. */
+ * gives bit-reproducible results. The nodal blocks, the assembled Jacobian (one launch over all
+ * cells) and the restriction of a transfer whose fine level is this problem scatter atomically
+ * unless COLOURED is set. */
 #define HFK_SCATTER_AUTO 0
 #define HFK_SCATTER_COLOURED 1
 #define HFK_SCATTER_ATOMIC 2
