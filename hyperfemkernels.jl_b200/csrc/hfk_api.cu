@@ -1272,17 +1272,21 @@ void pattern_build_dev(hfk_problem* p) {
 void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* nzval) {
   pattern_build_dev(p);
   HFK_CUDA(cudaMemsetAsync(nzval, 0, p->nnz * sizeof(double), p->stream));
-  AsmIO io{u, dvals, p->dNt.p, p->nzpos.p, nzval, p->np};
   const bool g = p->nn == 27;
   HFK_REQUIRE(p->nn == 27 || p->nn <= 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
-  const size_t smem = asm_smem_bytes(p->nn, p->np, g);
+  // 27-node cells: G_c padded (conflict-free, select-free tensor-core fragments) when it fits
+  const bool padded = g && asm_smem_bytes(p->nn, p->np, true, ASM_LDG_PADDED) <= 227 * 1024;
+  const int ldg = g ? (padded ? ASM_LDG_PADDED : 3 * p->nn) : 0;
+  AsmIO io{u, dvals, p->dNt.p, p->nzpos.p, nzval, p->np, ldg};
+  const size_t smem = asm_smem_bytes(p->nn, p->np, g, ldg);
   HFK_REQUIRE(smem <= 227 * 1024, HFK_ERR_UNSUPPORTED, "too many quadrature points for the assembly kernel");
   HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
   if (g) {
-    static size_t attr = 0;
-    if (smem > attr) {
-      HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_g<27>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = smem;
+    static size_t attr[2] = {0, 0};
+    if (smem > attr[padded]) {
+      HFK_CUDA(cudaFuncSetAttribute(padded ? jacobian_kernel_g<27, true> : jacobian_kernel_g<27, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr[padded] = smem;
     }
   } else {
     static size_t attr = 0;
@@ -1293,7 +1297,8 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   }
   auto launch = [&](const int32_t* cells, int n) {
     CellData cd = cell_data(p, cells, n);
-    if (g) jacobian_kernel_g<27><<<n, 256, smem, p->stream>>>(cd, io);
+    if (g && padded) jacobian_kernel_g<27, true><<<n, 256, smem, p->stream>>>(cd, io);
+    else if (g) jacobian_kernel_g<27, false><<<n, 256, smem, p->stream>>>(cd, io);
     else jacobian_kernel_direct<8><<<n, 256, smem, p->stream>>>(cd, io);
     check_launch(p);
   };

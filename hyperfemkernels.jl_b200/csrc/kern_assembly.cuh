@@ -6,8 +6,8 @@
 // only reads the reference tables (shared by all cells). For 27-node cells it is formed as the
 // reference forms it (element_jacobian_mm!, src/assembly.jl:1316-1342): per test component c,
 // G_c[(q,K),(m,k)] = sum_K' Dh[(c,K),(k,K')] dN^[m,K',q], then K_c = A^T G_c with A = dN^ as an
-// (np*3) x nn matrix, register-tiled. The entries are added at their precomputed positions
-// (scatter_jacobian!, src/assembly.jl:1402-1408) by reductions.
+// (np*3) x nn matrix, on the FP64 tensor cores (mma.sync m8n8k4). The entries are added at their
+// precomputed positions (scatter_jacobian!, src/assembly.jl:1402-1408) by reductions.
 #pragma once
 #include "hfk_internal.h"
 #include "pointwise.cuh"
@@ -21,7 +21,14 @@ struct AsmIO {
   const int32_t* nzpos;   // (ndl*ndl, ncells) 1-based
   double* nzval;
   int np;
+  int ldg;                // shared row stride of G_c[r][mk] (27-node cells, >= 3 nn)
 };
+
+// Row stride of G_c in the 27-node kernel when it fits: at least the 88 columns of the padded
+// product, with zeros past column 81, and 4 modulo 16 doubles, so that the 4 x 8 elements of a B
+// fragment (k rows apart by the stride, columns adjacent) fall on distinct 8-byte bank pairs within
+// each half-warp and two per pair over the warp: two wavefronts, the minimum for 32 doubles
+constexpr int ASM_LDG_PADDED = 100;
 
 // Phase 1 (shared by both variants): per point, physical gradient of u, geometry, pulled-back
 // tangent Dh[q][(c*3+K) + 9*(k*3+K')] in shared memory.
@@ -93,63 +100,111 @@ __device__ __forceinline__ void scatter_add(double* nzval, int32_t p, double v) 
   if (p > 0) atomicAdd(nzval + (p - 1), v);
 }
 
-// 27-node cells (Q2): G_c in shared memory, 3x3 register tiles of K_c
-template <int NN>
+// FP64 tensor-core product of an 8x4 and a 4x8 tile (mma.sync m8n8k4, PTX ISA "Matrix Fragments for
+// mma.m8n8k4 with .f64"): lane l holds a = A[l/4][l%4], b = B[l%4][l/4] and the accumulators
+// d[i] = D[l/4][2(l%4) + i].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 27-node cells (Q2): G_c in shared memory, K_c = A^T G_c on the FP64 tensor cores. Eight warps:
+// warp w takes the 8-row band w % 4 of K_c (rows n, 27 padded to 32) and every other 8-column tile
+// (columns mk, 81 padded to 88) from w / 4; the k dimension (r = 3 np) runs in steps of 4, padded
+// with zeros. A warp loads one fragment of A^T per k-step and reuses it for its five or six tiles.
+// PADDED: G_c has the row stride ASM_LDG_PADDED and zeros past its last row and column, so the B
+// fragments load without bounds selects; otherwise (large np) the stride is 81 and they select.
+template <int NN, bool PADDED>
 __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) {
   constexpr int NDL = 3 * NN;
+  constexpr int MT = (NN + 7) / 8, NT = (NDL + 7) / 8;  // 8-row bands of K_c, 8-column tiles
+  constexpr int TPW = (NT + 1) / 2;                      // column tiles per warp (two warps per band)
+  static_assert(MT == 4, "eight warps: four row bands x two column-tile sets");
   extern __shared__ __align__(16) double sm[];
-  const int np = io.np;
-  double* A = sm;                       // NN*3*np
-  double* xl = A + NN * 3 * np;         // NDL
+  const int np = io.np, ldg = io.ldg;
+  const int R = 3 * np, ksteps = (R + 3) / 4;
+  double* A = sm;                       // NN * R
+  double* xl = A + (size_t)NN * R;      // NDL
   double* Hs = xl + NDL;                // 9 np
   double* iJs = Hs + 9 * np;            // 9 np
   double* dVs = iJs + 9 * np;           // np
   double* Dh = dVs + np;                // 81 np
-  double* G = Dh + 81 * np;             // (3 np) x NDL
+  double* G = Dh + 81 * np;             // 4 ksteps x ldg
   const int li = blockIdx.x;
   if (li >= cd.ncells_list) return;
   const int cell = cd.cells ? cd.cells[li] : li;
   const int32_t* gid = cd.ids + (size_t)cell * NDL;
-  for (int i = threadIdx.x; i < NN * 3 * np; i += blockDim.x) A[i] = io.dNt[i];
+  for (int i = threadIdx.x; i < NN * R; i += blockDim.x) A[i] = io.dNt[i];
   for (int j = threadIdx.x; j < NDL; j += blockDim.x) {
     const int32_t id = gid[j];
     xl[j] = id > 0 ? io.u[id - 1] : (id < 0 ? io.dvals[-id - 1] : 0.0);
   }
+  if (PADDED) {  // the padding of G_c: columns NDL..NT*8-1 of every row, and the rows past R
+    constexpr int W = NT * 8 - NDL;
+    for (int i = threadIdx.x; i < R * W; i += blockDim.x) G[(i / W) * ldg + NDL + i % W] = 0.0;
+    for (int i = threadIdx.x; i < (4 * ksteps - R) * NT * 8; i += blockDim.x)
+      G[(R + i / (NT * 8)) * ldg + i % (NT * 8)] = 0.0;
+  }
   __syncthreads();
   asm_point_phase<NN>(cd, io, cell, A, xl, Hs, iJs, dVs, Dh);
   const int32_t* pos = io.nzpos + (size_t)NDL * NDL * cell;
-  const int R = 3 * np;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int band = warp % MT, tile0 = warp / MT;
+  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column of this lane
   for (int c = 0; c < 3; ++c) {
     // G_c[r = q*3 + K][mk = k*NN + m] = sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]
     for (int e = threadIdx.x; e < R * NDL; e += blockDim.x) {
       const int r = e / NDL, mk = e % NDL;
       const int q = r / 3, K = r % 3, k = mk / NN, m = mk % NN;
       const double* D = Dh + q * 81 + (c * 3 + K) + 9 * (k * 3);
-      G[e] = D[0] * A[m + NN * (0 + 3 * q)] + D[9] * A[m + NN * (1 + 3 * q)] + D[18] * A[m + NN * (2 + 3 * q)];
+      G[r * ldg + mk] = D[0] * A[m + NN * (0 + 3 * q)] + D[9] * A[m + NN * (1 + 3 * q)] + D[18] * A[m + NN * (2 + 3 * q)];
     }
     __syncthreads();
-    // K_c[n][mk] = sum_r A[n + NN*r] G[r][mk]; tiles of 3 rows x 3 columns
-    constexpr int TN = NN / 3, TM = NDL / 3;
-    for (int tile = threadIdx.x; tile < TN * TM; tile += blockDim.x) {
-      const int n0 = (tile % TN) * 3, mk0 = (tile / TN) * 3;
-      int32_t pp[3][3];  // positions loaded first: their latency overlaps the products
+    // this lane's output entries: rows n = band*8 + fr, columns mk = tile*8 + 2 fc + i; positions
+    // loaded first (their latency overlaps the products)
+    const int n = band * 8 + fr;
+    int32_t pp[TPW][2];
+    double acc[TPW][2];
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < TPW; ++j) {
+      const int tile = tile0 + 2 * j;
 #pragma unroll
-        for (int j = 0; j < 3; ++j) pp[i][j] = __ldg(pos + (c * NN + n0 + i) + NDL * (mk0 + j));
-      double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      for (int r = 0; r < R; ++r) {
-        const double a0 = A[n0 + NN * r], a1 = A[n0 + 1 + NN * r], a2 = A[n0 + 2 + NN * r];
-        const double g0 = G[r * NDL + mk0], g1 = G[r * NDL + mk0 + 1], g2 = G[r * NDL + mk0 + 2];
-        acc[0][0] += a0 * g0; acc[0][1] += a0 * g1; acc[0][2] += a0 * g2;
-        acc[1][0] += a1 * g0; acc[1][1] += a1 * g1; acc[1][2] += a1 * g2;
-        acc[2][0] += a2 * g0; acc[2][1] += a2 * g1; acc[2][2] += a2 * g2;
+      for (int i = 0; i < 2; ++i) {
+        const int mk = tile * 8 + 2 * fc + i;
+        pp[j][i] = (tile < NT && n < NN && mk < NDL) ? __ldg(pos + (c * NN + n) + NDL * mk) : 0;
+        acc[j][i] = 0.0;
       }
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) scatter_add(io.nzval, pp[i][j], acc[i][j]);
     }
+    // fragment elements past the matrices' edges are zeros: a lane whose element lies outside
+    // loads a valid address and selects zero, so the warp stays converged for mma.sync
+    const bool na = n < NN;
+    for (int ks = 0; ks < ksteps; ++ks) {
+      const int r = ks * 4 + fc;  // k index of this lane's A^T and B fragment elements
+      const bool ra = na && r < R;
+      double a = A[ra ? n + NN * r : 0];
+      a = ra ? a : 0.0;
+      const double* Gr = G + r * ldg + fr;
+#pragma unroll
+      for (int j = 0; j < TPW; ++j) {
+        const int tile = tile0 + 2 * j;
+        if (tile < NT) {  // uniform over the warp
+          double b;
+          if (PADDED) {
+            b = Gr[tile * 8];
+          } else {
+            const bool rb = r < R && tile * 8 + fr < NDL;
+            b = G[rb ? r * ldg + tile * 8 + fr : 0];
+            b = rb ? b : 0.0;
+          }
+          dmma_8x8x4(acc[j][0], acc[j][1], a, b);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TPW; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) scatter_add(io.nzval, pp[j][i], acc[j][i]);
     __syncthreads();
   }
 }
@@ -199,9 +254,10 @@ __global__ void __launch_bounds__(256) jacobian_kernel_direct(CellData cd, AsmIO
   }
 }
 
-inline size_t asm_smem_bytes(int nn, int np, bool with_g) {
+// with_g: G_c with row stride ldg and the rows of the padded k dimension (3 np rounded up to 4)
+inline size_t asm_smem_bytes(int nn, int np, bool with_g, int ldg) {
   size_t v = (size_t)nn * 3 * np + 3 * nn + 9 * np + 9 * np + np + 81 * np;
-  if (with_g) v += (size_t)3 * np * 3 * nn;
+  if (with_g) v += (size_t)((3 * np + 3) / 4 * 4) * ldg;
   return v * sizeof(double);
 }
 
