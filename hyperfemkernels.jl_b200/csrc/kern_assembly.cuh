@@ -152,20 +152,26 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int band = warp % MT, tile0 = warp / MT;
   const int fr = lane >> 2, fc = lane & 3;  // fragment row / column of this lane
+  constexpr int RG = 256 / NDL;  // thread groups of G_c's construction, one column per thread
   for (int c = 0; c < 3; ++c) {
-    // G_c[r = q*3 + K][mk = k*NN + m] = sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]
-    for (int e = threadIdx.x; e < R * NDL; e += blockDim.x) {
-      const int r = e / NDL, mk = e % NDL;
-      const int q = r / 3, K = r % 3, k = mk / NN, m = mk % NN;
-      const double* D = Dh + q * 81 + (c * 3 + K) + 9 * (k * 3);
-      G[r * ldg + mk] = D[0] * A[m + NN * (0 + 3 * q)] + D[9] * A[m + NN * (1 + 3 * q)] + D[18] * A[m + NN * (2 + 3 * q)];
+    // G_c[r = q*3 + K][mk = k*NN + m] = sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]: thread (g, mk) fills
+    // column mk for the points q = g, g + RG, ...; a point's three values of A serve its three rows
+    if (threadIdx.x < RG * NDL) {
+      const int g = threadIdx.x / NDL, mk = threadIdx.x - g * NDL;
+      const int k = mk / NN, m = mk - k * NN;
+      for (int q = g; q < np; q += RG) {
+        const double a0 = A[m + NN * (3 * q)], a1 = A[m + NN * (3 * q + 1)], a2 = A[m + NN * (3 * q + 2)];
+        const double* D = Dh + q * 81 + c * 3 + 27 * k;
+#pragma unroll
+        for (int K = 0; K < 3; ++K) G[(3 * q + K) * ldg + mk] = D[K] * a0 + D[K + 9] * a1 + D[K + 18] * a2;
+      }
     }
     __syncthreads();
     // this lane's output entries: rows n = band*8 + fr, columns mk = tile*8 + 2 fc + i; positions
     // loaded first (their latency overlaps the products)
     const int n = band * 8 + fr;
     int32_t pp[TPW][2];
-    double acc[TPW][2];
+    double acc[2][TPW][2];  // even and odd k-steps: two independent chains of tensor-core steps
 #pragma unroll
     for (int j = 0; j < TPW; ++j) {
       const int tile = tile0 + 2 * j;
@@ -173,13 +179,13 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
       for (int i = 0; i < 2; ++i) {
         const int mk = tile * 8 + 2 * fc + i;
         pp[j][i] = (tile < NT && n < NN && mk < NDL) ? __ldg(pos + (c * NN + n) + NDL * mk) : 0;
-        acc[j][i] = 0.0;
+        acc[0][j][i] = acc[1][j][i] = 0.0;
       }
     }
     // fragment elements past the matrices' edges are zeros: a lane whose element lies outside
     // loads a valid address and selects zero, so the warp stays converged for mma.sync
     const bool na = n < NN;
-    for (int ks = 0; ks < ksteps; ++ks) {
+    auto kstep = [&](int ks, double (&ac)[TPW][2]) {
       const int r = ks * 4 + fc;  // k index of this lane's A^T and B fragment elements
       const bool ra = na && r < R;
       double a = A[ra ? n + NN * r : 0];
@@ -197,14 +203,18 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
             b = G[rb ? r * ldg + tile * 8 + fr : 0];
             b = rb ? b : 0.0;
           }
-          dmma_8x8x4(acc[j][0], acc[j][1], a, b);
+          dmma_8x8x4(ac[j][0], ac[j][1], a, b);
         }
       }
+    };
+    for (int ks = 0; ks < ksteps; ks += 2) {
+      kstep(ks, acc[0]);
+      if (ks + 1 < ksteps) kstep(ks + 1, acc[1]);  // uniform over the block
     }
 #pragma unroll
     for (int j = 0; j < TPW; ++j)
 #pragma unroll
-      for (int i = 0; i < 2; ++i) scatter_add(io.nzval, pp[j][i], acc[j][i]);
+      for (int i = 0; i < 2; ++i) scatter_add(io.nzval, pp[j][i], acc[0][j][i] + acc[1][j][i]);
     __syncthreads();
   }
 }
