@@ -50,6 +50,37 @@ def test_subdomains_partition_properties(ghost):
             assert np.array_equal(s.peer_owns[p], space_owner(subs, s.free_global[idx]) == p)
     # slabs: each rank has one or two neighbours
     assert [sorted(s.shared) for s in subs] == [[1], [0, 2], [1]]
+    # every Dirichlet dof has exactly one owner, among the ranks whose cells reference it
+    downed = np.stack([s.dir_owned for s in subs])
+    assert np.array_equal(downed.sum(axis=0), np.ones(space.ndir))
+    for s in subs:
+        ids = s.space.cell_dof_ids
+        refd = np.unique(-ids[ids < 0].astype(np.int64) - 1)
+        assert set(np.nonzero(s.dir_owned)[0]) <= set(refd.tolist())
+
+
+def test_whole_mesh_multiplicity_counts_cells_per_dof():
+    """The restriction's multiplicity on a subdomain is the whole mesh's: the cells of every rank that
+    contain the dof (a Q2 vertex dof inside the mesh lies in 8 cells, an edge midpoint in 4, a face
+    midpoint in 2, a cell centre in 1)."""
+    from hfk.distributed import Subdomain, _global_multiplicity, slab_partition
+
+    space = svk_space((3, 3, 4), faces=("x0",))
+    mult = _global_multiplicity(space)
+    assert mult.shape == (space.nfree,) and mult.min() >= 1 and mult.max() == 8
+    assert sorted(set(mult.tolist())) == [1, 2, 4, 8]
+    cr = slab_partition(space.mesh, 2)
+    for r in range(2):
+        sub = Subdomain(space, cr, r)
+        ids = sub.space.cell_dof_ids
+        local = np.bincount(ids[ids > 0].astype(np.int64) - 1, minlength=sub.nfree)
+        whole = mult[sub.free_global]
+        assert np.all(whole >= local)
+        # interface dofs see fewer cells locally than on the whole mesh, interior ones the same
+        shared = np.zeros(sub.nfree, dtype=bool)
+        for idx in sub.shared.values():
+            shared[idx] = True
+        assert np.all(whole[~shared] == local[~shared]) and np.all(whole[shared] > local[shared])
 
 
 def space_owner(subs, glob):
