@@ -111,6 +111,20 @@ void check_launch(hfk_problem* p) {
   HFK_CUDA(cudaGetLastError());
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `smem` (`limit` caches what was set). The
+// limit only grows, under one lock: handles may be used from several host threads (one handle per
+// thread), and a thread about to launch with a large limit must not see it lowered by a thread that
+// needs less.
+std::mutex g_smem_limit_mu;
+template <typename K>
+void raise_smem_limit(K kernel, size_t smem, size_t& limit) {
+  std::lock_guard<std::mutex> lock(g_smem_limit_mu);
+  if (smem > limit) {
+    HFK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    limit = smem;
+  }
+}
+
 // ---- 1D Lagrange basis on [0,1], equispaced nodes (lagrange1d, src/tensorproduct.jl:24-47) ----
 void lagrange1d(int Q, double xi, double* N, double* dN) {
   std::vector<double> xs(Q);
@@ -250,10 +264,7 @@ void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>&
   using S = TPShape<Q, P>;
   const size_t smem = cell_smem_bytes<Q, P, R>(warps);
   static size_t attr = 0;
-  if (smem > attr) {
-    HFK_CUDA(cudaFuncSetAttribute(cell_kernel<Q, P, MODE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  raise_smem_limit(cell_kernel<Q, P, MODE, R>, smem, attr);
   const int per_cta = warps * S::CPW;
   const int grid = (ncl + per_cta - 1) / per_cta;
   if (grid == 0) return;
@@ -267,10 +278,7 @@ void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& 
   using S = JvpShape<Q, P, NT>;
   const size_t smem = jvp_smem_bytes<Q, P, R, NT>();
   static size_t attr = 0;
-  if (smem > attr) {
-    HFK_CUDA(cudaFuncSetAttribute(jvp_kernel<Q, P, R, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  raise_smem_limit(jvp_kernel<Q, P, R, NT>, smem, attr);
   const int grid = (ncl + S::C - 1) / S::C;
   if (grid == 0) return;
   jvp_kernel<Q, P, R, NT><<<grid, NT, smem, p->stream>>>(cell_data(p, cells, ncl), make_tab<R>(p), io);
@@ -722,10 +730,7 @@ template <int Q, int P>
 void blocks_tp_launch(hfk_problem* p, BlockIO io) {
   const size_t smem = blocks_tp_smem<Q, P>();
   static size_t attr = 0;
-  if (smem > attr) {
-    HFK_CUDA(cudaFuncSetAttribute(blocks_tp_kernel<Q, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  raise_smem_limit(blocks_tp_kernel<Q, P>, smem, attr);
   const Tab1D<double> tab = make_tab<double>(p);
   if (use_atomic_scatter(p)) {
     io.atomic = 1;
@@ -781,10 +786,7 @@ void blocks_update_dev(hfk_problem* p, int* ok) {
   }
   const size_t smem = ((size_t)3 * p->nn + 9 * p->np + 9 * p->np + p->np + 81 * p->np) * sizeof(double);
   static size_t attr = 0;
-  if (smem > attr) {
-    HFK_CUDA(cudaFuncSetAttribute(blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  raise_smem_limit(blocks_kernel, smem, attr);
   if (use_atomic_scatter(p)) {  // one launch over all cells, atomic accumulation of the blocks
     io.atomic = 1;
     blocks_kernel<<<p->ncells, 256, smem, p->stream>>>(cell_data(p, nullptr, p->ncells), io);
@@ -1283,17 +1285,10 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
   if (g) {
     static size_t attr[2] = {0, 0};
-    if (smem > attr[padded]) {
-      HFK_CUDA(cudaFuncSetAttribute(padded ? jacobian_kernel_g<27, true> : jacobian_kernel_g<27, false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr[padded] = smem;
-    }
+    raise_smem_limit(padded ? jacobian_kernel_g<27, true> : jacobian_kernel_g<27, false>, smem, attr[padded]);
   } else {
     static size_t attr = 0;
-    if (smem > attr) {
-      HFK_CUDA(cudaFuncSetAttribute(jacobian_kernel_direct<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = smem;
-    }
+    raise_smem_limit(jacobian_kernel_direct<8>, smem, attr);
   }
   auto launch = [&](const int32_t* cells, int n) {
     CellData cd = cell_data(p, cells, n);
@@ -3893,10 +3888,7 @@ void oseen_run(hfk_oseen* o, OseenIO io) {
   hfk_problem* p = &o->base;
   const size_t smem = (size_t)OseenSmem{o->nq}.total() * sizeof(double);
   static size_t attr = 0;
-  if (smem > attr) {
-    HFK_CUDA(cudaFuncSetAttribute(oseen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
+  raise_smem_limit(oseen_kernel, smem, attr);
   if (use_atomic_scatter(p)) {
     io.atomic = 1;
     oseen_kernel<<<p->ncells, OS_THREADS, smem, p->stream>>>(oseen_data(o, nullptr, p->ncells), io);
