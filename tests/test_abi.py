@@ -60,3 +60,19 @@ def test_operations_fail_loudly_without_a_device():
     with pytest.raises(_lib.HFKError) as e:
         KernelOperator(svk_residual(), svk_jacobian(), V)
     assert "CUDA" in str(e.value)
+
+
+def test_set_tolerance_is_the_forcing_term_hook():
+    # test/solvers/test_matrixfree_solver.jl:75-92 (the host side of it: the solve itself is on the GPU)
+    import types
+
+    from hfk import solvers as S
+
+    ns = types.SimpleNamespace(solver=S.MatrixFreeSolver(rtol=1e-10), rtol=1e-10)
+    assert S.tolerance(ns) == 1e-10
+    S.set_tolerance(ns, 1e-2)
+    assert S.tolerance(ns) == 1e-2
+    S.set_tolerance(ns, None)
+    assert S.tolerance(ns) == 1e-10
+    with pytest.raises(ValueError, match="HyperFEMKernels"):
+        S.set_tolerance(ns, 1.5)

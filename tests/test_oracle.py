@@ -366,3 +366,76 @@ def test_oracle_gmres_restarted_right_preconditioned():
     Ainv = sps.linalg.splu(A.tocsc())
     x, it, conv, _ = O.gmres(lambda v: A @ v, b, Ainv.solve, rtol=1e-10)
     assert conv and it == 1
+
+
+def test_vcycle_is_a_symmetric_positive_definite_operator():
+    # test/solvers/test_pmultigrid.jl:74-84: the cycle's matrix B (columns B e_j) is symmetric and SPD
+    m = CartesianMesh((2, 2, 2))
+    g = lambda x: np.stack([0.01 * x[:, 0], -0.02 * x[:, 1] * x[:, 2], 0.005 + 0 * x[:, 0]], axis=1)
+    Vs = [VectorLagrangeSpace(m, o, "boundary", g=g if o == 2 else None) for o in (2, 1)]
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_LINEAR, (2.0, 1.0))
+    mg.update(np.zeros(Vs[0].nfree), Vs[0].dirichlet_values)
+    B = np.stack([mg.ldiv(e) for e in np.eye(Vs[0].nfree)], axis=1)
+    assert np.linalg.norm(B - B.T) <= 1e-10 * np.linalg.norm(B)
+    assert np.linalg.eigvalsh((B + B.T) / 2).min() > 0
+
+
+@pytest.mark.parametrize("alpha,indefinite", [(0.8, True), (0.9, False)])
+def test_indefinite_tangent_gives_a_negative_ritz_value(alpha, indefinite):
+    # test/solvers/test_pmultigrid.jl:231-258 (there elasticity minus a mass term; here the SVK tangent
+    # under the uniform compression F = alpha I, whose compressive stress makes the shear modes
+    # negative at alpha = 0.8 and leaves the tangent definite at 0.9): a negative Ritz value in the
+    # smoother's estimate fails the hierarchy (the cycle returns NaN), and CG without a
+    # preconditioner meets the negative curvature; the definite case converges
+    m = CartesianMesh((3, 3, 3))
+    g = lambda x: (alpha - 1.0) * x
+    Vs = [VectorLagrangeSpace(m, o, "boundary", g=g if o == 2 else None) for o in (2, 1)]
+    x, _ = Vs[0].interpolate(g)
+    d = Vs[0].dirichlet_values
+    mg = O.OraclePMG(Vs, Quadrature.gauss(4), O.LAW_SVK, (2.0, 1.0))
+    A = mg.levels[0].jacobian(x, d).toarray()
+    lam = np.linalg.eigvalsh((A + A.T) / 2)
+    mg.update(x, d)
+    b = np.random.default_rng(0).standard_normal(Vs[0].nfree)
+    _, it, conv, _ = O.pcg(mg.levels[0].mf_apply, b, None, rtol=1e-8, maxiter=500)
+    if indefinite:
+        assert lam.min() < 0 < lam.max()
+        assert mg.smoothers[0].lmin < 0 and not mg.ok
+        assert np.all(np.isnan(mg.ldiv(b)))
+        assert not conv and it == 1
+    else:
+        assert lam.min() > 0 and mg.ok and mg.smoothers[0].lmin > 0
+        assert conv
+
+
+def test_nonlinear_coarse_tangent_differs_from_galerkin_by_O_h():
+    # test/solvers/test_pmultigrid_levels.jl:78-95: at a smooth state the coarse SVK tangent at the
+    # injected state differs from P^T A P by a first-order term in h
+    g = lambda x: np.stack([0.05 * np.sin(2 * x[:, 0]), 0.03 * x[:, 1] ** 2, 0.02 * x[:, 0] * x[:, 2]], axis=1)
+    errs = []
+    for k in (2, 4):
+        m = CartesianMesh((k, k, k))
+        Vf = VectorLagrangeSpace(m, 2, "boundary", g=g)
+        Vc = VectorLagrangeSpace(m, 1, "boundary")
+        q = Quadrature.gauss(4)
+        pf = O.OracleProblem(Vf, q, O.LAW_SVK, (2.0, 1.0))
+        pc = O.OracleProblem(Vc, q, O.LAW_SVK, (2.0, 1.0))
+        x, _ = Vf.interpolate(g)
+        df = Vf.dirichlet_values
+        T = O.OracleTransfer(Vf, Vc)
+        xc, dc = T.inject(x, df, Vc.nfree, Vc.ndir)
+        Af = pf.jacobian(x, df).toarray()
+        Ac = pc.jacobian(xc, dc).toarray()
+        P = np.stack([T.prolongate(e) for e in np.eye(Vc.nfree)], axis=1)
+        gal = P.T @ Af @ P
+        errs.append(np.linalg.norm(Ac - gal) / np.linalg.norm(gal))
+    assert errs[0] < 0.05
+    assert errs[0] / errs[1] > 1.5
+
+
+def test_embeddings_are_snapped():
+    # test/solvers/test_transfers.jl:135-143: entries within 1e-7 of 0 or 1 are exactly 0 or 1
+    for pc, pf in ((1, 3), (2, 3), (1, 2)):
+        for M in transfer_matrices(pf + 1, pc + 1):
+            e = np.asarray(M).ravel()
+            assert np.all((e == 0) | (e == 1) | ((np.abs(e) > 1e-7) & (np.abs(e - 1) > 1e-7)))
