@@ -439,3 +439,27 @@ def test_embeddings_are_snapped():
         for M in transfer_matrices(pf + 1, pc + 1):
             e = np.asarray(M).ravel()
             assert np.all((e == 0) | (e == 1) | ((np.abs(e) > 1e-7) & (np.abs(e - 1) > 1e-7)))
+
+
+def test_cell_dof_matrix_layout_and_dirichlet_ids():
+    # test/test_tables.jl:46-61: components of a node contiguous per cell (ldof = c*nn + n), free ids
+    # 1..nfree and Dirichlet ids -1..-ndir each used, a node's three components fixed or free together
+    m = CartesianMesh((3, 2, 2))
+    for order in (1, 2, 3):
+        V = VectorLagrangeSpace(m, order, ("x0", "y1"))
+        ids = V.cell_dof_ids.astype(np.int64)
+        assert ids.shape == (3 * V.nn, m.ncells)
+        assert set(np.unique(ids[ids > 0]).tolist()) == set(range(1, V.nfree + 1))
+        assert set(np.unique(-ids[ids < 0]).tolist()) == set(range(1, V.ndir + 1))
+        assert not (ids == 0).any()
+        per_comp = ids.reshape(3, V.nn, m.ncells)
+        assert np.array_equal(per_comp[0] > 0, per_comp[1] > 0) and np.array_equal(per_comp[0] > 0, per_comp[2] > 0)
+        free = per_comp[0] > 0  # node-major numbering: the components of a free node are consecutive ids
+        assert np.all(per_comp[1][free] == per_comp[0][free] + 1) and np.all(per_comp[2][free] == per_comp[0][free] + 2)
+        # the same global node carries the same ids in every cell that holds it
+        gid = {}
+        for c in range(m.ncells):
+            for n_ in range(V.nn):
+                key = int(V.cell_nodes[c, n_])
+                val = tuple(per_comp[:, n_, c])
+                assert gid.setdefault(key, val) == val
