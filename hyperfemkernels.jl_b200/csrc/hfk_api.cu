@@ -1492,6 +1492,10 @@ struct hfk_pmg {
   std::vector<double> a, b, lmin, lmax;
   std::vector<char> lok;
   bool ok = false, built = false;
+  // a failed update that met an indefinite tangent: on some smoothing level finite blocks and a
+  // finite estimate with a non-positive Ritz value (preconditioner_indefinite, src/pmultigrid.jl:343;
+  // smoother_indefinite, src/smoothers.jl:48)
+  bool indefinite = false;
   int since = 0, nupdate = 0, nbuild = 0;
   int band = -1;  // lower bandwidth of the coarse level's pattern (computed once)
   std::vector<std::unique_ptr<LevelWork<double>>> w64;
@@ -2824,7 +2828,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     coarse_factor_launch(m);
   }
   // smoothers: blocks and intervals (smoother_update!, src/smoothers.jl:86-107)
-  bool all_ok = true;
+  bool all_ok = true, indef = false;
   for (int l = 0; l + 1 < m->L; ++l) {
     hfk_problem* p = m->lv[l];
     int bok = 0;
@@ -2856,6 +2860,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
     for (int sgi = 0; sgi < ns; ++sgi) {
       const bool ok_s = std::isfinite(hi[sgi]) && hi[sgi] > 0 && lo[sgi] > 0;
       lok &= ok_s;
+      indef |= std::isfinite(hi[sgi]) && std::isfinite(lo[sgi]) && (lo[sgi] <= 0 || hi[sgi] <= 0);
       const double bs = ok_s ? m->inflate * hi[sgi] : 1.0;
       const std::vector<double> c = chebyshev_coefficients(bs / m->range, bs, m->degree);
       coefs.insert(coefs.end(), c.begin(), c.end());
@@ -2904,6 +2909,7 @@ int hfk_pmg_update(hfk_pmg* m, const double* x, const double* dvals, int* ok) {
   }
   all_ok &= m->coarse_ok;
   m->ok = all_ok;
+  m->indefinite = !all_ok && indef;
   m->built = true;
   m->nupdate++;
   *ok = all_ok;
@@ -2942,6 +2948,14 @@ int hfk_pmg_stats(hfk_pmg* m, double* out) {
   HFK_API_END
 }
 
+int hfk_pmg_status(hfk_pmg* m, int* ok, int* indefinite) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && ok && indefinite, HFK_ERR_ARG, "null argument");
+  *ok = m->ok;
+  *indefinite = m->indefinite;
+  HFK_API_END
+}
+
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b) {
   HFK_API_BEGIN
   HFK_REQUIRE(m && level >= 0 && level < m->L, HFK_ERR_ARG, "invalid level");
@@ -2972,10 +2986,11 @@ void solve_cg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x, do
   *converged = 0;
   if (indefinite) *indefinite = 0;
   if (relres) *relres = NAN;
-  if (prec && !prec->ok) {  // src/solvers.jl:114-121: no iteration, a failed solve
+  if (prec && !prec->ok) {  // src/solvers.jl:114-121: no iteration, a failed solve (indefinite or not)
     if (is_device_ptr(x)) HFK_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
     else std::fill(x, x + n, 0.0);
     HFK_CUDA(cudaStreamSynchronize(s));
+    if (indefinite) *indefinite = prec->indefinite;
     return;
   }
   hfk::CGWork& cw = op->cg;

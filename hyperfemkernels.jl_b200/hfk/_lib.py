@@ -82,6 +82,7 @@ SIGNATURES = {
     "hfk_pmg_vcycle": [_vp, _vp, _vp],
     "hfk_pmg_level_info": [_vp, _i, _pd, _pd, _pd, _pd],
     "hfk_pmg_stats": [_vp, _vp],
+    "hfk_pmg_status": [_vp, _pi, _pi],
     "hfk_solve_cg": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _pi, _pi, _pi, _pd],
     "hfk_solve_gmres": [_vp, _vp, _vp, _vp, _d, _d, _i, _i, _i, _pi, _pi, _pd],
     "hfk_slot_create": [ctypes.POINTER(_vp), _vp, _i, _i],

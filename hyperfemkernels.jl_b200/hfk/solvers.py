@@ -411,6 +411,11 @@ def solve(x, ns: MatrixFreeSolverNS, b):
         call("hfk_solve_cg", ns.mf.op.problem.h, prec, ptr(b), ptr(x), ns.rtol, s.atol, s.maxiter,
              1 if s.krylov == "fcg" else 0, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(ind), ctypes.byref(rel))
     ns.iters, ns.converged, ns.indefinite, ns.rnorm = it.value, bool(conv.value), bool(ind.value), rel.value
+    if prec is not None and s.krylov in ("gmres", "fgmres"):
+        # a failed preconditioner: no iteration, indefinite when it met an indefinite tangent
+        pok, pind = ctypes.c_int(), ctypes.c_int()
+        call("hfk_pmg_status", prec, ctypes.byref(pok), ctypes.byref(pind))
+        ns.indefinite = not pok.value and bool(pind.value)
     return x
 
 

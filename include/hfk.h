@@ -234,6 +234,12 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y);
  * V-cycles, in the Cholesky factorisation alone. The
  * V-cycle is replayed from a CUDA graph captured on the second cycle after each update. */
 int hfk_pmg_stats(hfk_pmg* m, double* out);
+/* State of the last update: ok (preconditioner_ok, src/solvers.jl:105-106) and, when it failed,
+ * whether it met an indefinite tangent: finite nodal blocks and a finite Ritz estimate with a
+ * non-positive value on some smoothing level (preconditioner_indefinite, src/pmultigrid.jl:342-343,
+ * the signal a Newton with a switching tangent reads). hfk_solve_cg reports the same flag in
+ * `indefinite` when it returns without iterating on a failed preconditioner. */
+int hfk_pmg_status(hfk_pmg* m, int* ok, int* indefinite);
 /* Interval and Ritz values of a level's smoother (with segments: the extreme Ritz values over the
  * segments and the interval of the largest). */
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);

@@ -602,3 +602,36 @@ def test_newton_pmg_load_stepping_matches_oracle_newton():
                     break
                 xo = xo - sp.linalg.spsolve(orc.jacobian(xo, d).tocsc(), r)
         assert reldiff(x.cpu().numpy(), xo) < 1e-8
+
+
+@pytest.mark.parametrize("alpha,indefinite", [(0.8, True), (0.9, False)])
+def test_indefinite_tangent_is_reported_by_the_solve(alpha, indefinite):
+    # test/solvers/test_pmultigrid.jl:231-258, with the SVK tangent under the uniform compression
+    # F = alpha I in place of the reference's elasticity-minus-mass form (indefinite at 0.8, definite
+    # at 0.9): a failed p-multigrid solve that met a negative Ritz value is reported indefinite
+    # (preconditioner_indefinite), CG without a preconditioner meets the negative curvature itself
+    m = CartesianMesh((3, 3, 3))
+    g = lambda x: (alpha - 1.0) * x
+    Vs = [VectorLagrangeSpace(m, o, "boundary", g=g if o == 2 else None) for o in (2, 1)]
+    res, jac = forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4)
+    op = KernelOperator(res, jac, Vs[0], jacobian="matrixfree")
+    x, _ = Vs[0].interpolate(g)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    b = np.random.default_rng(0).standard_normal(Vs[0].nfree)
+    for krylov in ("fcg", "gmres"):
+        ls = S.MatrixFreeSolver(krylov=krylov, rtol=1e-8, preconditioner=S.PMultigrid(Vs))
+        ns = S.numerical_setup(S.symbolic_setup(ls, mf), mf)
+        dx = np.zeros(Vs[0].nfree)
+        S.solve(dx, ns, b)
+        if indefinite:
+            assert not S.linear_converged(ns) and S.linear_iterations(ns) == 0 and S.linear_indefinite(ns)
+            assert np.all(dx == 0)
+        else:
+            assert S.linear_converged(ns) and not S.linear_indefinite(ns)
+    ls0 = S.MatrixFreeSolver(krylov="cg", rtol=1e-8, maxiter=500)
+    ns0 = S.numerical_setup(S.symbolic_setup(ls0, mf), mf)
+    dx = np.zeros(Vs[0].nfree)
+    S.solve(dx, ns0, b)
+    assert S.linear_converged(ns0) == (not indefinite) and S.linear_indefinite(ns0) == indefinite
+    assert np.all(np.isfinite(dx))
