@@ -463,3 +463,52 @@ def test_cell_dof_matrix_layout_and_dirichlet_ids():
                 key = int(V.cell_nodes[c, n_])
                 val = tuple(per_comp[:, n_, c])
                 assert gid.setdefault(key, val) == val
+
+
+@pytest.mark.parametrize("qc,qf", [(1, 2), (2, 3), (1, 3)])
+def test_prolongation_is_the_exact_embedding(qc, qf):
+    # test/solvers/test_transfers.jl:39-50: a field of the coarse space, prolongated, is the same field
+    # in the fine space (here checked against the fine nodal interpolation of a polynomial of the
+    # coarse degree, without Dirichlet dofs so that every dof takes part)
+    m = CartesianMesh((2, 2, 1))
+    Vc = VectorLagrangeSpace(m, qc, ())
+    Vf = VectorLagrangeSpace(m, qf, ())
+    assert Vc.ndir == 0 and Vf.ndir == 0
+
+    def f(x):
+        X, Y, Z = x[:, 0], x[:, 1], x[:, 2]
+        p = (X ** qc) * (Y ** qc) * (Z ** qc)
+        return np.stack([1 + X - 2 * Y + 0.5 * p, Z * Y - 0.3 * p, 2 - X * Z + p], axis=1)
+
+    xc, _ = Vc.interpolate(f)
+    xf, _ = Vf.interpolate(f)
+    T = O.OracleTransfer(Vf, Vc)
+    assert reldiff(T.prolongate(xc), xf) < 1e-12
+
+
+def test_chebyshev_zero_guess_residual_output_and_options():
+    # test/solvers/test_chebyshev.jl:100-126: a fixed start vector makes the interval reproducible;
+    # zero_guess ignores x; the residual output is b - A x; the smoother reduces the residual; the
+    # damping's closed form; invalid options rejected
+    from hfk import solvers as S
+
+    V = svk_space((3, 2, 2))
+    q = Quadrature.gauss(4)
+    p = O.OracleProblem(V, q, O.LAW_LINEAR, (2.0, 1.0))
+    p.mf_prepare(np.zeros(V.nfree), V.dirichlet_values)
+    st = O.OracleChebyshev(p, degree=2)
+    st2 = O.OracleChebyshev(p, degree=2)
+    assert st.ok and st.lmax == st2.lmax
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(V.nfree)
+    x1, _ = st.smooth(np.zeros(V.nfree), b)
+    x2, _ = st.smooth(rng.standard_normal(V.nfree), b, zero_guess=True)
+    assert reldiff(x2, x1) < 1e-13
+    x3, r = st.smooth(None, b, zero_guess=True, want_residual=True)
+    assert reldiff(x3, x1) < 1e-13
+    assert reldiff(r, b - p.mf_apply(x3)) < 1e-12
+    assert np.linalg.norm(r) < np.linalg.norm(b)
+    assert abs(S.chebyshev_damping(S.Chebyshev(degree=3, range=20.0)) - 1 / math.cosh(3 * math.acosh(21 / 19))) < 1e-15
+    for bad in (dict(degree=0), dict(range=1.0), dict(inflate=0.9), dict(eig_iters=1)):
+        with pytest.raises(ValueError, match="HyperFEMKernels"):
+            S.Chebyshev(**bad)
