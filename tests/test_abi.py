@@ -76,3 +76,31 @@ def test_set_tolerance_is_the_forcing_term_hook():
     assert S.tolerance(ns) == 1e-10
     with pytest.raises(ValueError, match="HyperFEMKernels"):
         S.set_tolerance(ns, 1.5)
+
+
+def test_solver_options_are_validated_before_any_device_work():
+    # test/solvers/test_matrixfree_solver.jl:55-73, test/solvers/test_operator.jl:89-95,
+    # test/solvers/test_pmultigrid_levels.jl:143 (the option checks; the GPU parts run in the gpu tests)
+    from hfk import forms
+    from hfk import solvers as S
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.operator import KernelOperator
+
+    for bad in (dict(krylov="bicgstab"), dict(restart=0), dict(rtol=1.0), dict(rtol=-1e-3), dict(atol=-1.0),
+                dict(maxiter=0)):
+        with pytest.raises(ValueError, match="HyperFEMKernels"):
+            S.MatrixFreeSolver(**bad)
+    m = CartesianMesh((2, 2, 2))
+    Vs = [VectorLagrangeSpace(m, o, ("x0",)) for o in (2, 1)]
+    for args, kw in (((Vs[:1],), {}), ((Vs,), dict(coarse_every=0)), ((Vs,), dict(precision="fp16")),
+                     ((Vs,), dict(coarse="amg")), ((Vs,), dict(coarse="cg", coarse_iters=0))):
+        with pytest.raises(ValueError, match="HyperFEMKernels"):
+            S.PMultigrid(*args, **kw)
+    for kw in (dict(solver="lu"), dict(every=0)):
+        with pytest.raises(ValueError, match="HyperFEMKernels"):
+            S.LaggedAssembled(**kw)
+    res, jac = forms.svk_residual(), forms.svk_jacobian()
+    with pytest.raises(ValueError, match="HyperFEMKernels"):
+        KernelOperator(res, jac, Vs[0], jacobian="dense")
+    with pytest.raises(ValueError, match="HyperFEMKernels"):
+        KernelOperator(res, forms.svk_jacobian(lam=3.0), Vs[0])  # residual and Jacobian of different laws
