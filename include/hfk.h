@@ -130,7 +130,8 @@ int hfk_nonzero_positions(hfk_problem* p, int32_t* nzpos);
  * x and Dirichlet values dvals. FP64. */
 int hfk_residual(hfk_problem* p, const double* x, const double* dvals, double* b);
 /* jacobian!(A, op, x) (src/assembly.jl:918-927): nzval (nnz) of the CSC Jacobian in rowval order
- * (zero-filled, then the fused element kernels and the colour-by-colour scatter). FP64. */
+ * (zero-filled, then the fused element kernels: one launch with atomic adds by default, colour by
+ * colour, bit-reproducible, under HFK_SCATTER_COLOURED). FP64. */
 int hfk_jacobian(hfk_problem* p, const double* x, const double* dvals, double* nzval);
 
 /* prepare!(mf, x) / jacobian!(mf, op, x) (src/matrixfree.jl:97-100, :140-159): bind the state.
