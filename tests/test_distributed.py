@@ -211,14 +211,17 @@ def _dd_rank(rank, world, port, out):
         dist.destroy_process_group()
 
 
-def test_gloo_two_ranks_product_residual_cg():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_product_residual_cg(world):
+    # world 3: the middle slab exchanges with both neighbours in one batch of sends and receives
     import torch
 
     import oracle as O
     from hfk.distributed import DistributedJacobian, Subdomain, cg, slab_partition
     from hfk.fespace import Quadrature
 
-    res = _spawn(_dd_rank, 2)
+    res = _spawn(_dd_rank, world)
+    assert len(res) == world
     space = svk_space((2, 3, 4))
     quad = Quadrature.gauss(4)
     x = _state(space)
@@ -249,10 +252,10 @@ def test_gloo_two_ranks_product_residual_cg():
         assert conv and abs(it - it1) <= 2
         assert np.linalg.norm(xl - xd[fg]) <= 1e-7 * np.linalg.norm(xd[fg])
         assert np.array_equal(v, fg.astype(np.float64))  # every copy holds its owner's value
-    # the two copies of an interface dof agree bitwise after the halo sum (two ranks per dof)
-    (_, f0, y0, *_), (_, f1, y1, *_) = res
-    common, i0, i1 = np.intersect1d(f0, f1, return_indices=True)
-    assert len(common) > 0 and np.array_equal(y0[i0], y1[i1])
+    # neighbouring slabs' copies of an interface dof agree bitwise after the halo sum (two ranks per dof)
+    for (_, f0, y0, *_), (_, f1, y1, *_) in zip(res[:-1], res[1:]):
+        common, i0, i1 = np.intersect1d(f0, f1, return_indices=True)
+        assert len(common) > 0 and np.array_equal(y0[i0], y1[i1])
 
 
 class _OracleOp:
