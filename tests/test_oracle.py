@@ -512,3 +512,31 @@ def test_chebyshev_zero_guess_residual_output_and_options():
     for bad in (dict(degree=0), dict(range=1.0), dict(inflate=0.9), dict(eig_iters=1)):
         with pytest.raises(ValueError, match="HyperFEMKernels"):
             S.Chebyshev(**bad)
+
+
+def test_arnoldi_bounds_against_the_dense_spectrum():
+    # test/solvers/test_matrixfree_solver.jl:172-197 (vector elasticity on Q2 in place of the 2D
+    # Poisson problem): the block-Jacobi preconditioned estimate within 10 % of the dense largest
+    # eigenvalue and positive smallest; without a preconditioner the operator's own spectrum; the
+    # same start vector gives the same bounds; an exact preconditioner breaks down at (1, 1)
+    V = svk_space((3, 2, 2))
+    p = O.OracleProblem(V, Quadrature.gauss(4), O.LAW_LINEAR, (2.0, 1.0))
+    x, d = np.zeros(V.nfree), V.dirichlet_values
+    p.mf_prepare(x, d)
+    p.blocks()
+    A = p.jacobian(x, d)
+    Ad = A.toarray()
+    n = V.nfree
+    Minv = np.stack([p.blocks_apply(e) for e in np.eye(n)], axis=1)
+    lam = np.linalg.eigvals(Ad @ Minv).real
+    b = O.chebyshev_start(n)
+    lo, hi, _ = O.arnoldi_bounds(p.mf_apply, p.blocks_apply, b, min(30, n))
+    assert 0.9 * lam.max() <= hi <= 1.1 * lam.max() and lo > 0
+    lo0, hi0, _ = O.arnoldi_bounds(p.mf_apply, lambda v: v, b, min(30, n))
+    lamA = np.linalg.eigvalsh((Ad + Ad.T) / 2).max()
+    assert 0.9 * lamA <= hi0 <= 1.1 * lamA
+    b0 = np.random.default_rng(3).standard_normal(n)
+    assert O.arnoldi_bounds(p.mf_apply, p.blocks_apply, b0, 10)[:2] == O.arnoldi_bounds(p.mf_apply, p.blocks_apply, b0, 10)[:2]
+    lu = sp.linalg.splu(A.tocsc())
+    le = O.arnoldi_bounds(p.mf_apply, lu.solve, b0, 10)[:2]
+    assert abs(le[0] - 1.0) < 1e-6 and abs(le[1] - 1.0) < 1e-6
