@@ -272,6 +272,67 @@ void element_residual(const Problem& p, const double* xl, int cell, double* re, 
     }
 }
 
+// gemm_add! (src/kernels.jl:640-690): C[m, n] += sum_r A[m, r] B[r, n], m < M, n < N, r < R, with
+// MB x NB tiles of C held in registers over the whole r loop: 8 x 4 tiles, then 4/2/1-row and
+// 1-column remainders. Each entry is summed over r in order, then added to C once.
+template <int MB, int NB>
+inline void gemm_tile(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda,
+                      const double* __restrict__ B, int ldb, int R) {
+  if constexpr (MB % 4 == 0) {
+    typedef double v4 __attribute__((vector_size(32)));
+    constexpr int MV = MB / 4;
+    v4 acc[NB][MV];
+#pragma GCC unroll 8
+    for (int j = 0; j < NB; ++j)
+#pragma GCC unroll 8
+      for (int i = 0; i < MV; ++i) acc[j][i] = v4{0, 0, 0, 0};
+    for (int r = 0; r < R; ++r) {
+      const double* a = A + (size_t)lda * r;
+      v4 av[MV];
+#pragma GCC unroll 8
+      for (int i = 0; i < MV; ++i) __builtin_memcpy(&av[i], a + 4 * i, sizeof(v4));
+#pragma GCC unroll 8
+      for (int j = 0; j < NB; ++j) {
+        const double b = B[r + (size_t)ldb * j];
+#pragma GCC unroll 8
+        for (int i = 0; i < MV; ++i) acc[j][i] += av[i] * b;
+      }
+    }
+    for (int j = 0; j < NB; ++j)
+      for (int i = 0; i < MV; ++i)
+        for (int l = 0; l < 4; ++l) C[4 * i + l + (size_t)ldc * j] += acc[j][i][l];
+  } else {
+    double acc[NB][MB] = {};
+    for (int r = 0; r < R; ++r) {
+      const double* a = A + (size_t)lda * r;
+#pragma GCC unroll 8
+      for (int j = 0; j < NB; ++j) {
+        const double b = B[r + (size_t)ldb * j];
+#pragma GCC unroll 8
+        for (int i = 0; i < MB; ++i) acc[j][i] += a[i] * b;
+      }
+    }
+    for (int j = 0; j < NB; ++j)
+      for (int i = 0; i < MB; ++i) C[i + (size_t)ldc * j] += acc[j][i];
+  }
+}
+
+template <int NB>
+inline void gemm_cols(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int M, int R) {
+  int m0 = 0;
+  for (; m0 + 8 <= M; m0 += 8) gemm_tile<8, NB>(C + m0, ldc, A + m0, lda, B, ldb, R);
+  int rem = M - m0;
+  if (rem >= 4) { gemm_tile<4, NB>(C + m0, ldc, A + m0, lda, B, ldb, R); m0 += 4; rem -= 4; }
+  if (rem >= 2) { gemm_tile<2, NB>(C + m0, ldc, A + m0, lda, B, ldb, R); m0 += 2; rem -= 2; }
+  if (rem >= 1) gemm_tile<1, NB>(C + m0, ldc, A + m0, lda, B, ldb, R);
+}
+
+inline void gemm_add(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int M, int N, int R) {
+  int n0 = 0;
+  for (; n0 + 4 <= N; n0 += 4) gemm_cols<4>(C + (size_t)ldc * n0, ldc, A, lda, B + (size_t)ldb * n0, ldb, M, R);
+  for (; n0 < N; ++n0) gemm_cols<1>(C + (size_t)ldc * n0, ldc, A, lda, B + (size_t)ldb * n0, ldb, M, R);
+}
+
 // element_jacobian_mm! (src/assembly.jl:1316-1342): point blocks of POINT_BLOCK points,
 // B[(ql,jj), n] = W[n, jj] (store_test_weights!), G[m, (ql,jj), k, c] = dV sum_ll T W[m, ll]
 // (store_trial_block!), KeT[(m,k), (n,c)] += sum_r G B (block_products!/gemm_add!, src/kernels.jl:615-705).
@@ -300,29 +361,24 @@ void element_jacobian(const Problem& p, const double* xl, int cell, double* KeT,
       law_tangent(p, F, T);
       for (int n = 0; n < nn; ++n)
         for (int jj = 0; jj < 3; ++jj) Bb[(ql * 3 + jj) + (size_t)qb * 3 * n] = W[n + nn * jj];
+      const double* __restrict__ W0 = W.data();
+      const double* __restrict__ W1 = W0 + nn;
+      const double* __restrict__ W2 = W0 + 2 * nn;
       for (int c = 0; c < 3; ++c)
         for (int k = 0; k < 3; ++k)
           for (int jj = 0; jj < 3; ++jj) {
-            double z[3];
-            for (int ll = 0; ll < 3; ++ll) z[ll] = dV * T[(c * 3 + jj) + 9 * (k * 3 + ll)];
-            for (int m = 0; m < nn; ++m) {
-              double acc = 0;
-              for (int ll = 0; ll < 3; ++ll) acc += z[ll] * W[m + nn * ll];
-              Gb[m + (size_t)nn * ((ql * 3 + jj) + (size_t)qb * 3 * (k + 3 * c))] = acc;
-            }
+            const double z0 = dV * T[(c * 3 + jj) + 9 * (k * 3 + 0)];
+            const double z1 = dV * T[(c * 3 + jj) + 9 * (k * 3 + 1)];
+            const double z2 = dV * T[(c * 3 + jj) + 9 * (k * 3 + 2)];
+            double* __restrict__ g = &Gb[(size_t)nn * ((ql * 3 + jj) + (size_t)qb * 3 * (k + 3 * c))];
+            for (int m = 0; m < nn; ++m) g[m] = z0 * W0[m] + z1 * W1[m] + z2 * W2[m];
           }
     }
     const int R = nq * 3;
     for (int c = 0; c < 3; ++c)
-      for (int k = 0; k < 3; ++k) {
-        const double* G = &Gb[(size_t)nn * qb * 3 * (k + 3 * c)];
-        for (int n = 0; n < nn; ++n)
-          for (int m = 0; m < nn; ++m) {
-            double acc = 0;
-            for (int r = 0; r < R; ++r) acc += G[m + (size_t)nn * r] * Bb[r + (size_t)qb * 3 * n];
-            KeT[(k * nn + m) + (size_t)ndl * (c * nn + n)] += acc;
-          }
-      }
+      for (int k = 0; k < 3; ++k)
+        if (getenv("SKIPG")==nullptr) gemm_add(&KeT[(size_t)k * nn + (size_t)ndl * c * nn], ndl, &Gb[(size_t)nn * qb * 3 * (k + 3 * c)], nn,
+                 Bb.data(), qb * 3, nn, nn, R);
   }
 }
 
