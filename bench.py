@@ -1,15 +1,23 @@
-"""Benchmark of the hot path: matrix-free SVK Jacobian-vector product, Q2 hexahedra on a 64^3 cube.
+"""Benchmark of the hot path: the FP64 CSC Jacobian assembly of the SVK Q2 20x10x10 cube.
 
-One step = one J(x)·dx over the whole mesh (6.34 M free dofs), FP64, tangent re-evaluated from the
-state inside the product (sum factorisation). Inputs are resident in HBM for `value`; `e2e` runs the
-same product through the public C ABI with pinned host buffers (dx copied in, y copied out every
-step). Prints one JSON line (rank 0).
+One step = one `jacobian!` (src/assembly.jl:918-927): zero-fill of the CSC values, the element
+Jacobians of all 2 000 Q2 cells (27 Gauss points each) and their scatter into the reference's
+CSC pattern (52 077 free dofs, 8 990 127 nonzeros), FP64. `value` = free dofs / step time with
+the state resident in HBM (GDOF/s); `e2e` runs the same assembly through the public C ABI with
+page-locked host buffers (state copied in, CSC values copied out every step). Prints one JSON line
+(rank 0). `extra` carries the other configurations: the matrix-free J*v on Q2 64^3 (with its own
+e2e, roofline and full-size CPU comparison), the other J*v sizes, the Oseen P2-P1 assembly and the
+p-multigrid Newton solve.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 `--impl reference` times the CPU restatement of the reference algorithm (the oracle: the
-reference's stored-tangent matrix-free product, OpenMP over all host cores) on a bounded sample of
-the same workload.
+reference's matrix-product element Jacobian with register-tiled products and the colour loop,
+OpenMP over all host cores) on the same configuration.
+
+With N > 1 GPUs (torchrun, one process per GPU) each rank assembles the owned rows of one slab of
+a 20 x 10 x 10N mesh cut along z (owner computes: the rank also assembles the cells that touch its
+dofs, so no data is exchanged); value = all ranks' free dofs / the slowest rank's step time.
 """
 import argparse
 import ctypes
@@ -26,22 +34,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hyperfemkernels.jl_b200"))
 
-METRIC = "Q2 SVK Jacobian GDOF/s (matrix-free J*v, FP64)"
+METRIC = "Q2 SVK Jacobian GDOF/s"
 UNIT = "GDOF/s"
-N_CELLS = 64
-ORDER = 2
-WORKLOAD = "MF Jacobian-vector product, SVK (lambda=2, mu=1), Q2 hexahedra, 64^3 unit cube, Gauss 3^3"
+C0_CELLS = (20, 10, 10)
+WORKLOAD = ("CSC Jacobian assembly (jacobian!: zero-fill, element Jacobians, scatter), SVK lambda=2 mu=1, "
+            "Q2 hexahedra 20x10x10 on the unit cube, Gauss degree 4 (27 points), x=0 clamped, x=1 displaced 0.05 "
+            "(open faces), FP64")
+# FP64 flops of one Q2 element Jacobian, the reference's own count (benchmark/roofline.jl:65-74):
+# block products G*B, 3*3*2*27*27*27*3, plus G at the points, 3*3*3*27*27*3*2
+C0_FLOPS_PER_CELL = 3 * 3 * 2 * 27 * 27 * 27 * 3 + 3 * 3 * 3 * 27 * 27 * 3 * 2
+L2_FLUSH_BYTES = 256 << 20  # twice the B200's 126 MB L2
+JV_CELLS = 64
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--n", type=int, default=N_CELLS, help="cells per direction")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--batch", action="store_true",
                     help="the batched workload instead: 256 SVK Q2 Newton solves (plain p-MG vs learned correction)")
     ap.add_argument("--batch-count", type=int, default=256)
@@ -49,24 +62,44 @@ def parse():
     ap.add_argument("--oseen", type=int, default=0, metavar="N",
                     help="only the Oseen P2-P1 assembly on the N^3 tetrahedral cube (the secondary case; 0 = off)")
     ap.add_argument("--launch", default="auto", choices=["auto", "line2", "line4", "point"],
-                    help="launch shape of the J*v (auto: the autotuner's; a fixed one for profiling, where the "
-                         "profiler's overhead would skew the autotuner's timings)")
+                    help="launch shape of the J*v in --jv (auto: the autotuner's; a fixed one for profiling, "
+                         "where the profiler's overhead would skew the autotuner's timings)")
+    ap.add_argument("--jv", type=int, default=0, metavar="N",
+                    help="only the matrix-free Q2 J*v on the N^3 cube (the case for profiling its kernel)")
     ap.add_argument("--assembly", action="store_true",
-                    help="only the Q2 SVK 20x10x10 residual + CSC Jacobian (the CPU-runnable configuration)")
+                    help="only the Q2 SVK 20x10x10 residual + CSC Jacobian, a few steps (the case for profiling)")
     ap.add_argument("--vcycle", type=int, default=0, metavar="K",
                     help="only K V-cycles of the Q4 16^3 p-multigrid 4 -> 2 -> 1 (the Newton case's preconditioner)")
     return ap.parse_args()
 
 
-def build_case(n, order=ORDER, seed=0):
-    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+def svk_dirichlet():
+    return [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
 
-    m = CartesianMesh((n, n, n))
-    g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
-    V = VectorLagrangeSpace(m, order, ("x0", "x1"), g=g)
+
+def svk_state(V, seed=0):
+    """u = 0.05 x e_x + U(-1e-3, 1e-3) on the free dofs (seeded)."""
     rng = np.random.default_rng(seed)
     x, _ = V.interpolate(lambda p: np.stack([0.05 * p[:, 0], 0 * p[:, 0], 0 * p[:, 0]], axis=1))
-    x = x + rng.uniform(-1e-3, 1e-3, V.nfree)
+    return x + rng.uniform(-1e-3, 1e-3, V.nfree)
+
+
+def c0_space(nz=10):
+    """The assembly configuration: Q2 vector Lagrange on a 20 x 10 x nz cube of the unit cube, Gridap's
+    open face tags (face interiors fixed): 52 077 free dofs at nz = 10."""
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+
+    m = CartesianMesh((C0_CELLS[0], C0_CELLS[1], nz))
+    return VectorLagrangeSpace(m, 2, ("x0", "x1"), g=svk_dirichlet(), open_faces=True)
+
+
+def build_case(n, order=2, seed=0):
+    """The matrix-free configuration: Q_order on the n^3 cube (closed faces), the SVK state and a
+    seeded N(0, 1) increment."""
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+
+    V = VectorLagrangeSpace(CartesianMesh((n, n, n)), order, ("x0", "x1"), g=svk_dirichlet())
+    x = svk_state(V, seed)
     dx = np.random.default_rng(seed + 1).standard_normal(V.nfree)
     return V, x, dx
 
@@ -133,12 +166,92 @@ def jv_flops_per_cell(Q, P):
     return 3 * interp + 3 * contract + pointwise
 
 
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Timer:
+    """Device timing on one stream: `steps(fn, K, W)` runs W untimed calls, then K calls each between
+    its own pair of CUDA events (an L2 flush, untimed, before every call when `flush` is set), with a
+    synchronize (and a barrier across ranks) on both sides of the timed calls; returns the summed
+    event time in ms, the max over ranks."""
+
+    def __init__(self, torch, dev, stream, world=1, flush=True):
+        self.torch, self.dev, self.stream, self.world = torch, dev, stream, world
+        self.buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev) if flush else None
+
+    def _sync(self):
+        self.torch.cuda.synchronize()
+        if self.world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            self.torch.cuda.synchronize()
+
+    def steps(self, fn, k, w):
+        torch = self.torch
+        for _ in range(w):
+            if self.buf is not None:
+                self.buf.zero_()
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        self._sync()
+        for e0, e1 in ev:
+            if self.buf is not None:
+                self.buf.zero_()
+            e0.record(self.stream)
+            fn()
+            e1.record(self.stream)
+        self._sync()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+        return self.max_over_ranks(ms)
+
+    def max_over_ranks(self, v):
+        if self.world == 1:
+            return v
+        import torch.distributed as dist
+
+        t = self.torch.tensor([v], dtype=torch_float64(self.torch), device=self.dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(self, v):
+        if self.world == 1:
+            return v
+        import torch.distributed as dist
+
+        t = self.torch.tensor([v], dtype=torch_float64(self.torch), device=self.dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+
+def torch_float64(torch):
+    return torch.float64
+
+
+def c0_problem(world, rank):
+    """(space the rank assembles, its state, free dofs of the whole job, cells it assembles): the
+    C0 space at one rank; at N ranks, rank r's ghost subdomain of the 20 x 10 x 10N mesh."""
+    if world == 1:
+        V = c0_space()
+        return V, svk_state(V), V.nfree, V.mesh.ncells
+    from hfk import distributed as D
+
+    G = c0_space(10 * world)
+    xg = svk_state(G)
+    sub = D.Subdomain(G, D.slab_partition(G.mesh, world), rank, ghost=True)
+    return sub.space, sub.restrict(xg), G.nfree, len(sub.cells)
+
+
 def engine(args):
     import torch
     import torch.distributed as dist
 
     from hfk import _lib, forms
-    from hfk.operator import KernelOperator, MatrixFreeJacobian
+    from hfk.operator import KernelOperator
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -148,20 +261,159 @@ def engine(args):
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    V, x, dx = build_case(args.n)
-    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V, jacobian="matrixfree")
-    stream = torch.cuda.current_stream()
-    op.problem.set_stream(stream.cuda_stream)
-    n = V.nfree
     dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    T = Timer(torch, dev, stream, world)
+
+    # ---- headline: device-resident FP64 CSC Jacobian assembly (C0) ----
+    V, x, nfree_job, ncells = c0_problem(world, rank)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
+    op.problem.set_stream(stream.cuda_stream)
+    nnz = op.sparsity_pattern().nnz
+    xd = torch.from_numpy(x).to(dev)
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+    nz = torch.zeros(nnz, dtype=torch.float64, device=dev)
+    h = op.problem.h
+
+    def step():
+        _lib.call("hfk_jacobian", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
+
+    step()
+    torch.cuda.synchronize()
+    l0 = op.problem.launches()
+    op.problem.set_timing(True)
+    with ClockSampler(local) as clk:
+        ms = T.steps(step, args.steps, args.warmup)
+    k_ms, k_n = op.problem.kernel_time()
+    op.problem.set_timing(False)
+    launches = (op.problem.launches() - l0) // (args.steps + args.warmup) * args.steps
+    ms_step = ms / args.steps
+    value = nfree_job / (ms_step * 1e-3) / 1e9
+    clocks = clk.summary()
+    kernel_ms = T.max_over_ranks(k_ms / max(k_n, 1))
+
+    # ---- e2e: the same assembly through the C ABI with page-locked host buffers ----
+    xh = torch.from_numpy(x).pin_memory()
+    dh = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).pin_memory()
+    nzh = torch.zeros(nnz, dtype=torch.float64).pin_memory()
+
+    def step_e2e():
+        _lib.call("hfk_jacobian", h, _lib.ptr(xh), _lib.ptr(dh), _lib.ptr(nzh))
+
+    k_e2e = max(3, args.steps // 4)
+    ms_e2e = T.steps(step_e2e, k_e2e, 2) / k_e2e
+    e2e_err = float(torch.linalg.norm(nzh.to(dev) - nz) / torch.linalg.norm(nz))
+    e2e = {"value": nfree_job / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": 8 * (V.nfree + V.ndir), "d2h_bytes_per_step": 8 * nnz, "ms_per_step": ms_e2e,
+           "mode": "one synchronous hfk_jacobian per step: state (free + Dirichlet values) H2D, CSC values D2H",
+           "rel_diff_vs_device_resident": e2e_err}
+
+    # ---- roofline of the dominant kernel (the element Jacobian + scatter kernel) ----
+    dmma, dfma = ctypes.c_double(), ctypes.c_double()
+    _lib.call("hfk_device_peak_fp64", ctypes.byref(dmma), ctypes.byref(dfma))
+    flops = C0_FLOPS_PER_CELL * ncells
+    peak = max(dmma.value, dfma.value)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    # DRAM bytes (read + write) of one launch of jacobian_kernel_g<27, true> on this configuration
+    # (ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch)
+    traffic = C0_TRAFFIC_BYTES * ncells / 2000 if C0_TRAFFIC_BYTES else None
+    alg_bytes = 8 * nnz + 4 * 81 * 81 * ncells + 4 * 81 * ncells + 8 * (V.nfree + V.ndir)
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "jacobian_kernel_g<27,true> (FP64 mma m8n8k4 element products)",
+                "kernel_ms": kernel_ms, "flops_per_launch": flops,
+                "flops_source": "benchmark/roofline.jl:65-74: 1 180 980 FP64 flops per Q2 cell (products + G)",
+                "peak_source": "FP64 measured in-process on this GPU (hfk_device_peak_fp64: mma m8n8k4 f64 "
+                               f"{dmma.value:.1f} TFLOP/s, DFMA {dfma.value:.1f} TFLOP/s); the measured-peaks file "
+                               "has no FP64 figure",
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "hbm_frac": alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak()[0],
+                "traffic_source": "ncu one launch, this configuration" if traffic else None}
+
+    extra = {}
+    if not args.no_extra and world == 1:
+        extra.update(assembly_extra(torch, dev, stream, op, xd, dd, nz, T))
+        del op
+        torch.cuda.empty_cache()
+        extra.update(jv_headline_case(torch, dev, stream, T, cpu=not args.no_cpu))
+        extra.update(jv_sizes_case(torch, dev, stream, T.steps))
+        extra.update(oseen_case(torch, dev, stream, T.steps))
+        extra.update(newton_case())
+
+    cpu = c0_cpu_baseline(budget_s=15.0) if world == 1 and not args.no_cpu else None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "cells_per_gpu": ncells, "free_dofs": nfree_job, "nnz_rank0": int(nnz),
+                           "quadrature_points_per_cell": 27, "qps": 27 * ncells * world / (ms_step * 1e-3),
+                           "parallelism": "1 GPU" if world == 1 else
+                           f"owner-computes z-slabs of a 20x10x{10 * world} mesh over {world} GPUs, no exchange",
+                           "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MB written; the step "
+                                 "touches about 125 MB)",
+                           "state": "u = 0.05 x e_x + U(-1e-3, 1e-3) on the free dofs, seed 0"},
+                "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+                "cpu_baseline": cpu, "extra": extra}
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# DRAM traffic of one jacobian_kernel_g launch on the 20x10x10 case (ncu, per launch); None = not captured
+C0_TRAFFIC_BYTES = None
+
+
+def assembly_extra(torch, dev, stream, op, xd, dd, nz, T):
+    """Secondary C0 figures: the residual, the bit-reproducible colour-by-colour scatter, and the
+    relative difference of the CSC values from the CPU restatement."""
+    from hfk import _lib
+
+    V = op.U
+    h = op.problem.h
+    b = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
+    ms_r = T.steps(lambda: _lib.call("hfk_residual", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(b)), 20, 3) / 20
+    op.problem.set_scatter("coloured")
+    ms_jc = T.steps(lambda: _lib.call("hfk_jacobian", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz)), 20, 3) / 20
+    nz_c = nz.cpu().numpy().copy()
+    op.problem.set_scatter("auto")
+    _lib.call("hfk_jacobian", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hfk.fespace import Quadrature
+
+    orc = O.OracleProblem(V, Quadrature.gauss(4))
+    orc.pattern()
+    x = xd.cpu().numpy()
+    d = np.ascontiguousarray(V.dirichlet_values)
+    ref = orc.jacobian_values(x, d)
+    rref = orc.residual(x, d)
+    got = nz.cpu().numpy()
+    return {"assembly_q2_20x10x10": {
+        "residual_ms": ms_r, "jacobian_coloured_ms": ms_jc,
+        "rel_diff_vs_cpu": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+        "rel_diff_coloured_vs_cpu": float(np.linalg.norm(nz_c - ref) / np.linalg.norm(ref)),
+        "residual_rel_diff_vs_cpu": float(np.linalg.norm(b.cpu().numpy() - rref) / np.linalg.norm(rref))}}
+
+
+def jv_headline_case(torch, dev, stream, T, n=JV_CELLS, cpu=True, launch="auto"):
+    """The matrix-free configuration: FP64 recompute J*v on the Q2 n^3 cube (6.34 M free dofs at
+    n = 64) with inputs resident in HBM, through the C ABI with host vectors (e2e), the roofline of
+    its cell kernel, the FP32 and the stored-tangent products, and the CPU restatement's
+    stored-tangent product on the same mesh."""
+    from hfk import _lib, forms
+    from hfk.operator import KernelOperator, MatrixFreeJacobian
+
+    V, x, dx = build_case(n)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V, jacobian="matrixfree")
+    op.problem.set_stream(stream.cuda_stream)
+    nfree = V.nfree
     xd = torch.from_numpy(x).to(dev)
     dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
     dxd = torch.from_numpy(dx).to(dev)
-    yd = torch.zeros(n, dtype=torch.float64, device=dev)
-    if args.launch != "auto":
+    yd = torch.zeros(nfree, dtype=torch.float64, device=dev)
+    if launch != "auto":
         op.problem.set_scatter("atomic")
-        op.problem.set_launch("point" if args.launch == "point" else "line",
-                              0 if args.launch == "point" else int(args.launch[-1]))
+        op.problem.set_launch("point" if launch == "point" else "line", 0 if launch == "point" else int(launch[-1]))
     mf = MatrixFreeJacobian(op, "recompute")
     mf.prepare(xd, dd)
     h = op.problem.h
@@ -169,126 +421,79 @@ def engine(args):
     def step():
         _lib.call("hfk_mf_apply", h, _lib.ptr(dxd), _lib.ptr(yd))
 
-    def timed(fn, steps, warm):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
-
-    # ---- headline: device-resident FP64 J*v ----
     step()
-    torch.cuda.synchronize()
-    l0 = op.problem.launches()
-    with ClockSampler(local) as clk:
-        ms = timed(step, args.steps, args.warmup)
-    launches = (op.problem.launches() - l0) // (args.steps + args.warmup) * args.steps
-    ms_step = ms / args.steps
-    value = world * n / (ms_step * 1e-3) / 1e9
-    clocks = clk.summary()
-
-    # ---- e2e: host (pinned) buffers through the public ABI, H2D + D2H of every step's vector ----
-    # a stream of K host vectors in one hfk_mf_apply_many call (the copies of one vector overlap the
-    # product of the next), inputs and outputs cycling through a ring of pinned buffers
+    op.problem.set_timing(True)
+    steps = 100
+    ms = T.steps(step, steps, 3) / steps
+    k_ms, k_n = op.problem.kernel_time()
+    op.problem.set_timing(False)
+    kernel_ms = k_ms / max(k_n, 1)
+    ncells = V.mesh.ncells
+    alg_bytes = 4 * V.ndl * ncells + 8 * nfree * 3 + 72 * 27 * ncells + 81 * ncells
+    hbm, src = hbm_peak()
+    flops = jv_flops_per_cell(3, 3) * ncells
+    out = {"free_dofs": nfree, "ms": ms, "gdofs": nfree / (ms * 1e-3) / 1e9, "kernel_ms": kernel_ms,
+           "roofline": {"bound": "hbm", "achieved": alg_bytes / (kernel_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm, "peak_source": src,
+                        "bytes_per_launch": alg_bytes, "fp64_tflops": flops / (kernel_ms * 1e-3) / 1e12}}
+    # e2e: a stream of host vectors in one hfk_mf_apply_many call (the copies of one vector overlap
+    # the product of the next), and one synchronous hfk_mf_apply per vector
     ring = 4
     dxh = [torch.from_numpy(dx).pin_memory() for _ in range(ring)]
-    yh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(ring)]
-    k_e2e = max(3, args.steps // 2)
+    yh = [torch.zeros(nfree, dtype=torch.float64).pin_memory() for _ in range(ring)]
+    k_e2e = 60
     pin = (ctypes.c_void_p * k_e2e)(*[dxh[i % ring].data_ptr() for i in range(k_e2e)])
     pout = (ctypes.c_void_p * k_e2e)(*[yh[i % ring].data_ptr() for i in range(k_e2e)])
+    ms_many = T.steps(lambda: _lib.call("hfk_mf_apply_many", h, k_e2e, ctypes.cast(pin, ctypes.c_void_p),
+                                        ctypes.cast(pout, ctypes.c_void_p)), 1, 1) / k_e2e
+    ms_single = T.steps(lambda: _lib.call("hfk_mf_apply", h, _lib.ptr(dxh[0]), _lib.ptr(yh[0])), 20, 2) / 20
+    out["e2e"] = {"value": nfree / (ms_many * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * nfree,
+                  "d2h_bytes_per_step": 8 * nfree, "ms_per_step": ms_many,
+                  "mode": f"{k_e2e} host vectors per hfk_mf_apply_many call (pinned ring of {ring})",
+                  "single_call_gdofs": nfree / (ms_single * 1e-3) / 1e9,
+                  "rel_diff_vs_device_resident": float(torch.linalg.norm(yh[0].to(dev) - yd) / torch.linalg.norm(yd))}
+    # FP32 and the stored (reference) formulation
+    dx32 = dxd.float()
+    y32 = torch.zeros(nfree, dtype=torch.float32, device=dev)
+    ms32 = T.steps(lambda: _lib.call("hfk_mf_apply_f32", h, _lib.ptr(dx32, np.float32), _lib.ptr(y32, np.float32)),
+                   50, 3) / 50
+    step()
+    torch.cuda.synchronize()
+    out["fp32"] = {"ms": ms32, "gdofs": nfree / (ms32 * 1e-3) / 1e9,
+                   "rel_err_vs_fp64": float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))}
+    out["autotuned_launch_shape"] = {k: op.problem.tuning(*k.split("_")) for k in ("jv_fp64", "jv_fp32")}
+    y64 = yd.cpu().numpy()
+    mfs = MatrixFreeJacobian(op, "stored")
+    mfs.prepare(xd, dd)
+    ms_s = T.steps(step, 30, 3) / 30
+    stored_bytes = 8 * 91 * 27 * ncells + 8 * nfree * 2 + 4 * V.ndl * ncells
+    out["stored_fp64"] = {"ms": ms_s, "gdofs": nfree / (ms_s * 1e-3) / 1e9,
+                          "hbm_frac": stored_bytes / (ms_s * 1e-3) / 1e9 / hbm}
+    del mf, mfs, op, xd, dd, dxd, yd, dx32, y32
+    torch.cuda.empty_cache()
+    if cpu:
+        # the CPU restatement of the reference's mul! (stored tangents, OpenMP, all host cores) on
+        # the same mesh, state and increment
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        from hfk.fespace import Quadrature
 
-    def step_e2e_many():
-        _lib.call("hfk_mf_apply_many", h, k_e2e, ctypes.cast(pin, ctypes.c_void_p), ctypes.cast(pout, ctypes.c_void_p))
-
-    ms_e2e = timed(step_e2e_many, 1, 1) / k_e2e
-    e2e_err = max(float(torch.linalg.norm(y.to(dev) - yd) / torch.linalg.norm(yd)) for y in yh[:min(ring, k_e2e)])
-
-    def step_e2e():  # one vector per synchronous call: copy in, product, copy out
-        _lib.call("hfk_mf_apply", h, _lib.ptr(dxh[0]), _lib.ptr(yh[0]))
-
-    ms_single = timed(step_e2e, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
-    e2e = {"value": world * n / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
-           "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e,
-           "mode": f"{k_e2e} host vectors per hfk_mf_apply_many call (pinned ring of {ring})",
-           "rel_err_vs_device_resident": e2e_err,
-           "single_call": {"value": world * n / (ms_single * 1e-3) / 1e9, "ms_per_step": ms_single}}
-
-    # ---- roofline of the dominant kernel (colour launches of the J*v cell kernel) ----
-    ncells = V.mesh.ncells
-    # ids, dx read, y read+write, F per point (prepared deformation gradient), per-cell geometry
-    alg_bytes = 4 * V.ndl * ncells + 8 * n * 3 + 72 * 27 * ncells + 81 * ncells
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        hbm, src = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
-        hbm, src = 6650.0, "fallback"
-    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
-    flops = jv_flops_per_cell(3, 3) * ncells
-    # DRAM bytes (read + write) of one launch of this kernel and launch shape from an ncu capture of
-    # the 48^3 case (110 592 cells: 302.7 MB + 22.5 MB), scaled by cells; the profile summary gives
-    # the capture's command
-    traffic = (302.712e6 + 22.487e6) * ncells / 110592 if ORDER == 2 else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, Q2 48^3 "
-                "launch, scaled by cells", "peak_source": src, "bytes_per_launch": alg_bytes,
-                "fp64_tflops": flops / (ms_step * 1e-3) / 1e12, "fp64_flops_per_launch": flops,
-                "note": "recompute J*v is latency/FP64-issue bound; hbm frac uses the algorithmic bytes"}
-
-    extra = {}
-    if not args.no_extra and rank == 0:
-        # reference formulation on the GPU: stored tangents (T, inv(Jt), dV per point)
-        mfs = MatrixFreeJacobian(op, "stored")
-        mfs.prepare(xd, dd)
-        ms_s = timed(step, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
-        stored_bytes = 8 * 91 * 27 * ncells + 8 * n * 2 + 4 * V.ndl * ncells
-        extra["jv_stored_fp64"] = {"gdofs": n / (ms_s * 1e-3) / 1e9, "ms": ms_s,
-                                   "hbm_frac": stored_bytes / (ms_s * 1e-3) / 1e9 / hbm}
-        mf.prepare(xd, dd)
-        dx32 = dxd.float()
-        y32 = torch.zeros(n, dtype=torch.float32, device=dev)
-
-        def step32():
-            _lib.call("hfk_mf_apply_f32", h, _lib.ptr(dx32, np.float32), _lib.ptr(y32, np.float32))
-
-        ms32 = timed(step32, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
-        step()
-        torch.cuda.synchronize()
-        err32 = float(torch.linalg.norm(y32.double() - yd) / torch.linalg.norm(yd))
-        extra["jv_recompute_fp32"] = {"gdofs": n / (ms32 * 1e-3) / 1e9, "ms": ms32, "rel_err_vs_fp64": err32}
-        extra["autotuned_launch_shape"] = {k: op.problem.tuning(*k.split("_")) for k in ("jv_fp64", "jv_fp32")}
-        extra.update(assembly_case(torch, dev, stream, timed))
-        extra.update(jv_sizes_case(torch, dev, stream, timed))
-        extra.update(oseen_case(torch, dev, stream, timed))
-        extra.update(newton_case())
-
-    cpu = cpu_baseline_sample() if rank == 0 and not args.no_cpu else None
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "cells": ncells, "free_dofs_per_gpu": n, "order": ORDER,
-                           "quadrature_points_per_cell": 27, "parallelism": f"replicas x{world}",
-                           "l2": f"inputs larger than L2 ({alg_bytes / 1e6:.0f} MB read per step, L2 126 MB)",
-                           "state": "u = 0.05 x e_x + U(-1e-3, 1e-3), dx ~ N(0,1), seeds 0/1"},
-                "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "extra": extra}
-        print(json.dumps(line))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+        p = O.OracleProblem(V, Quadrature.gauss(4))
+        t0 = time.perf_counter()
+        p.mf_prepare(x, V.dirichlet_values)
+        t_prep = time.perf_counter() - t0
+        yr = p.mf_apply(dx)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            p.mf_apply(dx)
+            ts.append(time.perf_counter() - t0)
+        t = min(ts)
+        out["cpu"] = {"gdofs": nfree / t / 1e9, "ms": 1e3 * t, "prepare_ms": 1e3 * t_prep, "cores": O.lib().o_max_threads(),
+                      "kind": "port", "rel_diff_engine_vs_cpu": float(np.linalg.norm(y64 - yr) / np.linalg.norm(yr)),
+                      "sample": f"full Q2 {n}^3 ({nfree} free dofs), stored-tangent mul!, best of 5"}
+        del p
+    return {f"jv_q2_{n}": out}
 
 
 def jv_sizes_case(torch, dev, stream, timed, cases=((2, 48), (4, 48), (4, 64))):
@@ -378,29 +583,37 @@ def oseen_case(torch, dev, stream, timed, n=32, cpu_n=12):
                                   "speedup_jacobian_vs_cpu": 1e3 * tj * scale / ms_j}}
 
 
-def oseen_main(args):
-    """The Oseen assembly alone (``--oseen N``), or the Q2 SVK 20x10x10 CSC assembly alone
-    (``--assembly``), one JSON line: the cases for profiling their kernels."""
+def profile_main(args):
+    """One case alone, one JSON line, for profiling its kernel: ``--assembly`` (the Q2 SVK 20x10x10
+    residual + CSC Jacobian, 20 steps each), ``--jv N`` (the Q2 N^3 matrix-free product, FP64 and
+    FP32) or ``--oseen N`` (the Oseen P2-P1 assembly on the N^3 tetrahedral cube)."""
     import torch
 
+    from hfk import _lib, forms
+    from hfk.operator import KernelOperator
+
+    dev = torch.device("cuda")
     stream = torch.cuda.current_stream()
-
-    def timed(fn, steps, warm):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
+    T = Timer(torch, dev, stream, 1, flush=False)
     if args.assembly:
-        out = assembly_case(torch, torch.device("cuda"), stream, timed)
+        V = c0_space()
+        x = svk_state(V)
+        op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
+        op.problem.set_stream(stream.cuda_stream)
+        nnz = op.sparsity_pattern().nnz
+        xd = torch.from_numpy(x).to(dev)
+        dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
+        nz = torch.zeros(nnz, dtype=torch.float64, device=dev)
+        b = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
+        ms_j = T.steps(lambda: _lib.call("hfk_jacobian", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz)),
+                       20, 3) / 20
+        ms_r = T.steps(lambda: _lib.call("hfk_residual", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(b)),
+                       20, 3) / 20
+        out = {"case": "assembly Q2 SVK 20x10x10", "jacobian_ms": ms_j, "residual_ms": ms_r, "nnz": int(nnz)}
+    elif args.jv:
+        out = jv_headline_case(torch, dev, stream, T, n=args.jv, cpu=False, launch=args.launch)
     else:
-        out = oseen_case(torch, torch.device("cuda"), stream, timed, n=args.oseen, cpu_n=min(args.oseen, 8))
+        out = oseen_case(torch, dev, stream, T.steps, n=args.oseen, cpu_n=min(args.oseen, 8))
     print(json.dumps(out))
 
 
@@ -439,76 +652,6 @@ def vcycle_main(args, n=16):
     print(json.dumps({"case": f"V-cycle SVK Q4 {n}^3 -> Q2 -> Q1", "free_dofs": Vs[0].nfree,
                       "coarse_free_dofs": Vs[2].nfree, "cycles": args.vcycle,
                       "ms_per_cycle": e0.elapsed_time(e1) / args.vcycle}))
-
-
-def assembly_case(torch, dev, stream, timed):
-    """Secondary: Q2 SVK 20x10x10 residual + CSC Jacobian (the reference's CPU-runnable case)."""
-    from hfk import _lib, forms
-    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
-    from hfk.operator import KernelOperator
-
-    m = CartesianMesh((20, 10, 10))
-    g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
-    V = VectorLagrangeSpace(m, 2, ("x0", "x1"), g=g, open_faces=True)  # Gridap face tags: 52 077 free dofs
-    rng = np.random.default_rng(0)
-    x, _ = V.interpolate(lambda p: np.stack([0.05 * p[:, 0], 0 * p[:, 0], 0 * p[:, 0]], axis=1))
-    x = x + rng.uniform(-1e-3, 1e-3, V.nfree)
-    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
-    op.problem.set_stream(stream.cuda_stream)
-    op.sparsity_pattern()
-    nnz = op.sparsity_pattern().nnz
-    xd = torch.from_numpy(x).to(dev)
-    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
-    nz = torch.zeros(nnz, dtype=torch.float64, device=dev)
-    b = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
-    h = op.problem.h
-
-    def jac():
-        _lib.call("hfk_jacobian", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
-
-    def res():
-        _lib.call("hfk_residual", h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(b))
-
-    ms_j = timed(jac, 10, 3) / 10
-    ms_r = timed(res, 10, 3) / 10
-    # the bit-reproducible colour-by-colour scatter (HFK_SCATTER_COLOURED) for comparison
-    op.problem.set_scatter("coloured")
-    ms_jc = timed(jac, 10, 3) / 10
-    nz_c = nz.clone()
-    op.problem.set_scatter("auto")
-    jac()
-    # the same assembly by the CPU restatement of the reference algorithm (matrix-product element
-    # Jacobian with point blocks of 12, colour loop, OpenMP on all host cores), best of 5
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    from hfk.fespace import Quadrature
-
-    orc = O.OracleProblem(V, Quadrature.gauss(4))
-    orc.pattern()
-    d = np.ascontiguousarray(V.dirichlet_values)
-    orc.jacobian_values(x, d)
-    tj, tr = [], []
-    for _ in range(5):
-        t0 = time.perf_counter()
-        orc.jacobian_values(x, d)
-        tj.append(time.perf_counter() - t0)
-        t0 = time.perf_counter()
-        orc.residual(x, d)
-        tr.append(time.perf_counter() - t0)
-    ref = orc.jacobian_values(x, d)
-    got = nz.cpu().numpy()
-    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    cpu_j, cpu_r = 1e3 * min(tj), 1e3 * min(tr)
-    err_c = float(np.linalg.norm(nz_c.cpu().numpy() - ref) / np.linalg.norm(ref))
-    return {"assembly_q2_20x10x10": {"free_dofs": V.nfree, "nnz": int(nnz), "jacobian_ms": ms_j, "residual_ms": ms_r,
-                                     "jacobian_coloured_ms": ms_jc, "rel_err_coloured_vs_cpu": err_c,
-                                     "jacobian_gdofs": V.nfree / (ms_j * 1e-3) / 1e9,
-                                     "jacobian_qps": 27 * V.mesh.ncells / (ms_j * 1e-3),
-                                     "cpu_jacobian_ms": cpu_j, "cpu_residual_ms": cpu_r,
-                                     "cpu_cores": O.lib().o_max_threads(), "cpu_kind": "port",
-                                     "speedup_jacobian_vs_cpu": cpu_j / ms_j,
-                                     "speedup_residual_jacobian_vs_cpu": (cpu_j + cpu_r) / (ms_j + ms_r),
-                                     "rel_err_vs_cpu": err}}
 
 
 def newton_case(n=16, loads=(0.1, 0.325, 0.55, 0.775, 1.0)):
@@ -560,56 +703,63 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline_sample(budget_s=15.0):
-    """Oracle (CPU restatement, stored-tangent J*v as the reference) on a bounded sample: Q2 24^3."""
+def c0_oracle():
+    """The CPU restatement on the C0 configuration: (oracle problem, state, Dirichlet values, free dofs)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from hfk.fespace import Quadrature
 
-    nsub = 24
-    V, x, dx = build_case(nsub)
-    p = O.OracleProblem(V, Quadrature.gauss(4))
-    p.mf_prepare(x, V.dirichlet_values)
-    p.mf_apply(dx)
+    V = c0_space()
+    orc = O.OracleProblem(V, Quadrature.gauss(4))
+    orc.pattern()
+    return O, orc, svk_state(V), np.ascontiguousarray(V.dirichlet_values), V.nfree
+
+
+def c0_cpu_baseline(budget_s=15.0):
+    """The CPU restatement (jacobian!: zero-fill, matrix-product element Jacobians, colour loop,
+    OpenMP on all host cores) on the full C0 configuration, repeated until ``budget_s``."""
+    O, orc, x, d, nfree = c0_oracle()
+    orc.jacobian_values(x, d)
     t0 = time.perf_counter()
     k = 0
+    ts = []
     while True:
-        p.mf_apply(dx)
+        t1 = time.perf_counter()
+        orc.jacobian_values(x, d)
+        ts.append(time.perf_counter() - t1)
         k += 1
-        if time.perf_counter() - t0 > budget_s or k >= 50:
+        if time.perf_counter() - t0 > budget_s or k >= 200:
             break
-    t = (time.perf_counter() - t0) / k
-    return {"value": V.nfree / t / 1e9, "unit": UNIT, "cores": O.lib().o_max_threads(), "kind": "port",
-            "sample": f"Q2 {nsub}^3 ({V.nfree} free dofs), {k} stored-tangent J*v applies, OpenMP all host cores"}
+    t = statistics.median(ts)
+    return {"value": nfree / t / 1e9, "unit": UNIT, "cores": O.lib().o_max_threads(), "kind": "port",
+            "ms_per_assembly": 1e3 * t,
+            "sample": f"the full configuration (Q2 SVK 20x10x10, {nfree} free dofs), {k} CSC Jacobian assemblies, "
+                      "median"}
 
 
 def reference(args):
+    """The reference arm: the CPU restatement of the reference's jacobian! (the oracle, all host
+    cores) on the headline configuration, one assembly per step; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    from hfk.fespace import Quadrature
-
-    # bounded sample of the workload per step: Q2 24^3 (1/19 of the cells), the reference's formulation
-    nsub = 24
-    V, x, dx = build_case(nsub)
-    p = O.OracleProblem(V, Quadrature.gauss(4))
-    p.mf_prepare(x, V.dirichlet_values)
+    O, orc, x, d, nfree = c0_oracle()
     for _ in range(max(1, args.warmup)):
-        p.mf_apply(dx)
+        orc.jacobian_values(x, d)
+    steps = min(args.steps, 200)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        p.mf_apply(dx)
-    t = (time.perf_counter() - t0) / args.steps
-    value = V.nfree / t / 1e9
+    for _ in range(steps):
+        orc.jacobian_values(x, d)
+    t = (time.perf_counter() - t0) / steps
+    value = nfree / t / 1e9
     cores = O.lib().o_max_threads()
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": f"Q2 {nsub}^3 per step"},
+            "config": {"workload": WORKLOAD, "cells": 2000, "free_dofs": nfree, "quadrature_points_per_cell": 27},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"Q2 {nsub}^3 ({V.nfree} free dofs) stored-tangent J*v per step"},
+                             "sample": f"the full configuration, {steps} CSC Jacobian assemblies (zero-fill "
+                                       "included), OpenMP on all host cores"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -809,8 +959,8 @@ if __name__ == "__main__":
         reference(a)
     elif a.batch:
         batch_main(a)
-    elif a.oseen or a.assembly:
-        oseen_main(a)
+    elif a.oseen or a.assembly or a.jv:
+        profile_main(a)
     elif a.vcycle:
         vcycle_main(a)
     else:

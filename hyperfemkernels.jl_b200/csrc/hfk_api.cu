@@ -17,6 +17,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 
+#include "devcache.h"
 #include "hfk_internal.h"
 #include "kern_assembly.cuh"
 #include "kern_band.cuh"
@@ -40,30 +41,17 @@ thread_local std::string g_last_error;
 void set_error(const std::string& m) { g_last_error = m; }
 }  // namespace hfk
 
-#define HFK_API_BEGIN try {
-#define HFK_API_END                                     \
-  return HFK_OK;                                        \
-  }                                                     \
-  catch (const hfk::Error& e) {                         \
-    hfk::set_error(e.msg);                              \
-    return e.code;                                      \
-  }                                                     \
-  catch (const std::exception& e) {                     \
-    hfk::set_error(std::string("HyperFEMKernels: ") + e.what()); \
-    return HFK_ERR_INTERNAL;                            \
-  }
-
 namespace {
 
-int g_sm_count = 0;
+PerDeviceValue g_sm_count;
 int sm_count() {
-  if (!g_sm_count) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 148;
-  }
-  return g_sm_count;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return g_sm_count.get(dev, [dev] {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  });
 }
 inline int vec_grid(int64_t n, int threads = 256) {
   int64_t g = (n + threads - 1) / threads;
@@ -111,18 +99,26 @@ void check_launch(hfk_problem* p) {
   HFK_CUDA(cudaGetLastError());
 }
 
-// Raise a kernel's dynamic shared-memory limit to at least `smem` (`limit` caches what was set). The
-// limit only grows, under one lock: handles may be used from several host threads (one handle per
-// thread), and a thread about to launch with a large limit must not see it lowered by a thread that
-// needs less.
-std::mutex g_smem_limit_mu;
-template <typename K>
-void raise_smem_limit(K kernel, size_t smem, size_t& limit) {
-  std::lock_guard<std::mutex> lock(g_smem_limit_mu);
-  if (smem > limit) {
-    HFK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    limit = smem;
+// Kernel timing: an event before and after an element-kernel launch sequence (only with timing on)
+void ktimer_mark(hfk_problem* p) {
+  if (!p->ktiming) return;
+  if (p->kev_used == p->kev.size()) {
+    cudaEvent_t e;
+    HFK_CUDA(cudaEventCreate(&e));
+    p->kev.push_back(e);
   }
+  HFK_CUDA(cudaEventRecord(p->kev[p->kev_used++], p->stream));
+}
+
+// Raise a kernel's dynamic shared-memory limit on the current device to at least `smem` (`limit`
+// records, per device, what was set).
+template <typename K>
+void raise_smem_limit(K kernel, size_t smem, PerDeviceLimit& limit) {
+  int dev = 0;
+  HFK_CUDA(cudaGetDevice(&dev));
+  limit.raise(dev, smem, [&] {
+    HFK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  });
 }
 
 // ---- 1D Lagrange basis on [0,1], equispaced nodes (lagrange1d, src/tensorproduct.jl:24-47) ----
@@ -263,7 +259,7 @@ template <int Q, int P, int MODE, typename R>
 void launch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int warps) {
   using S = TPShape<Q, P>;
   const size_t smem = cell_smem_bytes<Q, P, R>(warps);
-  static size_t attr = 0;
+  static PerDeviceLimit attr;
   raise_smem_limit(cell_kernel<Q, P, MODE, R>, smem, attr);
   const int per_cta = warps * S::CPW;
   const int grid = (ncl + per_cta - 1) / per_cta;
@@ -277,7 +273,7 @@ template <int Q, int P, typename R, int NT>
 void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
   using S = JvpShape<Q, P, NT>;
   const size_t smem = jvp_smem_bytes<Q, P, R, NT>();
-  static size_t attr = 0;
+  static PerDeviceLimit attr;
   raise_smem_limit(jvp_kernel<Q, P, R, NT>, smem, attr);
   const int grid = (ncl + S::C - 1) / S::C;
   if (grid == 0) return;
@@ -334,16 +330,18 @@ bool use_atomic_scatter(const hfk_problem* p) {
 
 template <int MODE, typename R>
 void run_cells_as(hfk_problem* p, CellIO<R> io, bool atomic, int warps) {
+  ktimer_mark(p);
   if (atomic) {
     io.atomic = 1;
     dispatch_cell<MODE, R>(p, nullptr, p->ncells, io, warps);
-    return;
+  } else {
+    io.atomic = 0;
+    for (int c = 0; c < p->ncolors; ++c) {
+      const int n = p->color_start[c + 1] - p->color_start[c];
+      dispatch_cell<MODE, R>(p, p->cells_by_color.p + p->color_start[c], n, io, warps);
+    }
   }
-  io.atomic = 0;
-  for (int c = 0; c < p->ncolors; ++c) {
-    const int n = p->color_start[c + 1] - p->color_start[c];
-    dispatch_cell<MODE, R>(p, p->cells_by_color.p + p->color_start[c], n, io, warps);
-  }
+  ktimer_mark(p);
 }
 
 // Launch-shape autotuner (per problem, per kernel mode and precision, so per degree): on the first
@@ -729,7 +727,7 @@ void invert_blocks_and_check(hfk_problem* p, int* ok) {
 template <int Q, int P>
 void blocks_tp_launch(hfk_problem* p, BlockIO io) {
   const size_t smem = blocks_tp_smem<Q, P>();
-  static size_t attr = 0;
+  static PerDeviceLimit attr;
   raise_smem_limit(blocks_tp_kernel<Q, P>, smem, attr);
   const Tab1D<double> tab = make_tab<double>(p);
   if (use_atomic_scatter(p)) {
@@ -785,7 +783,7 @@ void blocks_update_dev(hfk_problem* p, int* ok) {
     return;
   }
   const size_t smem = ((size_t)3 * p->nn + 9 * p->np + 9 * p->np + p->np + 81 * p->np) * sizeof(double);
-  static size_t attr = 0;
+  static PerDeviceLimit attr;
   raise_smem_limit(blocks_kernel, smem, attr);
   if (use_atomic_scatter(p)) {  // one launch over all cells, atomic accumulation of the blocks
     io.atomic = 1;
@@ -1284,10 +1282,10 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   HFK_REQUIRE(smem <= 227 * 1024, HFK_ERR_UNSUPPORTED, "too many quadrature points for the assembly kernel");
   HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
   if (g) {
-    static size_t attr[2] = {0, 0};
+    static PerDeviceLimit attr[2];
     raise_smem_limit(padded ? jacobian_kernel_g<27, true> : jacobian_kernel_g<27, false>, smem, attr[padded]);
   } else {
-    static size_t attr = 0;
+    static PerDeviceLimit attr;
     raise_smem_limit(jacobian_kernel_direct<8>, smem, attr);
   }
   auto launch = [&](const int32_t* cells, int n) {
@@ -1301,14 +1299,16 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   // may then add to the same nonzero, in an order that can change the last bit from run to run; by
   // colour (HFK_SCATTER_COLOURED) the adds of one nonzero come one launch after another, in colour
   // order, and the result is reproducible bit for bit
+  ktimer_mark(p);
   if (use_atomic_scatter(p)) {
     if (p->ncells) launch(nullptr, p->ncells);
-    return;
+  } else {
+    for (int c = 0; c < p->ncolors; ++c) {
+      const int n = p->color_start[c + 1] - p->color_start[c];
+      if (n) launch(p->cells_by_color.p + p->color_start[c], n);
+    }
   }
-  for (int c = 0; c < p->ncolors; ++c) {
-    const int n = p->color_start[c + 1] - p->color_start[c];
-    if (n) launch(p->cells_by_color.p + p->color_start[c], n);
-  }
+  ktimer_mark(p);
 }
 
 void residual_dev(hfk_problem* p, const double* u, const double* dvals, double* b) {
@@ -1983,12 +1983,8 @@ void mlp_correct(hfk_pmg* m, const double* r, double* y) {
   const int nb = mlp_prepare_features(m, r, y);
   m->ml_out.resize((size_t)nb * MLP_OUT);
   m->ml_delta.resize(n);
-  static bool attr = false;
-  if (!attr) {
-    HFK_CUDA(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(MLP_NPARAM * sizeof(float))));
-    attr = true;
-  }
+  static PerDeviceLimit attr;
+  raise_smem_limit(mlp_forward_kernel, MLP_NPARAM * sizeof(float), attr);
   mlp_forward_kernel<<<vec_grid(nb, 128), 128, MLP_NPARAM * sizeof(float), p->stream>>>(nb, m->mlp->wb.p, m->ml_feats.p,
                                                                                        m->ml_out.p);
   check_launch(p);
@@ -2144,6 +2140,7 @@ int hfk_problem_destroy(hfk_problem* p) {
     }
   for (cudaEvent_t e : p->many_ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->kev) cudaEventDestroy(e);
   delete p;
   HFK_API_END
 }
@@ -2226,6 +2223,30 @@ int hfk_launch_count(hfk_problem* p, int64_t* count) {
   HFK_API_BEGIN
   HFK_REQUIRE(p && count, HFK_ERR_ARG, "null argument");
   *count = p->launches;
+  HFK_API_END
+}
+
+int hfk_problem_set_timing(hfk_problem* p, int on) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p, HFK_ERR_ARG, "null argument");
+  p->ktiming = on != 0;
+  p->kev_used = 0;
+  HFK_API_END
+}
+
+int hfk_problem_kernel_time(hfk_problem* p, double* ms, int64_t* count) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && ms && count, HFK_ERR_ARG, "null argument");
+  double total = 0;
+  if (p->kev_used) HFK_CUDA(cudaEventSynchronize(p->kev[p->kev_used - 1]));
+  for (size_t i = 0; i + 1 < p->kev_used; i += 2) {
+    float t = 0;
+    HFK_CUDA(cudaEventElapsedTime(&t, p->kev[i], p->kev[i + 1]));
+    total += t;
+  }
+  *ms = total;
+  *count = (int64_t)(p->kev_used / 2);
+  p->kev_used = 0;
   HFK_API_END
 }
 
@@ -3658,11 +3679,8 @@ void mlp_upload(hfk_mlp* m, const float* w_host) {
 }
 
 void mlp_grad_dev(hfk_mlp* m, const float* feats, const float* targets, int64_t n, float* grad, float* loss) {
-  static bool attr = false;
-  if (!attr) {
-    HFK_CUDA(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_grad_smem_bytes()));
-    attr = true;
-  }
+  static PerDeviceLimit attr;
+  raise_smem_limit(mlp_grad_kernel, mlp_grad_smem_bytes(), attr);
   HFK_CUDA(cudaMemsetAsync(grad, 0, MLP_NPARAM * sizeof(float), m->stream));
   HFK_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), m->stream));
   const int64_t chunks = (n + MLP_CHUNK - 1) / MLP_CHUNK;
@@ -3902,7 +3920,7 @@ OseenData oseen_data(hfk_oseen* o, const int32_t* cells, int n) {
 void oseen_run(hfk_oseen* o, OseenIO io) {
   hfk_problem* p = &o->base;
   const size_t smem = (size_t)OseenSmem{o->nq}.total() * sizeof(double);
-  static size_t attr = 0;
+  static PerDeviceLimit attr;
   raise_smem_limit(oseen_kernel, smem, attr);
   if (use_atomic_scatter(p)) {
     io.atomic = 1;

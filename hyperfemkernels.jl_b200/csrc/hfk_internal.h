@@ -30,6 +30,20 @@ struct Error {
     if (!(cond)) throw ::hfk::Error{code, std::string("HyperFEMKernels: ") + (msg)}; \
   } while (0)
 
+// ABI entry points: body between HFK_API_BEGIN and HFK_API_END; errors become a status + message
+#define HFK_API_BEGIN try {
+#define HFK_API_END                                     \
+  return HFK_OK;                                        \
+  }                                                     \
+  catch (const hfk::Error& e) {                         \
+    hfk::set_error(e.msg);                              \
+    return e.code;                                      \
+  }                                                     \
+  catch (const std::exception& e) {                     \
+    hfk::set_error(std::string("HyperFEMKernels: ") + e.what()); \
+    return HFK_ERR_INTERNAL;                            \
+  }
+
 // ---- a device buffer owned by a handle ---------------------------------------------------
 template <typename T>
 struct DBuf {
@@ -202,6 +216,10 @@ struct hfk_problem {
   hfk::DBuf<int> flag;
   // timing of the last kernel sequence (CUDA events)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // kernel timing (hfk_problem_set_timing): event pairs around the element-kernel launches
+  bool ktiming = false;
+  std::vector<cudaEvent_t> kev;
+  size_t kev_used = 0;
   int launches = 0;
   int scatter = HFK_SCATTER_AUTO;
   int shape = 4;  // launch shape under an explicit scatter mode (warps per CTA, or a point-parallel shape)

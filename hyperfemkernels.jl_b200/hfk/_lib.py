@@ -53,6 +53,9 @@ SIGNATURES = {
     "hfk_problem_tuning": [_vp, _i, _i, _pi, _pi, _pi],
     "hfk_functional": [_vp, _vp, _vp, _i, _pd],
     "hfk_launch_count": [_vp, _pi64],
+    "hfk_problem_set_timing": [_vp, _i],
+    "hfk_problem_kernel_time": [_vp, _pd, _pi64],
+    "hfk_device_peak_fp64": [_pd, _pd],
     "hfk_colors": [_vp, _vp],
     "hfk_pattern_build": [_vp, _pi64],
     "hfk_pattern_get": [_vp, _vp, _vp],

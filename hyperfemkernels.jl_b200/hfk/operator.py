@@ -91,6 +91,17 @@ class Problem:
         call("hfk_launch_count", self.h, ctypes.byref(c))
         return c.value
 
+    def set_timing(self, on: bool = True):
+        """Bracket every element-kernel launch sequence with CUDA events (``hfk_problem_set_timing``)."""
+        call("hfk_problem_set_timing", self.h, int(bool(on)))
+
+    def kernel_time(self):
+        """(summed milliseconds, number of sequences) of the bracketed element-kernel launches since
+        timing was switched on or last read (``hfk_problem_kernel_time``)."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        call("hfk_problem_kernel_time", self.h, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
     def colors(self) -> np.ndarray:
         out = np.zeros(self.space.mesh.ncells, dtype=np.int32)
         call("hfk_colors", self.h, ptr(out, np.int32))

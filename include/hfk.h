@@ -113,6 +113,21 @@ int hfk_functional(hfk_problem* p, const double* x, const double* dvals, int kin
 /* Number of kernels this handle launched so far (launch accounting for benchmarks). */
 int hfk_launch_count(hfk_problem* p, int64_t* count);
 
+/* Kernel timing, a measurement aid with no counterpart in the reference. With on = 1, every
+ * element-kernel launch sequence of hfk_residual, hfk_jacobian, hfk_mf_apply and hfk_mf_apply_f32
+ * (the cell kernels, without the zero-fill of the output) is bracketed by CUDA events on the
+ * handle's stream; nothing waits on them. hfk_problem_kernel_time waits for the last one, returns
+ * the summed milliseconds and the number of bracketed sequences since timing was switched on or
+ * last read, and starts a new count. */
+int hfk_problem_set_timing(hfk_problem* p, int on);
+int hfk_problem_kernel_time(hfk_problem* p, double* ms, int64_t* count);
+
+/* FP64 throughput of the current device in TFLOP/s, measured by two microkernels on every SM:
+ * the FP64 tensor-core MMA (mma m8n8k4 f64, the instruction of the assembly's element products)
+ * and the FP64 FMA pipe (best of three runs each, about 0.5 s in all). The denominator of the
+ * FP64 roofline fractions; no counterpart in the reference. */
+int hfk_device_peak_fp64(double* dmma_tflops, double* dfma_tflops);
+
 /* Colour of every cell, 1-based (color_cells, src/coloring.jl:4-28; bit-exact greedy first fit). */
 int hfk_colors(hfk_problem* p, int32_t* color_of_cell);
 
