@@ -70,6 +70,17 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Device memory of GPU `device` (or managed memory, which every GPU can reach)
+bool is_device_ptr_on(const void* p, int device) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == device);
+}
+
 // An input vector on the device: the caller's device pointer, or a copy of host data in `stage`
 template <typename T>
 const T* dev_in(const T* p, size_t n, DBuf<T>& stage, cudaStream_t s) {
@@ -3643,6 +3654,9 @@ extern "C" int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, 
                   "); use hfk_chebyshev_smooth");
   HFK_REQUIRE(is_device_ptr(rhs) && is_device_ptr(x) && (!residual || is_device_ptr(residual)), HFK_ERR_ARG,
               "hfk_chebyshev_smooth_noalloc takes device pointers only (staging host data would allocate)");
+  HFK_REQUIRE(is_device_ptr_on(rhs, p->device) && is_device_ptr_on(x, p->device) &&
+                  (!residual || is_device_ptr_on(residual, p->device)),
+              HFK_ERR_ARG, "hfk_chebyshev_smooth_noalloc: rhs, x and residual must be memory of the operator's GPU");
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
   HFK_REQUIRE(p->nblocks > 0 && p->blocks_ok, HFK_ERR_STATE, "blocks not built (call hfk_blocks_update)");
   int dev = 0;

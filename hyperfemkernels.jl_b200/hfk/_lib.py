@@ -160,7 +160,12 @@ def call(name, *args):
 
 
 def ptr(a, dtype=np.float64):
-    """Address of a numpy array (checked dtype/contiguity) or a CUDA tensor (``data_ptr()``)."""
+    """Address of a numpy array (checked dtype/contiguity) or a CUDA tensor (``data_ptr()``).
+
+    The returned ``c_void_p`` holds a reference to the array, so a temporary passed straight into
+    a call (``call(..., ptr(np.asfortranarray(x)))``) stays alive until the call returns; a bare
+    address would let the temporary be freed, and its memory reused, before the library reads it.
+    """
     if a is None:
         return None
     if hasattr(a, "data_ptr"):
@@ -170,11 +175,14 @@ def ptr(a, dtype=np.float64):
                 np.int64: torch.int64}[np.dtype(dtype).type]
         if a.dtype != want or not a.is_contiguous():
             raise TypeError(f"HyperFEMKernels: expected a contiguous {want} tensor")
-        return ctypes.c_void_p(a.data_ptr())
-    if not isinstance(a, np.ndarray):
-        raise TypeError("HyperFEMKernels: expected a numpy array or a CUDA tensor")
-    if a.dtype != np.dtype(dtype):
-        raise TypeError(f"HyperFEMKernels: expected dtype {np.dtype(dtype)}, got {a.dtype}")
-    if not (a.flags.c_contiguous or a.flags.f_contiguous):
-        raise TypeError("HyperFEMKernels: expected a contiguous array")
-    return ctypes.c_void_p(a.ctypes.data)
+        p = ctypes.c_void_p(a.data_ptr())
+    else:
+        if not isinstance(a, np.ndarray):
+            raise TypeError("HyperFEMKernels: expected a numpy array or a CUDA tensor")
+        if a.dtype != np.dtype(dtype):
+            raise TypeError(f"HyperFEMKernels: expected dtype {np.dtype(dtype)}, got {a.dtype}")
+        if not (a.flags.c_contiguous or a.flags.f_contiguous):
+            raise TypeError("HyperFEMKernels: expected a contiguous array")
+        p = ctypes.c_void_p(a.ctypes.data)
+    p._owner = a
+    return p

@@ -1,4 +1,5 @@
 """The C ABI library loads and exports every symbol that include/hfk.h declares (no GPU needed)."""
+import ctypes
 import os
 import re
 
@@ -104,3 +105,18 @@ def test_solver_options_are_validated_before_any_device_work():
         KernelOperator(res, jac, Vs[0], jacobian="dense")
     with pytest.raises(ValueError, match="HyperFEMKernels"):
         KernelOperator(res, forms.svk_jacobian(lam=3.0), Vs[0])  # residual and Jacobian of different laws
+
+
+def test_pointer_keeps_a_temporary_alive():
+    # ptr() of a temporary copy: the pointer object must keep the copy alive until the call that
+    # receives it returns (the outlet normals are passed as np.asfortranarray(...) in place)
+    import gc
+
+    from hfk._lib import ptr
+
+    a = np.arange(12.0).reshape(3, 4)
+    p = ptr(np.asfortranarray(a))
+    gc.collect()
+    junk = [np.full(12, -1.0) for _ in range(64)]  # would reuse a freed block
+    view = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), shape=(12,))
+    assert np.array_equal(view, np.asfortranarray(a).ravel(order="K")) and len(junk) == 64

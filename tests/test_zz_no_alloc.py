@@ -63,6 +63,27 @@ def test_noalloc_smoother_matches_the_allocating_one_twice():
     assert float(torch.linalg.norm(x_na)) > 0
 
 
+def test_noalloc_smoother_leaves_free_device_memory_unchanged():
+    # the contract itself: after a first call (which resolves the scratch array's address and lets
+    # the launch-shape autotuner pick the product's kernel), further calls take no device memory
+    import torch
+
+    V, op, a, b = _prepared_operator()
+    n = V.nfree
+    rhs = torch.from_numpy(np.random.default_rng(3).standard_normal(n)).cuda()
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r = torch.zeros_like(x)
+    h = op.problem.h
+    call("hfk_chebyshev_smooth_noalloc", h, a, b, 3, ptr(rhs), ptr(x), 1, ptr(r))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in range(5):
+        call("hfk_chebyshev_smooth_noalloc", h, a, b, 2 + k % 3, ptr(rhs), ptr(x), 0, ptr(r))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_smoother_rejects_host_pointers_and_too_many_dofs():
     V, op, a, b = _prepared_operator()
     rhs = np.ones(V.nfree)
@@ -82,3 +103,10 @@ def test_noalloc_smoother_rejects_host_pointers_and_too_many_dofs():
     with pytest.raises(_lib.HFKError) as e:
         call("hfk_chebyshev_smooth_noalloc", opb.problem.h, a, b, 2, ptr(r), ptr(y), 1, None)
     assert e.value.code == 1 and "at most 524288 free dofs" in str(e.value)
+    # vectors on another GPU than the operator's (needs two GPUs)
+    if torch.cuda.device_count() > 1:
+        r1 = torch.ones(V.nfree, dtype=torch.float64, device="cuda:1")
+        x1 = torch.zeros_like(r1)
+        with pytest.raises(_lib.HFKError) as e:
+            call("hfk_chebyshev_smooth_noalloc", op.problem.h, a, b, 2, ptr(r1), ptr(x1), 1, None)
+        assert "operator's GPU" in str(e.value)
