@@ -1292,17 +1292,20 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   const size_t smem = asm_smem_bytes(p->nn, p->np, g, ldg);
   HFK_REQUIRE(smem <= 227 * 1024, HFK_ERR_UNSUPPORTED, "too many quadrature points for the assembly kernel");
   HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
+  // the recognised laws are hyperelastic (symmetric tangent): only the element blocks k >= c are formed
+  const bool sym = p->law == HFK_LAW_SVK || p->law == HFK_LAW_LINEAR_ELASTIC;
+  auto kern_g = padded ? (sym ? jacobian_kernel_g<27, true, true> : jacobian_kernel_g<27, true, false>)
+                       : (sym ? jacobian_kernel_g<27, false, true> : jacobian_kernel_g<27, false, false>);
   if (g) {
-    static PerDeviceLimit attr[2];
-    raise_smem_limit(padded ? jacobian_kernel_g<27, true> : jacobian_kernel_g<27, false>, smem, attr[padded]);
+    static PerDeviceLimit attr[4];
+    raise_smem_limit(kern_g, smem, attr[2 * padded + sym]);
   } else {
     static PerDeviceLimit attr;
     raise_smem_limit(jacobian_kernel_direct<8>, smem, attr);
   }
   auto launch = [&](const int32_t* cells, int n) {
     CellData cd = cell_data(p, cells, n);
-    if (g && padded) jacobian_kernel_g<27, true><<<n, 256, smem, p->stream>>>(cd, io);
-    else if (g) jacobian_kernel_g<27, false><<<n, 256, smem, p->stream>>>(cd, io);
+    if (g) kern_g<<<n, 256, smem, p->stream>>>(cd, io);
     else jacobian_kernel_direct<8><<<n, 256, smem, p->stream>>>(cd, io);
     check_launch(p);
   };

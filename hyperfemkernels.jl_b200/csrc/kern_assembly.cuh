@@ -109,17 +109,110 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                : "d"(a), "d"(b));
 }
 
+// One test component c of the 27-node kernel (below): G_c in shared memory, then K_c = A^T G_c on the
+// FP64 tensor cores and the scatter. C is a template parameter so that the first column tile
+// (TMIN, under SYM) is a constant: the tile loops and their bounds resolve at compile time.
+template <int NN, bool PADDED, bool SYM, int C>
+__device__ __forceinline__ void asm_component(const AsmIO& io, const int32_t* pos, const double* A, const double* Dh,
+                                              double* G) {
+  constexpr int NDL = 3 * NN;
+  constexpr int MT = (NN + 7) / 8, NT = (NDL + 7) / 8;  // 8-row bands of K_c, 8-column tiles
+  constexpr int MK0 = SYM ? C * NN : 0;                 // first column of K_c that is formed
+  constexpr int TMIN = MK0 / 8;                         // first column tile that reaches it
+  constexpr int TPW = (NT - TMIN + 1) / 2;              // column tiles per warp (two warps per band)
+  constexpr int RG = 256 / NDL;                         // thread groups of G_c's construction
+  const int np = io.np, ldg = io.ldg;
+  const int R = 3 * np, ksteps = (R + 3) / 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int band = warp % MT, tile0 = warp / MT;
+  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column of this lane
+  // G_c[r = q*3 + K][mk = k*NN + m] = sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]: thread (g, mk) fills
+  // column mk for the points q = g, g + RG, ...; a point's three values of A serve its three rows.
+  // Only the columns of the tiles the products read are formed (from the first tile's start; the
+  // few of its columns below MK0 are computed, but their entries are not scattered).
+  if (threadIdx.x < RG * NDL) {
+    const int g = threadIdx.x / NDL, mk = threadIdx.x - g * NDL;
+    const int k = mk / NN, m = mk - k * NN;
+    if (mk >= TMIN * 8)
+      for (int q = g; q < np; q += RG) {
+        const double a0 = A[m + NN * (3 * q)], a1 = A[m + NN * (3 * q + 1)], a2 = A[m + NN * (3 * q + 2)];
+        const double* D = Dh + q * 81 + C * 3 + 27 * k;
+#pragma unroll
+        for (int K = 0; K < 3; ++K) G[(3 * q + K) * ldg + mk] = D[K] * a0 + D[K + 9] * a1 + D[K + 18] * a2;
+      }
+  }
+  __syncthreads();
+  // this lane's output entries: rows n = band*8 + fr, columns mk = tile*8 + 2 fc + i; positions
+  // loaded first (their latency overlaps the products); under SYM also the transposed entry's
+  const int n = band * 8 + fr;
+  int32_t pp[TPW][2], pt[TPW][2];
+  double acc[2][TPW][2];  // even and odd k-steps: two independent chains of tensor-core steps
+#pragma unroll
+  for (int j = 0; j < TPW; ++j) {
+    const int tile = TMIN + tile0 + 2 * j;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int mk = tile * 8 + 2 * fc + i;
+      const bool own = tile < NT && n < NN && mk < NDL && mk >= MK0;
+      pp[j][i] = own ? __ldg(pos + (C * NN + n) + NDL * mk) : 0;
+      pt[j][i] = (SYM && own && mk >= MK0 + NN) ? __ldg(pos + mk + NDL * (C * NN + n)) : 0;
+      acc[0][j][i] = acc[1][j][i] = 0.0;
+    }
+  }
+  // fragment elements past the matrices' edges are zeros: a lane whose element lies outside
+  // loads a valid address and selects zero, so the warp stays converged for mma.sync
+  const bool na = n < NN;
+  auto kstep = [&](int ks, double (&ac)[TPW][2]) {
+    const int r = ks * 4 + fc;  // k index of this lane's A^T and B fragment elements
+    const bool ra = na && r < R;
+    double a = A[ra ? n + NN * r : 0];
+    a = ra ? a : 0.0;
+    const double* Gr = G + r * ldg + fr;
+#pragma unroll
+    for (int j = 0; j < TPW; ++j) {
+      const int tile = TMIN + tile0 + 2 * j;
+      if (tile < NT) {  // uniform over the warp
+        double b;
+        if (PADDED) {
+          b = Gr[tile * 8];
+        } else {
+          const bool rb = r < R && tile * 8 + fr < NDL;
+          b = G[rb ? r * ldg + tile * 8 + fr : 0];
+          b = rb ? b : 0.0;
+        }
+        dmma_8x8x4(ac[j][0], ac[j][1], a, b);
+      }
+    }
+  };
+  for (int ks = 0; ks < ksteps; ks += 2) {
+    kstep(ks, acc[0]);
+    if (ks + 1 < ksteps) kstep(ks + 1, acc[1]);  // uniform over the block
+  }
+#pragma unroll
+  for (int j = 0; j < TPW; ++j)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const double v = acc[0][j][i] + acc[1][j][i];
+      scatter_add(io.nzval, pp[j][i], v);
+      if (SYM) scatter_add(io.nzval, pt[j][i], v);
+    }
+  __syncthreads();
+}
+
 // 27-node cells (Q2): G_c in shared memory, K_c = A^T G_c on the FP64 tensor cores. Eight warps:
 // warp w takes the 8-row band w % 4 of K_c (rows n, 27 padded to 32) and every other 8-column tile
 // (columns mk, 81 padded to 88) from w / 4; the k dimension (r = 3 np) runs in steps of 4, padded
 // with zeros. A warp loads one fragment of A^T per k-step and reuses it for its five or six tiles.
 // PADDED: G_c has the row stride ASM_LDG_PADDED and zeros past its last row and column, so the B
 // fragments load without bounds selects; otherwise (large np) the stride is 81 and they select.
-template <int NN, bool PADDED>
+// SYM: the tangent has the major symmetry T[(c,J),(k,L)] = T[(k,L),(c,J)] (every hyperelastic law:
+// SVK, linear elasticity), so K[(n,c),(m,k)] = K[(m,k),(n,c)]: only the blocks k >= c are formed
+// (the column tiles that reach columns k*NN + m >= c*NN: 24 of 33 tiles, and the G_c columns of
+// those tiles), and each entry of a block k > c is added at its own position and at its transpose's.
+template <int NN, bool PADDED, bool SYM>
 __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) {
   constexpr int NDL = 3 * NN;
-  constexpr int MT = (NN + 7) / 8, NT = (NDL + 7) / 8;  // 8-row bands of K_c, 8-column tiles
-  constexpr int TPW = (NT + 1) / 2;                      // column tiles per warp (two warps per band)
+  constexpr int MT = (NN + 7) / 8, NT = (NDL + 7) / 8;
   static_assert(MT == 4, "eight warps: four row bands x two column-tile sets");
   extern __shared__ __align__(16) double sm[];
   const int np = io.np, ldg = io.ldg;
@@ -149,74 +242,9 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
   __syncthreads();
   asm_point_phase<NN>(cd, io, cell, A, xl, Hs, iJs, dVs, Dh);
   const int32_t* pos = io.nzpos + (size_t)NDL * NDL * cell;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int band = warp % MT, tile0 = warp / MT;
-  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column of this lane
-  constexpr int RG = 256 / NDL;  // thread groups of G_c's construction, one column per thread
-  for (int c = 0; c < 3; ++c) {
-    // G_c[r = q*3 + K][mk = k*NN + m] = sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]: thread (g, mk) fills
-    // column mk for the points q = g, g + RG, ...; a point's three values of A serve its three rows
-    if (threadIdx.x < RG * NDL) {
-      const int g = threadIdx.x / NDL, mk = threadIdx.x - g * NDL;
-      const int k = mk / NN, m = mk - k * NN;
-      for (int q = g; q < np; q += RG) {
-        const double a0 = A[m + NN * (3 * q)], a1 = A[m + NN * (3 * q + 1)], a2 = A[m + NN * (3 * q + 2)];
-        const double* D = Dh + q * 81 + c * 3 + 27 * k;
-#pragma unroll
-        for (int K = 0; K < 3; ++K) G[(3 * q + K) * ldg + mk] = D[K] * a0 + D[K + 9] * a1 + D[K + 18] * a2;
-      }
-    }
-    __syncthreads();
-    // this lane's output entries: rows n = band*8 + fr, columns mk = tile*8 + 2 fc + i; positions
-    // loaded first (their latency overlaps the products)
-    const int n = band * 8 + fr;
-    int32_t pp[TPW][2];
-    double acc[2][TPW][2];  // even and odd k-steps: two independent chains of tensor-core steps
-#pragma unroll
-    for (int j = 0; j < TPW; ++j) {
-      const int tile = tile0 + 2 * j;
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int mk = tile * 8 + 2 * fc + i;
-        pp[j][i] = (tile < NT && n < NN && mk < NDL) ? __ldg(pos + (c * NN + n) + NDL * mk) : 0;
-        acc[0][j][i] = acc[1][j][i] = 0.0;
-      }
-    }
-    // fragment elements past the matrices' edges are zeros: a lane whose element lies outside
-    // loads a valid address and selects zero, so the warp stays converged for mma.sync
-    const bool na = n < NN;
-    auto kstep = [&](int ks, double (&ac)[TPW][2]) {
-      const int r = ks * 4 + fc;  // k index of this lane's A^T and B fragment elements
-      const bool ra = na && r < R;
-      double a = A[ra ? n + NN * r : 0];
-      a = ra ? a : 0.0;
-      const double* Gr = G + r * ldg + fr;
-#pragma unroll
-      for (int j = 0; j < TPW; ++j) {
-        const int tile = tile0 + 2 * j;
-        if (tile < NT) {  // uniform over the warp
-          double b;
-          if (PADDED) {
-            b = Gr[tile * 8];
-          } else {
-            const bool rb = r < R && tile * 8 + fr < NDL;
-            b = G[rb ? r * ldg + tile * 8 + fr : 0];
-            b = rb ? b : 0.0;
-          }
-          dmma_8x8x4(ac[j][0], ac[j][1], a, b);
-        }
-      }
-    };
-    for (int ks = 0; ks < ksteps; ks += 2) {
-      kstep(ks, acc[0]);
-      if (ks + 1 < ksteps) kstep(ks + 1, acc[1]);  // uniform over the block
-    }
-#pragma unroll
-    for (int j = 0; j < TPW; ++j)
-#pragma unroll
-      for (int i = 0; i < 2; ++i) scatter_add(io.nzval, pp[j][i], acc[0][j][i] + acc[1][j][i]);
-    __syncthreads();
-  }
+  asm_component<NN, PADDED, SYM, 0>(io, pos, A, Dh, G);
+  asm_component<NN, PADDED, SYM, 1>(io, pos, A, Dh, G);
+  asm_component<NN, PADDED, SYM, 2>(io, pos, A, Dh, G);
 }
 
 // Small cells (Q1, any number of points): one thread per element entry
