@@ -1,7 +1,5 @@
 // C ABI of the B200 engine: construction (host C++), dispatch of the CUDA kernels, solver loops.
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <chrono>
@@ -22,17 +20,13 @@
 #include "kern_assembly.cuh"
 #include "kern_band.cuh"
 #include "kern_cell.cuh"
+#include "kern_chol.cuh"
 #include "kern_jvp.cuh"
 #include "kern_mlp.cuh"
 #include "kern_oseen.cuh"
 #include "kern_seg.cuh"
 #include "kern_vec.cuh"
 
-namespace hfk {
-GmresWork::~GmresWork() {
-  if (blas) cublasDestroy((cublasHandle_t)blas);
-}
-}  // namespace hfk
 
 using namespace hfk;
 
@@ -1518,14 +1512,14 @@ struct hfk_pmg {
   // fixed number of block-Jacobi CG steps per segment on the matrix-free coarse level
   int coarse_mode = HFK_COARSE_CHOLESKY, coarse_iters = 20;  // or COARSE_BLOCKS (a block-Jacobi slot)
   int eig_inner = HFK_EIG_EUCLIDEAN;  // inner product of the eigenvalue estimate
-  DBuf<double> Lc, cb, cx;
+  DBuf<double> Lb, cb, cx;  // Lb: the coarse Cholesky factor in band storage (kern_chol.cuh)
+  int cb_nbt = 0, cb_W = 0;  // its block rows and lower block bandwidth
+  DBuf<int> cb_info;         // first block column with a bad pivot (1-based), 0 = none
   DBuf<double> ccg_r, ccg_z, ccg_p, ccg_q, ccg_sc;
   bool coarse_ok = false;
   std::vector<std::unique_ptr<EigWork>> ew;          // per level (no reallocation between levels)
   std::vector<std::vector<double>> seg_lmin, seg_lmax;  // per level, per segment
   std::vector<std::unique_ptr<DBuf<double>>> start;  // per level: the fixed Arnoldi start vector
-  DBuf<double> potrf_work;
-  DBuf<int> potrf_info;
   // banded factor: the block tiles of both triangular solves (kern_band.cuh), rebuilt with the
   // factor; bs_sync holds both directions' tickets, then the error word
   bool bs_on = false;
@@ -1534,17 +1528,13 @@ struct hfk_pmg {
   // coarse_factor_launch, collected by coarse_factor_finish)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_c0 = nullptr, ev_c1 = nullptr, ev_p0 = nullptr, ev_p1 = nullptr;
-  bool cf_pending = false, cf_banded = false;
-  int cf_nt = 0;
+  bool cf_pending = false;
   DBuf<double> bs_tiles, bs_diag, bs_y;
   DBuf<int> bs_sync;
-  DBuf<const double*> bs_aptr;
-  DBuf<double*> bs_bptr;
   DBuf<double> top_r, top_y;
-  cusolverDnHandle_t solver = nullptr;
-  cublasHandle_t blas = nullptr;
-  DBuf<unsigned char> blas_ws;
-  double t_potrf = 0;
+  double t_potrf = 0;  // time of the factorisations proper (ms)
+  int bs_spin = BS_SPIN_LIMIT;  // polls before a wait of the block triangular solves gives up
+  int bs_skip = 0;              // test knob: the next forward solve starts its tickets at 1
   // learned correction after each cycle (null = plain cycle) and its work buffers
   hfk_mlp* mlp = nullptr;
   DBuf<double> ml_s, ml_t, ml_q, ml_delta, ml_scal;  // ml_scal: 8 per segment
@@ -1581,19 +1571,9 @@ __global__ void lower_bandwidth_kernel(int64_t n, const int64_t* colptr, const i
   atomicMax(band, mine);
 }
 
-void ensure_blas(hfk_pmg* m) {
-  if (m->blas) return;
-  if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
-  // a fixed workspace, so that the captured cycle never asks cuBLAS to allocate
-  m->blas_ws.resize(32u << 20);
-  if (cublasSetWorkspace(m->blas, m->blas_ws.p, m->blas_ws.n) != CUBLAS_STATUS_SUCCESS)
-    throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasSetWorkspace failed"};
-}
-
-// The tiles of the block triangular solves (kern_band.cuh) from the banded factor in m->Lc: the
-// band of each block row and block column copied into BS_T x BS_T tiles, then one batched
-// triangular solve per direction with the diagonal blocks turns them into D^-1 L tiles (and the
-// identity tile into D^-1).
+// The tiles of the block triangular solves (kern_band.cuh) from the band factor in m->Lb: the band
+// of each block row and block column copied into BS_T x BS_T tiles, then every tile multiplied by
+// the inverse of its step's diagonal block (tile_trsm_kernel; the identity tile becomes D^-1).
 void band_prepare(hfk_pmg* m, int64_t n) {
   hfk_problem* c = m->lv[m->L - 1];
   const int nb = (int)((n + BS_T - 1) / BS_T);
@@ -1605,36 +1585,25 @@ void band_prepare(hfk_pmg* m, int64_t n) {
   m->bs_y.resize(n);
   m->bs_sync.resize(3);  // the two directions' tickets, the error word
   if (m->bs_nb != nb || m->bs_wt != wt) {
-    std::vector<const double*> a(2 * nb);
-    std::vector<double*> b(2 * nb);
-    for (int q = 0; q < 2 * nb; ++q) {
-      a[q] = m->bs_diag.p + (size_t)q * tt;
-      b[q] = m->bs_tiles.p + (size_t)q * per;
-    }
-    m->bs_aptr.upload(a.data(), a.size(), c->stream);
-    m->bs_bptr.upload(b.data(), b.size(), c->stream);
     m->bs_sync.zero(c->stream);
     m->bs_nb = nb;
     m->bs_wt = wt;
   }
   const int64_t total = (int64_t)2 * nb * (wt + 2) * (int64_t)tt;
-  band_tiles_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 64), 256, 0, c->stream>>>(
-      n, nb, wt, m->Lc.p, m->bs_tiles.p, m->bs_diag.p);
+  band_tiles_kernel<<<(int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 64), 256, 0, c->stream>>>(
+      n, nb, wt, m->Lb.p, m->cb_W, m->bs_tiles.p, m->bs_diag.p);
   check_launch(c);
-  ensure_blas(m);
-  cublasSetStream(m->blas, c->stream);
-  const double one = 1.0;
-  for (int d = 0; d < 2; ++d)
-    if (cublasDtrsmBatched(m->blas, CUBLAS_SIDE_LEFT, d ? CUBLAS_FILL_MODE_UPPER : CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                           CUBLAS_DIAG_NON_UNIT, BS_T, (wt + 1) * BS_T, &one, m->bs_aptr.p + (size_t)d * nb, BS_T,
-                           m->bs_bptr.p + (size_t)d * nb, BS_T, nb) != CUBLAS_STATUS_SUCCESS)
-      throw Error{HFK_ERR_CUDA, "HyperFEMKernels: batched triangular solve of the coarse tiles failed"};
+  const size_t smem = tt * sizeof(double);
+  static PerDeviceLimit attr;
+  raise_smem_limit(tile_trsm_kernel<BS_T>, smem, attr);
+  tile_trsm_kernel<BS_T><<<2 * nb * (wt + 1), BS_T, smem, c->stream>>>(nb, wt, m->bs_diag.p, m->bs_tiles.p);
+  check_launch(c);
 }
 
 // the error word of the block triangular solves: a wait between blocks that ran out (the cycle's
 // coarse correction is then invalid)
 void band_check(hfk_pmg* m) {
-  if (!m->bs_on) return;
+  if (!m->bs_on || !m->bs_sync.p) return;
   int e = 0;
   hfk_problem* c = m->lv[m->L - 1];
   int* word = m->bs_sync.p + 2;
@@ -1647,12 +1616,11 @@ void band_check(hfk_pmg* m) {
 }
 
 // Cholesky factor of the assembled coarse level (in place of the reference's LU, the matrix being
-// symmetric positive definite). The coarse matrix is banded in the node-major numbering
-// (bandwidth b ~ 3 (n_x n_y + n_x + 1) dofs), and a Cholesky factor keeps the band, so the
-// factorisation runs over the band only: per block column of T = 256, a dense potrf of the
-// diagonal block, a triangular solve of the b rows below it and a symmetric rank-T update of the
-// b x b window that follows: O(n b^2) work instead of O(n^3). A matrix whose band is wide
-// (b >= n / 3) takes the dense potrf.
+// symmetric positive definite), hand-written over band storage (kern_chol.cuh): the lower triangle
+// of the assembled CSC matrix copied into CB_T x CB_T tiles of its band, then one panel launch and
+// one trailing-update launch per block column, O(n b^2) work and O(n b) memory for the lower
+// bandwidth b (a full lower triangle when the band is wide). Then the D^-1 L tiles of the cycle's
+// block triangular solves.
 void coarse_factor_launch(hfk_pmg* m) {
   hfk_problem* c = m->lv[m->L - 1];
   if (!m->ev_c0)
@@ -1661,17 +1629,15 @@ void coarse_factor_launch(hfk_pmg* m) {
   pattern_build_dev(c);
   jacobian_dev(c, c->x.p, c->dvals.p, c->nzval.p);
   const int64_t n = c->nfree;
-  HFK_REQUIRE(n <= 40000, HFK_ERR_UNSUPPORTED, "the dense coarse solve supports up to 40000 coarse dofs");
-  m->Lc.resize((size_t)n * n);
-  m->Lc.zero(c->stream);
-  csc_to_dense_kernel<<<(int)std::min<int64_t>(n, 65535), 128, 0, c->stream>>>(n, c->colptr.p, c->rowval.p, c->nzval.p,
-                                                                                m->Lc.p);
-  check_launch(c);
-  if (!m->solver) {
-    if (cusolverDnCreate(&m->solver) != CUSOLVER_STATUS_SUCCESS)
-      throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cusolverDnCreate failed"};
+  if (n == 0) {  // nothing to factor: the coarse solve is empty
+    m->cb_info.resize(1);
+    m->cb_info.zero(c->stream);
+    HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
+    HFK_CUDA(cudaEventRecord(m->ev_p1, c->stream));
+    HFK_CUDA(cudaEventRecord(m->ev_c1, c->stream));
+    m->cf_pending = true;
+    return;
   }
-  cusolverDnSetStream(m->solver, c->stream);
   if (m->band < 0) {  // the pattern's lower bandwidth, once
     DBuf<int> bd;
     bd.resize(1);
@@ -1681,67 +1647,55 @@ void coarse_factor_launch(hfk_pmg* m) {
     HFK_CUDA(cudaMemcpyAsync(&m->band, bd.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     HFK_CUDA(cudaStreamSynchronize(c->stream));
   }
-  constexpr int T = 256;
-  const bool banded = (int64_t)m->band * 3 < n;
-  const int nt = banded ? (int)((n + T - 1) / T) : 1;
-  int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(m->solver, CUBLAS_FILL_MODE_LOWER, banded ? T : (int)n, m->Lc.p, (int)n, &lwork) !=
-      CUSOLVER_STATUS_SUCCESS)
-    throw Error{HFK_ERR_CUDA, "HyperFEMKernels: potrf_bufferSize failed"};
-  if (m->potrf_work.n < (size_t)lwork + 1) m->potrf_work.resize((size_t)lwork + 1);
-  if (m->potrf_info.n < (size_t)nt) m->potrf_info.resize(nt);
-  m->potrf_info.zero(c->stream);
-  double* A = m->Lc.p;
-  int* info = m->potrf_info.p;
+  const int nbt = (int)((n + CB_T - 1) / CB_T);
+  const int W = std::min(nbt - 1, (m->band + CB_T - 1) / CB_T);
+  m->Lb.resize((size_t)nbt * (W + 1) * CB_T * CB_T);
+  m->Lb.zero(c->stream);
+  band_fill_kernel<<<(int)std::min<int64_t>((int64_t)nbt * CB_T, 65535), 128, 0, c->stream>>>(
+      n, nbt, W, c->colptr.p, c->rowval.p, c->nzval.p, m->Lb.p);
+  check_launch(c);
+  m->cb_nbt = nbt;
+  m->cb_W = W;
+  m->cb_info.resize(1);
+  m->cb_info.zero(c->stream);
+  const size_t smem = (size_t)2 * CB_T * CB_LD * sizeof(double);
+  static PerDeviceLimit attr_p, attr_u;
+  raise_smem_limit(band_panel_kernel, smem, attr_p);
+  raise_smem_limit(band_update_kernel, smem, attr_u);
   HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
-  if (!banded) {
-    cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, (int)n, A, (int)n, m->potrf_work.p, lwork, info);
-  } else {
-    ensure_blas(m);
-    cublasSetStream(m->blas, c->stream);
-    const double one = 1.0, minus = -1.0;
-    for (int k = 0; k < nt; ++k) {
-      const int64_t k0 = (int64_t)k * T;
-      const int kk = (int)std::min<int64_t>(T, n - k0);
-      double* Akk = A + k0 + n * k0;
-      cusolverDnDpotrf(m->solver, CUBLAS_FILL_MODE_LOWER, kk, Akk, (int)n, m->potrf_work.p, lwork, info + k);
-      const int64_t r0 = k0 + kk, r1 = std::min<int64_t>(n, k0 + kk + m->band);
-      const int nr = (int)(r1 - r0);
-      if (nr <= 0) continue;
-      double* Aik = A + r0 + n * k0;
-      if (cublasDtrsm(m->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nr, kk,
-                      &one, Akk, (int)n, Aik, (int)n) != CUBLAS_STATUS_SUCCESS ||
-          cublasDsyrk(m->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, nr, kk, &minus, Aik, (int)n, &one, A + r0 + n * r0,
-                      (int)n) != CUBLAS_STATUS_SUCCESS)
-        throw Error{HFK_ERR_CUDA, "HyperFEMKernels: banded Cholesky update of the coarse level failed"};
+  for (int k = 0; k < nbt; ++k) {
+    const int mq = std::min(W, nbt - 1 - k);
+    band_panel_kernel<<<mq + 1, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p);
+    check_launch(c);
+    if (mq > 0) {
+      band_update_kernel<<<mq * (mq + 1) / 2, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p);
+      check_launch(c);
     }
   }
   HFK_CUDA(cudaEventRecord(m->ev_p1, c->stream));
   // the block tiles of the cycle's triangular solves (used only if every pivot was positive)
-  if (banded) band_prepare(m, n);
+  band_prepare(m, n);
   HFK_CUDA(cudaEventRecord(m->ev_c1, c->stream));
-  m->cf_banded = banded;
-  m->cf_nt = nt;
   m->cf_pending = true;
 }
 
 // waits for the coarse build (on the coarse level's stream, the side stream) and reads the pivots'
-// status; the lower triangle of Lc then holds the Cholesky factor L (A = L L^T) and the cycle
-// applies A^-1 by two triangular solves
+// status; Lb then holds the band of the Cholesky factor L (A = L L^T) and the cycle applies A^-1 by
+// the two block triangular solves
 void coarse_factor_finish(hfk_pmg* m) {
   if (!m->cf_pending) return;
   hfk_problem* c = m->lv[m->L - 1];
   m->cf_pending = false;
-  std::vector<int> h_info(m->cf_nt, 0);
-  HFK_CUDA(cudaMemcpyAsync(h_info.data(), m->potrf_info.p, m->cf_nt * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  int info = 0;
+  HFK_CUDA(cudaMemcpyAsync(&info, m->cb_info.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HFK_CUDA(cudaStreamSynchronize(c->stream));
   float ms = 0;
   HFK_CUDA(cudaEventElapsedTime(&ms, m->ev_p0, m->ev_p1));
   m->t_potrf += ms;
   HFK_CUDA(cudaEventElapsedTime(&ms, m->ev_c0, m->ev_c1));
   m->t_coarse += ms;
-  m->coarse_ok = std::all_of(h_info.begin(), h_info.end(), [](int v) { return v == 0; });
-  m->bs_on = m->coarse_ok && m->cf_banded;
+  m->coarse_ok = info == 0;
+  m->bs_on = m->coarse_ok;
   if (m->coarse_ok) m->nbuild++;
 }
 
@@ -1793,37 +1747,30 @@ void coarse_cg_update(hfk_pmg* m) {
   if (m->coarse_ok) m->nbuild++;
 }
 
-// x = A^-1 b with the Cholesky factor: L y = b, L^T x = y, FP64 (the block solves over the band
-// when the factor is banded, else cuBLAS triangular solves)
+// x = A^-1 b with the Cholesky factor: L y = b, L^T x = y, FP64, by the block triangular solves of
+// kern_band.cuh (forward into bs_y, backward into x)
 void coarse_solve(hfk_pmg* m, const double* b, double* x) {
   hfk_problem* c = m->lv[m->L - 1];
   const int64_t n = c->nfree;
-  ensure_blas(m);
-  cublasSetStream(m->blas, c->stream);
-  if (m->bs_on) {
-    // banded factor: the block solves of kern_band.cuh, forward into bs_y, backward into x
-    const int nb = m->bs_nb;
-    int* sy = m->bs_sync.p;
-    HFK_CUDA(cudaMemsetAsync(sy, 0, 2 * sizeof(int), c->stream));
-    HFK_CUDA(cudaMemsetAsync(m->bs_y.p, 0xff, n * sizeof(double), c->stream));  // the sentinel
-    HFK_CUDA(cudaMemsetAsync(x, 0xff, n * sizeof(double), c->stream));
-    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 0, m->bs_tiles.p, b, m->bs_y.p, sy, sy + 2);
+  HFK_REQUIRE(m->bs_on, HFK_ERR_STATE, "the coarse factor is not available");
+  if (n == 0) return;
+  const int nb = m->bs_nb;
+  int* sy = m->bs_sync.p;
+  HFK_CUDA(cudaMemsetAsync(sy, 0, 2 * sizeof(int), c->stream));
+  if (m->bs_skip) {  // test knob: step 0 of the forward solve is never taken, so step 1 waits in vain
+    fill_int_kernel<<<1, 32, 0, c->stream>>>(1, sy, 1);
     check_launch(c);
-    band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 1,
-                                                        m->bs_tiles.p + (size_t)nb * (m->bs_wt + 1) * BS_T * BS_T,
-                                                        m->bs_y.p, x, sy + 1, sy + 2);
-    check_launch(c);
-    return;
+    m->bs_skip = 0;
   }
-  HFK_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  const double one = 1.0;
-  // dense triangular solves (zeros outside the band): measured faster here than block-column
-  // trsv/gemv calls over the band
-  if (cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
-                  m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS ||
-      cublasDtrsm(m->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
-                  m->Lc.p, (int)n, x, (int)n) != CUBLAS_STATUS_SUCCESS)
-    throw Error{HFK_ERR_CUDA, "HyperFEMKernels: triangular solve of the coarse level failed"};
+  HFK_CUDA(cudaMemsetAsync(m->bs_y.p, 0xff, n * sizeof(double), c->stream));  // the sentinel
+  HFK_CUDA(cudaMemsetAsync(x, 0xff, n * sizeof(double), c->stream));
+  band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 0, m->bs_tiles.p, b, m->bs_y.p, sy, sy + 2,
+                                                      m->bs_spin);
+  check_launch(c);
+  band_solve_kernel<<<nb, BS_THREADS, 0, c->stream>>>(n, nb, m->bs_wt, 1,
+                                                      m->bs_tiles.p + (size_t)nb * (m->bs_wt + 1) * BS_T * BS_T,
+                                                      m->bs_y.p, x, sy + 1, sy + 2, m->bs_spin);
+  check_launch(c);
 }
 
 // x ~= A^-1 b on the coarse level by coarse_iters steps of block-Jacobi preconditioned CG per
@@ -2156,6 +2103,7 @@ int hfk_problem_destroy(hfk_problem* p) {
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->kev) cudaEventDestroy(e);
   delete p;
+  cudaGetLastError();  // a release reports nothing: leave no error behind for the next checked call
   HFK_API_END
 }
 
@@ -2800,8 +2748,6 @@ int hfk_pmg_destroy(hfk_pmg* m) {
       m->lv[l]->stream = m->lv[l]->own_stream;
       if (m->lv[l]->seg_active) m->lv[l]->seg_active = m->lv[l]->seg_active_own.p;
     }
-    if (m->solver) cusolverDnDestroy(m->solver);
-    if (m->blas) cublasDestroy(m->blas);
     if (m->side) {
       cudaStreamSynchronize(m->side);
       cudaStreamDestroy(m->side);
@@ -2813,6 +2759,7 @@ int hfk_pmg_destroy(hfk_pmg* m) {
     if (m->ev1) cudaEventDestroy(m->ev1);
   }
   delete m;
+  cudaGetLastError();  // a release reports nothing: leave no error behind for the next checked call
   HFK_API_END
 }
 
@@ -3156,15 +3103,27 @@ void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x,
   gw.Z.resize((size_t)(flexible ? m : 1) * n);
   gw.w.resize(n);
   gw.h.resize(m + 1);
-  if (!gw.blas) {
-    cublasHandle_t hb = nullptr;
-    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cublasCreate failed"};
-    gw.blas = hb;
-  }
-  cublasHandle_t blas = (cublasHandle_t)gw.blas;
-  cublasSetStream(blas, s);
-  auto blas_ok = [](cublasStatus_t st) {
-    if (st != CUBLAS_STATUS_SUCCESS) throw Error{HFK_ERR_CUDA, "HyperFEMKernels: cuBLAS call of the GMRES solve failed"};
+  // Gram-Schmidt and basis combinations on the engine's multi-dot / multi-axpy kernels, over the
+  // whole vector (one range of reduction chunks for all segments)
+  ensure_seg_items(op);
+  gw.part.resize((size_t)std::max(op->nitems, 1) * SEG_MDOTS);
+  const int32_t all[2] = {0, op->nitems};
+  gw.all.upload(all, 2, s);
+  auto gram_dots = [&](int k, const double* Vb, const double* w, double* h) {  // h = Vb[:, :k]^T w
+    for (int c0 = 0; c0 < k; c0 += SEG_MDOTS) {
+      const int kc = std::min(SEG_MDOTS, k - c0);
+      if (op->nitems) {
+        seg_mdots_kernel<<<op->nitems, RED_THREADS, 0, s>>>(kc, op->item_lo.p, op->item_hi.p, Vb + (size_t)c0 * n, n,
+                                                             w, gw.part.p);
+        check_launch(op);
+      }
+      seg_mfinish_kernel<<<1, RED_THREADS, 0, s>>>(kc, gw.all.p, gw.part.p, h + c0, 0);
+      check_launch(op);
+    }
+  };
+  auto basis_sub = [&](int k, const double* c, const double* Vb, double* y) {  // y -= Vb[:, :k] c
+    seg_maxpy_kernel<<<vec_grid(n), 256, 0, s>>>(n, nullptr, k, c, 0, Vb, n, y);
+    check_launch(op);
   };
   auto apply_prec = [&](const double* in, double* outp) {
     if (prec) pmg_apply_dev(prec, in, outp);
@@ -3184,7 +3143,6 @@ void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x,
   bool conv = beta <= tol;
   int it = 0;
   std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), h1(m + 1), h2(m + 1);
-  const double one = 1.0, zero = 0.0, minus = -1.0;
   while (!conv && it < maxiter) {
     scale_kernel<<<vec_grid(n), 256, 0, s>>>(n, 1.0 / beta, V);
     check_launch(op);
@@ -3199,8 +3157,8 @@ void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x,
       mf_apply_dev(op, zj, vn);
       // classical Gram-Schmidt, twice
       for (int pass = 0; pass < 2; ++pass) {
-        blas_ok(cublasDgemv(blas, CUBLAS_OP_T, (int)n, j + 1, &one, V, (int)n, vn, 1, &zero, gw.h.p, 1));
-        blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, j + 1, &minus, V, (int)n, gw.h.p, 1, &one, vn, 1));
+        gram_dots(j + 1, V, vn, gw.h.p);
+        basis_sub(j + 1, gw.h.p, V, vn);
         HFK_CUDA(cudaMemcpyAsync(pass ? h2.data() : h1.data(), gw.h.p, (j + 1) * sizeof(double),
                                  cudaMemcpyDeviceToHost, s));
       }
@@ -3234,11 +3192,13 @@ void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x,
       const double d = H[(size_t)i * (m + 1) + i];
       y[i] = d != 0.0 ? t / d : 0.0;
     }
+    for (int i = 0; i < jend; ++i) y[i] = -y[i];  // the multi-axpy subtracts
     HFK_CUDA(cudaMemcpyAsync(gw.h.p, y.data(), jend * sizeof(double), cudaMemcpyHostToDevice, s));
     if (flexible) {
-      blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, jend, &one, gw.Z.p, (int)n, gw.h.p, 1, &one, xd, 1));
+      basis_sub(jend, gw.h.p, gw.Z.p, xd);
     } else {
-      blas_ok(cublasDgemv(blas, CUBLAS_OP_N, (int)n, jend, &one, V, (int)n, gw.h.p, 1, &zero, gw.w.p, 1));
+      HFK_CUDA(cudaMemsetAsync(gw.w.p, 0, n * sizeof(double), s));
+      basis_sub(jend, gw.h.p, V, gw.w.p);
       apply_prec(gw.w.p, gw.Z.p);
       axpby_kernel<double><<<vec_grid(n), 256, 0, s>>>(n, 1.0, gw.Z.p, 1.0, xd);
       check_launch(op);
@@ -3576,6 +3536,16 @@ int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters) {
   // the hierarchy is rebuilt by the next update
   m->built = false;
   m->ok = false;
+  HFK_API_END
+}
+
+int hfk_pmg_test_coarse_wait(hfk_pmg* m, int polls, int skip_first) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(m && polls >= 0, HFK_ERR_ARG, "invalid argument");
+  HFK_CUDA(cudaStreamSynchronize(m->lv[0]->stream));
+  m->bs_spin = polls > 0 ? polls : BS_SPIN_LIMIT;
+  m->bs_skip = skip_first != 0;
+  pmg_drop_graph(m);  // the captured cycle holds the old limit; the next cycle runs uncaptured
   HFK_API_END
 }
 

@@ -122,11 +122,11 @@ struct CGWork {
 };
 
 // Work of the restarted GMRES / FGMRES: the Krylov basis V ((restart + 1) n), the preconditioned
-// basis Z (restart n for FGMRES, one vector for GMRES), a work vector and the projections (device)
+// basis Z (restart n for FGMRES, one vector for GMRES), a work vector and the projections (device),
+// the multi-dot partial sums and the one reduction range {0, nitems}
 struct GmresWork {
-  DBuf<double> V, Z, w, h;
-  void* blas = nullptr;  // cublasHandle_t, created on first use
-  ~GmresWork();
+  DBuf<double> V, Z, w, h, part;
+  DBuf<int32_t> all;
 };
 
 // State of a matrix-free level in a precision

@@ -20,22 +20,24 @@
 #pragma once
 #include <cstdint>
 
+#include "kern_chol.cuh"
+
 namespace hfk {
 
 constexpr int BS_T = 128;                  // rows per block (one CTA per block)
 constexpr int BS_THREADS = 512;            // 4 threads per row, each over 32 columns of a tile
 constexpr int BS_H = BS_THREADS / BS_T;
 constexpr int BS_J = BS_T / BS_H;
-constexpr int BS_SPIN_LIMIT = 1 << 22;     // polls of a dependency flag before the wait gives up
+constexpr int BS_SPIN_LIMIT = 1 << 22;     // polls of a dependency before the wait gives up (default)
 
-// Tiles of both directions from the factor held in the lower triangle of the dense column-major
-// n x n array Lc (zeros outside the band). Direction d (0 forward on L, 1 backward on L^T), step s
+// Tiles of both directions from the factor's band (kern_chol.cuh storage, lower block bandwidth W
+// in CB_T tiles; zeros outside the band). Direction d (0 forward on L, 1 backward on L^T), step s
 // (block k = s, or nb - 1 - s backward) has wt + 1 tiles of BS_T x BS_T, column-major: tile t < wt
 // multiplies the output of step s - wt + t (zero when that step does not exist), tile wt is the
-// identity (it becomes D_k^-1 after the batched triangular solve). diag receives D_k (lower,
+// identity (it becomes D_k^-1 after the tile triangular solves). diag receives D_k (lower,
 // forward) or D_k^T (upper, backward), with unit diagonal on rows past n.
-__global__ void band_tiles_kernel(int64_t n, int nb, int wt, const double* __restrict__ Lc, double* __restrict__ tiles,
-                                  double* __restrict__ diag) {
+static __global__ void band_tiles_kernel(int64_t n, int nb, int wt, const double* __restrict__ Lb, int W,
+                                         double* __restrict__ tiles, double* __restrict__ diag) {
   const int64_t tt = (int64_t)BS_T * BS_T;
   const int64_t ntile = (int64_t)2 * nb * (wt + 1);
   const int64_t total = ntile * tt + (int64_t)2 * nb * tt;
@@ -57,7 +59,7 @@ __global__ void band_tiles_kernel(int64_t n, int nb, int wt, const double* __res
           // forward: L[k T + i, kb T + j] (kb < k); backward: L^T[k T + i, kb T + j] = L[kb T + j, k T + i]
           const int64_t r = d ? kb * BS_T + j : k * BS_T + i;
           const int64_t c = d ? k * BS_T + i : kb * BS_T + j;
-          if (r < n && c < n) v = Lc[r + n * c];
+          if (r < n && c < n) v = band_entry(Lb, W, r, c);
         }
       }
       tiles[e] = v;
@@ -71,11 +73,16 @@ __global__ void band_tiles_kernel(int64_t n, int nb, int wt, const double* __res
       double v = 0.0;
       if (d ? j >= i : i >= j) {
         const int64_t r = k * BS_T + (i > j ? i : j), c = k * BS_T + (i > j ? j : i);
-        v = r < n ? Lc[r + n * c] : (i == j ? 1.0 : 0.0);
+        v = r < n ? band_entry(Lb, W, r, c) : (i == j ? 1.0 : 0.0);
       }
       diag[q] = v;
     }
   }
+}
+
+// p[0 .. n) = v (a launch, so that it can sit inside a captured stream)
+static __global__ void fill_int_kernel(int n, int* p, int v) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
 }
 
 // the bit pattern the outputs are filled with before a launch (a negative NaN with every payload
@@ -94,10 +101,10 @@ __device__ __forceinline__ void bs_store_relaxed_u64(double* p, unsigned long lo
 
 // One direction of the solve: out_k = tile_wt(s) in_k - sum_t tile_t(s) out_{step s - wt + t}.
 // ticket: zeroed before the launch, out: filled with BS_SENTINEL before the launch. err: set to 1 when a
-// wait ran out. Launched with nb CTAs of BS_THREADS threads.
-__global__ void __launch_bounds__(BS_THREADS, 1)
+// wait ran out (after spin_limit polls of one value). Launched with nb CTAs of BS_THREADS threads.
+static __global__ void __launch_bounds__(BS_THREADS, 1)
     band_solve_kernel(int64_t n, int nb, int wt, int backward, const double* __restrict__ tiles,
-                      const double* __restrict__ in, double* out, int* ticket, int* err) {
+                      const double* __restrict__ in, double* out, int* ticket, int* err, int spin_limit) {
   __shared__ int s_step;
   __shared__ double yb[BS_T];
   __shared__ double part[BS_H][BS_T];
@@ -147,7 +154,7 @@ __global__ void __launch_bounds__(BS_THREADS, 1)
             v = __longlong_as_double((long long)bits);
             break;
           }
-          if (++polls > BS_SPIN_LIMIT || ((polls & 1023) == 0 && *((volatile int*)err))) {
+          if (++polls > spin_limit || ((polls & 1023) == 0 && *((volatile int*)err))) {
             atomicExch(err, 1);
             fail = 1;
             break;

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 
 import numpy as np
 
@@ -101,6 +102,7 @@ SIGNATURES = {
     "hfk_pmg_mlp_stats": [_vp, _pi64, _pi64],
     "hfk_pmg_mlp_sample": [_vp, _vp, _vp, _vp, _pi, _d],
     "hfk_pmg_set_coarse": [_vp, _i, _i],
+    "hfk_pmg_test_coarse_wait": [_vp, _i, _i],
     "hfk_pmg_segment_bounds": [_vp, _i, _vp, _vp],
     "hfk_pmg_set_eig_inner": [_vp, _i],
     "hfk_oseen_create": [ctypes.POINTER(_vp), _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _i],
@@ -148,6 +150,46 @@ def lib():
         L.hfk_last_error.restype = ctypes.c_char_p
         _LIB = L
     return _LIB
+
+
+# Destruction order of handles that refer to one another. A hierarchy (hfk_pmg) reads its level
+# problems when it is destroyed, so every level problem must outlive the hierarchies built on it.
+# Holding a reference does not guarantee that in Python: the cyclic garbage collector finalises the
+# objects of a reference cycle (a test frame kept alive by a caught exception's traceback, say) in
+# no particular order. The binding therefore orders it: a problem whose owner is finalised while
+# hierarchies still use it is destroyed when the last of those hierarchies is.
+_users: dict = {}     # problem handle (int) -> live hierarchies that use it
+_pending: set = set()  # problem handles whose owner is gone, waiting for their hierarchies
+_order_lock = threading.Lock()
+
+
+def retain_problem(hv: int) -> None:
+    """A hierarchy starts using problem handle ``hv``."""
+    with _order_lock:
+        _users[hv] = _users.get(hv, 0) + 1
+
+
+def release_problem(hv: int) -> None:
+    """A hierarchy that used ``hv`` is destroyed; destroy ``hv`` too if its owner already went."""
+    with _order_lock:
+        n = _users.get(hv, 0) - 1
+        if n > 0:
+            _users[hv] = n
+            return
+        _users.pop(hv, None)
+        if hv not in _pending:
+            return
+        _pending.discard(hv)
+    lib().hfk_problem_destroy(ctypes.c_void_p(hv))
+
+
+def destroy_problem(hv: int) -> None:
+    """The owner of problem handle ``hv`` is finalised: destroy it now, or once no hierarchy uses it."""
+    with _order_lock:
+        if _users.get(hv, 0) > 0:
+            _pending.add(hv)
+            return
+    lib().hfk_problem_destroy(ctypes.c_void_p(hv))
 
 
 def call(name, *args):

@@ -45,7 +45,7 @@ class Problem:
         h = getattr(self, "h", None)
         if h is not None and h.value:
             try:
-                _lib.lib().hfk_problem_destroy(h)
+                _lib.destroy_problem(h.value)  # deferred while a hierarchy still uses it
             except Exception:
                 pass
             self.h = None

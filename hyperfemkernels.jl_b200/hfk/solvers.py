@@ -201,6 +201,9 @@ class PMultigridState:
         call("hfk_pmg_create", ctypes.byref(h), L, lv, tr, c.degree, c.range, c.inflate, c.eig_iters, prec.coarse_every,
              _lib.FP32 if prec.precision == "fp32" else _lib.FP64)
         self.h = h
+        self._levels = [p.h.value for p in self.problems]
+        for hv in self._levels:
+            _lib.retain_problem(hv)
         if prec.coarse == "cg":
             call("hfk_pmg_set_coarse", h, _lib.COARSE_CG, prec.coarse_iters)
         if c.eig_inner == "preconditioner":
@@ -213,6 +216,8 @@ class PMultigridState:
         if h is not None and h.value:
             try:
                 _lib.lib().hfk_pmg_destroy(h)
+                for hv in getattr(self, "_levels", ()):
+                    _lib.release_problem(hv)
             except Exception:
                 pass
             self.h = None
@@ -296,8 +301,9 @@ class MatrixFreeSolver:
 class LaggedAssembled:
     """``LaggedAssembled(solver; every = 3)`` (src/preconditioners.jl:41-97): the operator's tangent
     assembled and factorised at the setup and then every ``every`` updates (a stale factor in
-    between). ``solver`` "cholesky": the GPU Cholesky of the assembled tangent (banded when the
-    numbering is, FP64; at most 40 000 free dofs), in place of the reference's Gridap solver."""
+    between). ``solver`` "cholesky": the GPU Cholesky of the assembled tangent, factored and stored
+    over the band of the matrix (FP64; memory about 8 n (b + 64) bytes for the lower bandwidth b),
+    in place of the reference's Gridap solver."""
 
     def __init__(self, solver: str = "cholesky", every: int = 3):
         if solver != "cholesky":
@@ -320,6 +326,8 @@ class SlotState:
         h = ctypes.c_void_p()
         call("hfk_slot_create", ctypes.byref(h), mf.op.problem.h, kind, getattr(slot, "every", 1))
         self.h, self.slot = h, slot
+        self._levels = [mf.op.problem.h.value]
+        _lib.retain_problem(self._levels[0])
         self.update(mf)
 
     def __del__(self):
@@ -327,6 +335,8 @@ class SlotState:
         if h is not None and h.value:
             try:
                 _lib.lib().hfk_pmg_destroy(h)
+                for hv in getattr(self, "_levels", ()):
+                    _lib.release_problem(hv)
             except Exception:
                 pass
             self.h = None

@@ -229,8 +229,9 @@ int hfk_inject(hfk_transfer* t, const double* xf, const double* df, double* xc, 
 
 /* ---- p-multigrid (src/pmultigrid.jl) ---------------------------------------------------------
  * levels[0] is the working level (its state is bound by hfk_pmg_update), levels[nlevels-1] the
- * assembled coarse level (solved by a dense Cholesky factorisation on the GPU and two triangular
- * solves per cycle, in place of the reference's LUSolver); transfers[l] goes from level l+1 to level l. Chebyshev(degree, range,
+ * assembled coarse level (solved by a Cholesky factorisation on the GPU, hand-written over the
+ * band of the matrix and stored in band form, and two block triangular solves per cycle, in place
+ * of the reference's LUSolver); transfers[l] goes from level l+1 to level l. Chebyshev(degree, range,
  * inflate, eig_iters) as src/smoothers.jl:21-33. precision HFK_FP64 or HFK_FP32: the arithmetic of
  * the smoothers and products on the levels above the coarse one (the coarse solve is always FP64). */
 #define HFK_FP64 0
@@ -261,8 +262,8 @@ int hfk_pmg_status(hfk_pmg* m, int* ok, int* indefinite);
 int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double* a, double* b);
 /* A one-level preconditioner slot on the prepared operator `op`, for hfk_solve_cg / hfk_solve_gmres
  * (the reference's preconditioner slots, src/preconditioners.jl): HFK_SLOT_LAGGED_ASSEMBLED, the
- * operator's tangent assembled on the GPU and factorised (banded or dense Cholesky, FP64, at most
- * 40000 free dofs) at the first update and then every `every` updates (LaggedAssembled(LUSolver();
+ * operator's tangent assembled on the GPU and factorised (Cholesky over the band, FP64, memory
+ * about 8 n (b + 64) bytes for the lower bandwidth b) at the first update and then every `every` updates (LaggedAssembled(LUSolver();
  * every), :41-97; a stale factor between builds); HFK_SLOT_BLOCK_JACOBI, the nodal 3x3 block
  * inverses of the tangent at every update (BlockJacobi, :151-344; `every` ignored). The slot is an
  * hfk_pmg handle with one level: updated by hfk_pmg_update, applied by the solvers or
@@ -270,11 +271,11 @@ int hfk_pmg_level_info(hfk_pmg* m, int level, double* lmin, double* lmax, double
 #define HFK_SLOT_LAGGED_ASSEMBLED 0
 #define HFK_SLOT_BLOCK_JACOBI 1
 int hfk_slot_create(hfk_pmg** out, hfk_problem* op, int kind, int every);
-/* Coarse solve of the hierarchy: HFK_COARSE_CHOLESKY (default; the assembled coarse level, dense
+/* Coarse solve of the hierarchy: HFK_COARSE_CHOLESKY (default; the assembled coarse level, band
  * Cholesky, in place of the reference's LUSolver, src/pmultigrid.jl:212-219) or HFK_COARSE_CG:
  * `iters` steps of block-Jacobi CG per segment on the matrix-free coarse level from zero (scalars on
  * the device, inside the captured cycle; a variable preconditioner, so use the flexible CG). The
- * second serves hierarchies whose coarse level is too large for a dense factor (many batched
+ * second serves hierarchies whose coarse level is too large for a direct factor (many batched
  * problems); it has no counterpart in the reference. Takes effect at the next hfk_pmg_update. */
 /* Ritz values (extremes) of a level's eigenvalue estimate per segment (nseg entries each; NaN
  * for a level without a smoother or before the first update). */
@@ -290,6 +291,12 @@ int hfk_pmg_set_eig_inner(hfk_pmg* m, int mode);
 #define HFK_COARSE_CHOLESKY 0
 #define HFK_COARSE_CG 1
 int hfk_pmg_set_coarse(hfk_pmg* m, int mode, int iters);
+/* Test knob of the coarse solve's bounded waits (no counterpart in the reference): the block
+ * triangular solves give up a wait after `polls` polls (0 = the default of 4 194 304), and with
+ * skip_first = 1 the next forward solve starts its step tickets at 1, so that step 0 never runs
+ * and the steps after it wait in vain: the wait runs out, the kernel sets its error word and
+ * returns, and the V-cycle returns HFK_ERR_INTERNAL ("... timed out"). Nothing faults or hangs. */
+int hfk_pmg_test_coarse_wait(hfk_pmg* m, int polls, int skip_first);
 
 /* ---- learned correction (no counterpart in the reference) ------------------------------------
  * A per-node MLP (16 -> 64 -> 64 -> 3, tanh, BF16 weights read by the forward pass, FP32 master

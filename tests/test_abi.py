@@ -120,3 +120,28 @@ def test_pointer_keeps_a_temporary_alive():
     junk = [np.full(12, -1.0) for _ in range(64)]  # would reuse a freed block
     view = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), shape=(12,))
     assert np.array_equal(view, np.asfortranarray(a).ravel(order="K")) and len(junk) == 64
+
+
+def test_problem_outlives_its_hierarchies_whatever_the_finalisation_order(monkeypatch):
+    # a hierarchy reads its level problems when destroyed: a problem whose owner is finalised first
+    # (cyclic garbage is finalised in no particular order) is destroyed with the last hierarchy
+    destroyed = []
+
+    class FakeLib:
+        def hfk_problem_destroy(self, h):
+            destroyed.append(h.value)
+
+    monkeypatch.setattr(_lib, "lib", lambda: FakeLib())
+    _lib.retain_problem(11)
+    _lib.retain_problem(11)
+    _lib.retain_problem(12)
+    _lib.destroy_problem(11)  # owner gone, two hierarchies still use it
+    _lib.destroy_problem(13)  # used by none: destroyed at once
+    assert destroyed == [13]
+    _lib.release_problem(11)
+    assert destroyed == [13]
+    _lib.release_problem(12)  # its owner is still alive: nothing destroyed
+    _lib.release_problem(11)  # the last user of 11
+    assert destroyed == [13, 11]
+    _lib.destroy_problem(12)
+    assert destroyed == [13, 11, 12] and not _lib._users and not _lib._pending
