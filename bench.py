@@ -68,6 +68,8 @@ def parse():
                     help="only the matrix-free Q2 J*v on the N^3 cube (the case for profiling its kernel)")
     ap.add_argument("--assembly", action="store_true",
                     help="only the Q2 SVK 20x10x10 residual + CSC Jacobian, a few steps (the case for profiling)")
+    ap.add_argument("--newton", type=int, default=0, metavar="N",
+                    help="only the matrix-free Newton + p-MG solve on the Q4 N^3 cube (FP64 and mixed)")
     ap.add_argument("--vcycle", type=int, default=0, metavar="K",
                     help="only K V-cycles of the Q4 16^3 p-multigrid 4 -> 2 -> 1 (the Newton case's preconditioner)")
     return ap.parse_args()
@@ -651,7 +653,7 @@ def vcycle_main(args, n=16):
     torch.cuda.synchronize()
     print(json.dumps({"case": f"V-cycle SVK Q4 {n}^3 -> Q2 -> Q1", "free_dofs": Vs[0].nfree,
                       "coarse_free_dofs": Vs[2].nfree, "cycles": args.vcycle,
-                      "ms_per_cycle": e0.elapsed_time(e1) / args.vcycle}))
+                      "ms_per_cycle": e0.elapsed_time(e1) / args.vcycle, "update_stats_ms": st.stats()}))
 
 
 def newton_case(n=16, loads=(0.1, 0.325, 0.55, 0.775, 1.0)):
@@ -692,7 +694,8 @@ def newton_case(n=16, loads=(0.1, 0.325, 0.55, 0.775, 1.0)):
                                         "final_residual": st.residual_norms[-1],
                                         "coarse_builds": st.pmg["coarse_builds"]}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
-    return {"newton_pmg_svk_q4_16": {"free_dofs": Vs[0].nfree, "levels": "Q4 -> Q2 -> Q1 (assembled, banded Cholesky)",
+    return {f"newton_pmg_svk_q4_{n}": {"free_dofs": Vs[0].nfree, "coarse_free_dofs": Vs[2].nfree,
+                                      "levels": "Q4 -> Q2 -> Q1 (assembled, Cholesky over the band)",
                                      "loads": list(loads), **out}}
 
 
@@ -963,5 +966,7 @@ if __name__ == "__main__":
         profile_main(a)
     elif a.vcycle:
         vcycle_main(a)
+    elif a.newton:
+        print(json.dumps(newton_case(n=a.newton)))
     else:
         engine(a)

@@ -1593,10 +1593,10 @@ void band_prepare(hfk_pmg* m, int64_t n) {
   band_tiles_kernel<<<(int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 64), 256, 0, c->stream>>>(
       n, nb, wt, m->Lb.p, m->cb_W, m->bs_tiles.p, m->bs_diag.p);
   check_launch(c);
-  const size_t smem = tt * sizeof(double);
+  const size_t smem = (tt + tt / 2 + BS_T) * sizeof(double);
   static PerDeviceLimit attr;
   raise_smem_limit(tile_trsm_kernel<BS_T>, smem, attr);
-  tile_trsm_kernel<BS_T><<<2 * nb * (wt + 1), BS_T, smem, c->stream>>>(nb, wt, m->bs_diag.p, m->bs_tiles.p);
+  tile_trsm_kernel<BS_T><<<2 * nb * (wt + 1), 2 * BS_T, smem, c->stream>>>(nb, wt, m->bs_diag.p, m->bs_tiles.p);
   check_launch(c);
 }
 
@@ -1665,7 +1665,7 @@ void coarse_factor_launch(hfk_pmg* m) {
   HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
   for (int k = 0; k < nbt; ++k) {
     const int mq = std::min(W, nbt - 1 - k);
-    band_panel_kernel<<<mq + 1, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p);
+    band_panel_kernel<<<mq + 1, CB_PANEL_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p);
     check_launch(c);
     if (mq > 0) {
       band_update_kernel<<<mq * (mq + 1) / 2, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p);

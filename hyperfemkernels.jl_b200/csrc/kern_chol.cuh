@@ -54,72 +54,132 @@ static __global__ void band_fill_kernel(int64_t n, int nbt, int W, const int64_t
   }
 }
 
-// Cholesky factor of the CB_T x CB_T tile in shared memory D (column-major, leading dimension
-// CB_LD, lower triangle used), in place, unblocked and right-looking: per column, the pivot's
-// square root, the column scaled below it, the trailing lower triangle updated by the column's
-// outer product. Returns (uniform over the CTA) whether every pivot was positive and finite.
-__device__ inline bool tile_cholesky(double* D) {
-  const int tid = threadIdx.x;
-  bool ok = true;
-  for (int c = 0; c < CB_T; ++c) {
-    __syncthreads();  // the previous column's trailing update is complete
-    const double piv = D[c + CB_LD * c];
-    const bool good = piv > 0.0 && piv < INFINITY;  // NaN fails both comparisons
-    ok = ok && good;
-    const double d = sqrt(good ? piv : 1.0);
-    const double inv = 1.0 / d;
-    for (int r = c + 1 + tid; r < CB_T; r += blockDim.x) D[r + CB_LD * c] *= inv;
-    __syncthreads();
-    // the diagonal entry is written here: the trailing update below never reads it
-    if (tid == 0) D[c + CB_LD * c] = d;
-    // trailing update: thread (r, s group) over the columns s = c+1+g, c+1+g+G, ... and row r >= s
-    constexpr int G = CB_THREADS / CB_T;
-    const int r = tid % CB_T;
-    const double lr = r > c ? D[r + CB_LD * c] : 0.0;
-    for (int s = c + 1 + tid / CB_T; s < CB_T; s += G)
-      if (r >= s) D[r + CB_LD * s] -= lr * D[s + CB_LD * c];
-  }
-  __syncthreads();
-  return ok;
-}
+// Panel k, blocked by 16 columns, the tile in shared memory (CB_PANEL_THREADS threads). Per block of
+// 16 columns: (1) one warp factors the 16 x 16 diagonal block, row i in lane i's registers, the
+// pivots and multipliers passed by shuffles (no barrier inside: the chain of dependent pivots is
+// the critical path of the whole factorisation, so it runs at warp latency, with one reciprocal
+// square root per pivot); (2) the rows below are solved against it, one thread per row; (3) the
+// trailing lower triangle takes the block's rank-16 update. Every CTA of the launch factors the
+// tile (no CTA waits for another); CTA 0 stores it. CTA q >= 1 then solves X L_kk^T = A_{k+q,k} by
+// the same blocks: a block of 16 columns of X, then the update of X's later columns.
+// A pivot that is not positive and finite records k + 1 in *info and is replaced by 1.
+constexpr int CB_PANEL_THREADS = 128;
+constexpr int CB_PB = 16;  // columns per block of the panel
 
-// Panel k: CTA 0 stores chol(A_kk); CTA q >= 1 solves X L_kk^T = A_{k+q,k} for the tile below.
-// Dynamic shared memory: two tiles of CB_T x CB_LD doubles.
-static __global__ void __launch_bounds__(CB_THREADS) band_panel_kernel(int nbt, int W, int k, double* Lb, int* info) {
+static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int nbt, int W, int k, double* Lb,
+                                                                             int* info) {
   extern __shared__ __align__(16) double cbs[];
-  double* D = cbs;                  // L_kk
-  double* X = cbs + CB_T * CB_LD;   // the panel tile
-  const int tid = threadIdx.x, q = blockIdx.x;
+  double* A = cbs;                 // the diagonal tile, becoming L_kk (column-major, leading dimension CB_LD)
+  double* X = cbs + CB_T * CB_LD;  // the panel tile below (CTA q >= 1)
+  __shared__ double s_inv[CB_T];   // reciprocals of L_kk's diagonal
+  __shared__ int s_bad;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, q = blockIdx.x;
   double* Akk = Lb + band_tile_offset(k, k, W);
-  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) D[(e % CB_T) + CB_LD * (e / CB_T)] = Akk[e];
+  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) A[(e % CB_T) + CB_LD * (e / CB_T)] = Akk[e];
+  if (tid == 0) s_bad = 0;
   __syncthreads();
-  const bool ok = tile_cholesky(D);
+#pragma unroll 1
+  for (int p0 = 0; p0 < CB_T; p0 += CB_PB) {
+    // (1) the diagonal block, by warp 0
+    if (warp == 0) {
+      const int i = lane & (CB_PB - 1);
+      double b[CB_PB];
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) b[c] = c <= i ? A[(p0 + i) + CB_LD * (p0 + c)] : 0.0;
+      bool ok = true;
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) {
+        const double piv = __shfl_sync(0xffffffffu, b[c], c);
+        const bool good = piv > 0.0 && piv < INFINITY;  // NaN fails both comparisons
+        ok = ok && good;
+        const double pv = good ? piv : 1.0;
+        const double iv = rsqrt(pv);
+        const double l = i > c ? b[c] * iv : (i == c ? pv * iv : 0.0);
+        b[c] = l;
+        if (lane == 0) s_inv[p0 + c] = iv;
+#pragma unroll
+        for (int s2 = c + 1; s2 < CB_PB; ++s2) {
+          const double ls = __shfl_sync(0xffffffffu, l, s2);
+          if (i >= s2) b[s2] = fma(-l, ls, b[s2]);
+        }
+      }
+      if (lane < CB_PB) {
+#pragma unroll
+        for (int c = 0; c < CB_PB; ++c)
+          if (c <= i) A[(p0 + i) + CB_LD * (p0 + c)] = b[c];
+      }
+      if (!ok && lane == 0) s_bad = 1;
+    }
+    __syncthreads();
+    // (2) the rows below the block: x L_pp^T = a, one thread per row
+    const int r = p0 + CB_PB + tid;
+    if (r < CB_T) {
+      double x[CB_PB];
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) x[c] = A[r + CB_LD * (p0 + c)];
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) {
+        const double v = x[c] * s_inv[p0 + c];
+        x[c] = v;
+#pragma unroll
+        for (int s2 = c + 1; s2 < CB_PB; ++s2) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
+      }
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) A[r + CB_LD * (p0 + c)] = x[c];
+    }
+    __syncthreads();
+    // (3) rank-16 update of the trailing lower triangle
+    const int t0 = p0 + CB_PB, m = CB_T - t0;
+    for (int e = tid; e < m * m; e += blockDim.x) {
+      const int rr = t0 + e % m, ss = t0 + e / m;
+      if (rr < ss) continue;
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) acc = fma(A[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], acc);
+      A[rr + CB_LD * ss] -= acc;
+    }
+    __syncthreads();
+  }
   if (q == 0) {
-    if (!ok && tid == 0) atomicCAS(info, 0, k + 1);
+    if (s_bad && tid == 0) atomicCAS(info, 0, k + 1);
     for (int e = tid; e < CB_T * CB_T; e += blockDim.x) {
-      const int r = e % CB_T, c = e / CB_T;
-      Akk[e] = r >= c ? D[r + CB_LD * c] : 0.0;
+      const int rr = e % CB_T, cc = e / CB_T;
+      Akk[e] = rr >= cc ? A[rr + CB_LD * cc] : 0.0;
     }
     return;
   }
-  const int i = k + q;
-  double* Aik = Lb + band_tile_offset(i, k, W);
+  double* Aik = Lb + band_tile_offset(k + q, k, W);
   for (int e = tid; e < CB_T * CB_T; e += blockDim.x) X[(e % CB_T) + CB_LD * (e / CB_T)] = Aik[e];
   __syncthreads();
-  // row r of X: X[r][c] = (A[r][c] - sum_{m<c} X[r][m] L[c][m]) / L[c][c], in place; four threads per
-  // row (h = 0..3) each sum the columns m = h, h + 4, ... and combine by shuffles within the warp
-  const int r = tid >> 2, h = tid & 3;
-  for (int c = 0; c < CB_T; ++c) {
-    double part = 0.0;
-    for (int m = h; m < c; m += 4) part += X[r + CB_LD * m] * D[c + CB_LD * m];
-    part += __shfl_xor_sync(0xffffffffu, part, 1);
-    part += __shfl_xor_sync(0xffffffffu, part, 2);
-    const double v = (X[r + CB_LD * c] - part) / D[c + CB_LD * c];
-    __syncwarp();
-    if (h == 0) X[r + CB_LD * c] = v;
-    __syncwarp();
+#pragma unroll 1
+  for (int p0 = 0; p0 < CB_T; p0 += CB_PB) {
+    // the block of 16 columns of X: row r solves x L_pp^T = a
+    if (tid < CB_T) {
+      double x[CB_PB];
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) x[c] = X[tid + CB_LD * (p0 + c)];
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) {
+        const double v = x[c] * s_inv[p0 + c];
+        x[c] = v;
+#pragma unroll
+        for (int s2 = c + 1; s2 < CB_PB; ++s2) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
+      }
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) X[tid + CB_LD * (p0 + c)] = x[c];
+    }
+    __syncthreads();
+    // the later columns of X: X[r][s] -= sum_c X[r][p0 + c] L[s][p0 + c]
+    const int t0 = p0 + CB_PB, m = CB_T - t0;
+    for (int e = tid; e < CB_T * m; e += blockDim.x) {
+      const int rr = e % CB_T, ss = t0 + e / CB_T;
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < CB_PB; ++c) acc = fma(X[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], acc);
+      X[rr + CB_LD * ss] -= acc;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   for (int e = tid; e < CB_T * CB_T; e += blockDim.x) Aik[e] = X[(e % CB_T) + CB_LD * (e / CB_T)];
 }
 
@@ -181,37 +241,83 @@ __device__ inline double band_entry(const double* Lb, int W, int64_t r, int64_t 
   return Lb[band_tile_offset(i, j, W) + (r % CB_T) + (size_t)CB_T * (c % CB_T)];
 }
 
+// x <- D_hh^-1 x for one half (rows r0 .. r0 + H - 1) of a column, D_hh the half's diagonal block
+// of the triangular D in shared memory (column-major, leading dimension BS): forward (lower) or
+// backward (upper) substitution, right-looking, the column half in registers.
+template <int BS, int H>
+__device__ __forceinline__ void trsm_half(double (&x)[H], const double* Ds, const double* dinv, int r0, bool upper) {
+  if (!upper) {
+#pragma unroll
+    for (int c = 0; c < H; ++c) {
+      const double v = x[c] * dinv[r0 + c];
+      x[c] = v;
+#pragma unroll
+      for (int s2 = c + 1; s2 < H; ++s2) x[s2] = fma(-v, Ds[(r0 + s2) + BS * (r0 + c)], x[s2]);
+    }
+  } else {
+#pragma unroll
+    for (int c = H - 1; c >= 0; --c) {
+      const double v = x[c] * dinv[r0 + c];
+      x[c] = v;
+#pragma unroll
+      for (int s2 = 0; s2 < c; ++s2) x[s2] = fma(-v, Ds[(r0 + s2) + BS * (r0 + c)], x[s2]);
+    }
+  }
+}
+
 // In place X <- D^-1 X for every tile of the block triangular solves (kern_band.cuh layout: 2 nb
 // steps of wt + 1 tiles of BS x BS, diag holding D of each step: lower for the forward direction,
-// upper for the backward one). One CTA per tile, one thread per column of the tile: forward
-// (d = 0) or backward (d = 1) substitution down its column, the column in shared memory and the
-// triangular block read with warp-uniform loads.
+// upper for the backward one). One CTA per tile, D in shared memory, two threads per column of the
+// tile, one per half of it, the half in registers: the half that comes first (top for forward,
+// bottom for backward) is solved with its diagonal block and published in shared memory, then the
+// other half subtracts its coupling to it and is solved with its own diagonal block. The reads of D
+// are uniform over each warp (both halves of a warp's columns run the same instruction stream).
 template <int BS>
-static __global__ void __launch_bounds__(BS) tile_trsm_kernel(int nb, int wt, const double* __restrict__ diag,
-                                                               double* __restrict__ tiles) {
-  extern __shared__ __align__(16) double xs[];  // BS x BS: xs[m * BS + j] = column j's entry m
+static __global__ void __launch_bounds__(2 * BS) tile_trsm_kernel(int nb, int wt, const double* __restrict__ diag,
+                                                                   double* __restrict__ tiles) {
+  constexpr int H = BS / 2;
+  extern __shared__ __align__(16) double trs[];
+  double* Ds = trs;               // BS x BS, column-major
+  double* Xs = trs + BS * BS;     // H x BS: the first half solved, Xs[m * BS + j]
+  double* dinv = Xs + H * BS;     // BS reciprocals of the diagonal
   const int64_t tt = (int64_t)BS * BS;
   const int64_t tile = blockIdx.x;  // d * nb * (wt + 1) + s * (wt + 1) + t
   const int64_t ds = tile / (wt + 1);
-  const int d = (int)(ds / nb);
+  const bool upper = ds / nb != 0;
   const double* Dk = diag + ds * tt;
   double* X = tiles + tile * tt;
-  const int j = threadIdx.x;
-  for (int m = 0; m < BS; ++m) xs[m * BS + j] = X[m + (int64_t)BS * j];
-  if (d == 0) {
-    for (int r = 0; r < BS; ++r) {
-      double s = xs[r * BS + j];
-      for (int m = 0; m < r; ++m) s -= Dk[r + (int64_t)BS * m] * xs[m * BS + j];
-      xs[r * BS + j] = s / Dk[r + (int64_t)BS * r];
-    }
-  } else {
-    for (int r = BS - 1; r >= 0; --r) {
-      double s = xs[r * BS + j];
-      for (int m = r + 1; m < BS; ++m) s -= Dk[r + (int64_t)BS * m] * xs[m * BS + j];
-      xs[r * BS + j] = s / Dk[r + (int64_t)BS * r];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < BS * BS; e += blockDim.x) Ds[e] = Dk[e];
+  for (int e = tid; e < BS; e += blockDim.x) dinv[e] = 1.0 / Dk[e + (int64_t)BS * e];
+  __syncthreads();
+  const int j = tid % BS, h = tid / BS;
+  const int first = upper ? 1 : 0;
+  const int r0 = h * H;
+  double x[H];
+  if (h == first) {
+#pragma unroll
+    for (int i = 0; i < H; ++i) x[i] = X[(r0 + i) + (int64_t)BS * j];
+    trsm_half<BS, H>(x, Ds, dinv, r0, upper);
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      Xs[i * BS + j] = x[i];
+      X[(r0 + i) + (int64_t)BS * j] = x[i];
     }
   }
-  for (int m = 0; m < BS; ++m) X[m + (int64_t)BS * j] = xs[m * BS + j];
+  __syncthreads();
+  if (h != first) {
+    const int m0 = first * H;
+#pragma unroll
+    for (int i = 0; i < H; ++i) x[i] = X[(r0 + i) + (int64_t)BS * j];
+    for (int m = 0; m < H; ++m) {
+      const double xm = Xs[m * BS + j];
+#pragma unroll
+      for (int i = 0; i < H; ++i) x[i] = fma(-Ds[(r0 + i) + BS * (m0 + m)], xm, x[i]);
+    }
+    trsm_half<BS, H>(x, Ds, dinv, r0, upper);
+#pragma unroll
+    for (int i = 0; i < H; ++i) X[(r0 + i) + (int64_t)BS * j] = x[i];
+  }
 }
 
 }  // namespace hfk
