@@ -9,6 +9,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -21,6 +22,7 @@
 #include "kern_band.cuh"
 #include "kern_cell.cuh"
 #include "kern_chol.cuh"
+#include "kern_jv_tc.cuh"
 #include "kern_jvp.cuh"
 #include "kern_mlp.cuh"
 #include "kern_oseen.cuh"
@@ -289,9 +291,41 @@ void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& 
 // Launch shapes: 2 or 4 = warps per CTA of the line-mapped kernel; SHAPE_PT_NARROW / SHAPE_PT_WIDE =
 // the point-parallel product (matrix-free product only) with one cell per CTA or 256 threads
 constexpr int SHAPE_PT_NARROW = 100, SHAPE_PT_WIDE = 108;
+// SHAPE_TC: the FP32 product of Q2 cells with both contractions on the tensor cores (kern_jv_tc.cuh)
+constexpr int SHAPE_TC = 120;
+
+void launch_jv_tc(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<float>& io) {
+  if (!p->tc_tabs.p) {  // the B operands, once per problem (the reference gradients do not change)
+    p->tc_tabs.resize(TC_TAB_FLOATS);
+    tc_tables_kernel<<<16, 256, 0, p->stream>>>(p->dNt.p, p->tc_tabs.p);
+    check_launch(p);
+  }
+  if (!p->tc_err.p) {
+    p->tc_err.resize(1);
+    p->tc_err.zero(p->stream);
+  }
+  static PerDeviceLimit attr;
+  raise_smem_limit(jv_tc_kernel, TC_SMEM, attr);
+  const int grid = (ncl + TC_CELLS - 1) / TC_CELLS;
+  if (grid == 0) return;
+  jv_tc_kernel<<<grid, TC_CELLS, TC_SMEM, p->stream>>>(cell_data(p, cells, ncl), p->tc_tabs.p, io, p->tc_err.p);
+  check_launch(p);
+}
+
+// whether the tensor-core product serves this problem and precision
+template <int MODE, typename R>
+bool tc_eligible(const hfk_problem* p) {
+  return MODE == MODE_JV && std::is_same<R, float>::value && p->Q == 3 && p->P == 3;
+}
 
 template <int Q, int P, int MODE, typename R>
 void launch_shape(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io, int shape) {
+  if constexpr (MODE == MODE_JV && Q == 3 && P == 3 && std::is_same<R, float>::value) {
+    if (shape == SHAPE_TC) {
+      launch_jv_tc(p, cells, ncl, io);
+      return;
+    }
+  }
   if (MODE == MODE_JV && shape == SHAPE_PT_NARROW) launch_jvp<Q, P, R, jvp_narrow<P>()>(p, cells, ncl, io);
   else if (MODE == MODE_JV && shape == SHAPE_PT_WIDE) launch_jvp<Q, P, R, JVP_WIDE>(p, cells, ncl, io);
   else launch_cell<Q, P, MODE, R>(p, cells, ncl, io, shape >= SHAPE_PT_NARROW ? 4 : shape);
@@ -371,24 +405,27 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
       return;
     }
     // (atomic, warps per CTA); the matrix-free product also tries the point-parallel kernel
-    const int cand[8][2] = {{1, 4},
+    const int cand[9][2] = {{1, 4},
                             {1, 2},
                             {0, 4},
                             {0, 2},
                             {1, SHAPE_PT_NARROW},
                             {1, SHAPE_PT_WIDE},
                             {0, SHAPE_PT_NARROW},
-                            {0, SHAPE_PT_WIDE}};
+                            {0, SHAPE_PT_WIDE},
+                            {1, SHAPE_TC}};
     // batched problems keep the line-mapped kernels: the tuning call has every problem active, but
     // most of a batched solve runs with converged problems masked, where the line-mapped kernels'
     // per-warp exit measured better (256 SVK Q2 problems: 22.3 s against 23.9 s with the
     // point-parallel product picked for the Q1 level)
-    const int ncand = MODE == MODE_JV && p->nseg <= 1 ? 8 : 4;
+    const bool tc = tc_eligible<MODE, R>(p) && p->nseg <= 1;
+    const int ncand = MODE == MODE_JV && p->nseg <= 1 ? (tc ? 9 : 8) : 4;
     cudaEvent_t e0, e1;
     HFK_CUDA(cudaEventCreate(&e0));
     HFK_CUDA(cudaEventCreate(&e1));
     float best = 0;
     int pick = 0;
+    std::vector<R> ref, got;  // the tensor-core candidate is kept only if it agrees with the first one
     for (int c = 0; c < ncand; ++c) {
       float t = 1e30f;
       for (int rep = 0; rep < 2; ++rep) {
@@ -400,6 +437,23 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
         float ms = 0;
         HFK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         t = std::min(t, ms);
+      }
+      if (tc && (c == 0 || cand[c][1] == SHAPE_TC)) {
+        std::vector<R>& v = c == 0 ? ref : got;
+        v.resize(p->nfree);
+        HFK_CUDA(cudaMemcpyAsync(v.data(), io.y, p->nfree * sizeof(R), cudaMemcpyDeviceToHost, p->stream));
+        HFK_CUDA(cudaStreamSynchronize(p->stream));
+        if (c > 0) {
+          int err = 0;
+          HFK_CUDA(cudaMemcpy(&err, p->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+          double dmax = 0, rmax = 0;
+          for (int64_t i = 0; i < p->nfree; ++i) {
+            dmax = std::max(dmax, (double)std::fabs((double)got[i] - (double)ref[i]));
+            rmax = std::max(rmax, (double)std::fabs((double)ref[i]));
+          }
+          if (err || !(dmax <= 1e-5 * rmax)) t = 1e30f;  // not eligible
+          if (err) HFK_CUDA(cudaMemset(p->tc_err.p, 0, sizeof(int)));
+        }
       }
       if (c == 0 || t < best) {
         best = t;
@@ -2147,18 +2201,23 @@ int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int
   auto it = p->tuned.find(internal * 2 + (precision == HFK_FP32 ? 1 : 0));
   *atomic = it == p->tuned.end() ? -1 : (int)it->second.first;
   const int shape = it == p->tuned.end() ? 0 : it->second.second;
-  *kernel = shape >= SHAPE_PT_NARROW ? 1 : 0;
-  *warps = shape == SHAPE_PT_NARROW ? (p->P * p->P * p->P + 31) / 32 : (shape == SHAPE_PT_WIDE ? JVP_WIDE / 32 : shape);
+  *kernel = shape == SHAPE_TC ? 2 : (shape >= SHAPE_PT_NARROW ? 1 : 0);
+  *warps = shape == SHAPE_TC ? TC_CELLS / 32
+                             : (shape == SHAPE_PT_NARROW ? (p->P * p->P * p->P + 31) / 32
+                                                         : (shape == SHAPE_PT_WIDE ? JVP_WIDE / 32 : shape));
   HFK_API_END
 }
 
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps) {
   HFK_API_BEGIN
-  HFK_REQUIRE(p && (kernel == 0 || kernel == 1), HFK_ERR_ARG, "kernel must be 0 (line-mapped) or 1 (point-parallel)");
-  HFK_REQUIRE(kernel == 1 || warps == 2 || warps == 4, HFK_ERR_ARG, "the line-mapped kernels take 2 or 4 warps per CTA");
-  HFK_REQUIRE(kernel == 0 || warps == 0 || warps == JVP_WIDE / 32, HFK_ERR_ARG,
+  HFK_REQUIRE(p && kernel >= 0 && kernel <= 2, HFK_ERR_ARG,
+              "kernel must be 0 (line-mapped), 1 (point-parallel) or 2 (tensor cores)");
+  HFK_REQUIRE(kernel != 0 || warps == 2 || warps == 4, HFK_ERR_ARG, "the line-mapped kernels take 2 or 4 warps per CTA");
+  HFK_REQUIRE(kernel != 1 || warps == 0 || warps == JVP_WIDE / 32, HFK_ERR_ARG,
               "the point-parallel product takes 0 (one cell per CTA) or 8 warps per CTA");
-  p->shape = kernel == 0 ? warps : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE);
+  HFK_REQUIRE(kernel != 2 || (p->Q == 3 && p->P == 3), HFK_ERR_UNSUPPORTED,
+              "the tensor-core product serves Q2 cells with 3^3 Gauss points");
+  p->shape = kernel == 0 ? warps : (kernel == 2 ? SHAPE_TC : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE));
   HFK_API_END
 }
 
@@ -2185,6 +2244,18 @@ int hfk_launch_count(hfk_problem* p, int64_t* count) {
   HFK_API_BEGIN
   HFK_REQUIRE(p && count, HFK_ERR_ARG, "null argument");
   *count = p->launches;
+  HFK_API_END
+}
+
+int hfk_problem_device_errors(hfk_problem* p, int* errors) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && errors, HFK_ERR_ARG, "null argument");
+  *errors = 0;
+  if (p->tc_err.p) {
+    HFK_CUDA(cudaMemcpyAsync(errors, p->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    HFK_CUDA(cudaStreamSynchronize(p->stream));
+    HFK_CUDA(cudaMemsetAsync(p->tc_err.p, 0, sizeof(int), p->stream));
+  }
   HFK_API_END
 }
 

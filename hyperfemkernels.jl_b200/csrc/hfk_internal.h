@@ -212,6 +212,9 @@ struct hfk_problem {
   cudaEvent_t many_ev[7] = {};
   hfk::DBuf<int64_t> stage_l;
   hfk::DBuf<float> tmp32a, tmp32b;
+  // the tensor-core product: its B operands (once per problem) and the error word of its bounded waits
+  hfk::DBuf<float> tc_tabs;
+  hfk::DBuf<int> tc_err;
   // error flag for numerical checks
   hfk::DBuf<int> flag;
   // timing of the last kernel sequence (CUDA events)

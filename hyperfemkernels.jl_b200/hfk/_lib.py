@@ -55,6 +55,7 @@ SIGNATURES = {
     "hfk_functional": [_vp, _vp, _vp, _i, _pd],
     "hfk_launch_count": [_vp, _pi64],
     "hfk_problem_set_timing": [_vp, _i],
+    "hfk_problem_device_errors": [_vp, _pi],
     "hfk_problem_kernel_time": [_vp, _pd, _pi64],
     "hfk_device_peak_fp64": [_pd, _pd],
     "hfk_colors": [_vp, _vp],

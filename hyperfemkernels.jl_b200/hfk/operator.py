@@ -73,9 +73,10 @@ class Problem:
 
     def set_launch(self, kernel: str = "line", warps: int = 4):
         """Launch shape under an explicit scatter mode: "line" (the line-mapped kernels, 2 or 4 warps
-        per CTA) or "point" (the point-parallel matrix-free product, warps 0 = one cell per CTA or
-        8)."""
-        call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1}[kernel], int(warps))
+        per CTA), "point" (the point-parallel matrix-free product, warps 0 = one cell per CTA or
+        8) or "tensor" (the FP32 product of Q2 cells with both contractions on the tensor cores;
+        the other kernels then take the line-mapped shape of 4 warps)."""
+        call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1, "tensor": 2}[kernel], int(warps))
 
     def tuning(self, kernel: str = "jv", precision: str = "fp64"):
         """The launch-shape autotuner's choice: {"atomic": bool, "kernel": "line" | "point",
@@ -83,13 +84,20 @@ class Problem:
         a, k, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hfk_problem_tuning", self.h, {"jv": 0, "residual": 1, "jv_stored": 2}[kernel],
              _lib.FP32 if precision == "fp32" else _lib.FP64, ctypes.byref(a), ctypes.byref(k), ctypes.byref(w))
-        return None if a.value < 0 else {"atomic": bool(a.value), "kernel": ("line", "point")[k.value],
+        return None if a.value < 0 else {"atomic": bool(a.value), "kernel": ("line", "point", "tensor")[k.value],
                                          "warps": w.value}
 
     def launches(self) -> int:
         c = ctypes.c_int64()
         call("hfk_launch_count", self.h, ctypes.byref(c))
         return c.value
+
+    def device_errors(self) -> int:
+        """Bounded device waits of this problem's kernels that ran out since the last call
+        (``hfk_problem_device_errors``; 0 in a healthy run)."""
+        e = ctypes.c_int()
+        call("hfk_problem_device_errors", self.h, ctypes.byref(e))
+        return e.value
 
     def set_timing(self, on: bool = True):
         """Bracket every element-kernel launch sequence with CUDA events (``hfk_problem_set_timing``)."""

@@ -91,8 +91,12 @@ int hfk_problem_info(hfk_problem* p, int64_t* nfree, int* Q, int* P, int* ncolor
 int hfk_problem_set_scatter(hfk_problem* p, int mode);
 /* Launch shape under an explicit scatter mode (COLOURED or ATOMIC; AUTO tunes its own): kernel 0,
  * the line-mapped kernels with 2 or 4 warps per CTA (default 4); kernel 1, the point-parallel
- * matrix-free product with one cell per CTA (warps = 0) or 8 warps per CTA (the other kernels
- * then take the line-mapped shape of 4 warps). */
+ * matrix-free product with one cell per CTA (warps = 0) or 8 warps per CTA; kernel 2, the FP32
+ * product of Q2 cells (3^3 Gauss points) with both sum-factorisation contractions as GEMMs on the
+ * tensor cores (tcgen05.mma kind::tf32, operands split hi + lo for FP32 accuracy, 128 cells per
+ * CTA; warps ignored). The other kernels then take the line-mapped shape of 4 warps. Under AUTO
+ * the tensor-core product is a candidate of the FP32 product, kept only when its result agrees
+ * with the line-mapped kernel's to 1e-5. */
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
@@ -120,6 +124,10 @@ int hfk_launch_count(hfk_problem* p, int64_t* count);
  * the summed milliseconds and the number of bracketed sequences since timing was switched on or
  * last read, and starts a new count. */
 int hfk_problem_set_timing(hfk_problem* p, int on);
+/* Bounded device waits of this problem's kernels that ran out since the last call (the tensor-core
+ * product's waits for its MMAs; a kernel whose wait runs out skips its remaining work, frees its
+ * tensor memory and returns), then cleared. 0 in a healthy run; no counterpart in the reference. */
+int hfk_problem_device_errors(hfk_problem* p, int* errors);
 int hfk_problem_kernel_time(hfk_problem* p, double* ms, int64_t* count);
 
 /* FP64 throughput of the current device in TFLOP/s, measured by two microkernels on every SM:
