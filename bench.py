@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--oseen", type=int, default=0, metavar="N",
                     help="only the Oseen P2-P1 assembly on the N^3 tetrahedral cube (the secondary case; 0 = off)")
-    ap.add_argument("--launch", default="auto", choices=["auto", "line2", "line4", "point"],
+    ap.add_argument("--launch", default="auto", choices=["auto", "line2", "line4", "point", "tensor"],
                     help="launch shape of the J*v in --jv (auto: the autotuner's; a fixed one for profiling, "
                          "where the profiler's overhead would skew the autotuner's timings)")
     ap.add_argument("--jv", type=int, default=0, metavar="N",
@@ -415,7 +415,10 @@ def jv_headline_case(torch, dev, stream, T, n=JV_CELLS, cpu=True, launch="auto")
     yd = torch.zeros(nfree, dtype=torch.float64, device=dev)
     if launch != "auto":
         op.problem.set_scatter("atomic")
-        op.problem.set_launch("point" if launch == "point" else "line", 0 if launch == "point" else int(launch[-1]))
+        if launch in ("point", "tensor"):
+            op.problem.set_launch(launch, 0)
+        else:
+            op.problem.set_launch("line", int(launch[-1]))
     mf = MatrixFreeJacobian(op, "recompute")
     mf.prepare(xd, dd)
     h = op.problem.h

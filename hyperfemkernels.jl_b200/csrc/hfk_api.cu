@@ -17,15 +17,14 @@
 #include <cub/device/device_select.cuh>
 
 #include "devcache.h"
+#include "engine.h"
 #include "hfk_internal.h"
 #include "kern_assembly.cuh"
 #include "kern_band.cuh"
 #include "kern_cell.cuh"
 #include "kern_chol.cuh"
-#include "kern_jv_tc.cuh"
 #include "kern_jvp.cuh"
 #include "kern_mlp.cuh"
-#include "kern_oseen.cuh"
 #include "kern_seg.cuh"
 #include "kern_vec.cuh"
 
@@ -38,95 +37,6 @@ void set_error(const std::string& m) { g_last_error = m; }
 }  // namespace hfk
 
 namespace {
-
-PerDeviceValue g_sm_count;
-int sm_count() {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  return g_sm_count.get(dev, [dev] {
-    int n = 0;
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n > 0 ? n : 148;
-  });
-}
-inline int vec_grid(int64_t n, int threads = 256) {
-  int64_t g = (n + threads - 1) / threads;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)sm_count() * 8));
-}
-
-// ---- pointer classification: device-accessible or host ---------------------------------------
-bool is_device_ptr(const void* p) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  cudaError_t e = cudaPointerGetAttributes(&a, p);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
-// Device memory of GPU `device` (or managed memory, which every GPU can reach)
-bool is_device_ptr_on(const void* p, int device) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == device);
-}
-
-// An input vector on the device: the caller's device pointer, or a copy of host data in `stage`
-template <typename T>
-const T* dev_in(const T* p, size_t n, DBuf<T>& stage, cudaStream_t s) {
-  if (!p) return nullptr;
-  if (is_device_ptr(p)) return p;
-  stage.resize(std::max(stage.n, n));
-  if (n) HFK_CUDA(cudaMemcpyAsync(stage.p, p, n * sizeof(T), cudaMemcpyHostToDevice, s));
-  return stage.p;
-}
-// An output vector: device pointer written directly, or staged and copied back by `finish_out`
-template <typename T>
-T* dev_out(T* p, size_t n, DBuf<T>& stage) {
-  if (is_device_ptr(p)) return p;
-  stage.resize(std::max(stage.n, n));
-  return stage.p;
-}
-template <typename T>
-void finish_out(T* p, const T* d, size_t n, cudaStream_t s) {
-  if (p != d && n) {
-    HFK_CUDA(cudaMemcpyAsync(p, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
-    HFK_CUDA(cudaStreamSynchronize(s));
-  }
-}
-
-void check_launch(hfk_problem* p) {
-  p->launches++;
-  HFK_CUDA(cudaGetLastError());
-}
-
-// Kernel timing: an event before and after an element-kernel launch sequence (only with timing on)
-void ktimer_mark(hfk_problem* p) {
-  if (!p->ktiming) return;
-  if (p->kev_used == p->kev.size()) {
-    cudaEvent_t e;
-    HFK_CUDA(cudaEventCreate(&e));
-    p->kev.push_back(e);
-  }
-  HFK_CUDA(cudaEventRecord(p->kev[p->kev_used++], p->stream));
-}
-
-// Raise a kernel's dynamic shared-memory limit on the current device to at least `smem` (`limit`
-// records, per device, what was set).
-template <typename K>
-void raise_smem_limit(K kernel, size_t smem, PerDeviceLimit& limit) {
-  int dev = 0;
-  HFK_CUDA(cudaGetDevice(&dev));
-  limit.raise(dev, smem, [&] {
-    HFK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  });
-}
 
 // ---- 1D Lagrange basis on [0,1], equispaced nodes (lagrange1d, src/tensorproduct.jl:24-47) ----
 void lagrange1d(int Q, double xi, double* N, double* dN) {
@@ -239,7 +149,8 @@ Tab1D<R> make_tab(const hfk_problem* p) {
   return t;
 }
 
-CellData cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) {
+}  // namespace
+CellData hfk::cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) {
   CellData cd;
   cd.ids = p->ids.p;
   cd.cells = cells;
@@ -260,6 +171,7 @@ CellData cell_data(const hfk_problem* p, const int32_t* cells, int ncells_list) 
   for (int c = 0; c < 3; ++c) cd.body[c] = p->params[2 + c];
   return cd;
 }
+namespace {
 
 // ---- cell-kernel dispatch over (Q, P) ----------------------------------------------------------
 template <int Q, int P, int MODE, typename R>
@@ -293,24 +205,6 @@ void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& 
 constexpr int SHAPE_PT_NARROW = 100, SHAPE_PT_WIDE = 108;
 // SHAPE_TC: the FP32 product of Q2 cells with both contractions on the tensor cores (kern_jv_tc.cuh)
 constexpr int SHAPE_TC = 120;
-
-void launch_jv_tc(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<float>& io) {
-  if (!p->tc_tabs.p) {  // the B operands, once per problem (the reference gradients do not change)
-    p->tc_tabs.resize(TC_TAB_FLOATS);
-    tc_tables_kernel<<<16, 256, 0, p->stream>>>(p->dNt.p, p->tc_tabs.p);
-    check_launch(p);
-  }
-  if (!p->tc_err.p) {
-    p->tc_err.resize(1);
-    p->tc_err.zero(p->stream);
-  }
-  static PerDeviceLimit attr;
-  raise_smem_limit(jv_tc_kernel, TC_SMEM, attr);
-  const int grid = (ncl + TC_CELLS - 1) / TC_CELLS;
-  if (grid == 0) return;
-  jv_tc_kernel<<<grid, TC_CELLS, TC_SMEM, p->stream>>>(cell_data(p, cells, ncl), p->tc_tabs.p, io, p->tc_err.p);
-  check_launch(p);
-}
 
 // whether the tensor-core product serves this problem and precision
 template <int MODE, typename R>
@@ -360,12 +254,14 @@ void dispatch_cell(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R
 // Scatter policy: colour by colour (deterministic) unless the colours are too small to fill the
 // GPU, then one launch over all cells with atomicAdd (an order-dependent last bit). A colour needs
 // about 4 warps per SM to hide the gather latency.
-bool use_atomic_scatter(const hfk_problem* p) {
+}  // namespace
+bool hfk::use_atomic_scatter(const hfk_problem* p) {
   // AUTO scatters with atomics: one launch instead of one per colour (no wave tails, no launch
   // gaps), and a fire-and-forget reduction in L2 instead of a dependent read of y before the
   // write (measured on B200, Q2 64^3 J*v: 0.55 ms against 0.75 ms by colour)
   return p->scatter != HFK_SCATTER_COLOURED;
 }
+namespace {
 
 template <int MODE, typename R>
 void run_cells_as(hfk_problem* p, CellIO<R> io, bool atomic, int warps) {
@@ -469,7 +365,8 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
 }
 
 // ---- colouring (color_cells, src/coloring.jl:4-28) --------------------------------------------
-void color_cells(hfk_problem* p) {
+}  // namespace
+void hfk::color_cells(hfk_problem* p) {
   std::vector<unsigned __int128> masks(p->nfree + 1, 0);
   p->h_color_of.assign(p->ncells, 0);
   int ncol = 0;
@@ -496,6 +393,7 @@ void color_cells(hfk_problem* p) {
   for (int cell = 0; cell < p->ncells; ++cell) order[fill[p->h_color_of[cell] - 1]++] = cell;
   p->cells_by_color.upload(order.data(), order.size(), p->stream);
 }
+namespace {
 
 // ---- affine cells and per-cell geometry (affine_cells, src/tables.jl:128-156) ------------------
 void cell_geometry(hfk_problem* p, const double* coords, const double* dMt_caller) {
@@ -633,7 +531,8 @@ void build_seg_of_block(hfk_problem* p, const std::vector<int32_t>& dofs) {
 }
 
 // ---- matrix-free products on device vectors ---------------------------------------------------
-void mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
+}  // namespace
+void hfk::mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
   HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
   HFK_CUDA(cudaMemsetAsync(y, 0, p->nfree * sizeof(double), p->stream));
   CellIO<double> io{};
@@ -649,6 +548,7 @@ void mf_apply_dev(hfk_problem* p, const double* dx, double* y) {
     run_cells<MODE_JV, double>(p, io);
   }
 }
+namespace {
 
 // the FP32 copy of the stored deformation gradients (made on first use after a prepare)
 void ensure_F32(hfk_problem* p) {
@@ -1279,7 +1179,8 @@ __global__ void nzpos_kernel(int ncells, int ndl, const int32_t* ids, const int6
   }
 }
 
-void pattern_build_dev(hfk_problem* p) {
+}  // namespace
+void hfk::pattern_build_dev(hfk_problem* p) {
   if (p->nnz > 0) return;
   HFK_REQUIRE(p->ndl <= 384, HFK_ERR_UNSUPPORTED, "pattern construction supports up to 384 dofs per cell");
   // count keys
@@ -1327,6 +1228,7 @@ void pattern_build_dev(hfk_problem* p) {
   p->nzval.resize(std::max<int64_t>(nnz, 1));
   HFK_CUDA(cudaStreamSynchronize(p->stream));
 }
+namespace {
 
 void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* nzval) {
   pattern_build_dev(p);
@@ -2202,7 +2104,7 @@ int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int
   *atomic = it == p->tuned.end() ? -1 : (int)it->second.first;
   const int shape = it == p->tuned.end() ? 0 : it->second.second;
   *kernel = shape == SHAPE_TC ? 2 : (shape >= SHAPE_PT_NARROW ? 1 : 0);
-  *warps = shape == SHAPE_TC ? TC_CELLS / 32
+  *warps = shape == SHAPE_TC ? JV_TC_WARPS
                              : (shape == SHAPE_PT_NARROW ? (p->P * p->P * p->P + 31) / 32
                                                          : (shape == SHAPE_PT_WIDE ? JVP_WIDE / 32 : shape));
   HFK_API_END
@@ -3623,102 +3525,6 @@ int hfk_pmg_test_coarse_wait(hfk_pmg* m, int polls, int skip_first) {
 }  // extern "C"
 
 // =================================================================================================
-// Allocation-free Chebyshev smoothing
-//
-// hfk_chebyshev_smooth allocates its three work vectors (residual, product, direction) on every
-// call. This variant takes them from one file-scope device array instead, so that a caller whose
-// device memory is fixed after set-up (a host that draws every GPU buffer from a pre-sized pool, or
-// an application that forbids further allocation once its solver is built, since cudaMalloc and
-// cudaFree synchronise the device and may fail once memory is committed) can smooth without any
-// allocation. The array is sized for HFK_NOALLOC_MAX_DOFS free dofs and is held on every GPU that
-// loads the library until the process exits.
-// =================================================================================================
-namespace {
-
-static __device__ __align__(256) double g_noalloc_cheb_scratch[3 * (size_t)HFK_NOALLOC_MAX_DOFS];
-
-constexpr int kNoAllocMaxDevices = 64;
-double* g_noalloc_cheb_addr[kNoAllocMaxDevices] = {nullptr};
-std::mutex g_noalloc_mutex;
-
-// Device address of the scratch array on the current device (resolved once per device).
-double* noalloc_scratch_on(int device) {
-  HFK_REQUIRE(device >= 0 && device < kNoAllocMaxDevices, HFK_ERR_UNSUPPORTED, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_cheb_addr[device]) {
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_cheb_scratch);
-    if (e != cudaSuccess || !ptr)
-      throw Error{HFK_ERR_CUDA, std::string("HyperFEMKernels: cudaGetSymbolAddress of the smoother scratch failed: ") +
-                                    cudaGetErrorString(e)};
-    g_noalloc_cheb_addr[device] = static_cast<double*>(ptr);
-  }
-  return g_noalloc_cheb_addr[device];
-}
-
-// smooth! (src/smoothers.jl:116-146) on caller-provided work vectors r, z, d (same kernels and
-// recurrence as cheb_smooth_dev)
-void cheb_smooth_on(hfk_problem* p, double* r, double* z, double* d, double a, double b, int degree, const double* rhs,
-                    double* x, bool zero_guess, double* residual) {
-  const int64_t n = p->nfree;
-  const double th = (b + a) / 2, de = (b - a) / 2, sg = th / de;
-  if (!zero_guess) mf_apply_dev(p, x, z);
-  cheb_start_kernel<double><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, p->Binv.p, rhs, z, r,
-                                                                         d, x, 1.0 / th, zero_guess ? 1 : 0);
-  check_launch(p);
-  double rho = 1.0 / sg;
-  for (int i = 1; i <= degree; ++i) {
-    if (i == degree && !residual) break;
-    mf_apply_dev(p, d, z);
-    const bool last = i == degree;
-    double c1 = 0, c2 = 0, rn = 0;
-    if (!last) {
-      rn = 1.0 / (2 * sg - rho);
-      c1 = rn * rho;
-      c2 = 2 * rn / de;
-    }
-    cheb_step_kernel<double><<<vec_grid(p->nblocks), 256, 0, p->stream>>>(p->nblocks, p->bdofs.p, p->Binv.p, z, r, d, x,
-                                                                          c1, c2, last ? 0 : 1);
-    check_launch(p);
-    if (last) break;
-    rho = rn;
-  }
-  if (residual) HFK_CUDA(cudaMemcpyAsync(residual, r, n * sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
-}
-
-}  // namespace
-
-extern "C" int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, int degree, const double* rhs,
-                                            double* x, int zero_guess, double* residual) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(p && rhs && x && degree >= 1 && b > a, HFK_ERR_ARG, "invalid argument");
-  HFK_REQUIRE(p->nfree <= (int64_t)HFK_NOALLOC_MAX_DOFS, HFK_ERR_ARG,
-              "hfk_chebyshev_smooth_noalloc supports at most " + std::to_string((long long)HFK_NOALLOC_MAX_DOFS) +
-                  " free dofs (this operator has " + std::to_string((long long)p->nfree) +
-                  "); use hfk_chebyshev_smooth");
-  HFK_REQUIRE(is_device_ptr(rhs) && is_device_ptr(x) && (!residual || is_device_ptr(residual)), HFK_ERR_ARG,
-              "hfk_chebyshev_smooth_noalloc takes device pointers only (staging host data would allocate)");
-  HFK_REQUIRE(is_device_ptr_on(rhs, p->device) && is_device_ptr_on(x, p->device) &&
-                  (!residual || is_device_ptr_on(residual, p->device)),
-              HFK_ERR_ARG, "hfk_chebyshev_smooth_noalloc: rhs, x and residual must be memory of the operator's GPU");
-  HFK_REQUIRE(p->prepared, HFK_ERR_STATE, "the matrix-free Jacobian has not been prepared (call hfk_mf_prepare)");
-  HFK_REQUIRE(p->nblocks > 0 && p->blocks_ok, HFK_ERR_STATE, "blocks not built (call hfk_blocks_update)");
-  int dev = 0;
-  HFK_CUDA(cudaGetDevice(&dev));
-  HFK_REQUIRE(dev == p->device, HFK_ERR_STATE, "the current device is not the operator's device");
-  double* scratch = noalloc_scratch_on(dev);
-  const int64_t n = p->nfree;
-  double* r = scratch;
-  double* z = scratch + n;
-  double* d = scratch + 2 * n;
-  // the array keeps the previous call's values: start from zeros
-  HFK_CUDA(cudaMemsetAsync(scratch, 0, 3 * n * sizeof(double), p->stream));
-  cheb_smooth_on(p, r, z, d, a, b, degree, rhs, x, zero_guess != 0, residual);
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-// =================================================================================================
 // Learned correction: the network, its training, and its place after the V-cycle
 // =================================================================================================
 namespace {
@@ -3926,280 +3732,6 @@ int hfk_pmg_mlp_sample(hfk_pmg* m, const double* r, float* feats, float* targets
     throw;
   }
   m->mlp = net;
-  HFK_API_END
-}
-
-}  // extern "C"
-
-// =================================================================================================
-// Oseen–BDF step on Taylor–Hood P2–P1 tetrahedra (the reference's Oseen volume group,
-// test/common.jl:164-228; assembly driver src/assembly.jl:909-927, :1413-1505)
-// =================================================================================================
-struct hfk_oseen {
-  hfk_problem base;  // ids, colours, CSC pattern and positions (34 local dofs, the caller's order)
-  int nq = 0;
-  DBuf<double> w, N2, dN2, H2, N1, dN1, un, und, unm1, unm1d;
-  double rho = 1, mu = 1e-3, dt = 1e-3;
-  int bdf2 = 1;
-  // outlet boundary group (0 facets: none)
-  int nf = 0, nqf = 0;
-  DBuf<int32_t> fcell, fface;
-  DBuf<double> farea, fnormal, fw, fN;
-  double Pc = 0.7, ZA = 2.3;
-};
-
-namespace {
-OseenData oseen_data(hfk_oseen* o, const int32_t* cells, int n) {
-  OseenData d;
-  d.ids = o->base.ids.p;
-  d.cells = cells;
-  d.ncells_list = n;
-  d.coords = o->base.coords.p;
-  d.w = o->w.p;
-  d.N2 = o->N2.p;
-  d.dN2 = o->dN2.p;
-  d.H2 = o->H2.p;
-  d.N1 = o->N1.p;
-  d.dN1 = o->dN1.p;
-  d.un = o->un.p;
-  d.und = o->und.p;
-  d.unm1 = o->unm1.p;
-  d.unm1d = o->unm1d.p;
-  d.nq = o->nq;
-  d.rho = o->rho;
-  d.mu = o->mu;
-  d.bdf2 = o->bdf2;
-  d.c0 = o->bdf2 ? 1.5 / o->dt : 1.0 / o->dt;  // BDF coefficients (test/common.jl:183-185)
-  d.c1 = o->bdf2 ? 2.0 / o->dt : 1.0 / o->dt;
-  d.c2 = o->bdf2 ? 0.5 / o->dt : 0.0;
-  return d;
-}
-
-void oseen_run(hfk_oseen* o, OseenIO io) {
-  hfk_problem* p = &o->base;
-  const size_t smem = (size_t)OseenSmem{o->nq}.total() * sizeof(double);
-  static PerDeviceLimit attr;
-  raise_smem_limit(oseen_kernel, smem, attr);
-  if (use_atomic_scatter(p)) {
-    io.atomic = 1;
-    oseen_kernel<<<p->ncells, OS_THREADS, smem, p->stream>>>(oseen_data(o, nullptr, p->ncells), io);
-    check_launch(p);
-    return;
-  }
-  io.atomic = 0;
-  for (int c = 0; c < p->ncolors; ++c) {
-    const int n = p->color_start[c + 1] - p->color_start[c];
-    if (!n) continue;
-    oseen_kernel<<<n, OS_THREADS, smem, p->stream>>>(oseen_data(o, p->cells_by_color.p + p->color_start[c], n), io);
-    check_launch(p);
-  }
-}
-
-// the outlet boundary group after the volume terms (atomic scatter: its facets are few)
-void oseen_run_outlet(hfk_oseen* o, OseenIO io) {
-  if (!o->nf) return;
-  hfk_problem* p = &o->base;
-  OutletData fd{o->nf, o->nqf, o->fcell.p, o->fface.p, o->farea.p, o->fnormal.p, o->fw.p, o->fN.p, o->Pc, o->ZA};
-  oseen_outlet_kernel<<<o->nf, 128, 0, p->stream>>>(oseen_data(o, nullptr, p->ncells), fd, io);
-  check_launch(p);
-}
-
-void oseen_set_params(hfk_oseen* o, const double* params, int nparams) {
-  HFK_REQUIRE(params && nparams == 4, HFK_ERR_ARG, "Oseen parameters: rho, mu, dt, bdf2 (0 or 1)");
-  HFK_REQUIRE(params[0] > 0 && params[1] > 0 && params[2] > 0, HFK_ERR_ARG, "rho, mu and dt must be positive");
-  o->rho = params[0];
-  o->mu = params[1];
-  o->dt = params[2];
-  o->bdf2 = params[3] != 0;
-}
-}  // namespace
-
-extern "C" {
-
-int hfk_oseen_create(hfk_oseen** out, int ncells, int nq, const double* w, const double* N2, const double* dN2,
-                     const double* H2, const double* N1, const double* dN1, const double* coords,
-                     const int32_t* cell_dof_ids, int64_t nfree, int64_t ndir, const double* params, int nparams) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(out, HFK_ERR_ARG, "null output handle");
-  *out = nullptr;
-  HFK_REQUIRE(ncells > 0 && nq > 0 && nq <= OS_MAXQ, HFK_ERR_ARG, "invalid sizes (ncells > 0, 0 < nq <= 64)");
-  HFK_REQUIRE(w && N2 && dN2 && H2 && N1 && dN1 && coords && cell_dof_ids, HFK_ERR_ARG, "null input array");
-  HFK_REQUIRE(nfree >= 0 && ndir >= 0 && nfree < (1ll << 31), HFK_ERR_ARG, "invalid dof counts");
-  auto o = std::make_unique<hfk_oseen>();
-  oseen_set_params(o.get(), params, nparams);
-  hfk_problem* p = &o->base;
-  p->ncells = ncells;
-  p->ndl = OS_NDL;
-  p->nn = OS_NDL;
-  p->np = nq;
-  p->nfree = nfree;
-  p->ndir = ndir;
-  HFK_CUDA(cudaGetDevice(&p->device));
-  HFK_CUDA(cudaStreamCreate(&p->own_stream));
-  p->stream = p->own_stream;
-  const size_t nids = (size_t)OS_NDL * ncells;
-  for (size_t k = 0; k < nids; ++k)
-    HFK_REQUIRE(cell_dof_ids[k] <= nfree && -(int64_t)cell_dof_ids[k] <= ndir, HFK_ERR_ARG, "cell dof id out of range");
-  p->h_ids.assign(cell_dof_ids, cell_dof_ids + nids);
-  p->nodeperm.resize(OS_NDL);
-  for (int i = 0; i < OS_NDL; ++i) p->nodeperm[i] = i;
-  p->ids.upload(cell_dof_ids, nids, p->stream);
-  p->coords.upload(coords, (size_t)12 * ncells, p->stream);
-  o->nq = nq;
-  o->w.upload(w, nq, p->stream);
-  o->N2.upload(N2, (size_t)OS_NV * nq, p->stream);
-  o->dN2.upload(dN2, (size_t)OS_NV * 3 * nq, p->stream);
-  o->H2.upload(H2, (size_t)OS_NV * 9, p->stream);
-  o->N1.upload(N1, (size_t)OS_NP * nq, p->stream);
-  o->dN1.upload(dN1, (size_t)OS_NP * 3 * nq, p->stream);
-  for (auto* b : {&o->un, &o->unm1}) {
-    b->resize(std::max<int64_t>(nfree, 1));
-    b->zero(p->stream);
-  }
-  for (auto* b : {&o->und, &o->unm1d}) {
-    b->resize(std::max<int64_t>(ndir, 1));
-    b->zero(p->stream);
-  }
-  color_cells(p);
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  *out = o.release();
-  HFK_API_END
-}
-
-int hfk_oseen_destroy(hfk_oseen* o) {
-  HFK_API_BEGIN
-  if (!o) return HFK_OK;
-  if (o->base.own_stream) {
-    cudaStreamSynchronize(o->base.own_stream);
-    cudaStreamDestroy(o->base.own_stream);
-  }
-  delete o;
-  HFK_API_END
-}
-
-int hfk_oseen_set_params(hfk_oseen* o, const double* params, int nparams) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o, HFK_ERR_ARG, "null handle");
-  oseen_set_params(o, params, nparams);
-  HFK_API_END
-}
-
-int hfk_oseen_set_scatter(hfk_oseen* o, int mode) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && (mode == HFK_SCATTER_AUTO || mode == HFK_SCATTER_COLOURED || mode == HFK_SCATTER_ATOMIC),
-              HFK_ERR_ARG, "scatter mode must be HFK_SCATTER_AUTO, _COLOURED or _ATOMIC");
-  o->base.scatter = mode;
-  HFK_API_END
-}
-
-int hfk_oseen_set_history(hfk_oseen* o, const double* un, const double* und, const double* unm1, const double* unm1d) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && un && unm1 && ((und && unm1d) || o->base.ndir == 0), HFK_ERR_ARG, "null argument");
-  hfk_problem* p = &o->base;
-  auto copy_in = [&](DBuf<double>& dst, const double* src, int64_t n) {
-    if (n) HFK_CUDA(cudaMemcpyAsync(dst.p, src, n * sizeof(double), cudaMemcpyDefault, p->stream));
-  };
-  copy_in(o->un, un, p->nfree);
-  copy_in(o->unm1, unm1, p->nfree);
-  if (p->ndir) {
-    copy_in(o->und, und, p->ndir);
-    copy_in(o->unm1d, unm1d, p->ndir);
-  }
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-int hfk_oseen_pattern(hfk_oseen* o, int64_t* nnz) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && nnz, HFK_ERR_ARG, "null argument");
-  pattern_build_dev(&o->base);
-  *nnz = o->base.nnz;
-  HFK_API_END
-}
-
-int hfk_oseen_pattern_get(hfk_oseen* o, int64_t* colptr, int64_t* rowval) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o, HFK_ERR_ARG, "null handle");
-  hfk_problem* p = &o->base;
-  pattern_build_dev(p);
-  if (colptr) {
-    int64_t* d = dev_out(colptr, p->nfree + 1, p->stage_l);
-    HFK_CUDA(cudaMemcpyAsync(d, p->colptr.p, (p->nfree + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, p->stream));
-    finish_out(colptr, d, p->nfree + 1, p->stream);
-  }
-  if (rowval) {
-    int64_t* d = dev_out(rowval, p->nnz, p->stage_l);
-    HFK_CUDA(cudaMemcpyAsync(d, p->rowval.p, p->nnz * sizeof(int64_t), cudaMemcpyDeviceToDevice, p->stream));
-    finish_out(rowval, d, p->nnz, p->stream);
-  }
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-int hfk_oseen_residual(hfk_oseen* o, const double* x, const double* dvals, double* b) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && x && b && (dvals || o->base.ndir == 0), HFK_ERR_ARG, "null argument");
-  hfk_problem* p = &o->base;
-  OseenIO io{};
-  io.mode = 0;
-  io.x = dev_in(x, p->nfree, p->stage_in, p->stream);
-  io.dvals = dvals ? dev_in(dvals, p->ndir, p->stage_in2, p->stream) : nullptr;
-  io.b = dev_out(b, p->nfree, p->stage_out);
-  HFK_CUDA(cudaMemsetAsync(io.b, 0, p->nfree * sizeof(double), p->stream));
-  oseen_run(o, io);
-  oseen_run_outlet(o, io);
-  finish_out(b, io.b, p->nfree, p->stream);
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-int hfk_oseen_jacobian(hfk_oseen* o, double* nzval) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && nzval, HFK_ERR_ARG, "null argument");
-  hfk_problem* p = &o->base;
-  pattern_build_dev(p);
-  OseenIO io{};
-  io.mode = 1;
-  io.nzpos = p->nzpos.p;
-  io.nzval = is_device_ptr(nzval) ? nzval : p->nzval.p;
-  HFK_CUDA(cudaMemsetAsync(io.nzval, 0, p->nnz * sizeof(double), p->stream));
-  oseen_run(o, io);
-  oseen_run_outlet(o, io);
-  finish_out(nzval, io.nzval, p->nnz, p->stream);
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-int hfk_oseen_set_outlet(hfk_oseen* o, int nfacets, const int32_t* cells, const int32_t* faces, const double* areas,
-                         const double* normals, int nq, const double* w, const double* N, double Pc, double ZA) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && nfacets >= 0, HFK_ERR_ARG, "invalid argument");
-  HFK_REQUIRE(nfacets == 0 || (cells && faces && areas && normals && w && N && nq > 0 && nq <= OS_MAXQF), HFK_ERR_ARG,
-              "outlet facets: null array or 0 < nq <= 32 violated");
-  hfk_problem* p = &o->base;
-  for (int f = 0; f < nfacets; ++f)
-    HFK_REQUIRE(cells[f] >= 0 && cells[f] < p->ncells && faces[f] >= 0 && faces[f] < 4, HFK_ERR_ARG,
-                "outlet facet: cell or local face out of range");
-  o->nf = nfacets;
-  o->nqf = nq;
-  o->Pc = Pc;
-  o->ZA = ZA;
-  if (nfacets) {
-    o->fcell.upload(cells, nfacets, p->stream);
-    o->fface.upload(faces, nfacets, p->stream);
-    o->farea.upload(areas, nfacets, p->stream);
-    o->fnormal.upload(normals, 3 * (size_t)nfacets, p->stream);
-    o->fw.upload(w, nq, p->stream);
-    o->fN.upload(N, (size_t)OS_NV * nq * 4, p->stream);
-  }
-  HFK_CUDA(cudaStreamSynchronize(p->stream));
-  HFK_API_END
-}
-
-int hfk_oseen_launch_count(hfk_oseen* o, int64_t* count) {
-  HFK_API_BEGIN
-  HFK_REQUIRE(o && count, HFK_ERR_ARG, "null argument");
-  *count = o->base.launches;
   HFK_API_END
 }
 

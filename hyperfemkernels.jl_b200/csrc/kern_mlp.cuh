@@ -57,7 +57,7 @@ __device__ __forceinline__ void mlp_forward_one(const float* ws, const float* x,
 }
 
 // inference: out (n x 3) = MLP(feats (n x 16))
-__global__ void __launch_bounds__(128) mlp_forward_kernel(int64_t n, const __nv_bfloat16* wb, const float* feats,
+static __global__ void __launch_bounds__(128) mlp_forward_kernel(int64_t n, const __nv_bfloat16* wb, const float* feats,
                                                           float* out) {
   extern __shared__ float mlp_ws[];
   float* ws = mlp_ws;
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(int64_t n, const __nv_
 // one atomicAdd per parameter and block into the FP32 gradient vector.
 constexpr int MLP_CHUNK = 64;
 
-__global__ void __launch_bounds__(128) mlp_grad_kernel(int64_t n, const __nv_bfloat16* wb, const float* feats,
+static __global__ void __launch_bounds__(128) mlp_grad_kernel(int64_t n, const __nv_bfloat16* wb, const float* feats,
                                                        const float* targets, float inv_count, float* grad,
                                                        float* loss) {
   extern __shared__ float mlp_sm[];
@@ -178,7 +178,7 @@ constexpr size_t mlp_grad_smem_bytes() {
 }
 
 // Adam on the FP32 master weights, then the BF16 copy the forward pass reads
-__global__ void mlp_adam_kernel(int np, float* w, __nv_bfloat16* wb, const float* g, float* m1, float* m2, float lr,
+static __global__ void mlp_adam_kernel(int np, float* w, __nv_bfloat16* wb, const float* g, float* m1, float* m2, float lr,
                                 float b1, float b2, float eps, float c1, float c2) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
     const float gi = g[i];
@@ -190,7 +190,7 @@ __global__ void mlp_adam_kernel(int np, float* w, __nv_bfloat16* wb, const float
   }
 }
 
-__global__ void mlp_to_bf16_kernel(int np, const float* w, __nv_bfloat16* wb) {
+static __global__ void mlp_to_bf16_kernel(int np, const float* w, __nv_bfloat16* wb) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) wb[i] = __float2bfloat16(w[i]);
 }
 
@@ -198,7 +198,7 @@ __global__ void mlp_to_bf16_kernel(int np, const float* w, __nv_bfloat16* wb) {
 // feats[b] = [s/ss, (Binv s)/sm, r/sr, y/sy, log lam, log mu, 0, 0]; the dofs of block b = bdofs[3b..]
 // Per-segment scales: scales[seg * sstride + j], j = 0..3 the root mean squares of s, Binv s, r, y;
 // loglm[2 seg], loglm[2 seg + 1] = log lambda, log mu of the segment (one segment: segb null).
-__global__ void mlp_features_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* Binv,
+static __global__ void mlp_features_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* Binv,
                                     const double* s, const double* r, const double* y, const double* scales,
                                     int sstride, const float* loglm, float* feats) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
@@ -226,7 +226,7 @@ __global__ void mlp_features_kernel(int nb, const int32_t* dofs, const int32_t* 
     f[15] = 0.f;
   }
 }
-__global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* segb, const float* out,
+static __global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* segb, const float* out,
                                    const double* scales, int sstride, double* delta) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     const double sc = scales[(size_t)(segb ? segb[b] : 0) * sstride + 3];
@@ -236,7 +236,7 @@ __global__ void mlp_scatter_kernel(int nb, const int32_t* dofs, const int32_t* s
     }
   }
 }
-__global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* e,
+static __global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* segb, const double* e,
                                    const double* scales, int sstride, float* t) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     const double s1 = scales[(size_t)(segb ? segb[b] : 0) * sstride + 3];
@@ -252,7 +252,7 @@ __global__ void mlp_targets_kernel(int nb, const int32_t* dofs, const int32_t* s
 // minimises (a residual-norm test would reject any prediction with small high-frequency noise).
 // c = nrm + seg * stride: c[0] = delta . s, c[1] = delta . A delta.
 __device__ __forceinline__ double mlp_step(const double* c) { return (c[0] > 0 && c[1] > 0) ? c[0] / c[1] : 0.0; }
-__global__ void mlp_accept_kernel(int64_t n, const int32_t* seg, const double* nrm, int stride, const double* delta,
+static __global__ void mlp_accept_kernel(int64_t n, const int32_t* seg, const double* nrm, int stride, const double* delta,
                                   double* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double w = mlp_step(nrm + (size_t)(seg ? seg[i] : 0) * stride);
@@ -260,7 +260,7 @@ __global__ void mlp_accept_kernel(int64_t n, const int32_t* seg, const double* n
   }
 }
 // one CTA: *accepted += the number of segments with a positive step
-__global__ void mlp_accept_count_kernel(int nseg, const double* nrm, int stride, int* accepted) {
+static __global__ void mlp_accept_count_kernel(int nseg, const double* nrm, int stride, int* accepted) {
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();

@@ -72,7 +72,7 @@ struct OseenSmem {
   __host__ __device__ int total() const { return rc() + 20 * nq; }
 };
 
-__global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO io) {
+static __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO io) {
   extern __shared__ __align__(16) double osm[];
   __shared__ int32_t sid[OS_NDL];
   const OseenSmem L{d.nq};
@@ -316,7 +316,7 @@ struct OutletData {
   double Pc, ZA;
 };
 
-__global__ void __launch_bounds__(128) oseen_outlet_kernel(OseenData d, OutletData fd, OseenIO io) {
+static __global__ void __launch_bounds__(128) oseen_outlet_kernel(OseenData d, OutletData fd, OseenIO io) {
   __shared__ double phi[OS_MAXQF][OS_NV], c1[OS_MAXQF], c2[OS_MAXQF], dS[OS_MAXQF], uq[OS_MAXQF][3];
   __shared__ double unl[30], uml[30], xl[30];
   __shared__ int32_t sid[OS_NDL];

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(RED_THREADS) seg_dots_kernel(int k, const int6
 }
 
 // out[s * stride + j] = sum over the chunks of segment s (one CTA per segment)
-__global__ void __launch_bounds__(RED_THREADS) seg_finish_kernel(int k, const int32_t* first, const double* partial,
+static __global__ void __launch_bounds__(RED_THREADS) seg_finish_kernel(int k, const int32_t* first, const double* partial,
                                                                  double* out, int stride) {
   const int s = blockIdx.x;
   const int f = first[s], e = first[s + 1];
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(RED_THREADS) seg_finish_kernel(int k, const in
 constexpr int SEG_MDOTS = 16;  // vectors per multi-dot launch
 
 // partial[it * SEG_MDOTS + j] = sum over chunk it of V_j[i] w[i], j < k <= SEG_MDOTS (V_j = V + j ldv)
-__global__ void __launch_bounds__(RED_THREADS) seg_mdots_kernel(int k, const int64_t* lo, const int64_t* hi,
+static __global__ void __launch_bounds__(RED_THREADS) seg_mdots_kernel(int k, const int64_t* lo, const int64_t* hi,
                                                                 const double* V, int64_t ldv, const double* w,
                                                                 double* partial) {
   const int it = blockIdx.x;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(RED_THREADS) seg_mdots_kernel(int k, const int
 }
 
 // out[s * stride + j] = sum over the chunks of segment s, j < k (one CTA per segment)
-__global__ void __launch_bounds__(RED_THREADS) seg_mfinish_kernel(int k, const int32_t* first, const double* partial,
+static __global__ void __launch_bounds__(RED_THREADS) seg_mfinish_kernel(int k, const int32_t* first, const double* partial,
                                                                   double* out, int stride) {
   const int s = blockIdx.x;
   const int f = first[s], e = first[s + 1];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(RED_THREADS) seg_mfinish_kernel(int k, const i
 }
 
 // y[i] -= sum_{j<k} c[seg(i) * stride + j] V_j[i]
-__global__ void seg_maxpy_kernel(int64_t n, const int32_t* seg, int k, const double* c, int stride, const double* V,
+static __global__ void seg_maxpy_kernel(int64_t n, const int32_t* seg, int k, const double* c, int stride, const double* V,
                                  int64_t ldv, double* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double* cs = c + (size_t)seg_at(seg, i) * stride;
@@ -102,7 +102,7 @@ __global__ void seg_maxpy_kernel(int64_t n, const int32_t* seg, int k, const dou
 }
 
 // dst[s * stride + j] += src[s * stride + j], j < k, every segment s
-__global__ void seg_add_kernel(int ns, int k, const double* src, double* dst, int stride) {
+static __global__ void seg_add_kernel(int ns, int k, const double* src, double* dst, int stride) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ns * k; e += gridDim.x * blockDim.x) {
     const int s = e / k, j = e - s * k;
     dst[(size_t)s * stride + j] += src[(size_t)s * stride + j];
@@ -110,14 +110,14 @@ __global__ void seg_add_kernel(int ns, int k, const double* src, double* dst, in
 }
 
 // y[i] += sign * a[seg(i) * stride] x[i]
-__global__ void seg_axpy_kernel(int64_t n, const int32_t* seg, const double* a, int stride, double sign,
+static __global__ void seg_axpy_kernel(int64_t n, const int32_t* seg, const double* a, int stride, double sign,
                                 const double* x, double* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] += sign * a[(size_t)seg_at(seg, i) * stride] * x[i];
 }
 
 // y[i] = x[i] / s[seg(i) * stride] (0 where the scale is 0)
-__global__ void seg_scale_kernel(int64_t n, const int32_t* seg, const double* s, int stride, const double* x,
+static __global__ void seg_scale_kernel(int64_t n, const int32_t* seg, const double* s, int stride, const double* x,
                                  double* y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double v = s[(size_t)seg_at(seg, i) * stride];
@@ -127,14 +127,14 @@ __global__ void seg_scale_kernel(int64_t n, const int32_t* seg, const double* s,
 
 // s[j * stride] = sqrt(max(s[j * stride], 0)) for every segment j (a rounding-negative square of a
 // vanished vector, possible in the P^-1 inner product, is a breakdown, not a NaN)
-__global__ void seg_sqrt_kernel(int nseg, double* s, int stride) {
+static __global__ void seg_sqrt_kernel(int nseg, double* s, int stride) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nseg; j += gridDim.x * blockDim.x)
     s[(size_t)j * stride] = sqrt(fmax(s[(size_t)j * stride], 0.0));
 }
 
 // sc[out] = sc[den] > 0 ? sc[num] / sc[den] : 0 per segment; then sc[den] = sc[num] when `shift`
 // (the fixed-count CG of the inexact coarse solve: alpha = rz / pq, beta = rz' / rz)
-__global__ void seg_ratio_kernel(int nseg, double* sc, int num, int den, int out, int shift) {
+static __global__ void seg_ratio_kernel(int nseg, double* sc, int num, int den, int out, int shift) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     double* c = sc + (size_t)s * SEG_NS;
     const double d = c[den];
@@ -144,7 +144,7 @@ __global__ void seg_ratio_kernel(int nseg, double* sc, int num, int den, int out
 }
 
 // one CTA: count the active segments into *nactive
-__device__ void seg_count_active(int nseg, const int* fl, int* nactive) {
+static __device__ void seg_count_active(int nseg, const int* fl, int* nactive) {
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
@@ -156,7 +156,7 @@ __device__ void seg_count_active(int nseg, const int* fl, int* nactive) {
 }
 
 // start of a solve: tol = atol + rtol ||b||; a segment is active while ||r|| > tol
-__global__ void seg_cg_init_kernel(int nseg, double* sc, int* fl, double rtol, double atol, int* nactive) {
+static __global__ void seg_cg_init_kernel(int nseg, double* sc, int* fl, double rtol, double atol, int* nactive) {
   for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
     double* c = sc + (size_t)s * SEG_NS;
     int* f = fl + (size_t)s * SEG_NF;
@@ -174,7 +174,7 @@ __global__ void seg_cg_init_kernel(int nseg, double* sc, int* fl, double rtol, d
 
 // alpha = rz / pq for the active segments; a non-positive curvature stops the segment as
 // indefinite (src/solvers.jl:135-139); inactive segments get alpha = 0 (their iterates stay)
-__global__ void seg_cg_alpha_kernel(int nseg, double* sc, int* fl) {
+static __global__ void seg_cg_alpha_kernel(int nseg, double* sc, int* fl) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     double* c = sc + (size_t)s * SEG_NS;
     int* f = fl + (size_t)s * SEG_NF;
@@ -193,7 +193,7 @@ __global__ void seg_cg_alpha_kernel(int nseg, double* sc, int* fl) {
 }
 
 // x += alpha p, r -= alpha q per segment (rold = r before the update, for the flexible beta)
-__global__ void seg_cg_update_kernel(int64_t n, const int32_t* seg, const double* sc, const double* p, const double* q,
+static __global__ void seg_cg_update_kernel(int64_t n, const int32_t* seg, const double* sc, const double* p, const double* q,
                                      double* x, double* r, double* rold) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double a = sc[(size_t)seg_at(seg, i) * SEG_NS + S_ALPHA];
@@ -205,7 +205,7 @@ __global__ void seg_cg_update_kernel(int64_t n, const int32_t* seg, const double
 }
 
 // convergence test on the recursive residual; counts the segments still active
-__global__ void seg_cg_check_kernel(int nseg, const double* sc, int* fl, int* nactive) {
+static __global__ void seg_cg_check_kernel(int nseg, const double* sc, int* fl, int* nactive) {
   for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
     const double* c = sc + (size_t)s * SEG_NS;
     int* f = fl + (size_t)s * SEG_NF;
@@ -219,7 +219,7 @@ __global__ void seg_cg_check_kernel(int nseg, const double* sc, int* fl, int* na
 }
 
 // beta per segment: Polak-Ribiere (flexible) (z.r - z.rold) / rz, else z.r / rz; rz <- z.r
-__global__ void seg_cg_beta_kernel(int nseg, double* sc, const int* fl, int flexible) {
+static __global__ void seg_cg_beta_kernel(int nseg, double* sc, const int* fl, int flexible) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     double* c = sc + (size_t)s * SEG_NS;
     double b = 0;
@@ -230,25 +230,25 @@ __global__ void seg_cg_beta_kernel(int nseg, double* sc, const int* fl, int flex
 }
 
 // p = z + sc[slot] p per segment
-__global__ void seg_xpby_kernel(int64_t n, const int32_t* seg, const double* sc, int slot, const double* z, double* p) {
+static __global__ void seg_xpby_kernel(int64_t n, const int32_t* seg, const double* sc, int slot, const double* z, double* p) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = z[i] + sc[(size_t)seg_at(seg, i) * SEG_NS + slot] * p[i];
 }
 
 // the cell kernels' segment flags from a batched solve's flags (value = -1: set every flag to 1)
-__global__ void seg_mask_kernel(int nseg, const int* fl, int32_t* mask, int value) {
+static __global__ void seg_mask_kernel(int nseg, const int* fl, int32_t* mask, int value) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
     mask[s] = value < 0 ? fl[(size_t)s * SEG_NF + F_ACTIVE] : value;
 }
 
 // x[i] *= f[seg(i)]
-__global__ void seg_mul_kernel(int64_t n, const int32_t* seg, const double* f, double* x) {
+static __global__ void seg_mul_kernel(int64_t n, const int32_t* seg, const double* f, double* x) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] *= f[seg_at(seg, i)];
 }
 
 // v[s * stride + j] = sqrt(v[s * stride + j] / n_s) for j < k (root mean squares per segment)
-__global__ void seg_rms_kernel(int nseg, double* v, int stride, int k, const int64_t* off) {
+static __global__ void seg_rms_kernel(int nseg, double* v, int stride, int k, const int64_t* off) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     const double ns = (double)(off[s + 1] - off[s]);
     for (int j = 0; j < k; ++j) {

@@ -47,7 +47,7 @@ __global__ void dots_kernel(int64_t n, int k, const R* a0, const R* b0, const R*
   if (k > 2) block_sum_store(s2, partial + 2 * gridDim.x + blockIdx.x);
 }
 
-__global__ void finish_sums_kernel(int nparts, int k, const double* partial, double* out) {
+static __global__ void finish_sums_kernel(int nparts, int k, const double* partial, double* out) {
   for (int j = 0; j < k; ++j) {
     double s = 0;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += partial[j * nparts + i];
@@ -71,7 +71,7 @@ __global__ void axpby_kernel(int64_t n, R a, const R* x, R b, R* y) {
 }
 // z = a x + b y
 // x *= a
-__global__ void scale_kernel(int64_t n, double a, double* x) {
+static __global__ void scale_kernel(int64_t n, double a, double* x) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] *= a;
 }
 template <typename R>
@@ -79,7 +79,7 @@ __global__ void axpbyz_kernel(int64_t n, R a, const R* x, R b, const R* y, R* z)
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) z[i] = a * x[i] + b * y[i];
 }
 // CG update: x += alpha p; rold = r; r -= alpha q
-__global__ void cg_update_kernel(int64_t n, double alpha, const double* p, const double* q, double* x, double* r,
+static __global__ void cg_update_kernel(int64_t n, double alpha, const double* p, const double* q, double* x, double* r,
                                  double* rold) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const double ri = r[i];
@@ -103,7 +103,7 @@ struct BlockIO {
   int atomic;              // 1: atomicAdd into B (all cells in one launch)
 };
 
-__global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
+static __global__ void __launch_bounds__(256) blocks_kernel(CellData cd, BlockIO io) {
   extern __shared__ __align__(16) double sm[];
   const int np = io.np, nn = io.nn, ndl = 3 * nn;
   double* xl = sm;               // ndl
@@ -350,7 +350,7 @@ constexpr size_t blocks_tp_smem() {
 }
 
 // _invert_blocks! (src/preconditioners.jl:312-327): fixed components -> identity rows/columns
-__global__ void invert_blocks_kernel(int nb, const int32_t* dofs, const double* B, double* Binv, float* Binv32,
+static __global__ void invert_blocks_kernel(int nb, const int32_t* dofs, const double* B, double* Binv, float* Binv32,
                                      int* bad) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     double M[9];
@@ -664,7 +664,7 @@ __global__ void prolongate_tp_kernel(XferData t, XferTP tp, const R* __restrict_
 }
 
 // inject_field! (src/transfers.jl:295-313)
-__global__ void inject_kernel(XferData t, int ncells, const double* xf, const double* df, double* xc, double* dc) {
+static __global__ void inject_kernel(XferData t, int ncells, const double* xf, const double* df, double* xc, double* dc) {
   const int per = 3 * t.NC;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)ncells * per;
        e += (int64_t)gridDim.x * blockDim.x) {
@@ -686,7 +686,7 @@ __global__ void inject_kernel(XferData t, int ncells, const double* xf, const do
 
 // ---- dense coarse solve -----------------------------------------------------------------------
 // CSC (1-based) -> dense column-major n x n
-__global__ void csc_to_dense_kernel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+static __global__ void csc_to_dense_kernel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                                     double* A) {
   for (int64_t c = blockIdx.x; c < n; c += gridDim.x)
     for (int64_t k = colptr[c] - 1 + threadIdx.x; k < colptr[c + 1] - 1; k += blockDim.x)
