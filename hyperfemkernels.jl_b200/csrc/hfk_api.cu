@@ -1230,7 +1230,10 @@ void hfk::pattern_build_dev(hfk_problem* p) {
 }
 namespace {
 
-void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* nzval) {
+// after_chunk (atomic scatter only): the cells are launched in the chunks of jc_start, and
+// after_chunk(k) runs (on the host, in launch order) right after chunk k's launch
+void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* nzval,
+                  const std::function<void(int)>* after_chunk = nullptr) {
   pattern_build_dev(p);
   HFK_CUDA(cudaMemsetAsync(nzval, 0, p->nnz * sizeof(double), p->stream));
   const bool g = p->nn == 27;
@@ -1264,7 +1267,13 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   // colour (HFK_SCATTER_COLOURED) the adds of one nonzero come one launch after another, in colour
   // order, and the result is reproducible bit for bit
   ktimer_mark(p);
-  if (use_atomic_scatter(p)) {
+  if (use_atomic_scatter(p) && after_chunk) {
+    for (size_t k = 0; k + 1 < p->jc_start.size(); ++k) {
+      const int c0 = p->jc_start[k], n = p->jc_start[k + 1] - c0;
+      if (n) launch(p->jc_cells.p + c0, n);
+      (*after_chunk)((int)k);
+    }
+  } else if (use_atomic_scatter(p)) {
     if (p->ncells) launch(nullptr, p->ncells);
   } else {
     for (int c = 0; c < p->ncolors; ++c) {
@@ -1273,6 +1282,38 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
     }
   }
   ktimer_mark(p);
+}
+
+// The chunks of the host-output assembly (once per problem): at least two full waves of CTAs each,
+// at most 8; per chunk the CSC values that are complete once it has run: the columns below the
+// smallest free dof any later chunk's cells touch (every cell of a later chunk adds only to the
+// columns of its own dofs)
+void jacobian_chunks(hfk_problem* p) {
+  if (!p->jc_start.empty()) return;
+  const int K = (int)std::max<int64_t>(1, std::min<int64_t>(8, p->ncells / (2 * (int64_t)sm_count() * 2)));
+  p->jc_start.assign(K + 1, 0);
+  for (int k = 0; k <= K; ++k) p->jc_start[k] = (int)((int64_t)p->ncells * k / K);
+  std::vector<int32_t> all(p->ncells);
+  for (int c = 0; c < p->ncells; ++c) all[c] = c;
+  p->jc_cells.upload(all.data(), all.size(), p->stream);
+  std::vector<int64_t> colptr(p->nfree + 1);
+  HFK_CUDA(cudaMemcpyAsync(colptr.data(), p->colptr.p, colptr.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                           p->stream));
+  HFK_CUDA(cudaStreamSynchronize(p->stream));
+  // smallest free id (1-based) over the cells from chunk k on, for k = K-1 .. 1
+  std::vector<int64_t> minid(K + 1, p->nfree + 1);
+  for (int k = K - 1; k >= 0; --k) {
+    int64_t m = minid[k + 1];
+    for (int c = p->jc_start[k]; c < p->jc_start[k + 1]; ++c)
+      for (int j = 0; j < p->ndl; ++j) {
+        const int32_t id = p->h_ids[(size_t)c * p->ndl + j];
+        if (id > 0) m = std::min<int64_t>(m, id);
+      }
+    minid[k] = m;
+  }
+  p->jc_done.assign(K, p->nnz);
+  for (int k = 0; k + 1 < K; ++k) p->jc_done[k] = colptr[minid[k + 1] - 1] - 1;  // columns < minid - 1
+  p->jc_done[K - 1] = p->nnz;
 }
 
 void residual_dev(hfk_problem* p, const double* u, const double* dvals, double* b) {
@@ -2058,6 +2099,11 @@ int hfk_problem_destroy(hfk_problem* p) {
   for (cudaEvent_t e : p->many_ev)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->kev) cudaEventDestroy(e);
+  if (p->jc_copy) {
+    cudaStreamSynchronize(p->jc_copy);
+    cudaStreamDestroy(p->jc_copy);
+  }
+  for (cudaEvent_t e : p->jc_ev) cudaEventDestroy(e);
   delete p;
   cudaGetLastError();  // a release reports nothing: leave no error behind for the next checked call
   HFK_API_END
@@ -2255,8 +2301,34 @@ int hfk_jacobian(hfk_problem* p, const double* x, const double* dvals, double* n
   const double* dx = dev_in(x, p->nfree, p->stage_in, p->stream);
   const double* dd = dvals ? dev_in(dvals, p->ndir, p->stage_in2, p->stream) : nullptr;
   double* dn = dev_out(nzval, p->nnz, p->stage_out);
-  jacobian_dev(p, dx, dd, dn);
-  finish_out(nzval, dn, p->nnz, p->stream);
+  if (dn != nzval && use_atomic_scatter(p) && p->ncells > 0 && p->nnz > 0) {
+    // host output: each chunk's finished prefix of the values travels to the host while the next
+    // chunk is assembled (the copies on their own stream, ordered after the chunk by an event)
+    jacobian_chunks(p);
+    const int K = (int)p->jc_done.size();
+    if (!p->jc_copy) HFK_CUDA(cudaStreamCreateWithFlags(&p->jc_copy, cudaStreamNonBlocking));
+    while ((int)p->jc_ev.size() < K) {
+      cudaEvent_t e;
+      HFK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      p->jc_ev.push_back(e);
+    }
+    int64_t sent = 0;
+    const std::function<void(int)> after = [&](int k) {
+      HFK_CUDA(cudaEventRecord(p->jc_ev[k], p->stream));
+      HFK_CUDA(cudaStreamWaitEvent(p->jc_copy, p->jc_ev[k], 0));
+      const int64_t upto = p->jc_done[k];
+      if (upto > sent) {
+        HFK_CUDA(cudaMemcpyAsync(nzval + sent, dn + sent, (upto - sent) * sizeof(double), cudaMemcpyDeviceToHost,
+                                 p->jc_copy));
+        sent = upto;
+      }
+    };
+    jacobian_dev(p, dx, dd, dn, &after);
+    HFK_CUDA(cudaStreamSynchronize(p->jc_copy));
+  } else {
+    jacobian_dev(p, dx, dd, dn);
+    finish_out(nzval, dn, p->nnz, p->stream);
+  }
   HFK_API_END
 }
 

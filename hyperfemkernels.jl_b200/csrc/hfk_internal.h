@@ -212,6 +212,13 @@ struct hfk_problem {
   cudaEvent_t many_ev[7] = {};
   hfk::DBuf<int64_t> stage_l;
   hfk::DBuf<float> tmp32a, tmp32b;
+  // hfk_jacobian into host memory: the cells in chunks; once a chunk has run, the prefix of the CSC
+  // values that no later chunk touches is copied back on jc_copy while the next chunk is assembled
+  hfk::DBuf<int32_t> jc_cells;            // 0 .. ncells - 1
+  std::vector<int> jc_start;              // chunk boundaries (cells), nchunks + 1
+  std::vector<int64_t> jc_done;           // per chunk: the CSC values complete once it has run
+  cudaStream_t jc_copy = nullptr;
+  std::vector<cudaEvent_t> jc_ev;
   // the tensor-core product: its B operands (once per problem) and the error word of its bounded waits
   hfk::DBuf<float> tc_tabs;
   hfk::DBuf<int> tc_err;
