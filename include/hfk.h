@@ -100,8 +100,8 @@ int hfk_problem_set_scatter(hfk_problem* p, int mode);
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
- * warp's lanes on the tensor lines of a few cells) or 1 (point-parallel product: one thread per
- * quadrature point), warps per CTA; atomic = -1 if that kernel has not run under AUTO yet. No
+ * warp's lanes on the tensor lines of a few cells), 1 (point-parallel product: one thread per
+ * quadrature point) or 2 (the FP32 Q2 product on the tensor cores), warps per CTA; atomic = -1 if that kernel has not run under AUTO yet. No
  * counterpart in the reference. */
 int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* kernel, int* warps);
 
@@ -124,11 +124,11 @@ int hfk_launch_count(hfk_problem* p, int64_t* count);
  * the summed milliseconds and the number of bracketed sequences since timing was switched on or
  * last read, and starts a new count. */
 int hfk_problem_set_timing(hfk_problem* p, int on);
+int hfk_problem_kernel_time(hfk_problem* p, double* ms, int64_t* count);
 /* Bounded device waits of this problem's kernels that ran out since the last call (the tensor-core
  * product's waits for its MMAs; a kernel whose wait runs out skips its remaining work, frees its
  * tensor memory and returns), then cleared. 0 in a healthy run; no counterpart in the reference. */
 int hfk_problem_device_errors(hfk_problem* p, int* errors);
-int hfk_problem_kernel_time(hfk_problem* p, double* ms, int64_t* count);
 
 /* FP64 throughput of the current device in TFLOP/s, measured by two microkernels on every SM:
  * the FP64 tensor-core MMA (mma m8n8k4 f64, the instruction of the assembly's element products)
