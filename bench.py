@@ -316,14 +316,18 @@ def engine(args):
     flops = C0_FLOPS_PER_CELL * ncells
     peak = max(dmma.value, dfma.value)
     achieved = flops / (kernel_ms * 1e-3) / 1e12
-    # DRAM bytes (read + write) of one launch of jacobian_kernel_g<27, true> on this configuration
-    # (ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch)
+    # DRAM bytes (read + write) of one launch of the assembly kernel on this configuration (ncu
+    # dram__bytes_read.sum + dram__bytes_write.sum, one launch), scaled by the cells of this rank
     traffic = C0_TRAFFIC_BYTES * ncells / 2000 if C0_TRAFFIC_BYTES else None
     alg_bytes = 8 * nnz + 4 * 81 * 81 * ncells + 4 * 81 * ncells + 8 * (V.nfree + V.ndir)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "jacobian_kernel_g<27,true> (FP64 mma m8n8k4 element products)",
+                "traffic": traffic,
+                "kernel": "jacobian_kernel_sym27<TP> (FP64 FMA: symmetric element blocks, sum-factorised "
+                          "contraction, persistent CTAs)",
                 "kernel_ms": kernel_ms, "flops_per_launch": flops,
-                "flops_source": "benchmark/roofline.jl:65-74: 1 180 980 FP64 flops per Q2 cell (products + G)",
+                "flops_source": "benchmark/roofline.jl:65-74: 1 180 980 FP64 flops per Q2 cell (products + G), the "
+                                "reference's dense formulation; the kernel executes about 0.37 MFLOP per cell "
+                                "(symmetric blocks only, sum-factorised contraction)",
                 "peak_source": "FP64 measured in-process on this GPU (hfk_device_peak_fp64: mma m8n8k4 f64 "
                                f"{dmma.value:.1f} TFLOP/s, DFMA {dfma.value:.1f} TFLOP/s); the measured-peaks file "
                                "has no FP64 figure",
@@ -361,8 +365,9 @@ def engine(args):
         dist.destroy_process_group()
 
 
-# DRAM traffic of one jacobian_kernel_g launch on the 20x10x10 case (ncu, per launch); None = not captured
-C0_TRAFFIC_BYTES = None
+# DRAM traffic of one jacobian_kernel_sym27<TP> launch on the 20x10x10 case (ncu, one launch:
+# 125 709 312 B read + 18 921 472 B written); None = not captured
+C0_TRAFFIC_BYTES = 144630784
 
 
 def assembly_extra(torch, dev, stream, op, xd, dd, nz, T):
@@ -610,11 +615,27 @@ def profile_main(args):
         dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).to(dev)
         nz = torch.zeros(nnz, dtype=torch.float64, device=dev)
         b = torch.zeros(V.nfree, dtype=torch.float64, device=dev)
-        ms_j = T.steps(lambda: _lib.call("hfk_jacobian", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz)),
-                       20, 3) / 20
-        ms_r = T.steps(lambda: _lib.call("hfk_residual", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(b)),
-                       20, 3) / 20
-        out = {"case": "assembly Q2 SVK 20x10x10", "jacobian_ms": ms_j, "residual_ms": ms_r, "nnz": int(nnz)}
+        def jac():
+            _lib.call("hfk_jacobian", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
+
+        # both element-block kernels: the FP64 FMA one (default) and the FP64 tensor-core one
+        out = {"case": "assembly Q2 SVK 20x10x10", "nnz": int(nnz)}
+        vals = {}
+        for kern in ("fma", "tensor"):
+            op.problem.set_assembly_kernel(kern)
+            jac()
+            op.problem.set_timing(True)
+            ms_j = T.steps(jac, 20, 3) / 20
+            k_ms, k_n = op.problem.kernel_time()
+            op.problem.set_timing(False)
+            vals[kern] = nz.cpu().numpy().copy()
+            out[f"jacobian_ms_{kern}"] = ms_j
+            out[f"kernel_ms_{kern}"] = k_ms / max(k_n, 1)
+        op.problem.set_assembly_kernel("fma")
+        out["rel_diff_fma_vs_tensor"] = float(np.linalg.norm(vals["fma"] - vals["tensor"]) /
+                                              np.linalg.norm(vals["tensor"]))
+        out["residual_ms"] = T.steps(lambda: _lib.call("hfk_residual", op.problem.h, _lib.ptr(xd), _lib.ptr(dd),
+                                                       _lib.ptr(b)), 20, 3) / 20
     elif args.jv:
         out = jv_headline_case(torch, dev, stream, T, n=args.jv, cpu=False, launch=args.launch)
     else:

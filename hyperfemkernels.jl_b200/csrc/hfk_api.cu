@@ -284,7 +284,8 @@ void run_cells_as(hfk_problem* p, CellIO<R> io, bool atomic, int warps) {
 // per CTA of the line-mapped kernel and, for the matrix-free product, the point-parallel kernel of
 // 8 warps), timed with CUDA events, and the fastest is kept. Outputs are zeroed before each
 // candidate and once more before the real run. No tuning while the stream is being captured (the
-// V-cycle is captured from its second application, when every kernel of it has run once).
+// V-cycle is captured from its second application, when every kernel of it has run once) nor inside
+// the allocation-free smoother (an untuned kernel runs with the atomic scatter and 4 warps there).
 template <int MODE, typename R>
 void run_cells(hfk_problem* p, CellIO<R> io) {
   if (p->scatter != HFK_SCATTER_AUTO) {
@@ -296,7 +297,7 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
   if (it == p->tuned.end()) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     HFK_CUDA(cudaStreamIsCapturing(p->stream, &cs));
-    if (cs != cudaStreamCaptureStatusNone || !io.y) {
+    if (cs != cudaStreamCaptureStatusNone || !io.y || p->no_tune) {
       run_cells_as<MODE, R>(p, io, true, 4);
       return;
     }
@@ -1220,7 +1221,9 @@ void hfk::pattern_build_dev(hfk_problem* p) {
   p->colptr.resize(p->nfree + 1);
   pattern_csc_kernel<<<vec_grid(nnz), 256, 0, p->stream>>>(nnz, p->nfree, keys.p, p->rowval.p, p->colptr.p);
   check_launch(p);
-  p->nzpos.resize((size_t)p->ndl * p->ndl * p->ncells);
+  // 16 bytes of slack: the assembly kernels copy a cell's positions in 16-byte pieces from the
+  // 16-byte boundary below its first one, so the last cell's copy may reach 12 bytes past its end
+  p->nzpos.resize((size_t)p->ndl * p->ndl * p->ncells + 4);
   nzpos_kernel<<<vec_grid((int64_t)p->ndl * p->ndl * p->ncells), 256, 0, p->stream>>>(p->ncells, p->ndl, p->ids.p,
                                                                                       p->colptr.p, p->rowval.p,
                                                                                       p->nzpos.p);
@@ -1245,11 +1248,33 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   const size_t smem = asm_smem_bytes(p->nn, p->np, g, ldg);
   HFK_REQUIRE(smem <= 227 * 1024, HFK_ERR_UNSUPPORTED, "too many quadrature points for the assembly kernel");
   HFK_REQUIRE(g || p->nn == 8, HFK_ERR_UNSUPPORTED, "assembled Jacobians support 8- and 27-node cells");
-  // the recognised laws are hyperelastic (symmetric tangent): only the element blocks k >= c are formed
+  // the recognised laws are hyperelastic (symmetric tangent): only the element blocks k >= c are
+  // formed; on 27-node cells by the FP64 FMA kernel when its shared memory fits, else on the FP64
+  // tensor cores
   const bool sym = p->law == HFK_LAW_SVK || p->law == HFK_LAW_LINEAR_ELASTIC;
+  const size_t smem_s = sym27_smem_bytes(p->np, ASM_SYM27_QC);
+  const bool fma27 = g && sym && p->asm_kernel != 1 && smem_s <= 227 * 1024 && sym27_fits(p->np, ASM_SYM27_QC);
   auto kern_g = padded ? (sym ? jacobian_kernel_g<27, true, true> : jacobian_kernel_g<27, true, false>)
                        : (sym ? jacobian_kernel_g<27, false, true> : jacobian_kernel_g<27, false, false>);
-  if (g) {
+  // on Q2 cells with 3^3 Gauss points the product is the sum-factorised contraction
+  const bool tp27 = p->Q == 3 && p->P == 3 && ASM_SYM27_QC == 9;
+  auto kern_s = tp27 ? jacobian_kernel_sym27<true, 9, ASM_SYM27_MINB_TP>
+                     : jacobian_kernel_sym27<false, ASM_SYM27_QC, ASM_SYM27_MINB>;
+  const Tab1D<double> tab = make_tab<double>(p);
+  int grid_s = 0;  // the FMA kernel's persistent CTAs: as many as are resident at once
+  if (fma27) {
+    static PerDeviceLimit attr[2];
+    raise_smem_limit(kern_s, smem_s, attr[tp27]);
+    static PerDeviceValue occ[2];
+    int dev = 0;
+    HFK_CUDA(cudaGetDevice(&dev));
+    const int per_sm = occ[tp27].get(dev, [&] {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern_s, 256, smem_s) != cudaSuccess) b = 1;
+      return std::max(b, 1);
+    });
+    grid_s = per_sm * sm_count();
+  } else if (g) {
     static PerDeviceLimit attr[4];
     raise_smem_limit(kern_g, smem, attr[2 * padded + sym]);
   } else {
@@ -1258,7 +1283,8 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   }
   auto launch = [&](const int32_t* cells, int n) {
     CellData cd = cell_data(p, cells, n);
-    if (g) kern_g<<<n, 256, smem, p->stream>>>(cd, io);
+    if (fma27) kern_s<<<std::min(n, grid_s), 256, smem_s, p->stream>>>(cd, io, tab);
+    else if (g) kern_g<<<n, 256, smem, p->stream>>>(cd, io);
     else jacobian_kernel_direct<8><<<n, 256, smem, p->stream>>>(cd, io);
     check_launch(p);
   };
@@ -2166,6 +2192,14 @@ int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps) {
   HFK_REQUIRE(kernel != 2 || (p->Q == 3 && p->P == 3), HFK_ERR_UNSUPPORTED,
               "the tensor-core product serves Q2 cells with 3^3 Gauss points");
   p->shape = kernel == 0 ? warps : (kernel == 2 ? SHAPE_TC : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE));
+  HFK_API_END
+}
+
+int hfk_problem_set_assembly_kernel(hfk_problem* p, int kernel) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p && (kernel == 0 || kernel == 1), HFK_ERR_ARG,
+              "kernel must be 0 (the default choice) or 1 (the FP64 tensor-core kernel)");
+  p->asm_kernel = kernel;
   HFK_API_END
 }
 

@@ -233,8 +233,10 @@ struct hfk_problem {
   int launches = 0;
   int scatter = HFK_SCATTER_AUTO;
   int shape = 4;  // launch shape under an explicit scatter mode (warps per CTA, or a point-parallel shape)
+  int asm_kernel = 0;  // assembled Jacobian of 27-node cells: 0 the default choice, 1 the FP64 tensor-core kernel
   hfk::DBuf<double> func_red;             // per-warp partials of the functionals
   std::map<int, std::pair<bool, int>> tuned;  // autotuned (atomic scatter, warps per CTA) per kernel mode
+  bool no_tune = false;  // set while a call that must not tune (allocation-free smoothing) runs
   hfk::CGWork cg;
   hfk::GmresWork gm;
 };

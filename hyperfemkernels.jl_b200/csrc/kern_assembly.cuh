@@ -247,6 +247,314 @@ __global__ void __launch_bounds__(256) jacobian_kernel_g(CellData cd, AsmIO io) 
   asm_component<NN, PADDED, SYM, 2>(io, pos, A, Dh, G);
 }
 
+// ---- symmetric tangents on 27-node cells: the element blocks on the FP64 FMA pipe --------------
+// The recognised laws have the major symmetry T[(c,J),(k,L)] = T[(k,L),(c,J)], so the element
+// matrix is symmetric and the blocks k >= c determine it. Their columns form one index j in [0, 162):
+// pair p = 0..5 for (c, k) = (0,0) (0,1) (0,2) (1,1) (1,2) (2,2) and j = 27 p + m. The matrix of
+// all six blocks, K_sym[n][j] = sum_r A^T[n][r] G[r][j] with G[(q,K)][j] = G_c[(q,K)][(k,m)], is
+// one 27 x 162 x 3np product: 243 threads each hold a 3-row x 6-column tile of it in registers and,
+// per k-step, read 3 values of A (9 distinct addresses per warp) and 6 of G (in 16-byte pairs,
+// about 5 distinct column groups per warp) for 18 FMAs. G is built QC points at a time so that
+// three CTAs share an SM; a thread builds three columns (m, m + 9, m + 18) of one pair and point
+// from the pair's 3 x 3 block held in registers. The CTAs are persistent: each loads the reference
+// tables once and then takes cell after cell. Against the tensor-core kernel above this forms
+// 27 x 162 instead of 32 x 192 entries per k-step, on the FP64 FMA pipe, whose measured rate on
+// B200 is above the FP64 MMA's.
+#ifndef HFK_ASM_SYM27_QC
+#define HFK_ASM_SYM27_QC 9  // points per G chunk (73 KB of shared memory per CTA at 27 points: 3 CTAs per SM)
+#endif
+#ifndef HFK_ASM_SYM27_MINB
+#define HFK_ASM_SYM27_MINB 3  // CTAs per SM the register budget is sized for
+#endif
+#ifndef HFK_ASM_SYM27_MINB_TP
+#define HFK_ASM_SYM27_MINB_TP 2  // the same for the tensor-product contraction (27 results per thread)
+#endif
+constexpr int ASM_SYM27_QC = HFK_ASM_SYM27_QC, ASM_SYM27_MINB = HFK_ASM_SYM27_MINB;
+constexpr int ASM_SYM27_MINB_TP = HFK_ASM_SYM27_MINB_TP;
+constexpr int SYM27_COLS = 162;
+constexpr int SYM27_LDG = 164;  // row stride of the G chunk: even, so each row starts on 16 bytes
+constexpr int SYM27_LDK = 29;   // column stride of the staged element blocks
+
+// (c, k) of pair p and the first combined column of component c
+__device__ __forceinline__ void sym27_pair(int p, int& c, int& k) {
+  c = p < 3 ? 0 : (p < 5 ? 1 : 2);
+  k = p < 3 ? p : (p < 5 ? p - 2 : 2);
+}
+
+// staged per cell after the doubles: its positions (81 x 81 from the 16-byte boundary at or below
+// the first: at most 1641 pieces of 16 bytes) and the dof ids of this cell and the next
+constexpr int SYM27_POS_INTS = 6568, SYM27_IDS_INTS = 84;
+__host__ __device__ inline size_t sym27_g_offset(int np) { return ((size_t)181 * np + 91 + 1) & ~(size_t)1; }
+inline size_t sym27_smem_bytes(int np, int qc) {
+  return (sym27_g_offset(np) + (size_t)3 * qc * SYM27_LDG) * sizeof(double) +
+         (SYM27_POS_INTS + 2 * SYM27_IDS_INTS) * sizeof(int32_t);
+}
+
+// asynchronous copies global -> shared (cp.async, completion by wait_group: no polling)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// the staged element blocks (162 columns of stride SYM27_LDK) fit over Dh and the G chunk
+// (Dh starts 100 np + 91 doubles in; from there to the end: 81 np + the chunk, at least)
+inline bool sym27_fits(int np, int qc) { return (size_t)81 * np + 3 * qc * SYM27_LDG >= (size_t)SYM27_COLS * SYM27_LDK; }
+
+// TP: the cell's tables are the tensor product of the 1D tables tab (3 nodes and 3 Gauss points per
+// direction, points in chunks of QC = 9, one z-layer each): the product is then a sum-factorised
+// contraction per column (x and y within a chunk, z accumulated over the chunks), 729 FMAs per
+// column instead of 2187, one thread per column with its 27 results in registers, reading only its
+// own column of G.
+template <bool TP, int QC, int MINB>
+__global__ void __launch_bounds__(256, MINB) jacobian_kernel_sym27(CellData cd, AsmIO io, Tab1D<double> tab) {
+  constexpr int NN = 27, NDL = 81, NT = 256;
+  extern __shared__ __align__(16) double sm[];
+  __shared__ int s_affine;
+  const int np = io.np, R = 3 * np;
+  double* A = sm;                       // (NN, 3, np): A[m + NN * (K + 3q)]
+  double* xl = A + NN * R;              // NDL
+  double* gs = xl + NDL;                // 10: the cell's affine geometry (iJt, |det|)
+  double* Gq = gs + 10;                 // 9 np: reference gradient of u, Gq[q*9 + c*3 + K]
+  double* iJs = Gq + 9 * np;            // 9 np
+  double* dVs = iJs + 9 * np;           // np
+  double* Dh = dVs + np;                // 81 np (the blocks k >= c)
+  double* G = sm + sym27_g_offset(np);  // 3 QC rows x SYM27_LDG
+  int32_t* posS = reinterpret_cast<int32_t*>(G + 3 * QC * SYM27_LDG);  // 16-byte aligned (even offsets)
+  int32_t* idsS = posS + SYM27_POS_INTS;                                // two buffers of SYM27_IDS_INTS
+  const int t = threadIdx.x;
+  // the reference tables, once per CTA (four loads in flight per thread)
+  {
+    const int n = NN * R;
+    int i = t;
+    for (; i + 3 * NT < n; i += 4 * NT) {
+      const double v0 = __ldg(io.dNt + i), v1 = __ldg(io.dNt + i + NT), v2 = __ldg(io.dNt + i + 2 * NT),
+                   v3 = __ldg(io.dNt + i + 3 * NT);
+      A[i] = v0;
+      A[i + NT] = v1;
+      A[i + 2 * NT] = v2;
+      A[i + 3 * NT] = v3;
+    }
+    for (; i < n; i += NT) A[i] = __ldg(io.dNt + i);
+  }
+  static_assert(!TP || QC == 9, "the tensor-product contraction takes one z-layer of 3 x 3 points per chunk");
+  const bool prod = t < 243;
+  const int ig = t % 9, jg = t / 9;  // dense product tile: rows 3 ig .. 3 ig + 2, columns 6 jg .. 6 jg + 5
+  // tensor-product contraction: column jt, 21 per warp so that every scheduler gets two warps
+  const int jt = (t >> 5) * 21 + (t & 31);
+  const bool tcol = (t & 31) < 21 && jt < SYM27_COLS;
+  if (blockIdx.x < cd.ncells_list && t < NDL) {  // the first cell's dof ids
+    const int cell0 = cd.cells ? cd.cells[blockIdx.x] : blockIdx.x;
+    cp_async4(idsS + t, cd.ids + (size_t)cell0 * NDL + t);
+  }
+  cp_async_commit();
+  int buf = 0;
+  for (int li = blockIdx.x; li < cd.ncells_list; li += gridDim.x, buf ^= 1) {
+    const int cell = cd.cells ? cd.cells[li] : li;
+    cp_async_wait_all();
+    __syncthreads();  // this cell's ids have arrived; the previous cell's scatter has read its positions
+    // staged asynchronously while this cell is computed: the next cell's ids and this cell's positions
+    const int lnext = li + gridDim.x;
+    if (lnext < cd.ncells_list && t < NDL) {
+      const int cn = cd.cells ? cd.cells[lnext] : lnext;
+      cp_async4(idsS + SYM27_IDS_INTS * (buf ^ 1) + t, cd.ids + (size_t)cn * NDL + t);
+    }
+    const size_t pa = reinterpret_cast<size_t>(io.nzpos + (size_t)NDL * NDL * cell);
+    const int pofs = (int)((pa & 15) >> 2);
+    {
+      const char* src = reinterpret_cast<const char*>(pa & ~(size_t)15);
+      const int npiece = (int)(((pa & 15) + NDL * NDL * sizeof(int32_t) + 15) >> 4);
+      for (int i = t; i < npiece; i += NT) cp_async16(posS + 4 * i, src + 16 * (size_t)i);
+    }
+    cp_async_commit();
+    // the cell's values, its affine geometry and flag (the previous cell's readers of these are
+    // behind at least three barriers)
+    if (t < NDL) {
+      const int32_t id = idsS[SYM27_IDS_INTS * buf + t];
+      xl[t] = id > 0 ? io.u[id - 1] : (id < 0 ? io.dvals[-id - 1] : 0.0);
+    } else if (t >= 96 && t < 106) {
+      gs[t - 96] = cd.geo[(size_t)cell * 10 + (t - 96)];
+    } else if (t == 128) {
+      s_affine = cd.affine[cell];
+    }
+    __syncthreads();
+    // reference gradient of u per point and component (one thread per entry), geometry per point
+    for (int e = t; e < 9 * np; e += NT) {
+      const int q = e / 9, cK = e - 9 * q, c = cK / 3, K = cK - 3 * c;
+      const double* a = A + NN * (K + 3 * q);
+      const double* x = xl + c * NN;
+      double s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+      for (int n = 0; n < NN; n += 3) {
+        s0 += x[n] * a[n];
+        s1 += x[n + 1] * a[n + 1];
+        s2 += x[n + 2] * a[n + 2];
+      }
+      Gq[e] = s0 + s1 + s2;
+    }
+    const bool aff = s_affine != 0;
+    for (int q = t; q < np; q += NT) {
+      double Jt[9], iJ[9], det;
+      if (aff) {
+        for (int i = 0; i < 9; ++i) iJ[i] = gs[i];
+        det = gs[9];
+      } else {
+        point_jacobian_dev(cd, cell, q, Jt);
+        det = det3(Jt);
+        inv3(Jt, det, iJ);
+        det = fabs(det);
+      }
+      for (int i = 0; i < 9; ++i) iJs[q * 9 + i] = iJ[i];
+      dVs[q] = cd.w[q] * det;
+    }
+    __syncthreads();
+    // per (point, pair): the pulled-back tangent block Dh_q[(c,K),(k,K')]
+    for (int e = t; e < 6 * np; e += NT) {
+      const int q = e / 6;
+      int c, k;
+      sym27_pair(e - 6 * q, c, k);
+      const double* iJ = iJs + q * 9;
+      const double* g = Gq + q * 9;
+      double H[9];  // H[c' + 3J] = sum_K iJ[J + 3K] Gq[c'][K]
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int J = 0; J < 3; ++J)
+          H[cc + 3 * J] = iJ[J] * g[cc * 3] + iJ[J + 3] * g[cc * 3 + 1] + iJ[J + 6] * g[cc * 3 + 2];
+      double Tb[9];
+      law_tangent_block(cd.law, cd.lam_of(cell), cd.mu_of(cell), H, c, k, Tb);
+      double X[3][3];
+#pragma unroll
+      for (int J = 0; J < 3; ++J)
+#pragma unroll
+        for (int Kp = 0; Kp < 3; ++Kp)
+          X[J][Kp] = Tb[J] * iJ[3 * Kp] + Tb[J + 3] * iJ[1 + 3 * Kp] + Tb[J + 6] * iJ[2 + 3 * Kp];
+      const double dV = dVs[q];
+#pragma unroll
+      for (int K = 0; K < 3; ++K)
+#pragma unroll
+        for (int Kp = 0; Kp < 3; ++Kp)
+          Dh[q * 81 + (c * 3 + K) + 9 * (k * 3 + Kp)] =
+              dV * (iJ[3 * K] * X[0][Kp] + iJ[1 + 3 * K] * X[1][Kp] + iJ[2 + 3 * K] * X[2][Kp]);
+    }
+    __syncthreads();
+    double acc[3][6];  // dense product
+    double out[27];    // tensor-product contraction: column jt of the element blocks
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+      for (int h = 0; h < 6; ++h) acc[s][h] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 27; ++i) out[i] = 0.0;
+    for (int q0 = 0; q0 < np; q0 += QC) {
+      const int nq = min(QC, np - q0);
+      // G rows 3 (q - q0) + K, columns 27 p + m: sum_K' Dh_q[(c,K),(k,K')] dN^[m,K',q]; a thread
+      // takes one point and pair and the nodes m = mg, mg + 9, mg + 18
+      for (int e = t; e < nq * 54; e += NT) {
+        const int mg = e % 9, rest = e / 9, pr = rest % 6, qq = rest / 6;
+        int c, k;
+        sym27_pair(pr, c, k);
+        const int q = q0 + qq;
+        const double* D = Dh + q * 81 + c * 3 + 27 * k;  // D[K + 9 K'] = Dh_q[(c,K),(k,K')]
+        const double* a = A + mg + NN * 3 * q;
+        double av[3][3];  // av[i][K'] = dN^[mg + 9 i, K', q]
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int Kp = 0; Kp < 3; ++Kp) av[i][Kp] = a[9 * i + NN * Kp];
+        double* g = G + 3 * qq * SYM27_LDG + 27 * pr + mg;
+#pragma unroll
+        for (int K = 0; K < 3; ++K) {
+          const double d0 = D[K], d1 = D[K + 9], d2 = D[K + 18];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) g[K * SYM27_LDG + 9 * i] = d0 * av[i][0] + d1 * av[i][1] + d2 * av[i][2];
+        }
+      }
+      __syncthreads();
+      if (TP && tcol) {
+        // out[n1 + 3 n2 + 9 n3] += sum_K sum_{q1,q2} Tx(n1,q1) Ty(n2,q2) Tz(n3,q3) G[(q,K)][jt], with T
+        // the derivative table in direction K and the basis table in the others (T(n, q) = N1[3q + n])
+        const int q3 = q0 / 9;
+#pragma unroll
+        for (int K = 0; K < 3; ++K) {
+          const double* Tx = K == 0 ? tab.dN1 : tab.N1;
+          const double* Ty = K == 1 ? tab.dN1 : tab.N1;
+          const double* Tz = K == 2 ? tab.dN1 : tab.N1;
+          double g[9];  // g[q1 + 3 q2]
+#pragma unroll
+          for (int i = 0; i < 9; ++i) g[i] = G[(3 * i + K) * SYM27_LDG + jt];
+          double sx[9];  // sx[n1 + 3 q2]
+#pragma unroll
+          for (int q2 = 0; q2 < 3; ++q2)
+#pragma unroll
+            for (int n1 = 0; n1 < 3; ++n1)
+              sx[n1 + 3 * q2] = Tx[n1] * g[3 * q2] + Tx[3 + n1] * g[1 + 3 * q2] + Tx[6 + n1] * g[2 + 3 * q2];
+#pragma unroll
+          for (int n2 = 0; n2 < 3; ++n2)
+#pragma unroll
+            for (int n1 = 0; n1 < 3; ++n1) {
+              const double u = Ty[n2] * sx[n1] + Ty[3 + n2] * sx[n1 + 3] + Ty[6 + n2] * sx[n1 + 6];
+#pragma unroll
+              for (int n3 = 0; n3 < 3; ++n3) out[n1 + 3 * n2 + 9 * n3] += Tz[3 * q3 + n3] * u;
+            }
+        }
+      }
+      if (!TP && prod) {
+        const double* Ar = A + 3 * ig + NN * 3 * q0;
+        const double* Gr = G + 6 * jg;
+#pragma unroll 3
+        for (int rr = 0; rr < 3 * nq; ++rr) {
+          const double a[3] = {Ar[0], Ar[1], Ar[2]};
+          const double2 b01 = *reinterpret_cast<const double2*>(Gr);
+          const double2 b23 = *reinterpret_cast<const double2*>(Gr + 2);
+          const double2 b45 = *reinterpret_cast<const double2*>(Gr + 4);
+          const double b[6] = {b01.x, b01.y, b23.x, b23.y, b45.x, b45.y};
+#pragma unroll
+          for (int s = 0; s < 3; ++s)
+#pragma unroll
+            for (int h = 0; h < 6; ++h) acc[s][h] += a[s] * b[h];
+          Ar += NN;
+          Gr += SYM27_LDG;
+        }
+      }
+      __syncthreads();
+    }
+    // the element blocks into shared memory, over Dh and the G chunk (both dead now), column by
+    // column: Kt[j * SYM27_LDK + n] (odd stride: both scatter loops below read it without conflicts)
+    double* Kt = Dh;
+    if (TP && tcol)
+#pragma unroll
+      for (int n = 0; n < 27; ++n) Kt[jt * SYM27_LDK + n] = out[n];
+    if (!TP && prod)
+#pragma unroll
+      for (int h = 0; h < 6; ++h)
+#pragma unroll
+        for (int s = 0; s < 3; ++s) Kt[(6 * jg + h) * SYM27_LDK + 3 * ig + s] = acc[s][h];
+    cp_async_wait_all();  // the positions
+    __syncthreads();
+    // scatter: entry (n, c) x (m, k) at its position, n fastest (27 consecutive positions of one
+    // CSC column per 27 threads); then the blocks k > c at the transposed positions, m fastest
+    const int32_t* pos = posS + pofs;
+#pragma unroll 4
+    for (int e = t; e < NN * SYM27_COLS; e += NT) {
+      const int j = e / NN, n = e - NN * j, pr = j / NN, m = j - NN * pr;
+      int c, k;
+      sym27_pair(pr, c, k);
+      scatter_add(io.nzval, pos[(c * NN + n) + NDL * (k * NN + m)], Kt[j * SYM27_LDK + n]);
+    }
+#pragma unroll 4
+    for (int e = t; e < NN * NN * 3; e += NT) {
+      const int m = e % NN, rest = e / NN, n = rest % NN, b = rest / NN;
+      const int pr = b == 0 ? 1 : (b == 1 ? 2 : 4);  // (0,1) (0,2) (1,2)
+      int c, k;
+      sym27_pair(pr, c, k);
+      scatter_add(io.nzval, pos[(k * NN + m) + NDL * (c * NN + n)], Kt[(NN * pr + m) * SYM27_LDK + n]);
+    }
+  }
+}
+
 // Small cells (Q1, any number of points): one thread per element entry
 template <int NN>
 __global__ void __launch_bounds__(256) jacobian_kernel_direct(CellData cd, AsmIO io) {

@@ -100,6 +100,14 @@ extern "C" int hfk_chebyshev_smooth_noalloc(hfk_problem* p, double a, double b, 
   double* d = scratch + 2 * n;
   // the array keeps the previous call's values: start from zeros
   HFK_CUDA(cudaMemsetAsync(scratch, 0, 3 * n * sizeof(double), p->stream));
+  // no autotuning inside this call: the tuner's candidate launches, events and host copies are
+  // work the caller did not ask for (a product not tuned yet runs with the default shape)
+  struct NoTune {
+    hfk_problem* p;
+    bool old;
+    ~NoTune() { p->no_tune = old; }
+  } guard{p, p->no_tune};
+  p->no_tune = true;
   cheb_smooth_on(p, r, z, d, a, b, degree, rhs, x, zero_guess != 0, residual);
   HFK_CUDA(cudaStreamSynchronize(p->stream));
   HFK_API_END

@@ -78,6 +78,11 @@ class Problem:
         the other kernels then take the line-mapped shape of 4 warps)."""
         call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1, "tensor": 2}[kernel], int(warps))
 
+    def set_assembly_kernel(self, kernel: str = "fma"):
+        """Kernel of the assembled Jacobian on 27-node cells: "fma" (default: the element blocks of the
+        symmetric tangent on the FP64 FMA pipe) or "tensor" (on the FP64 tensor cores)."""
+        call("hfk_problem_set_assembly_kernel", self.h, {"fma": 0, "tensor": 1}[kernel])
+
     def tuning(self, kernel: str = "jv", precision: str = "fp64"):
         """The launch-shape autotuner's choice: {"atomic": bool, "kernel": "line" | "point",
         "warps": int} or None (not run yet)."""

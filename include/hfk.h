@@ -98,6 +98,12 @@ int hfk_problem_set_scatter(hfk_problem* p, int mode);
  * the tensor-core product is a candidate of the FP32 product, kept only when its result agrees
  * with the line-mapped kernel's to 1e-5. */
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
+/* Kernel of the assembled Jacobian (hfk_jacobian) on 27-node cells: 0 (default) forms the element
+ * blocks of a symmetric tangent (the recognised laws) on the FP64 FMA pipe, a 27 x 162 register-
+ * tiled product per cell; 1 forms them on the FP64 tensor cores (mma m8n8k4 f64, 8 x 8 tiles). Both
+ * give the reference's jacobian! (src/assembly.jl:918-927) to round-off; no counterpart in the
+ * reference. */
+int hfk_problem_set_assembly_kernel(hfk_problem* p, int kernel);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
  * warp's lanes on the tensor lines of a few cells), 1 (point-parallel product: one thread per
@@ -208,7 +214,9 @@ int hfk_chebyshev_smooth(hfk_problem* p, double a, double b, int degree, const d
  * nothing: its three work vectors live in one file-scope device array sized for
  * HFK_NOALLOC_MAX_DOFS free dofs (3 * 2^19 doubles = 12 MiB, held on every GPU that loads the
  * library until the process exits); larger operators are rejected with HFK_ERR_ARG. rhs, x and
- * residual (NULL allowed) must be device pointers. The first call on a device does the set-up (it
+ * residual (NULL allowed) must be device pointers on the operator's GPU. The launch-shape autotuner
+ * does not run inside this call: a product not tuned yet runs with the default shape (atomic scatter,
+ * 4 warps per CTA). The first call on a device does the set-up (it
  * resolves the array's device address with cudaGetSymbolAddress); make that first call before any
  * stream capture. Every call shares the array and starts by clearing it; calls that overlap on the
  * GPU (from other streams or threads) race on it. The call returns after the smoothing has finished. */

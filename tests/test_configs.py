@@ -6,7 +6,8 @@
   oracle (color_cells, src/coloring.jl:4-28; sparsity / cell_positions!, src/assembly.jl:773-899), the
   FP64 residual and CSC Jacobian within 1e-12 relative (jacobian!, src/assembly.jl:918-927), with the
   atomic and the colour-by-colour scatter. This is what the reference's own equality tests check
-  against Gridap (test/test_gridap_equality.jl:18-36, test/test_assembly.jl:3-21).
+  against Gridap (test/test_gridap_equality.jl:18-36, test/test_assembly.jl:3-21). The element
+  blocks are formed on the FP64 FMA pipe (default) and, once, on the FP64 tensor cores.
 * Matrix-free product at sizes the oracle finishes in seconds: Q2 24^3 (338 541 free dofs) and Q4
   12^3 (the Q4 element of the Newton case): FP64 within 1e-12 of the oracle's stored-tangent mul!
   (src/matrixfree.jl:341-424), FP32 within 2e-6 of it. The FP32 error is printed and must be above
@@ -65,11 +66,12 @@ def test_c0_colours_pattern_and_positions_bit_exact(c0):
     assert np.array_equal(op.nonzero_positions(), orc.nzpos)
 
 
-@pytest.mark.parametrize("scatter", ["atomic", "coloured"])
-def test_c0_residual_and_jacobian_parity(c0, scatter):
+@pytest.mark.parametrize("scatter,kernel", [("atomic", "fma"), ("coloured", "fma"), ("atomic", "tensor")])
+def test_c0_residual_and_jacobian_parity(c0, scatter, kernel):
     V, orc, x = c0
     op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
     op.problem.set_scatter(scatter)
+    op.problem.set_assembly_kernel(kernel)
     d = V.dirichlet_values
     b = op.residual(np.zeros(V.nfree), x)
     assert reldiff(b, orc.residual(x, d)) < TOL64

@@ -62,10 +62,13 @@ def test_residual_parity(order, perturb, law):
     assert reldiff(b, orc.residual(x, V.dirichlet_values)) < TOL64
 
 
-@pytest.mark.parametrize("order,perturb", [(1, 0.0), (2, 0.0), (2, 0.2)])
+@pytest.mark.parametrize("order,perturb,kernel", [(1, 0.0, "fma"), (2, 0.0, "fma"), (2, 0.2, "fma"),
+                                                  (2, 0.0, "tensor"), (2, 0.2, "tensor")])
 @pytest.mark.parametrize("law", ["svk", "linear"])
-def test_jacobian_parity(order, perturb, law):
+def test_jacobian_parity(order, perturb, kernel, law):
+    # Q2: the element blocks on the FP64 FMA pipe (default) and on the FP64 tensor cores
     V, op, orc = make(order, perturb=perturb, law=law)
+    op.problem.set_assembly_kernel(kernel)
     x = svk_state(V, amp=1e-2)
     A = op.allocate_jacobian(x)
     op.jacobian(A, x)
@@ -74,6 +77,19 @@ def test_jacobian_parity(order, perturb, law):
     # a second assembly into the same matrix (zero-fill) gives the same values
     op.jacobian(A, x)
     assert reldiff(A.data, ref) < TOL64
+
+
+@pytest.mark.parametrize("kernel", ["fma", "tensor"])
+def test_jacobian_parity_q2_with_64_points(kernel):
+    # Gauss degree 6 on Q2 cells: 64 points, so the FMA kernel's last chunk of points is partial
+    V = svk_space(n=(3, 2, 2), order=2, perturb=0.1)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 6), forms.svk_jacobian(2.0, 1.0, 6), V)
+    op.problem.set_assembly_kernel(kernel)
+    orc = O.OracleProblem(V, Quadrature.gauss(6))
+    x = svk_state(V, amp=1e-2)
+    A = op.allocate_jacobian(x)
+    op.jacobian(A, x)
+    assert reldiff(A.data, orc.jacobian_values(x, V.dirichlet_values)) < TOL64
 
 
 @pytest.mark.parametrize("order,perturb", CASES)
