@@ -101,3 +101,65 @@ def test_learned_correction_inside_the_pmg():
           f"accepted {st['accepted']}/{st['tried']}")
     assert st["tried"] > 0
     assert its[True] <= its[False] + 2
+
+
+def test_trained_correction_lowers_the_error_of_a_cycle():
+    # What the trained network gains over the method without it, per application of the V-cycle:
+    # the energy-norm error left by one cycle on held-out right-hand sides b = A x* (exact error
+    # known), plain cycle vs cycle + correction with an untrained network vs with the trained one.
+    # The step along the prediction minimises the energy error, so no variant can be worse than the
+    # plain cycle; training must add a clear margin over the untrained network.
+    import torch
+
+    from hfk import forms
+    from hfk import solvers as S
+    from hfk.fespace import CartesianMesh, VectorLagrangeSpace
+    from hfk.learned import MLP, attach, collect_samples
+    from hfk.operator import KernelOperator
+
+    m = CartesianMesh((6, 6, 6))
+    g = [lambda x: 0 * x, lambda x: np.tile([0.05, 0.0, 0.0], (len(x), 1))]
+    Vs = [VectorLagrangeSpace(m, o, ("x0", "x1"), g=g if o == 2 else None) for o in (2, 1)]
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), Vs[0], jacobian="matrixfree")
+    x = torch.from_numpy(np.random.default_rng(0).uniform(-1e-3, 1e-3, Vs[0].nfree)).cuda()
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    st = S.PMultigridState(S.PMultigrid(Vs, S.Chebyshev(degree=2)), mf)
+    assert st.ok
+    feats, targets = [], []
+    for seed in range(4):
+        b = torch.from_numpy(np.random.default_rng(10 + seed).standard_normal(Vs[0].nfree)).cuda()
+        f, t = collect_samples(st, mf, b, cycles=3)
+        feats.append(f)
+        targets.append(t)
+    feats, targets = torch.cat(feats), torch.cat(targets)
+    perm = torch.randperm(feats.shape[0], device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    feats, targets = feats[perm].contiguous(), targets[perm].contiguous()
+    trained = MLP(seed=0)
+    trained.train(feats, targets, steps=800, batch=4096, lr=2e-3)
+    untrained = MLP(seed=7)
+
+    def energy(e):
+        Ae = torch.zeros_like(e)
+        mf.mul(Ae, e)
+        return float(torch.dot(e, Ae)) ** 0.5
+
+    ratios = {}
+    for name, net in (("plain", None), ("untrained", untrained), ("trained", trained)):
+        attach(st, net)
+        rs = []
+        for seed in range(100, 104):  # held out: not among the training right-hand sides
+            xs = torch.from_numpy(np.random.default_rng(seed).standard_normal(Vs[0].nfree)).cuda()
+            b = torch.zeros_like(xs)
+            mf.mul(b, xs)
+            y = torch.zeros_like(xs)
+            st.ldiv(y, b)
+            rs.append(energy(xs - y) / energy(xs))
+        ratios[name] = float(np.mean(rs))
+    attach(st, None)
+    print("energy error left by one cycle (mean of 4 held-out right-hand sides): "
+          + ", ".join(f"{k} {v:.4f}" for k, v in ratios.items()))
+    assert ratios["untrained"] <= ratios["plain"] * (1 + 1e-12)
+    assert ratios["trained"] <= ratios["plain"] * (1 + 1e-12)
+    assert ratios["trained"] < ratios["untrained"]
+    assert ratios["trained"] < 0.95 * ratios["plain"]
