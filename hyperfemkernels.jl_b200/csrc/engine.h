@@ -83,6 +83,8 @@ inline void check_launch(hfk_problem* p) {
 // Kernel timing: an event before and after an element-kernel launch sequence (only with timing on)
 inline void ktimer_mark(hfk_problem* p) {
   if (!p->ktiming) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;  // no event nodes in captured graphs
+  if (cudaStreamIsCapturing(p->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
   if (p->kev_used == p->kev.size()) {
     cudaEvent_t e;
     HFK_CUDA(cudaEventCreate(&e));

@@ -1904,6 +1904,15 @@ void pmg_collect_cycle_time(hfk_pmg* m) {
 void pmg_cycle_on_buffers(hfk_pmg* m) {
   hfk_problem* p0 = m->lv[0];
   cudaStream_t s = p0->stream;
+  // inside a capture of the caller's (the device-driven batched solve) the cycle's kernels are
+  // recorded into that graph directly
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HFK_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    if (m->precision == HFK_FP32) vcycle_dev<float>(m, 0);
+    else vcycle_dev<double>(m, 0);
+    return;
+  }
   // the legacy default stream cannot be captured (a caller that launches its own work there, such
   // as a partitioned solve ordering the engine with torch, gets the cycle uncaptured)
   if (!m->graph_exec && m->cycles_since_update >= 1 && s != cudaStreamLegacy) {
@@ -1995,12 +2004,19 @@ void pmg_apply_dev(hfk_pmg* m, const double* r, double* y) {
     check_launch(p0);
     return;
   }
-  pmg_collect_cycle_time(m);
-  if (!m->ev0) {
-    HFK_CUDA(cudaEventCreate(&m->ev0));
-    HFK_CUDA(cudaEventCreate(&m->ev1));
+  // the cycle is timed with events, except while the stream is being captured (a graph body may
+  // hold no event nodes)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HFK_CUDA(cudaStreamIsCapturing(p0->stream, &cs));
+  const bool timed = cs == cudaStreamCaptureStatusNone;
+  if (timed) {
+    pmg_collect_cycle_time(m);
+    if (!m->ev0) {
+      HFK_CUDA(cudaEventCreate(&m->ev0));
+      HFK_CUDA(cudaEventCreate(&m->ev1));
+    }
+    HFK_CUDA(cudaEventRecord(m->ev0, p0->stream));
   }
-  HFK_CUDA(cudaEventRecord(m->ev0, p0->stream));
   if (m->precision == HFK_FP32) {
     LevelWork<float>& w = *m->w32[0];
     convert_kernel<double, float><<<vec_grid(n), 256, 0, p0->stream>>>(n, r, w.b.p);
@@ -2015,8 +2031,10 @@ void pmg_apply_dev(hfk_pmg* m, const double* r, double* y) {
     HFK_CUDA(cudaMemcpyAsync(y, w.x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, p0->stream));
   }
   if (m->mlp) mlp_correct(m, r, y);
-  HFK_CUDA(cudaEventRecord(m->ev1, p0->stream));
-  m->ev_pending = true;
+  if (timed) {
+    HFK_CUDA(cudaEventRecord(m->ev1, p0->stream));
+    m->ev_pending = true;
+  }
   m->ncycles++;
 }
 
@@ -2192,6 +2210,13 @@ int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps) {
   HFK_REQUIRE(kernel != 2 || (p->Q == 3 && p->P == 3), HFK_ERR_UNSUPPORTED,
               "the tensor-core product serves Q2 cells with 3^3 Gauss points");
   p->shape = kernel == 0 ? warps : (kernel == 2 ? SHAPE_TC : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE));
+  HFK_API_END
+}
+
+int hfk_problem_set_solve_graph(hfk_problem* p, int on) {
+  HFK_API_BEGIN
+  HFK_REQUIRE(p, HFK_ERR_ARG, "null handle");
+  p->solve_graph = on != 0;
   HFK_API_END
 }
 
@@ -3298,6 +3323,67 @@ void solve_gmres_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x,
   *converged = conv;
 }
 
+// The remaining iterations of the batched CG as one CUDA graph: a while node whose body is one
+// iteration (both halves, captured from the engine's own launches) and a last kernel that counts
+// the iteration and sets the loop condition (a segment still active, the limit not reached). The
+// host launches it once and waits. After the last check finds no active segment the body's second
+// half still runs once; it changes only the direction and its scalars, which nothing reads after
+// the loop. Returns the iteration count reached, or -1 (nothing launched) if the graph could not be
+// built, in which case the caller continues on the host.
+int seg_cg_device_loop(hfk_problem* op, const std::function<void()>& step_half,
+                       const std::function<void()>& direction_half, hfk::CGWork& cw, int it0, int maxiter) {
+  cudaStream_t s = op->stream;
+  cw.itd.resize(1);
+  set_int_kernel<<<1, 1, 0, s>>>(cw.itd.p, it0);
+  check_launch(op);
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  bool built = false;
+  if (cudaGraphCreate(&g, 0) == cudaSuccess) {
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams np{};
+    cudaGraphNode_t node;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess) {
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      if (cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess &&
+          cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        bool captured = true;
+        try {
+          step_half();
+          direction_half();
+          seg_cg_loop_kernel<<<1, 32, 0, s>>>(h, cw.cnt.p, cw.itd.p, maxiter);
+          check_launch(op);
+        } catch (...) {
+          captured = false;
+        }
+        cudaGraph_t body = nullptr;
+        captured = cudaStreamEndCapture(s, &body) == cudaSuccess && captured;
+        built = captured && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
+      }
+    }
+  }
+  if (!built) {
+    cudaGetLastError();  // the failed build's error state, not a launch error
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    return -1;
+  }
+  int reached = it0;
+  const cudaError_t e = cudaGraphLaunch(ge, s);
+  if (e == cudaSuccess) {
+    HFK_CUDA(cudaMemcpyAsync(&reached, cw.itd.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HFK_CUDA(cudaStreamSynchronize(s));
+  }
+  cudaGraphExecDestroy(ge);
+  cudaGraphDestroy(g);
+  HFK_CUDA(e);
+  return reached;
+}
+
 // MatrixFreeSolver.solve! (src/solvers.jl:111-159) on every segment of op at once: one FP64
 // (flexible) CG per segment with its own alpha, beta, tolerance atol + rtol ||b_s|| and stopping
 // test; every product and preconditioner application covers all segments in one launch sequence.
@@ -3383,30 +3469,51 @@ void solve_cg_seg_dev(hfk_problem* op, hfk_pmg* prec, const double* b, double* x
     if (prec) pmg_apply_dev(prec, in, outp);
     else HFK_CUDA(cudaMemcpyAsync(outp, in, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   };
+  // one iteration in two halves: the product, step and convergence check; then the preconditioner
+  // and the new direction (skipped on the host when no segment is active any more)
+  auto step_half = [&]() {
+    mf_apply_dev(op, pp.p, q.p);
+    seg_dots<double>(op, 1, sc + S_PQ, SEG_NS, pp.p, q.p);
+    seg_cg_alpha_kernel<<<sg, 256, 0, s>>>(ns, sc, fl);
+    check_launch(op);
+    seg_cg_update_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, pp.p, q.p, xd, r.p, flexible ? rold.p : nullptr);
+    check_launch(op);
+    seg_dots<double>(op, 1, sc + S_RR, SEG_NS, r.p, r.p);
+    seg_cg_check_kernel<<<1, 256, 0, s>>>(ns, sc, fl, cw.cnt.p);
+    check_launch(op);
+    set_mask(-1);
+  };
+  auto direction_half = [&]() {
+    apply_prec(r.p, z.p);
+    if (flexible) seg_dots<double>(op, 2, sc + S_ZR, SEG_NS, z.p, r.p, z.p, rold.p);
+    else seg_dots<double>(op, 1, sc + S_ZR, SEG_NS, z.p, r.p);
+    seg_cg_beta_kernel<<<sg, 256, 0, s>>>(ns, sc, fl, flexible);
+    check_launch(op);
+    seg_xpby_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, S_BETA, z.p, pp.p);
+    check_launch(op);
+  };
+  bool device_loop = op->solve_graph && s != cudaStreamLegacy;
   if (nact > 0) {
     apply_prec(r.p, z.p);
     HFK_CUDA(cudaMemcpyAsync(pp.p, z.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     seg_dots<double>(op, 1, sc + S_RZ, SEG_NS, r.p, z.p);
     while (it < maxiter) {
       ++it;
-      mf_apply_dev(op, pp.p, q.p);
-      seg_dots<double>(op, 1, sc + S_PQ, SEG_NS, pp.p, q.p);
-      seg_cg_alpha_kernel<<<sg, 256, 0, s>>>(ns, sc, fl);
-      check_launch(op);
-      seg_cg_update_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, pp.p, q.p, xd, r.p, flexible ? rold.p : nullptr);
-      check_launch(op);
-      seg_dots<double>(op, 1, sc + S_RR, SEG_NS, r.p, r.p);
-      seg_cg_check_kernel<<<1, 256, 0, s>>>(ns, sc, fl, cw.cnt.p);
-      check_launch(op);
-      set_mask(-1);
+      step_half();
       if (active_count() == 0) break;
-      apply_prec(r.p, z.p);
-      if (flexible) seg_dots<double>(op, 2, sc + S_ZR, SEG_NS, z.p, r.p, z.p, rold.p);
-      else seg_dots<double>(op, 1, sc + S_ZR, SEG_NS, z.p, r.p);
-      seg_cg_beta_kernel<<<sg, 256, 0, s>>>(ns, sc, fl, flexible);
-      check_launch(op);
-      seg_xpby_kernel<<<vec_grid(n), 256, 0, s>>>(n, seg, sc, S_BETA, z.p, pp.p);
-      check_launch(op);
+      direction_half();
+      // two host-driven iterations have created every buffer and tuned every launch shape: the
+      // remaining iterations run as one graph launch, the loop itself on the device
+      if (device_loop && it >= 2 && it < maxiter) {
+        const int reached = seg_cg_device_loop(op, step_half, direction_half, cw, it, maxiter);
+        if (reached >= 0) {
+          // one cycle per body run; the capture itself counted one
+          if (prec) prec->ncycles += reached - it - 1;
+          it = reached;
+          break;
+        }
+        device_loop = false;  // the graph could not be built: carry on from the host
+      }
     }
   }
   // true residual check per segment (src/solvers.jl:150-157), on every problem

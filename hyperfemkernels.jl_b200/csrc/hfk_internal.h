@@ -119,6 +119,7 @@ struct CGWork {
   Reducer red;
   DBuf<double> sc;  // per-segment scalars of the batched solve
   DBuf<int> fl, cnt;
+  DBuf<int> itd;  // the batched solve's iteration count, when its loop runs on the device
 };
 
 // Work of the restarted GMRES / FGMRES: the Krylov basis V ((restart + 1) n), the preconditioned
@@ -236,7 +237,9 @@ struct hfk_problem {
   int asm_kernel = 0;  // assembled Jacobian of 27-node cells: 0 the default choice, 1 the FP64 tensor-core kernel
   hfk::DBuf<double> func_red;             // per-warp partials of the functionals
   std::map<int, std::pair<bool, int>> tuned;  // autotuned (atomic scatter, warps per CTA) per kernel mode
-  bool no_tune = false;  // set while a call that must not tune (allocation-free smoothing) runs
+  bool no_tune = false;
+  bool solve_graph = true;  // batched CG: after two host-driven iterations, the rest as one CUDA graph
+                            // whose while node loops on the device  // set while a call that must not tune (allocation-free smoothing) runs
   hfk::CGWork cg;
   hfk::GmresWork gm;
 };

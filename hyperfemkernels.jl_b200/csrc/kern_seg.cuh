@@ -218,6 +218,19 @@ static __global__ void seg_cg_check_kernel(int nseg, const double* sc, int* fl, 
   seg_count_active(nseg, fl, nactive);
 }
 
+// End of one iteration of the device-driven batched CG (the body of a CUDA graph while node): count
+// the iteration and continue while a segment is active and the iteration limit is not reached.
+static __global__ void seg_cg_loop_kernel(cudaGraphConditionalHandle h, const int* nactive, int* it, int maxiter) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int i = *it + 1;
+    *it = i;
+    cudaGraphSetConditional(h, (*nactive > 0 && i < maxiter) ? 1u : 0u);
+  }
+}
+static __global__ void set_int_kernel(int* p, int v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *p = v;
+}
+
 // beta per segment: Polak-Ribiere (flexible) (z.r - z.rold) / rz, else z.r / rz; rz <- z.r
 static __global__ void seg_cg_beta_kernel(int nseg, double* sc, const int* fl, int flexible) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {

@@ -51,6 +51,7 @@ SIGNATURES = {
     "hfk_problem_set_scatter": [_vp, _i],
     "hfk_problem_set_launch": [_vp, _i, _i],
     "hfk_problem_set_assembly_kernel": [_vp, _i],
+    "hfk_problem_set_solve_graph": [_vp, _i],
     "hfk_mf_apply_many": [_vp, _i, _vp, _vp],
     "hfk_problem_tuning": [_vp, _i, _i, _pi, _pi, _pi],
     "hfk_functional": [_vp, _vp, _vp, _i, _pd],

@@ -83,6 +83,11 @@ class Problem:
         symmetric tangent on the FP64 FMA pipe) or "tensor" (on the FP64 tensor cores)."""
         call("hfk_problem_set_assembly_kernel", self.h, {"fma": 0, "tensor": 1}[kernel])
 
+    def set_solve_graph(self, on: bool = True):
+        """Batched CG on this operator: the iterations after the second as one CUDA graph launch that
+        loops on the device (default), or the host-driven loop."""
+        call("hfk_problem_set_solve_graph", self.h, 1 if on else 0)
+
     def tuning(self, kernel: str = "jv", precision: str = "fp64"):
         """The launch-shape autotuner's choice: {"atomic": bool, "kernel": "line" | "point",
         "warps": int} or None (not run yet)."""

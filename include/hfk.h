@@ -104,6 +104,13 @@ int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
  * give the reference's jacobian! (src/assembly.jl:918-927) to round-off; no counterpart in the
  * reference. */
 int hfk_problem_set_assembly_kernel(hfk_problem* p, int kernel);
+/* The batched CG (hfk_solve_cg_batched) on this operator: on = 1 (default) runs the iterations after
+ * the second as one CUDA graph launch whose while node loops on the device (the iteration, captured
+ * from the engine's launches, ends with a kernel that sets the loop condition: a problem still
+ * active and the iteration limit not reached), so the host launches once and waits instead of
+ * reading a flag count every iteration; on = 0 keeps the host-driven loop. Same iterates either
+ * way. No counterpart in the reference. */
+int hfk_problem_set_solve_graph(hfk_problem* p, int on);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
  * warp's lanes on the tensor lines of a few cells), 1 (point-parallel product: one thread per
@@ -265,7 +272,9 @@ int hfk_pmg_vcycle(hfk_pmg* m, const double* r, double* y);
 /* Counters and times (ms) of a hierarchy: out[9] = updates, coarse factorisations, V-cycles, time in
  * updates, in coarse assembly + factorisation, in block extraction, in eigenvalue estimates, in
  * V-cycles, in the Cholesky factorisation alone. The
- * V-cycle is replayed from a CUDA graph captured on the second cycle after each update. */
+ * V-cycle is replayed from a CUDA graph captured on the second cycle after each update. Cycles run
+ * inside the device-driven loop of a batched solve (hfk_problem_set_solve_graph) are counted but
+ * not timed (a graph loop body holds no events). */
 int hfk_pmg_stats(hfk_pmg* m, double* out);
 /* State of the last update: ok (preconditioner_ok, src/solvers.jl:105-106) and, when it failed,
  * whether it met an indefinite tangent: finite nodal blocks and a finite Ritz estimate with a

@@ -204,6 +204,40 @@ def test_batched_solve_matches_each_problem_solved_alone():
 
 
 @pytest.mark.gpu
+def test_device_driven_batched_loop_equals_the_host_loop():
+    # the iterations after the second as one CUDA graph launch looping on the device (default)
+    # against the host-driven loop: the same iterates, counts and residuals
+    op, (U2, U1), _ = _union_operator()
+    x = _states(U2)
+    mf = op.allocate_jacobian(x)
+    op.jacobian(mf, x)
+    b = -op.residual(np.zeros(U2.nfree), x)
+    pm = dict(smoother=S.Chebyshev(degree=3), coarse="cg", coarse_iters=12)
+    out = {}
+    for graph in (False, True):
+        op.problem.set_solve_graph(graph)
+        ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-10, preconditioner=S.PMultigrid([U2, U1], **pm))
+        ns = S.numerical_setup(ls, mf)
+        dx = S.solve(np.zeros(U2.nfree), ns, b)
+        res = ns.batched
+        assert res.converged.all() and res.sweeps > 2
+        out[graph] = (dx, res.iters.copy(), res.sweeps, res.relres.copy())
+    op.problem.set_solve_graph(True)
+    assert np.array_equal(out[True][1], out[False][1]) and out[True][2] == out[False][2]
+    assert reldiff(out[True][0], out[False][0]) < 1e-14
+    # the true residuals (about 4e-11 of b: round-off after cancellation, with the atomic scatter's
+    # add order free from run to run) agree to a few digits and meet the tolerance either way
+    assert np.allclose(out[True][3], out[False][3], rtol=1e-4, atol=0)
+    assert (out[True][3] <= 1e-10 * 1.01).all()
+    # a limit reached inside the device loop stops it there
+    op.problem.set_solve_graph(True)
+    ls = S.MatrixFreeSolver(krylov="fcg", rtol=1e-14, maxiter=5, preconditioner=S.PMultigrid([U2, U1], **pm))
+    ns = S.numerical_setup(ls, mf)
+    S.solve(np.zeros(U2.nfree), ns, b)
+    assert ns.batched.sweeps == 5 and not ns.batched.converged.any()
+
+
+@pytest.mark.gpu
 def test_batched_newton_matches_each_problem_solved_alone():
     from hfk.newton import newton_solve
     from hfk.operator import KernelOperator
