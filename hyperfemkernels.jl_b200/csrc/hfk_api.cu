@@ -1551,6 +1551,8 @@ struct hfk_pmg {
   // coarse_factor_launch, collected by coarse_factor_finish)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_c0 = nullptr, ev_c1 = nullptr, ev_p0 = nullptr, ev_p1 = nullptr;
+  cudaStream_t cb_stream = nullptr;  // the factorisation's lookahead stream (the trailing updates)
+  std::vector<cudaEvent_t> cb_ev;    // its two ordering events (panel done, update rest done)
   bool cf_pending = false;
   DBuf<double> bs_tiles, bs_diag, bs_y;
   DBuf<int> bs_sync;
@@ -1686,15 +1688,43 @@ void coarse_factor_launch(hfk_pmg* m) {
   raise_smem_limit(band_panel_kernel, smem, attr_p);
   raise_smem_limit(band_update_kernel, smem, attr_u);
   HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
+  // Lookahead: after panel k, the tiles of block column k + 1 are updated on the coarse stream
+  // (the next panel needs only them) and the rest of the trailing window on a second stream, where
+  // it overlaps panel k + 1. A tile of block column k + 1 is also written by the rest of update
+  // k - 1, so the column part of update k waits for that (event rest[k - 1]); the rest of update k
+  // waits for panel k (event pan[k]) and follows the rest of update k - 1 on its stream.
+  if (!m->cb_stream) HFK_CUDA(cudaStreamCreateWithFlags(&m->cb_stream, cudaStreamNonBlocking));
+  while ((int)m->cb_ev.size() < 2) {
+    cudaEvent_t e;
+    HFK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    m->cb_ev.push_back(e);
+  }
+  cudaEvent_t ev_pan = m->cb_ev[0], ev_rest = m->cb_ev[1];
+  HFK_CUDA(cudaEventRecord(ev_pan, c->stream));  // the band storage is filled
+  HFK_CUDA(cudaStreamWaitEvent(m->cb_stream, ev_pan, 0));
+  bool rest_pending = false;
   for (int k = 0; k < nbt; ++k) {
     const int mq = std::min(W, nbt - 1 - k);
     band_panel_kernel<<<mq + 1, CB_PANEL_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p);
     check_launch(c);
     if (mq > 0) {
-      band_update_kernel<<<mq * (mq + 1) / 2, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p);
+      if (mq > 1) {
+        HFK_CUDA(cudaEventRecord(ev_pan, c->stream));
+        HFK_CUDA(cudaStreamWaitEvent(m->cb_stream, ev_pan, 0));
+      }
+      if (rest_pending) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest, 0));
+      band_update_kernel<<<mq, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, 1);
       check_launch(c);
+      rest_pending = false;
+      if (mq > 1) {
+        band_update_kernel<<<(mq - 1) * mq / 2, CB_THREADS, smem, m->cb_stream>>>(nbt, W, k, m->Lb.p, 2);
+        check_launch(c);
+        HFK_CUDA(cudaEventRecord(ev_rest, m->cb_stream));
+        rest_pending = true;
+      }
     }
   }
+  if (rest_pending) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest, 0));
   HFK_CUDA(cudaEventRecord(m->ev_p1, c->stream));
   // the block tiles of the cycle's triangular solves (used only if every pivot was positive)
   band_prepare(m, n);
@@ -2856,6 +2886,11 @@ int hfk_pmg_destroy(hfk_pmg* m) {
       cudaStreamSynchronize(m->side);
       cudaStreamDestroy(m->side);
     }
+    if (m->cb_stream) {
+      cudaStreamSynchronize(m->cb_stream);
+      cudaStreamDestroy(m->cb_stream);
+    }
+    for (cudaEvent_t e : m->cb_ev) cudaEventDestroy(e);
     for (cudaEvent_t e : {m->ev_fork, m->ev_c0, m->ev_c1, m->ev_p0, m->ev_p1})
       if (e) cudaEventDestroy(e);
     pmg_drop_graph(m);

@@ -54,6 +54,36 @@ static __global__ void band_fill_kernel(int64_t n, int nbt, int W, const int64_t
   }
 }
 
+// A CB_T x CB_T tile between global memory (contiguous, column-major) and shared memory (leading
+// dimension CB_LD), by NT threads: 16-byte global accesses, the loop unrolled so that every
+// thread's loads are in flight together (the tiles are read on the factorisation's critical path).
+template <int NT>
+__device__ __forceinline__ void tile_to_shared(double* S, const double* __restrict__ G, int tid) {
+  constexpr int N2 = CB_T * CB_T / 2;
+  static_assert(N2 % NT == 0, "whole pairs per thread");
+  double2 v[N2 / NT];
+#pragma unroll
+  for (int k = 0; k < N2 / NT; ++k) v[k] = reinterpret_cast<const double2*>(G)[tid + NT * k];
+#pragma unroll
+  for (int k = 0; k < N2 / NT; ++k) {
+    const int e = 2 * (tid + NT * k), r = e % CB_T, c = e / CB_T;  // r even: r + 1 in the same column
+    S[r + CB_LD * c] = v[k].x;
+    S[r + 1 + CB_LD * c] = v[k].y;
+  }
+}
+template <int NT, bool LOWER>
+__device__ __forceinline__ void tile_to_global(double* __restrict__ G, const double* S, int tid) {
+  constexpr int N2 = CB_T * CB_T / 2;
+#pragma unroll 8
+  for (int k = 0; k < N2 / NT; ++k) {
+    const int e = 2 * (tid + NT * k), r = e % CB_T, c = e / CB_T;
+    double2 v;
+    v.x = (!LOWER || r >= c) ? S[r + CB_LD * c] : 0.0;
+    v.y = (!LOWER || r + 1 >= c) ? S[r + 1 + CB_LD * c] : 0.0;
+    reinterpret_cast<double2*>(G)[tid + NT * k] = v;
+  }
+}
+
 // Panel k, blocked by 16 columns, the tile in shared memory (CB_PANEL_THREADS threads). Per block of
 // 16 columns: (1) one warp factors the 16 x 16 diagonal block, row i in lane i's registers, the
 // pivots and multipliers passed by shuffles (no barrier inside: the chain of dependent pivots is
@@ -75,7 +105,7 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
   __shared__ int s_bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, q = blockIdx.x;
   double* Akk = Lb + band_tile_offset(k, k, W);
-  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) A[(e % CB_T) + CB_LD * (e / CB_T)] = Akk[e];
+  tile_to_shared<CB_PANEL_THREADS>(A, Akk, tid);
   if (tid == 0) s_bad = 0;
   __syncthreads();
 #pragma unroll 1
@@ -97,10 +127,14 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
         const double l = i > c ? b[c] * iv : (i == c ? pv * iv : 0.0);
         b[c] = l;
         if (lane == 0) s_inv[p0 + c] = iv;
+        // a constant trip count with a predicate (not s2 = c + 1 ..): the loops unroll completely
+        // and b stays in registers
 #pragma unroll
-        for (int s2 = c + 1; s2 < CB_PB; ++s2) {
-          const double ls = __shfl_sync(0xffffffffu, l, s2);
-          if (i >= s2) b[s2] = fma(-l, ls, b[s2]);
+        for (int s2 = 0; s2 < CB_PB; ++s2) {
+          if (s2 > c) {
+            const double ls = __shfl_sync(0xffffffffu, l, s2);
+            if (i >= s2) b[s2] = fma(-l, ls, b[s2]);
+          }
         }
       }
       if (lane < CB_PB) {
@@ -122,34 +156,32 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
         const double v = x[c] * s_inv[p0 + c];
         x[c] = v;
 #pragma unroll
-        for (int s2 = c + 1; s2 < CB_PB; ++s2) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
+        for (int s2 = 0; s2 < CB_PB; ++s2)
+          if (s2 > c) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
       }
 #pragma unroll
       for (int c = 0; c < CB_PB; ++c) A[r + CB_LD * (p0 + c)] = x[c];
     }
     __syncthreads();
-    // (3) rank-16 update of the trailing lower triangle
+    // (3) rank-16 update of the trailing lower triangle (four partial sums: short FMA chains)
     const int t0 = p0 + CB_PB, m = CB_T - t0;
-    for (int e = tid; e < m * m; e += blockDim.x) {
+    for (int e = tid; e < m * m; e += CB_PANEL_THREADS) {
       const int rr = t0 + e % m, ss = t0 + e / m;
       if (rr < ss) continue;
-      double acc = 0.0;
+      double a4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-      for (int c = 0; c < CB_PB; ++c) acc = fma(A[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], acc);
-      A[rr + CB_LD * ss] -= acc;
+      for (int c = 0; c < CB_PB; ++c) a4[c & 3] = fma(A[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], a4[c & 3]);
+      A[rr + CB_LD * ss] -= (a4[0] + a4[1]) + (a4[2] + a4[3]);
     }
     __syncthreads();
   }
   if (q == 0) {
     if (s_bad && tid == 0) atomicCAS(info, 0, k + 1);
-    for (int e = tid; e < CB_T * CB_T; e += blockDim.x) {
-      const int rr = e % CB_T, cc = e / CB_T;
-      Akk[e] = rr >= cc ? A[rr + CB_LD * cc] : 0.0;
-    }
+    tile_to_global<CB_PANEL_THREADS, true>(Akk, A, tid);
     return;
   }
   double* Aik = Lb + band_tile_offset(k + q, k, W);
-  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) X[(e % CB_T) + CB_LD * (e / CB_T)] = Aik[e];
+  tile_to_shared<CB_PANEL_THREADS>(X, Aik, tid);
   __syncthreads();
 #pragma unroll 1
   for (int p0 = 0; p0 < CB_T; p0 += CB_PB) {
@@ -163,48 +195,59 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
         const double v = x[c] * s_inv[p0 + c];
         x[c] = v;
 #pragma unroll
-        for (int s2 = c + 1; s2 < CB_PB; ++s2) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
+        for (int s2 = 0; s2 < CB_PB; ++s2)
+          if (s2 > c) x[s2] = fma(-v, A[(p0 + s2) + CB_LD * (p0 + c)], x[s2]);
       }
 #pragma unroll
       for (int c = 0; c < CB_PB; ++c) X[tid + CB_LD * (p0 + c)] = x[c];
     }
     __syncthreads();
-    // the later columns of X: X[r][s] -= sum_c X[r][p0 + c] L[s][p0 + c]
+    // the later columns of X: X[r][s] -= sum_c X[r][p0 + c] L[s][p0 + c] (four partial sums)
     const int t0 = p0 + CB_PB, m = CB_T - t0;
-    for (int e = tid; e < CB_T * m; e += blockDim.x) {
+    for (int e = tid; e < CB_T * m; e += CB_PANEL_THREADS) {
       const int rr = e % CB_T, ss = t0 + e / CB_T;
-      double acc = 0.0;
+      double a4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-      for (int c = 0; c < CB_PB; ++c) acc = fma(X[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], acc);
-      X[rr + CB_LD * ss] -= acc;
+      for (int c = 0; c < CB_PB; ++c) a4[c & 3] = fma(X[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], a4[c & 3]);
+      X[rr + CB_LD * ss] -= (a4[0] + a4[1]) + (a4[2] + a4[3]);
     }
     __syncthreads();
   }
-  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) Aik[e] = X[(e % CB_T) + CB_LD * (e / CB_T)];
+  tile_to_global<CB_PANEL_THREADS, false>(Aik, X, tid);
 }
 
 // Update k: tile (i, j) -= L_ik L_jk^T for the m (m + 1) / 2 tiles k < j <= i <= k + m (m = min(W,
 // nbt - 1 - k)); CTA b takes the b-th tile in the order (i, j) = (k+1, k+1), (k+2, k+1), (k+2, k+2),
-// ... Each thread forms a 4 x 4 block of the product (rows tr + 16 a, columns ts + 16 b). On a
+// ... part = 1 takes only the tiles of block column k + 1 (CTA b: i = k + 1 + b), the ones the next
+// panel needs; part = 2 the others (j >= k + 2, in the same order over that smaller triangle); 0
+// all. Each thread forms a 4 x 4 block of the product (rows tr + 16 a, columns ts + 16 b). On a
 // diagonal tile only the lower triangle is written. Dynamic shared memory: two tiles.
-static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt, int W, int k, double* Lb) {
+static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt, int W, int k, double* Lb, int part) {
   extern __shared__ __align__(16) double cbs[];
   double* Li = cbs;
   double* Lj = cbs + CB_T * CB_LD;
   const int tid = threadIdx.x;
   // b -> (ii, jj), jj <= ii: ii (ii + 1) / 2 <= b < (ii + 1) (ii + 2) / 2
   const int b = blockIdx.x;
-  int ii = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-  while ((ii + 1) * (ii + 2) / 2 <= b) ++ii;
-  while (ii * (ii + 1) / 2 > b) --ii;
-  const int jj = b - ii * (ii + 1) / 2;
+  int ii, jj;
+  if (part == 1) {
+    ii = b;
+    jj = 0;
+  } else {
+    ii = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+    while ((ii + 1) * (ii + 2) / 2 <= b) ++ii;
+    while (ii * (ii + 1) / 2 > b) --ii;
+    jj = b - ii * (ii + 1) / 2;
+    if (part == 2) {
+      ++ii;
+      ++jj;
+    }
+  }
   const int i = k + 1 + ii, j = k + 1 + jj;
   const double* Lik = Lb + band_tile_offset(i, k, W);
   const double* Ljk = Lb + band_tile_offset(j, k, W);
-  for (int e = tid; e < CB_T * CB_T; e += blockDim.x) {
-    Li[(e % CB_T) + CB_LD * (e / CB_T)] = Lik[e];
-    Lj[(e % CB_T) + CB_LD * (e / CB_T)] = Ljk[e];
-  }
+  tile_to_shared<CB_THREADS>(Li, Lik, tid);
+  tile_to_shared<CB_THREADS>(Lj, Ljk, tid);
   __syncthreads();
   const int tr = tid % 16, ts = tid / 16;
   double acc[4][4];
