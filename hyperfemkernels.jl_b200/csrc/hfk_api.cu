@@ -7,8 +7,10 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -1265,14 +1267,23 @@ void jacobian_dev(hfk_problem* p, const double* u, const double* dvals, double* 
   if (fma27) {
     static PerDeviceLimit attr[2];
     raise_smem_limit(kern_s, smem_s, attr[tp27]);
-    static PerDeviceValue occ[2];
+    // resident CTAs per SM, per (device, variant, shared-memory size): the dense variant's size
+    // depends on the number of points
+    static std::mutex occ_mutex;
+    static std::map<std::tuple<int, bool, size_t>, int> occ;
     int dev = 0;
     HFK_CUDA(cudaGetDevice(&dev));
-    const int per_sm = occ[tp27].get(dev, [&] {
-      int b = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern_s, 256, smem_s) != cudaSuccess) b = 1;
-      return std::max(b, 1);
-    });
+    int per_sm = 0;
+    {
+      std::lock_guard<std::mutex> lock(occ_mutex);
+      auto it = occ.find({dev, tp27, smem_s});
+      if (it == occ.end()) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern_s, 256, smem_s) != cudaSuccess) b = 1;
+        it = occ.emplace(std::make_tuple(dev, tp27, smem_s), std::max(b, 1)).first;
+      }
+      per_sm = it->second;
+    }
     grid_s = per_sm * sm_count();
   } else if (g) {
     static PerDeviceLimit attr[4];
