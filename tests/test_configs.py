@@ -127,3 +127,26 @@ def test_c2_oseen_assembly_parity(scatter):
     x = np.random.default_rng(0).standard_normal(V.nfree)
     d = V.dirichlet_values
     assert reldiff(op.residual(np.zeros(V.nfree), x, d), orc.residual(x, d)) < TOL64
+
+
+def test_c0_jacobian_into_device_memory_repeatedly(c0):
+    # device-resident state and values (the single-launch path of the persistent FMA kernel, the one
+    # the benchmark times): five assemblies into the same array, with other values written in
+    # between, all equal the oracle's (the zero-fill comes first every time)
+    import torch
+
+    from hfk import _lib
+
+    V, orc, x = c0
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 4), forms.svk_jacobian(2.0, 1.0, 4), V)
+    nnz = op.sparsity_pattern().nnz
+    ref = orc.jacobian_values(x, V.dirichlet_values)
+    xd = torch.from_numpy(x).cuda()
+    dd = torch.from_numpy(np.ascontiguousarray(V.dirichlet_values)).cuda()
+    nz = torch.full((nnz,), 7.0, dtype=torch.float64, device="cuda")
+    for k in range(5):
+        _lib.call("hfk_jacobian", op.problem.h, _lib.ptr(xd), _lib.ptr(dd), _lib.ptr(nz))
+        torch.cuda.synchronize()
+        assert reldiff(nz.cpu().numpy(), ref) < TOL64, k
+        nz.fill_(float(k + 1))
+    assert op.problem.device_errors() == 0
