@@ -3,7 +3,7 @@
 // TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA engine and the timed CPU
 // baseline ("CPU restatement of the reference algorithm"). Nothing in the product links it.
 //
-// Parity status: the reference (Julia + Gridap) cannot run in this build environment and ships
+// Parity status: the reference (Julia + Gridap) cannot run without Julia, which is absent, and ships
 // no golden vectors (its tests compare against a live Gridap). The restatement is pinned by the
 // reference's own known-answer and property tests, restated in tests/ (partition of unity,
 // exact affine gradients, tensor-product == dense tables, matrix-free == assembled,
