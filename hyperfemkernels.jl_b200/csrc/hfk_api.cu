@@ -1694,48 +1694,43 @@ void coarse_factor_launch(hfk_pmg* m) {
   m->cb_W = W;
   m->cb_info.resize(1);
   m->cb_info.zero(c->stream);
-  const size_t smem = (size_t)2 * CB_T * CB_LD * sizeof(double);
+  const size_t smem = (size_t)2 * CB_T * CB_LD * sizeof(double), smem_p = 2 * smem;
   static PerDeviceLimit attr_p, attr_u;
-  raise_smem_limit(band_panel_kernel, smem, attr_p);
+  raise_smem_limit(band_panel_kernel, smem_p, attr_p);
   raise_smem_limit(band_update_kernel, smem, attr_u);
   HFK_CUDA(cudaEventRecord(m->ev_p0, c->stream));
-  // Lookahead: after panel k, the tiles of block column k + 1 are updated on the coarse stream
-  // (the next panel needs only them) and the rest of the trailing window on a second stream, where
-  // it overlaps panel k + 1. A tile of block column k + 1 is also written by the rest of update
-  // k - 1, so the column part of update k waits for that (event rest[k - 1]); the rest of update k
-  // waits for panel k (event pan[k]) and follows the rest of update k - 1 on its stream.
+  // Lookahead: panel k + 1 applies the update of block column k + 1 by block column k itself (the
+  // only tiles it needs), and the rest of that trailing update (block columns k + 2 ..) runs on a
+  // second stream, where it overlaps panel k + 1. Block column k is last written by the rest of
+  // update k - 2, so panel k waits for that (two alternating events); the rest of update k waits
+  // for panel k and follows the rest of update k - 1 on its stream.
   if (!m->cb_stream) HFK_CUDA(cudaStreamCreateWithFlags(&m->cb_stream, cudaStreamNonBlocking));
-  while ((int)m->cb_ev.size() < 2) {
+  while ((int)m->cb_ev.size() < 3) {
     cudaEvent_t e;
     HFK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     m->cb_ev.push_back(e);
   }
-  cudaEvent_t ev_pan = m->cb_ev[0], ev_rest = m->cb_ev[1];
+  cudaEvent_t ev_pan = m->cb_ev[0], ev_rest[2] = {m->cb_ev[1], m->cb_ev[2]};
+  bool rest_rec[2] = {false, false};
   HFK_CUDA(cudaEventRecord(ev_pan, c->stream));  // the band storage is filled
   HFK_CUDA(cudaStreamWaitEvent(m->cb_stream, ev_pan, 0));
-  bool rest_pending = false;
   for (int k = 0; k < nbt; ++k) {
     const int mq = std::min(W, nbt - 1 - k);
-    band_panel_kernel<<<mq + 1, CB_PANEL_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p);
+    if (rest_rec[k % 2]) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest[k % 2], 0));  // the rest of update k - 2
+    band_panel_kernel<<<mq + 1, CB_PANEL_THREADS, smem_p, c->stream>>>(nbt, W, k, m->Lb.p, m->cb_info.p, 1);
     check_launch(c);
-    if (mq > 0) {
-      if (mq > 1) {
-        HFK_CUDA(cudaEventRecord(ev_pan, c->stream));
-        HFK_CUDA(cudaStreamWaitEvent(m->cb_stream, ev_pan, 0));
-      }
-      if (rest_pending) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest, 0));
-      band_update_kernel<<<mq, CB_THREADS, smem, c->stream>>>(nbt, W, k, m->Lb.p, 1);
+    rest_rec[k % 2] = false;
+    if (mq > 1) {
+      HFK_CUDA(cudaEventRecord(ev_pan, c->stream));
+      HFK_CUDA(cudaStreamWaitEvent(m->cb_stream, ev_pan, 0));
+      band_update_kernel<<<(mq - 1) * mq / 2, CB_THREADS, smem, m->cb_stream>>>(nbt, W, k, m->Lb.p, 2);
       check_launch(c);
-      rest_pending = false;
-      if (mq > 1) {
-        band_update_kernel<<<(mq - 1) * mq / 2, CB_THREADS, smem, m->cb_stream>>>(nbt, W, k, m->Lb.p, 2);
-        check_launch(c);
-        HFK_CUDA(cudaEventRecord(ev_rest, m->cb_stream));
-        rest_pending = true;
-      }
+      HFK_CUDA(cudaEventRecord(ev_rest[k % 2], m->cb_stream));
+      rest_rec[k % 2] = true;
     }
   }
-  if (rest_pending) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest, 0));
+  for (int i = 0; i < 2; ++i)
+    if (rest_rec[i]) HFK_CUDA(cudaStreamWaitEvent(c->stream, ev_rest[i], 0));
   HFK_CUDA(cudaEventRecord(m->ev_p1, c->stream));
   // the block tiles of the cycle's triangular solves (used only if every pivot was positive)
   band_prepare(m, n);

@@ -10,9 +10,11 @@
 // of n^2: a Q1 32^3 coarse level (101 277 dofs, b = 3 369) takes 2.9 GB.
 //
 // Right-looking blocked factorisation, two launches per block column k:
-//   panel k:  tile (k, k) <- chol(A_kk) (every CTA of the launch factors it in shared memory; CTA 0
-//             stores it), tile (k + q, k) <- A_{k+q,k} L_kk^-T (CTA q >= 1);
-//   update k: tile (i, j) -= L_ik L_jk^T for k < j <= i <= k + W (one CTA per tile).
+//   panel k:  the update of block column k by block column k - 1, then tile (k, k) <- chol(A_kk)
+//             (every CTA of the launch updates and factors it in shared memory; CTA 0 stores it),
+//             tile (k + q, k) <- A_{k+q,k} L_kk^-T (CTA q >= 1);
+//   update k: tile (i, j) -= L_ik L_jk^T for k + 1 < j <= i <= k + W (one CTA per tile), on a
+//             second stream, where it overlaps panel k + 1.
 // A pivot that is not positive and finite records the block column (1-based) in *info (the first
 // one wins) and is replaced by 1 so that the remaining work stays finite; the host rejects the
 // factor.
@@ -84,6 +86,36 @@ __device__ __forceinline__ void tile_to_global(double* __restrict__ G, const dou
   }
 }
 
+// S -= Li Lj^T for CB_T x CB_T tiles in shared memory (leading dimension CB_LD), by 128 threads,
+// each a 4 x 8 block of the product; lower: only the lower triangle of S is written.
+__device__ __forceinline__ void tile_sub_prod128(double* S, const double* Li, const double* Lj, int tid, bool lower) {
+  const int tr = tid % 16, ts = tid / 16;  // rows tr + 16 a, columns ts + 8 b
+  double acc[4][8];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+#pragma unroll 4
+  for (int m = 0; m < CB_T; ++m) {
+    double x[4], y[8];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) x[a] = Li[tr + 16 * a + CB_LD * m];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) y[b] = Lj[ts + 8 * b + CB_LD * m];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int r = tr + 16 * a, c = ts + 8 * b;
+      if (!lower || r >= c) S[r + CB_LD * c] -= acc[a][b];
+    }
+}
+
 // Panel k, blocked by 16 columns, the tile in shared memory (CB_PANEL_THREADS threads). Per block of
 // 16 columns: (1) one warp factors the 16 x 16 diagonal block, row i in lane i's registers, the
 // pivots and multipliers passed by shuffles (no barrier inside: the chain of dependent pivots is
@@ -96,18 +128,34 @@ __device__ __forceinline__ void tile_to_global(double* __restrict__ G, const dou
 constexpr int CB_PANEL_THREADS = 128;
 constexpr int CB_PB = 16;  // columns per block of the panel
 
+// fuse: block column k first takes its update by block column k - 1 (the tiles (k + q, k) -= L_{k+q,k-1}
+// L_{k,k-1}^T, the diagonal one by every CTA, as it factors it), so that no separate launch sits
+// between two panels on the factorisation's critical path; four tiles of shared memory then.
 static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int nbt, int W, int k, double* Lb,
-                                                                             int* info) {
+                                                                             int* info, int fuse) {
   extern __shared__ __align__(16) double cbs[];
   double* A = cbs;                 // the diagonal tile, becoming L_kk (column-major, leading dimension CB_LD)
   double* X = cbs + CB_T * CB_LD;  // the panel tile below (CTA q >= 1)
+  double* Ld = X + CB_T * CB_LD;   // fuse: L_{k,k-1}
+  double* Lq = Ld + CB_T * CB_LD;  // fuse: L_{k+q,k-1}
   __shared__ double s_inv[CB_T];   // reciprocals of L_kk's diagonal
   __shared__ int s_bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, q = blockIdx.x;
   double* Akk = Lb + band_tile_offset(k, k, W);
+  double* Aik = Lb + band_tile_offset(k + q, k, W);
+  const bool fz = fuse && k > 0 && W >= 1;
+  const bool fq = fz && q >= 1 && q + 1 <= W;  // tile (k + q, k - 1) lies in the band
   tile_to_shared<CB_PANEL_THREADS>(A, Akk, tid);
+  if (q >= 1) tile_to_shared<CB_PANEL_THREADS>(X, Aik, tid);
+  if (fz) tile_to_shared<CB_PANEL_THREADS>(Ld, Lb + band_tile_offset(k, k - 1, W), tid);
+  if (fq) tile_to_shared<CB_PANEL_THREADS>(Lq, Lb + band_tile_offset(k + q, k - 1, W), tid);
   if (tid == 0) s_bad = 0;
   __syncthreads();
+  if (fz) {
+    tile_sub_prod128(A, Ld, Ld, tid, true);
+    if (fq) tile_sub_prod128(X, Lq, Ld, tid, false);
+    __syncthreads();
+  }
 #pragma unroll 1
   for (int p0 = 0; p0 < CB_T; p0 += CB_PB) {
     // (1) the diagonal block, by warp 0
@@ -180,9 +228,6 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
     tile_to_global<CB_PANEL_THREADS, true>(Akk, A, tid);
     return;
   }
-  double* Aik = Lb + band_tile_offset(k + q, k, W);
-  tile_to_shared<CB_PANEL_THREADS>(X, Aik, tid);
-  __syncthreads();
 #pragma unroll 1
   for (int p0 = 0; p0 < CB_T; p0 += CB_PB) {
     // the block of 16 columns of X: row r solves x L_pp^T = a
@@ -218,9 +263,8 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
 
 // Update k: tile (i, j) -= L_ik L_jk^T for the m (m + 1) / 2 tiles k < j <= i <= k + m (m = min(W,
 // nbt - 1 - k)); CTA b takes the b-th tile in the order (i, j) = (k+1, k+1), (k+2, k+1), (k+2, k+2),
-// ... part = 1 takes only the tiles of block column k + 1 (CTA b: i = k + 1 + b), the ones the next
-// panel needs; part = 2 the others (j >= k + 2, in the same order over that smaller triangle); 0
-// all. Each thread forms a 4 x 4 block of the product (rows tr + 16 a, columns ts + 16 b). On a
+// ... part = 2 takes only the tiles j >= k + 2 (in the same order over that smaller triangle; block
+// column k + 1 is updated inside the next panel launch), 0 all. Each thread forms a 4 x 4 block of the product (rows tr + 16 a, columns ts + 16 b). On a
 // diagonal tile only the lower triangle is written. Dynamic shared memory: two tiles.
 static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt, int W, int k, double* Lb, int part) {
   extern __shared__ __align__(16) double cbs[];
@@ -229,19 +273,13 @@ static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt,
   const int tid = threadIdx.x;
   // b -> (ii, jj), jj <= ii: ii (ii + 1) / 2 <= b < (ii + 1) (ii + 2) / 2
   const int b = blockIdx.x;
-  int ii, jj;
-  if (part == 1) {
-    ii = b;
-    jj = 0;
-  } else {
-    ii = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-    while ((ii + 1) * (ii + 2) / 2 <= b) ++ii;
-    while (ii * (ii + 1) / 2 > b) --ii;
-    jj = b - ii * (ii + 1) / 2;
-    if (part == 2) {
-      ++ii;
-      ++jj;
-    }
+  int ii = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+  while ((ii + 1) * (ii + 2) / 2 <= b) ++ii;
+  while (ii * (ii + 1) / 2 > b) --ii;
+  int jj = b - ii * (ii + 1) / 2;
+  if (part == 2) {
+    ++ii;
+    ++jj;
   }
   const int i = k + 1 + ii, j = k + 1 + jj;
   const double* Lik = Lb + band_tile_offset(i, k, W);
