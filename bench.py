@@ -50,7 +50,7 @@ JV_CELLS = 64
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
@@ -107,15 +107,23 @@ def build_case(n, order=2, seed=0):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms; the summary keeps the samples
+    taken inside the window marked by ``start()`` / ``stop()`` (the timed region)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        self.t0 = time.time()
+
+    def stop(self):
+        self.t1 = time.time()
 
     def __enter__(self):
         try:
@@ -139,24 +147,27 @@ class ClockSampler:
             self.lines = [l for l in out.splitlines() if l.strip()]
 
     def summary(self):
-        sms, maxs, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        import datetime
+
+        rows = []
         for l in self.lines:
             f = [s.strip() for s in l.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sms.append(float(f[1]))
-                maxs.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sms:
+        inside = [r for r in rows if self.t0 is not None and self.t1 is not None and self.t0 <= r[0] <= self.t1]
+        window = "timed region" if inside else "whole sampler run (no sample fell inside the timed region)"
+        use = inside or rows
+        if not use:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
-                "samples": len(sms)}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {nm for r in use for nm, v in zip(names, r[3]) if v.lower() == "active"}
+        return {"sm_mhz": statistics.median(r[1] for r in use), "sm_max_mhz": max(r[2] for r in use),
+                "reasons": sorted(reasons), "samples": len(use), "window": window}
 
 
 def jv_flops_per_cell(Q, P):
@@ -193,7 +204,7 @@ class Timer:
             dist.barrier()
             self.torch.cuda.synchronize()
 
-    def steps(self, fn, k, w):
+    def steps(self, fn, k, w, on_start=None, on_stop=None):
         torch = self.torch
         for _ in range(w):
             if self.buf is not None:
@@ -201,6 +212,8 @@ class Timer:
             fn()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
         self._sync()
+        if on_start:
+            on_start()
         for e0, e1 in ev:
             if self.buf is not None:
                 self.buf.zero_()
@@ -208,6 +221,8 @@ class Timer:
             fn()
             e1.record(self.stream)
         self._sync()
+        if on_stop:
+            on_stop()
         ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
         return self.max_over_ranks(ms)
 
@@ -285,7 +300,7 @@ def engine(args):
     l0 = op.problem.launches()
     op.problem.set_timing(True)
     with ClockSampler(local) as clk:
-        ms = T.steps(step, args.steps, args.warmup)
+        ms = T.steps(step, args.steps, args.warmup, on_start=clk.start, on_stop=clk.stop)
     k_ms, k_n = op.problem.kernel_time()
     op.problem.set_timing(False)
     launches = (op.problem.launches() - l0) // (args.steps + args.warmup) * args.steps
@@ -906,7 +921,9 @@ def batch_main(args):
         torch.cuda.synchronize()
         dist.barrier()
     with clocks:
+        clocks.start()
         x, st = B.newton_solve_batched(op, _batch_solver(U2, U1, args.batch_precision), g, BATCH_LOADS, lift=lift)
+        clocks.stop()
     st.seconds = max_over_ranks(st.seconds)
     plain = {"seconds": st.seconds, "newton_sweeps": st.newton_sweeps, "krylov_sweeps": int(sum(st.krylov_sweeps)),
              "newton_iters_mean": float(st.newton_iters.mean()), "krylov_iters_mean": float(st.krylov_iters.mean()),
