@@ -22,6 +22,7 @@
 #include "engine.h"
 #include "hfk_internal.h"
 #include "kern_assembly.cuh"
+#include "kern_q1.cuh"
 #include "kern_band.cuh"
 #include "kern_cell.cuh"
 #include "kern_chol.cuh"
@@ -207,6 +208,16 @@ void launch_jvp(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& 
 constexpr int SHAPE_PT_NARROW = 100, SHAPE_PT_WIDE = 108;
 // SHAPE_TC: the FP32 product of Q2 cells with both contractions on the tensor cores (kern_jv_tc.cuh)
 constexpr int SHAPE_TC = 120;
+// SHAPE_Q1: the warp-synchronous product of Q1 cells with 2^3 Gauss points (kern_q1.cuh)
+constexpr int SHAPE_Q1 = 130;
+
+template <typename R>
+void launch_q1(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>& io) {
+  const int grid = (ncl + Q1_THREADS / 8 - 1) / (Q1_THREADS / 8);
+  if (grid == 0) return;
+  q1_jv_kernel<R><<<grid, Q1_THREADS, 0, p->stream>>>(cell_data(p, cells, ncl), make_tab<R>(p), io);
+  check_launch(p);
+}
 
 // whether the tensor-core product serves this problem and precision
 template <int MODE, typename R>
@@ -222,9 +233,15 @@ void launch_shape(hfk_problem* p, const int32_t* cells, int ncl, const CellIO<R>
       return;
     }
   }
+  if constexpr (MODE == MODE_JV && Q == 2 && P == 2) {
+    if (shape == SHAPE_Q1) {
+      launch_q1<R>(p, cells, ncl, io);
+      return;
+    }
+  }
   if (MODE == MODE_JV && shape == SHAPE_PT_NARROW) launch_jvp<Q, P, R, jvp_narrow<P>()>(p, cells, ncl, io);
   else if (MODE == MODE_JV && shape == SHAPE_PT_WIDE) launch_jvp<Q, P, R, JVP_WIDE>(p, cells, ncl, io);
-  else launch_cell<Q, P, MODE, R>(p, cells, ncl, io, shape >= SHAPE_PT_NARROW ? 4 : shape);
+  else launch_cell<Q, P, MODE, R>(p, cells, ncl, io, shape >= SHAPE_PT_NARROW ? 4 : shape);  // SHAPE_TC/Q1 elsewhere: 4 warps
 }
 
 template <int MODE, typename R>
@@ -304,21 +321,21 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
       return;
     }
     // (atomic, warps per CTA); the matrix-free product also tries the point-parallel kernel
-    const int cand[9][2] = {{1, 4},
-                            {1, 2},
-                            {0, 4},
-                            {0, 2},
-                            {1, SHAPE_PT_NARROW},
-                            {1, SHAPE_PT_WIDE},
-                            {0, SHAPE_PT_NARROW},
-                            {0, SHAPE_PT_WIDE},
-                            {1, SHAPE_TC}};
-    // batched problems keep the line-mapped kernels: the tuning call has every problem active, but
-    // most of a batched solve runs with converged problems masked, where the line-mapped kernels'
-    // per-warp exit measured better (256 SVK Q2 problems: 22.3 s against 23.9 s with the
-    // point-parallel product picked for the Q1 level)
+    std::vector<std::pair<int, int>> cand = {{1, 4}, {1, 2}, {0, 4}, {0, 2}};
+    // batched problems keep the line-mapped kernels (and the Q1 one): the tuning call has every
+    // problem active, but most of a batched solve runs with converged problems masked, where the
+    // per-warp exit of these kernels measured better (256 SVK Q2 problems: 22.3 s against 23.9 s
+    // with the point-parallel product picked for the Q1 level)
+    if (MODE == MODE_JV && p->nseg <= 1)
+      for (int a : {1, 0})
+        for (int sh : {SHAPE_PT_NARROW, SHAPE_PT_WIDE}) cand.push_back({a, sh});
     const bool tc = tc_eligible<MODE, R>(p) && p->nseg <= 1;
-    const int ncand = MODE == MODE_JV && p->nseg <= 1 ? (tc ? 9 : 8) : 4;
+    if (tc) cand.push_back({1, SHAPE_TC});
+    if (MODE == MODE_JV && p->Q == 2 && p->P == 2) {
+      cand.push_back({1, SHAPE_Q1});
+      cand.push_back({0, SHAPE_Q1});
+    }
+    const int ncand = (int)cand.size();
     cudaEvent_t e0, e1;
     HFK_CUDA(cudaEventCreate(&e0));
     HFK_CUDA(cudaEventCreate(&e1));
@@ -330,14 +347,14 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
       for (int rep = 0; rep < 2; ++rep) {
         HFK_CUDA(cudaMemsetAsync(io.y, 0, p->nfree * sizeof(R), p->stream));
         HFK_CUDA(cudaEventRecord(e0, p->stream));
-        run_cells_as<MODE, R>(p, io, cand[c][0] != 0, cand[c][1]);
+        run_cells_as<MODE, R>(p, io, cand[c].first != 0, cand[c].second);
         HFK_CUDA(cudaEventRecord(e1, p->stream));
         HFK_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         HFK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         t = std::min(t, ms);
       }
-      if (tc && (c == 0 || cand[c][1] == SHAPE_TC)) {
+      if (tc && (c == 0 || cand[c].second == SHAPE_TC)) {
         std::vector<R>& v = c == 0 ? ref : got;
         v.resize(p->nfree);
         HFK_CUDA(cudaMemcpyAsync(v.data(), io.y, p->nfree * sizeof(R), cudaMemcpyDeviceToHost, p->stream));
@@ -361,7 +378,7 @@ void run_cells(hfk_problem* p, CellIO<R> io) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    it = p->tuned.emplace(key, std::make_pair(cand[pick][0] != 0, cand[pick][1])).first;
+    it = p->tuned.emplace(key, std::make_pair(cand[pick].first != 0, cand[pick].second)).first;
     HFK_CUDA(cudaMemsetAsync(io.y, 0, p->nfree * sizeof(R), p->stream));
   }
   run_cells_as<MODE, R>(p, io, it->second.first, it->second.second);
@@ -2229,8 +2246,9 @@ int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int
   auto it = p->tuned.find(internal * 2 + (precision == HFK_FP32 ? 1 : 0));
   *atomic = it == p->tuned.end() ? -1 : (int)it->second.first;
   const int shape = it == p->tuned.end() ? 0 : it->second.second;
-  *kernel = shape == SHAPE_TC ? 2 : (shape >= SHAPE_PT_NARROW ? 1 : 0);
-  *warps = shape == SHAPE_TC ? JV_TC_WARPS
+  *kernel = shape == SHAPE_Q1 ? 3 : (shape == SHAPE_TC ? 2 : (shape >= SHAPE_PT_NARROW ? 1 : 0));
+  *warps = shape == SHAPE_Q1 ? Q1_THREADS / 32
+         : shape == SHAPE_TC ? JV_TC_WARPS
                              : (shape == SHAPE_PT_NARROW ? (p->P * p->P * p->P + 31) / 32
                                                          : (shape == SHAPE_PT_WIDE ? JVP_WIDE / 32 : shape));
   HFK_API_END
@@ -2238,14 +2256,18 @@ int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int
 
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps) {
   HFK_API_BEGIN
-  HFK_REQUIRE(p && kernel >= 0 && kernel <= 2, HFK_ERR_ARG,
-              "kernel must be 0 (line-mapped), 1 (point-parallel) or 2 (tensor cores)");
+  HFK_REQUIRE(p && kernel >= 0 && kernel <= 3, HFK_ERR_ARG,
+              "kernel must be 0 (line-mapped), 1 (point-parallel), 2 (tensor cores) or 3 (Q1 warp-synchronous)");
   HFK_REQUIRE(kernel != 0 || warps == 2 || warps == 4, HFK_ERR_ARG, "the line-mapped kernels take 2 or 4 warps per CTA");
   HFK_REQUIRE(kernel != 1 || warps == 0 || warps == JVP_WIDE / 32, HFK_ERR_ARG,
               "the point-parallel product takes 0 (one cell per CTA) or 8 warps per CTA");
   HFK_REQUIRE(kernel != 2 || (p->Q == 3 && p->P == 3), HFK_ERR_UNSUPPORTED,
               "the tensor-core product serves Q2 cells with 3^3 Gauss points");
-  p->shape = kernel == 0 ? warps : (kernel == 2 ? SHAPE_TC : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE));
+  HFK_REQUIRE(kernel != 3 || (p->Q == 2 && p->P == 2), HFK_ERR_UNSUPPORTED,
+              "the warp-synchronous Q1 product serves Q1 cells with 2^3 Gauss points");
+  p->shape = kernel == 0 ? warps
+                         : (kernel == 2 ? SHAPE_TC
+                                        : (kernel == 3 ? SHAPE_Q1 : (warps == 0 ? SHAPE_PT_NARROW : SHAPE_PT_WIDE)));
   HFK_API_END
 }
 

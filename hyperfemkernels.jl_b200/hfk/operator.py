@@ -74,9 +74,10 @@ class Problem:
     def set_launch(self, kernel: str = "line", warps: int = 4):
         """Launch shape under an explicit scatter mode: "line" (the line-mapped kernels, 2 or 4 warps
         per CTA), "point" (the point-parallel matrix-free product, warps 0 = one cell per CTA or
-        8) or "tensor" (the FP32 product of Q2 cells with both contractions on the tensor cores;
-        the other kernels then take the line-mapped shape of 4 warps)."""
-        call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1, "tensor": 2}[kernel], int(warps))
+        8), "tensor" (the FP32 product of Q2 cells with both contractions on the tensor cores) or
+        "q1" (the warp-synchronous product of Q1 cells with 2^3 points); with the last two the other
+        kernels take the line-mapped shape of 4 warps."""
+        call("hfk_problem_set_launch", self.h, {"line": 0, "point": 1, "tensor": 2, "q1": 3}[kernel], int(warps))
 
     def set_assembly_kernel(self, kernel: str = "fma"):
         """Kernel of the assembled Jacobian on 27-node cells: "fma" (default: the element blocks of the
@@ -94,7 +95,7 @@ class Problem:
         a, k, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("hfk_problem_tuning", self.h, {"jv": 0, "residual": 1, "jv_stored": 2}[kernel],
              _lib.FP32 if precision == "fp32" else _lib.FP64, ctypes.byref(a), ctypes.byref(k), ctypes.byref(w))
-        return None if a.value < 0 else {"atomic": bool(a.value), "kernel": ("line", "point", "tensor")[k.value],
+        return None if a.value < 0 else {"atomic": bool(a.value), "kernel": ("line", "point", "tensor", "q1")[k.value],
                                          "warps": w.value}
 
     def launches(self) -> int:

@@ -94,9 +94,11 @@ int hfk_problem_set_scatter(hfk_problem* p, int mode);
  * matrix-free product with one cell per CTA (warps = 0) or 8 warps per CTA; kernel 2, the FP32
  * product of Q2 cells (3^3 Gauss points) with both sum-factorisation contractions as GEMMs on the
  * tensor cores (tcgen05.mma kind::tf32, operands split hi + lo for FP32 accuracy, 128 cells per
- * CTA; warps ignored). The other kernels then take the line-mapped shape of 4 warps. Under AUTO
- * the tensor-core product is a candidate of the FP32 product, kept only when its result agrees
- * with the line-mapped kernel's to 1e-5. */
+ * CTA; warps ignored); kernel 3, the matrix-free product of Q1 cells (2^3 Gauss points) by a
+ * warp-synchronous kernel, 8 lanes per cell, one per point, the nodal sums by shuffles (warps
+ * ignored). With kernels 2 and 3 the other kernels take the line-mapped shape of 4 warps. Under
+ * AUTO the tensor-core product is a candidate of the FP32 product, kept only when its result
+ * agrees with the line-mapped kernel's to 1e-5, and the Q1 kernel a candidate of every Q1 product. */
 int hfk_problem_set_launch(hfk_problem* p, int kernel, int warps);
 /* Kernel of the assembled Jacobian (hfk_jacobian) on 27-node cells: 0 (default) forms the element
  * blocks of a symmetric tangent (the recognised laws) on the FP64 FMA pipe, a 27 x 162 register-
@@ -114,7 +116,8 @@ int hfk_problem_set_solve_graph(hfk_problem* p, int on);
 /* The autotuner's choice for a kernel (mode 0: matrix-free product, 1: residual, 2: stored-tangent
  * product; precision HFK_FP64 / HFK_FP32): atomic = 1/0 (scatter), kernel = 0 (line-mapped: a
  * warp's lanes on the tensor lines of a few cells), 1 (point-parallel product: one thread per
- * quadrature point) or 2 (the FP32 Q2 product on the tensor cores), warps per CTA; atomic = -1 if that kernel has not run under AUTO yet. No
+ * quadrature point), 2 (the FP32 Q2 product on the tensor cores) or 3 (the warp-synchronous Q1
+ * product), warps per CTA; atomic = -1 if that kernel has not run under AUTO yet. No
  * counterpart in the reference. */
 int hfk_problem_tuning(hfk_problem* p, int mode, int precision, int* atomic, int* kernel, int* warps);
 

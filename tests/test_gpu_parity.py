@@ -105,6 +105,50 @@ def test_matrix_free_product_parity(order, perturb, mode):
     assert reldiff(y, orc.mf_apply(dx)) < TOL64
 
 
+@pytest.mark.parametrize("n,perturb,law", [((3, 2, 2), 0.0, "svk"), ((7, 5, 6), 0.25, "svk"), ((7, 5, 6), 0.0, "linear"),
+                                             ((2, 1, 1), 0.0, "svk")])
+@pytest.mark.parametrize("scatter", ["coloured", "atomic"])
+def test_q1_warp_synchronous_product_parity(n, perturb, law, scatter):
+    # the Q1 kernel (8 lanes per cell, one per Gauss point, the nodal sums by shuffles) against the
+    # oracle, FP64 and FP32: affine and perturbed (trilinear) cells, a partial last warp and CTA,
+    # two cells
+    V = svk_space(n=n, order=1, perturb=perturb)
+    if law == "svk":
+        res, jf, olaw = forms.svk_residual(2.0, 1.0, 2), forms.svk_jacobian(2.0, 1.0, 2), O.LAW_SVK
+    else:
+        res, jf = forms.linear_elastic_residual(2.0, 1.0, 2), forms.linear_elastic_jacobian(2.0, 1.0, 2)
+        olaw = O.LAW_LINEAR
+    op = KernelOperator(res, jf, V, V, jacobian="matrixfree")
+    orc = O.OracleProblem(V, Quadrature.gauss(2), olaw, (2.0, 1.0))
+    op.problem.set_scatter(scatter)
+    op.problem.set_launch("q1")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    orc.mf_prepare(x, V.dirichlet_values)
+    dx = np.random.default_rng(1).standard_normal(V.nfree)
+    ref = orc.mf_apply(dx)
+    assert reldiff(mf.mul(np.zeros(V.nfree), dx), ref) < TOL64
+    y32 = mf.mul_f32(np.zeros(V.nfree, dtype=np.float32), dx.astype(np.float32))
+    assert reldiff(y32.astype(np.float64), ref) < 2e-6
+
+
+def test_q1_kernel_is_an_autotuner_candidate():
+    V = svk_space(n=(8, 8, 8), order=1)
+    op = KernelOperator(forms.svk_residual(2.0, 1.0, 2), forms.svk_jacobian(2.0, 1.0, 2), V, V, jacobian="matrixfree")
+    x = svk_state(V, amp=1e-2)
+    mf = MatrixFreeJacobian(op)
+    op.jacobian(mf, x)
+    dx = np.random.default_rng(3).standard_normal(V.nfree)
+    y = mf.mul(np.zeros(V.nfree), dx)
+    assert op.problem.tuning("jv", "fp64")["kernel"] in ("line", "point", "q1")
+    orc = O.OracleProblem(V, Quadrature.gauss(2))
+    orc.mf_prepare(x, V.dirichlet_values)
+    assert reldiff(y, orc.mf_apply(dx)) < TOL64
+    with pytest.raises(Exception):  # Q2 cells: not served by the Q1 kernel
+        make(2)[1].problem.set_launch("q1")
+
+
 @pytest.mark.parametrize("order,perturb", CASES)
 @pytest.mark.parametrize("scatter,warps", [("coloured", 8), ("atomic", 8), ("atomic", 0)])
 def test_point_parallel_product_parity(order, perturb, scatter, warps):
