@@ -176,9 +176,12 @@ class OracleProblem:
         lib().o_residual(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)), _d(b), nthreads)
         return b
 
-    def jacobian_values(self, x, dvals, nthreads=0, point_block=12):
+    def jacobian_values(self, x, dvals, nthreads=0, point_block=12, out=None):
+        """The CSC values of jacobian! (the restatement zero-fills them first); ``out``: a float64
+        array of nnz entries to assemble into in place, as jacobian!(A, ...) does into A."""
         self.pattern()
-        nz = np.zeros(self.nnz)
+        nz = np.zeros(self.nnz) if out is None else out
+        assert nz.dtype == np.float64 and nz.size == self.nnz and nz.flags.c_contiguous
         lib().o_jacobian(self.h, _d(np.ascontiguousarray(x, float)), _d(np.ascontiguousarray(dvals, float)), _d(nz),
                          nthreads, point_block)
         return nz
