@@ -219,8 +219,11 @@ class OracleProblem:
         lib().o_mf_get(self.h, _d(T), _d(iJt), _d(dV))
         return T, iJt, dV
 
-    def mf_apply(self, dx, nthreads=0):
-        y = np.zeros(self.nfree)
+    def mf_apply(self, dx, nthreads=0, out=None):
+        """y = J dx (the restatement zero-fills y first); ``out``: a float64 array of nfree entries
+        to write in place, as mul!(y, J, dx) does."""
+        y = np.zeros(self.nfree) if out is None else out
+        assert y.dtype == np.float64 and y.size == self.nfree and y.flags.c_contiguous
         rc = lib().o_mf_apply(self.h, _d(np.ascontiguousarray(dx, float)), _d(y), nthreads)
         if rc != 0:
             raise RuntimeError("oracle: mf_apply needs a tensor-product table and prepare()")
@@ -699,9 +702,12 @@ class OracleOseen:
                                _d(b), nthreads)
         return b
 
-    def jacobian_values(self, nthreads=0):
+    def jacobian_values(self, nthreads=0, out=None):
+        """The CSC values (zero-filled first by the restatement); ``out``: nnz float64 entries to
+        assemble into in place."""
         self.pattern()
-        nz = np.zeros(self.nnz)
+        nz = np.zeros(self.nnz) if out is None else out
+        assert nz.dtype == np.float64 and nz.size == self.nnz and nz.flags.c_contiguous
         lib().o_oseen_jacobian(self.h, _d(nz), nthreads)
         return nz
 
