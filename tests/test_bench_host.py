@@ -43,3 +43,26 @@ def test_clock_summary_without_samples_in_the_window():
     assert s["samples"] == 1 and s["window"].startswith("whole sampler run")
     c.lines = []
     assert c.summary()["reasons"] == ["unsampled"]
+
+
+def test_multi_rank_slabs_of_the_headline_configuration():
+    # what each of N ranks assembles in `bench.py --gpus N` (owner computes on z-slabs of the
+    # 20 x 10 x 10N mesh): about 2 000 cells and at most one ghost layer on each side; the owned free
+    # dofs of the ranks partition the job's free dofs
+    import numpy as np
+
+    from hfk import distributed as D
+
+    b = _bench()
+    for world in (2, 4):
+        G = b.c0_space(10 * world)
+        owned = np.zeros(G.nfree, dtype=np.int32)
+        for rank in range(world):
+            V, x, nfree_job, ncells = b.c0_problem(world, rank)
+            assert nfree_job == G.nfree
+            assert 2000 <= ncells <= 2000 + 2 * 200
+            assert len(x) == V.nfree and np.isfinite(x).all()
+            sub = D.Subdomain(G, D.slab_partition(G.mesh, world), rank, ghost=True)
+            assert V.nfree == len(sub.free_global) and len(sub.cells) == ncells
+            owned[sub.free_global[sub.owned]] += 1
+        assert (owned == 1).all()
