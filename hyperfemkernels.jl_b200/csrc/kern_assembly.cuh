@@ -10,6 +10,7 @@
 // precomputed positions (scatter_jacobian!, src/assembly.jl:1402-1408) by reductions.
 #pragma once
 #include "hfk_internal.h"
+#include "kern_async.cuh"
 #include "pointwise.cuh"
 
 namespace hfk {
@@ -290,15 +291,7 @@ inline size_t sym27_smem_bytes(int np, int qc) {
          (SYM27_POS_INTS + 2 * SYM27_IDS_INTS) * sizeof(int32_t);
 }
 
-// asynchronous copies global -> shared (cp.async, completion by wait_group: no polling)
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // the staged element blocks (162 columns of stride SYM27_LDK) fit over Dh and the G chunk
 // (Dh starts 100 np + 91 doubles in; from there to the end: 81 np + the chunk, at least)
 inline bool sym27_fits(int np, int qc) { return (size_t)81 * np + 3 * qc * SYM27_LDG >= (size_t)SYM27_COLS * SYM27_LDK; }

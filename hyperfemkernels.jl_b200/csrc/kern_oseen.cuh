@@ -19,6 +19,7 @@
 // thread per test function contracts them over the points (no element matrix).
 #pragma once
 #include "hfk_internal.h"
+#include "kern_async.cuh"
 #include "pointwise.cuh"
 
 namespace hfk {
@@ -75,11 +76,18 @@ struct OseenSmem {
 static __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, OseenIO io) {
   extern __shared__ __align__(16) double osm[];
   __shared__ int32_t sid[OS_NDL];
+  __shared__ __align__(16) int32_t spos[OS_NDL * OS_NDL];  // Jacobian: the cell's positions
   const OseenSmem L{d.nq};
   const int t = threadIdx.x;
   const int li = blockIdx.x;
   if (li >= d.ncells_list) return;
   const int cell = d.cells ? d.cells[li] : li;
+  if (io.mode == 1) {  // the cell's 34 x 34 positions (4 624 bytes, 16-byte aligned blocks), in flight
+                       // while the cell's data and point tables are computed
+    const char* src = reinterpret_cast<const char*>(io.nzpos + (size_t)OS_NDL * OS_NDL * cell);
+    for (int i = t; i < OS_NDL * OS_NDL * 4 / 16; i += blockDim.x) cp_async16(spos + 4 * i, src + 16 * i);
+    cp_async_commit();
+  }
   const int nq = d.nq;
   double* cv = osm + L.cellv();
   double* xl = osm + L.loc();
@@ -240,8 +248,10 @@ static __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, O
     return;
   }
   // ---- Jacobian: one thread per basis pair --------------------------------------------------
+  cp_async_wait_all();
+  __syncthreads();  // every thread's pieces of the positions have arrived
   const double* gpsi = cv + 11;
-  const int32_t* pos = io.nzpos + (size_t)OS_NDL * OS_NDL * cell;
+  const int32_t* pos = spos;
   auto put = [&](int te, int tr, double v) {
     const int32_t ps = pos[te + OS_NDL * tr];
     if (ps > 0) {
