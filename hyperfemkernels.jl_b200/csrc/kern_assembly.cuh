@@ -1,12 +1,20 @@
 // Fused element Jacobian + scatter into the CSC nonzeros.
 //
-// One CTA per cell (all cells in one launch, or the cells of one colour per launch). Per point the
-// tangent is pulled back to the reference gradients once, Dh_q[(c,K),(k,K')] = dV sum_{J,L} iJt[J,K] T[(c,J),(k,L)] iJt[L,K'], so the element matrix
+// Per point the tangent is pulled back to the reference gradients once,
+//   Dh_q[(c,K),(k,K')] = dV sum_{J,L} iJt[J,K] T[(c,J),(k,L)] iJt[L,K'],
+// so that the element matrix
 //   K[(n,c),(m,k)] = sum_q sum_{K,K'} dN^[n,K,q] Dh_q[(c,K),(k,K')] dN^[m,K',q]
 // only reads the reference tables (shared by all cells). For 27-node cells it is formed as the
 // reference forms it (element_jacobian_mm!, src/assembly.jl:1316-1342): per test component c,
 // G_c[(q,K),(m,k)] = sum_K' Dh[(c,K),(k,K')] dN^[m,K',q], then K_c = A^T G_c with A = dN^ as an
-// (np*3) x nn matrix, on the FP64 tensor cores (mma.sync m8n8k4). The entries are added at their
+// (np*3) x nn matrix. Three kernels:
+//   jacobian_kernel_sym27 (the default for the symmetric tangents of the recognised laws): the
+//     blocks k >= c only, on the FP64 FMA pipe, with a sum-factorised contraction when the tables
+//     are tensor products; persistent CTAs;
+//   jacobian_kernel_g (27-node cells, any tangent; selectable for the symmetric ones): K_c on the
+//     FP64 tensor cores (mma.sync m8n8k4), one CTA per cell;
+//   jacobian_kernel_direct (8-node cells): one thread per element entry, one CTA per cell.
+// All cells in one launch, or the cells of one colour per launch. The entries are added at their
 // precomputed positions (scatter_jacobian!, src/assembly.jl:1402-1408) by reductions.
 #pragma once
 #include "hfk_internal.h"
