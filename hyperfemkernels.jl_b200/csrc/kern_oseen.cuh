@@ -136,19 +136,21 @@ static __global__ void __launch_bounds__(OS_THREADS) oseen_kernel(OseenData d, O
   }
   __syncthreads();
   // ---- point data -------------------------------------------------------------------------
+  // the basis values and physical gradients per (point, basis function): all threads
+  for (int e = t; e < nq * OS_NV; e += blockDim.x) {
+    const int q = e / OS_NV, a = e - OS_NV * q;
+    osm[L.phi() + 10 * q + a] = d.N2[a + OS_NV * q];
+    const double g0 = d.dN2[a + OS_NV * (3 * q)], g1 = d.dN2[a + OS_NV * (1 + 3 * q)], g2 = d.dN2[a + OS_NV * (2 + 3 * q)];
+    double* gphi = osm + L.gphi() + 30 * q + a * 3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gphi[c] = cv[3 * c] * g0 + cv[1 + 3 * c] * g1 + cv[2 + 3 * c] * g2;
+    if (a < OS_NP) osm[L.psi() + 4 * q + a] = d.N1[a + OS_NP * q];
+  }
+  __syncthreads();
   for (int q = t; q < nq; q += blockDim.x) {
     double* phi = osm + L.phi() + 10 * q;
     double* gphi = osm + L.gphi() + 30 * q;
     double* psi = osm + L.psi() + 4 * q;
-    for (int a = 0; a < OS_NV; ++a) {
-      phi[a] = d.N2[a + OS_NV * q];
-      for (int c = 0; c < 3; ++c) {
-        double s = 0;
-        for (int K = 0; K < 3; ++K) s += cv[K + 3 * c] * d.dN2[a + OS_NV * (K + 3 * q)];
-        gphi[a * 3 + c] = s;
-      }
-    }
-    for (int a = 0; a < OS_NP; ++a) psi[a] = d.N1[a + OS_NP * q];
     double w[3], f[3], nrm = 0;
     for (int c = 0; c < 3; ++c) {
       double u0 = 0, u1 = 0;
