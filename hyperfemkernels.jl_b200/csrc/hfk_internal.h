@@ -1,5 +1,6 @@
 // Internal definitions of the B200 engine (not part of the C ABI).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
@@ -139,6 +140,14 @@ struct LevelState {
 }  // namespace hfk
 
 // The opaque handles of the ABI
+// the learned correction's network (hfk_mlp_*): FP32 master weights, their BF16 copy, Adam moments
+struct hfk_mlp {
+  hfk::DBuf<float> w, m1, m2, grad, loss;
+  hfk::DBuf<__nv_bfloat16> wb;
+  int64_t steps = 0;
+  cudaStream_t stream = nullptr;
+};
+
 struct hfk_problem {
   int D = 3, nn = 0, nc = 3, np = 0, ng = 8, ndl = 0, ncells = 0;
   int Q = 0, P = 0;             // tensor-product structure (0 = none)
