@@ -1704,7 +1704,7 @@ void coarse_factor_launch(hfk_pmg* m) {
   m->cb_W = W;
   m->cb_info.resize(1);
   m->cb_info.zero(c->stream);
-  const size_t smem = (size_t)2 * CB_T * CB_LD * sizeof(double), smem_p = 2 * smem;
+  const size_t smem_p = (size_t)4 * CB_T * CB_LD * sizeof(double), smem = (size_t)2 * CB_T * CB_LDU * sizeof(double);
   static PerDeviceLimit attr_p, attr_u;
   raise_smem_limit(band_panel_kernel, smem_p, attr_p);
   raise_smem_limit(band_update_kernel, smem, attr_u);

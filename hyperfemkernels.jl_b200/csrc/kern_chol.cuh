@@ -26,6 +26,8 @@ namespace hfk {
 constexpr int CB_T = 64;         // tile size of the band storage
 constexpr int CB_THREADS = 256;  // threads per CTA of the factorisation kernels
 constexpr int CB_LD = CB_T + 1;  // padded leading dimension of a tile in shared memory
+constexpr int CB_LDU = CB_T + 4;  // the same for the trailing update's tiles: the 8 x 4 fragments of
+                                  // each half-warp fall on distinct banks
 
 // offset (in doubles) of tile (i, j), j <= i <= j + W, in the band storage
 __host__ __device__ inline size_t band_tile_offset(int i, int j, int W) {
@@ -59,7 +61,7 @@ static __global__ void band_fill_kernel(int64_t n, int nbt, int W, const int64_t
 // A CB_T x CB_T tile between global memory (contiguous, column-major) and shared memory (leading
 // dimension CB_LD), by NT threads: 16-byte global accesses, the loop unrolled so that every
 // thread's loads are in flight together (the tiles are read on the factorisation's critical path).
-template <int NT>
+template <int NT, int LD = CB_LD>
 __device__ __forceinline__ void tile_to_shared(double* S, const double* __restrict__ G, int tid) {
   constexpr int N2 = CB_T * CB_T / 2;
   static_assert(N2 % NT == 0, "whole pairs per thread");
@@ -69,8 +71,8 @@ __device__ __forceinline__ void tile_to_shared(double* S, const double* __restri
 #pragma unroll
   for (int k = 0; k < N2 / NT; ++k) {
     const int e = 2 * (tid + NT * k), r = e % CB_T, c = e / CB_T;  // r even: r + 1 in the same column
-    S[r + CB_LD * c] = v[k].x;
-    S[r + 1 + CB_LD * c] = v[k].y;
+    S[r + LD * c] = v[k].x;
+    S[r + 1 + LD * c] = v[k].y;
   }
 }
 template <int NT, bool LOWER>
@@ -264,12 +266,13 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
 // Update k: tile (i, j) -= L_ik L_jk^T for the m (m + 1) / 2 tiles k < j <= i <= k + m (m = min(W,
 // nbt - 1 - k)); CTA b takes the b-th tile in the order (i, j) = (k+1, k+1), (k+2, k+1), (k+2, k+2),
 // ... part = 2 takes only the tiles j >= k + 2 (in the same order over that smaller triangle; block
-// column k + 1 is updated inside the next panel launch), 0 all. Each thread forms a 4 x 4 block of the product (rows tr + 16 a, columns ts + 16 b). On a
-// diagonal tile only the lower triangle is written. Dynamic shared memory: two tiles.
+// column k + 1 is updated inside the next panel launch), 0 all. Each warp forms 8 rows of the
+// product on the FP64 tensor cores. On a diagonal tile only the lower triangle is written. Dynamic
+// shared memory: two tiles of leading dimension CB_LDU.
 static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt, int W, int k, double* Lb, int part) {
   extern __shared__ __align__(16) double cbs[];
   double* Li = cbs;
-  double* Lj = cbs + CB_T * CB_LD;
+  double* Lj = cbs + CB_T * CB_LDU;
   const int tid = threadIdx.x;
   // b -> (ii, jj), jj <= ii: ii (ii + 1) / 2 <= b < (ii + 1) (ii + 2) / 2
   const int b = blockIdx.x;
@@ -284,34 +287,35 @@ static __global__ void __launch_bounds__(CB_THREADS) band_update_kernel(int nbt,
   const int i = k + 1 + ii, j = k + 1 + jj;
   const double* Lik = Lb + band_tile_offset(i, k, W);
   const double* Ljk = Lb + band_tile_offset(j, k, W);
-  tile_to_shared<CB_THREADS>(Li, Lik, tid);
-  tile_to_shared<CB_THREADS>(Lj, Ljk, tid);
+  tile_to_shared<CB_THREADS, CB_LDU>(Li, Lik, tid);
+  tile_to_shared<CB_THREADS, CB_LDU>(Lj, Ljk, tid);
   __syncthreads();
-  const int tr = tid % 16, ts = tid / 16;
-  double acc[4][4];
+  // L_ik L_jk^T on the FP64 tensor cores (mma.sync m8n8k4): warp w the rows 8w .. 8w + 7, all eight
+  // 8-column tiles; per k-step of 4 one fragment of L_ik and eight of L_jk (the same index pattern:
+  // lane l holds entry (8 t + l / 4, m + l % 4) of its tile)
+  const int warp = tid >> 5, lane = tid & 31, fr = lane >> 2, fc = lane & 3;
+  double acc[8][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = 0.0;
+#pragma unroll 4
+  for (int m = 0; m < CB_T; m += 4) {
+    const double a = Li[(8 * warp + fr) + CB_LDU * (m + fc)];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
-  for (int m = 0; m < CB_T; ++m) {
-    double x[4], y[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      x[a] = Li[tr + 16 * a + CB_LD * m];
-      y[a] = Lj[ts + 16 * a + CB_LD * m];
+    for (int t = 0; t < 8; ++t) {
+      const double b = Lj[(8 * t + fr) + CB_LDU * (m + fc)];
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(acc[t][0]), "+d"(acc[t][1])
+                   : "d"(a), "d"(b));
     }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[a][c] = fma(x[a], y[c], acc[a][c]);
   }
   double* Aij = Lb + band_tile_offset(i, j, W);
+  const int r = 8 * warp + fr;
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int t = 0; t < 8; ++t)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int r = tr + 16 * a, s = ts + 16 * c;
-      if (i != j || r >= s) Aij[r + (size_t)CB_T * s] -= acc[a][c];
+    for (int h = 0; h < 2; ++h) {
+      const int c = 8 * t + 2 * fc + h;
+      if (i != j || r >= c) Aij[r + (size_t)CB_T * c] -= acc[t][h];
     }
 }
 
