@@ -88,34 +88,42 @@ __device__ __forceinline__ void tile_to_global(double* __restrict__ G, const dou
   }
 }
 
-// S -= Li Lj^T for CB_T x CB_T tiles in shared memory (leading dimension CB_LD), by 128 threads,
-// each a 4 x 8 block of the product; lower: only the lower triangle of S is written.
+// S -= Li Lj^T for CB_T x CB_T tiles in shared memory (leading dimension CB_LD), by 128 threads on
+// the FP64 tensor cores (mma.sync m8n8k4): warp w the rows 16 w .. 16 w + 15 (two 8-row bands), all
+// eight 8-column tiles; lane l holds fragment entries (row l / 4, k l % 4) and accumulator entries
+// (row l / 4, columns 2 (l % 4), + 1). lower: only the lower triangle of S is written.
 __device__ __forceinline__ void tile_sub_prod128(double* S, const double* Li, const double* Lj, int tid, bool lower) {
-  const int tr = tid % 16, ts = tid / 16;  // rows tr + 16 a, columns ts + 8 b
-  double acc[4][8];
+  const int warp = tid >> 5, lane = tid & 31, fr = lane >> 2, fc = lane & 3;
+  double acc[2][8][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int rb = 0; rb < 2; ++rb)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
-#pragma unroll 4
-  for (int m = 0; m < CB_T; ++m) {
-    double x[4], y[8];
+    for (int t = 0; t < 8; ++t) acc[rb][t][0] = acc[rb][t][1] = 0.0;
+#pragma unroll 2
+  for (int m = 0; m < CB_T; m += 4) {
+    double a[2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) x[a] = Li[tr + 16 * a + CB_LD * m];
+    for (int rb = 0; rb < 2; ++rb) a[rb] = Li[(16 * warp + 8 * rb + fr) + CB_LD * (m + fc)];
 #pragma unroll
-    for (int b = 0; b < 8; ++b) y[b] = Lj[ts + 8 * b + CB_LD * m];
+    for (int t = 0; t < 8; ++t) {
+      const double b = Lj[(8 * t + fr) + CB_LD * (m + fc)];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 8; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
-  }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int r = tr + 16 * a, c = ts + 8 * b;
-      if (!lower || r >= c) S[r + CB_LD * c] -= acc[a][b];
+      for (int rb = 0; rb < 2; ++rb)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(acc[rb][t][0]), "+d"(acc[rb][t][1])
+                     : "d"(a[rb]), "d"(b));
     }
+  }
+  // S is neither Li nor Lj: its entries are written without waiting for the other warps
+#pragma unroll
+  for (int rb = 0; rb < 2; ++rb)
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = 16 * warp + 8 * rb + fr, c = 8 * t + 2 * fc + h;
+        if (!lower || r >= c) S[r + CB_LD * c] -= acc[rb][t][h];
+      }
 }
 
 // Panel k, blocked by 16 columns, the tile in shared memory (CB_PANEL_THREADS threads). Per block of
