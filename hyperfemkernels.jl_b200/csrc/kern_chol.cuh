@@ -126,6 +126,37 @@ __device__ __forceinline__ void tile_sub_prod128(double* S, const double* Li, co
       }
 }
 
+constexpr int CB_PANEL_THREADS = 128;
+constexpr int CB_PB = 16;  // columns per block of the panel
+
+// S[r][c] -= sum_{j < 16} P[r][p0 + j] Q[c][p0 + j] for r0 <= r < CB_T, t0 <= c < CB_T (r0 and t0
+// multiples of 8; tiles in shared memory, leading dimension CB_LD), by 128 threads on the FP64 tensor
+// cores: the 8 x 8 output tiles round-robin over the 4 warps, 4 MMAs each. lower: tiles above the
+// diagonal skipped, diagonal tiles written below it only. S's columns t0.. never overlap the read
+// columns p0 .. p0 + 15.
+__device__ __forceinline__ void panel_rank16_dmma(double* S, const double* P, const double* Q, int p0, int r0, int t0,
+                                                  int tid, bool lower) {
+  const int warp = tid >> 5, lane = tid & 31, fr = lane >> 2, fc = lane & 3;
+  const int nr = (CB_T - r0) / 8, nt = nr * ((CB_T - t0) / 8);
+  for (int e = warp; e < nt; e += CB_PANEL_THREADS / 32) {
+    const int tr = e % nr, tc = e / nr;
+    const int rb = r0 + 8 * tr, cb = t0 + 8 * tc;
+    if (lower && rb + 7 < cb) continue;  // above the diagonal (uniform over the warp)
+    double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+    for (int j = 0; j < CB_PB; j += 4) {
+      const double a = P[(rb + fr) + CB_LD * (p0 + j + fc)];
+      const double b = Q[(cb + fr) + CB_LD * (p0 + j + fc)];
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(d0), "+d"(d1)
+                   : "d"(a), "d"(b));
+    }
+    const int r = rb + fr, c = cb + 2 * fc;
+    if (!lower || r >= c) S[r + CB_LD * c] -= d0;
+    if (!lower || r >= c + 1) S[r + CB_LD * (c + 1)] -= d1;
+  }
+}
+
 // Panel k, blocked by 16 columns, the tile in shared memory (CB_PANEL_THREADS threads). Per block of
 // 16 columns: (1) one warp factors the 16 x 16 diagonal block, row i in lane i's registers, the
 // pivots and multipliers passed by shuffles (no barrier inside: the chain of dependent pivots is
@@ -135,8 +166,6 @@ __device__ __forceinline__ void tile_sub_prod128(double* S, const double* Li, co
 // tile (no CTA waits for another); CTA 0 stores it. CTA q >= 1 then solves X L_kk^T = A_{k+q,k} by
 // the same blocks: a block of 16 columns of X, then the update of X's later columns.
 // A pivot that is not positive and finite records k + 1 in *info and is replaced by 1.
-constexpr int CB_PANEL_THREADS = 128;
-constexpr int CB_PB = 16;  // columns per block of the panel
 
 // fuse: block column k first takes its update by block column k - 1 (the tiles (k + q, k) -= L_{k+q,k-1}
 // L_{k,k-1}^T, the diagonal one by every CTA, as it factors it), so that no separate launch sits
@@ -221,16 +250,9 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
       for (int c = 0; c < CB_PB; ++c) A[r + CB_LD * (p0 + c)] = x[c];
     }
     __syncthreads();
-    // (3) rank-16 update of the trailing lower triangle (four partial sums: short FMA chains)
-    const int t0 = p0 + CB_PB, m = CB_T - t0;
-    for (int e = tid; e < m * m; e += CB_PANEL_THREADS) {
-      const int rr = t0 + e % m, ss = t0 + e / m;
-      if (rr < ss) continue;
-      double a4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int c = 0; c < CB_PB; ++c) a4[c & 3] = fma(A[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], a4[c & 3]);
-      A[rr + CB_LD * ss] -= (a4[0] + a4[1]) + (a4[2] + a4[3]);
-    }
+    // (3) rank-16 update of the trailing lower triangle (FP64 tensor cores)
+    const int t0 = p0 + CB_PB;
+    if (t0 < CB_T) panel_rank16_dmma(A, A, A, p0, t0, t0, tid, true);
     __syncthreads();
   }
   if (q == 0) {
@@ -257,15 +279,9 @@ static __global__ void __launch_bounds__(CB_PANEL_THREADS) band_panel_kernel(int
       for (int c = 0; c < CB_PB; ++c) X[tid + CB_LD * (p0 + c)] = x[c];
     }
     __syncthreads();
-    // the later columns of X: X[r][s] -= sum_c X[r][p0 + c] L[s][p0 + c] (four partial sums)
-    const int t0 = p0 + CB_PB, m = CB_T - t0;
-    for (int e = tid; e < CB_T * m; e += CB_PANEL_THREADS) {
-      const int rr = e % CB_T, ss = t0 + e / CB_T;
-      double a4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int c = 0; c < CB_PB; ++c) a4[c & 3] = fma(X[rr + CB_LD * (p0 + c)], A[ss + CB_LD * (p0 + c)], a4[c & 3]);
-      X[rr + CB_LD * ss] -= (a4[0] + a4[1]) + (a4[2] + a4[3]);
-    }
+    // the later columns of X: X[r][s] -= sum_c X[r][p0 + c] L[s][p0 + c] (FP64 tensor cores)
+    const int t0 = p0 + CB_PB;
+    if (t0 < CB_T) panel_rank16_dmma(X, X, A, p0, 0, t0, tid, false);
     __syncthreads();
   }
   tile_to_global<CB_PANEL_THREADS, false>(Aik, X, tid);
